@@ -1,0 +1,189 @@
+/*
+ * yeti_b200 -- B200-native (sm_100a) implementation of YETI's U1 solid NURBS
+ * path behind a C ABI.
+ *
+ * All entry points return an int status (YETI_OK == 0).  On failure,
+ * yeti_last_error() returns a thread-local message.  Buffers are owned by the
+ * caller.  A pointer argument documented as "mem" is host or device memory
+ * according to the accompanying `mem` flag (YETI_MEM_HOST / YETI_MEM_DEVICE);
+ * model descriptions are always host memory.  Contexts are independent: the
+ * library keeps no global mutable state besides the thread-local error text.
+ *
+ * Reference interfaces replaced (paths relative to the reference's tree):
+ *   yeti_assemble_u1_coo   <- stiffmtrx_elemstorage.sys_linmat_lindef_static
+ *                             (src/yeti_iga/main/build_system_elemStorage.f90:24,
+ *                              called at src/yeti_iga/overlay/iga_model.py:387-389)
+ *   yeti_wq_*              <- iga_wq_mf assembly/solver f2py modules used by
+ *                             ThermoMechaIGA/pysrc/lib/fortran_mf_wq.py:29-560
+ *                             (mf_wq_get_ku_3d  src/yeti_iga/iga_wq_mf/fsrc/mf_wq_solver.f90:284,
+ *                              wq_mf_cg_3d      mf_wq_solver.f90:642,
+ *                              eval_mech_coefficient, jacobien_physicalposition_3d,
+ *                              wq_get_force_3d  src/yeti_iga/iga_wq_mf/fsrc/wq_assembly.f90:52,233,1193)
+ *   yeti_grad_lin_elast_work <- optim.gradadjointwork.gradlinelastwork_an
+ *                             (src/yeti_iga/optim/gradtotalwork_fullAN.f90:17,
+ *                              called at preprocessing/igaparametrization/OPT_modelling.py:474-477)
+ */
+#ifndef YETI_B200_H
+#define YETI_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define YETI_OK 0
+#define YETI_EINVAL (-1)        /* invalid argument / malformed model */
+#define YETI_ECUDA (-2)         /* CUDA runtime error */
+#define YETI_ENOMEM (-3)        /* device allocation failed or over budget */
+#define YETI_EUNSUPPORTED (-4)  /* element type / load type not on this path */
+#define YETI_ETIMEDOUT (-5)     /* bounded device wait gave up */
+#define YETI_EBREAKDOWN (-6)    /* Krylov breakdown (p.Ap <= 0 or NaN) */
+#define YETI_ENUMERIC (-7)      /* non-positive Jacobian / NaN in setup */
+#define YETI_ENOTCONV (-8)      /* iteration limit reached before tolerance */
+
+#define YETI_MEM_HOST 0
+#define YETI_MEM_DEVICE 1
+
+#define YETI_PREC_F64 0
+#define YETI_PREC_F32 1
+
+typedef struct yeti_ctx yeti_ctx;
+
+/* Thread-local description of the last failure of a yeti_* call. */
+const char *yeti_last_error(void);
+/* Library version string. */
+const char *yeti_version(void);
+
+/* Create a context on CUDA device `device`.  The context owns a stream
+ * (non-blocking) unless yeti_ctx_set_stream() supplies one.  hbm_budget_bytes
+ * bounds the device memory the context's operators may hold (0 = no bound). */
+int yeti_ctx_create(int device, size_t hbm_budget_bytes, yeti_ctx **out);
+int yeti_ctx_destroy(yeti_ctx *ctx);
+/* Use an existing cudaStream_t (passed as void*) for all work of the
+ * context; NULL restores the context's own stream. */
+int yeti_ctx_set_stream(yeti_ctx *ctx, void *stream);
+int yeti_ctx_synchronize(yeti_ctx *ctx);
+/* Bytes of device memory currently held by the context's objects. */
+size_t yeti_ctx_bytes_in_use(const yeti_ctx *ctx);
+
+/* ------------------------------------------------------------------------
+ * U1 element stiffness + COO assembly (drop-in for sys_linmat_lindef_static)
+ * ------------------------------------------------------------------------
+ * The model arrays are exactly those IGAparametrization.get_inputs4system_
+ * elemStorage() passes (IGA_parametrization.py:1705-1716), flattened in
+ * Fortran (column-major) order, integers as int64.  Only U1 patches with
+ * TENSOR=THREED and MCRD=3 are on this path; a patch of another element type
+ * that is marked active returns YETI_EUNSUPPORTED.
+ */
+typedef struct {
+    int64_t nb_patch, nb_elem, nb_cp;
+    const double *coords;            /* (3, nb_cp)                         */
+    const int64_t *ien;              /* sum_p nnode_p*nb_elem_p, 1-based    */
+    const int64_t *nb_elem_patch;    /* (nb_patch)                          */
+    const int64_t *nkv;              /* (3, nb_patch) knot vector lengths   */
+    const double *ukv;               /* concatenated knot vectors           */
+    const int64_t *nijk;             /* (3, nb_elem) 1-based knot spans     */
+    const double *weight;            /* sum_p nnode_p*nb_elem_p             */
+    const int64_t *jpqr;             /* (3, nb_patch) degrees               */
+    const int64_t *nnode;            /* (nb_patch)                          */
+    const int64_t *nbint;            /* (nb_patch) Gauss points / element   */
+    const int32_t *is_u1;            /* (nb_patch) 1 if U1/THREED           */
+    const double *matprops;          /* (2, nb_patch): E, nu                */
+    const double *rho;               /* (nb_patch) density                  */
+    const int64_t *active;           /* (nb_elem) 1 = assemble              */
+    int64_t nb_load;
+    const int64_t *inddload;         /* element (or CP) lists of the loads  */
+    const int64_t *jdltype;          /* (nb_load) load codes                */
+    const double *adlmag;            /* (nb_load) magnitudes                */
+    const int64_t *load_target_nbelem; /* (nb_load) list lengths           */
+    const double *load_addinfos;     /* additional load data                */
+    int64_t len_load_addinfos;
+    const int64_t *nb_load_addinfos; /* (nb_load)                           */
+    int64_t nb_n_dist;               /* rows of nodal_dist                  */
+    const double *nodal_dist;        /* (nb_n_dist, nb_cp)                  */
+} yeti_u1_model;
+
+/* Replaces sys_linmat_lindef_static (build_system_elemStorage.f90:24-315).
+ * Writes the upper-triangle element blocks in the reference's COO slot order
+ * (slots compacted over active elements, diagonal blocks halved) and the
+ * load vector F (concentrated loads assigned, then element loads added).
+ * kdata/krow/kcol: nb_data entries, F: 3*nb_cp entries; all `mem`. */
+int yeti_assemble_u1_coo(yeti_ctx *ctx, const yeti_u1_model *model,
+                         int64_t nb_data, double *kdata, int32_t *krow,
+                         int32_t *kcol, double *F, int mem);
+
+/* ------------------------------------------------------------------------
+ * Weighted-quadrature (WQ) matrix-free elasticity on one NURBS patch
+ * ------------------------------------------------------------------------
+ * Patch: degree p[d], nel[d] uniform elements per direction on an open
+ * uniform knot vector (the reference's WQ hypothesis,
+ * iga_wq_mf/fsrc/iga_wq_methods.f90:1-10), control points cps (3, ncp) and
+ * weights (ncp), CP index = iu + n_u*(iv + n_v*iw).  Vectors are
+ * component-major [c][iw][iv][iu] (the layout of wq_get_force_3d,
+ * wq_assembly.f90:1239-1249).  dirichlet[6*c + f] != 0 clamps component c on
+ * face f (0:u=0 1:u=1 2:v=0 3:v=1 4:w=0 5:w=1); clamped dofs are kept in the
+ * vectors and held at zero (the reference erases their rows,
+ * fortran_mf_wq.py:240-267).
+ */
+typedef struct yeti_wq_op yeti_wq_op;
+
+typedef struct {
+    int32_t iterations;        /* total inner (Krylov) iterations        */
+    int32_t outer_iterations;  /* FP64 refinement steps (mixed mode)      */
+    int32_t fp64_applies;      /* operator applications in FP64           */
+    int32_t fp32_applies;      /* operator applications in FP32           */
+    double rel_residual;       /* ||b - A x||_2 / ||b||_2 (FP64, true)    */
+    double rel_residual_inf;   /* max|b - A x| / max|b| (reference's
+                                  criterion, mf_wq_solver.f90:931)        */
+    double solve_ms;           /* device time of the solve                */
+    int32_t status;            /* YETI_OK / YETI_ENOTCONV / ...           */
+} yeti_cg_stats;
+
+#define YETI_WQ_F64 1     /* keep FP64 operator data                    */
+#define YETI_WQ_F32 2     /* keep FP32 operator data                    */
+
+int yeti_wq_setup(yeti_ctx *ctx, const int32_t p[3], const int32_t nel[3],
+                  const double *cps, const double *weights, double E,
+                  double nu, const uint8_t dirichlet[18], int prec_mask,
+                  yeti_wq_op **out);
+int yeti_wq_destroy(yeti_wq_op *op);
+/* Sizes: number of control points, total dofs (3*ncp), free dofs,
+ * quadrature points, bytes of operator data held on the device. */
+int yeti_wq_info(const yeti_wq_op *op, int64_t *ncp, int64_t *ndof,
+                 int64_t *nfree, int64_t *nqp, int64_t *bytes);
+/* Ku = K u.  prec YETI_PREC_F64: u, Ku are double; YETI_PREC_F32: float. */
+int yeti_wq_apply(yeti_wq_op *op, const void *u, void *Ku, int prec, int mem);
+/* Diagonal of K (3*ncp doubles; clamped dofs hold 1). */
+int yeti_wq_diag(yeti_wq_op *op, double *d, int mem);
+/* Body-force load vector for a constant force density f[3]
+ * (wq_get_force_3d, wq_assembly.f90:1193-1251). */
+int yeti_wq_body_force(yeti_wq_op *op, const double f[3], double *F, int mem);
+/* Jacobi-preconditioned CG on K x = b (x holds the initial guess).
+ * mode 0: plain FP64.  mode 1: FP32 operator and inner PCG with FP64
+ * residual and iterative-refinement correction.  Stops when the FP64 true
+ * residual satisfies ||r||_2 <= rtol ||b||_2. */
+int yeti_wq_pcg(yeti_wq_op *op, const double *b, double *x, double rtol,
+                int maxit, int mode, yeti_cg_stats *stats, int mem);
+
+/* ------------------------------------------------------------------------
+ * Adjoint shape gradient of the linear-elastic work (U1, 3D)
+ * ------------------------------------------------------------------------
+ * Replaces gradLinElastWork_AN (gradtotalwork_fullAN.f90:17-300): for each
+ * adjoint field a, gWint[a] = d(-ADJ_a^T K U)/dP and gWext[a] = d(ADJ_a^T F)/dP
+ * with respect to the control-point coordinates P (3, nb_cp).
+ * sol: (3, nb_cp); adj: (nadj, 3, nb_cp) Fortran order; outputs
+ * (nadj, 3, nb_cp) Fortran order.  include_surface_loads: 0 reproduces the
+ * reference (surface-load sensitivity left out, gradUELMAT_solid.f90:463-477);
+ * 1 adds the traction term.  sol/adj/outputs are `mem`. */
+int yeti_grad_lin_elast_work(yeti_ctx *ctx, const yeti_u1_model *model,
+                             const double *sol, const double *adj,
+                             int64_t nadj, int compute_wint, int compute_wext,
+                             int include_surface_loads, double *gwint,
+                             double *gwext, int mem);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* YETI_B200_H */

@@ -1,0 +1,148 @@
+"""U1 element stiffness + COO assembly: oracle pins (CPU) and GPU parity.
+
+Parity bar (the reference's own seq-vs-OpenMP test style,
+benchs/omp/test_build_stifmatrix_omp.py:41-73): identical Krow/Kcol,
+||dKdata||/||Kdata|| <= 1e-12 and max|dKdata| <= 1e-12 max|Kdata|,
+||dF||/||F|| <= 1e-12, and the direct-solve displacement within 1e-12.
+"""
+import numpy as np
+import pytest
+import scipy.sparse as sp
+import scipy.sparse.linalg as spla
+
+import oracle
+from conftest import load_fixture
+
+FIXTURES = ["cantilever_p2_16x4x4", "dload_beam_dist", "volume_force_3d",
+            "omp_beam_dist", "grad_unit_cube", "quarter_annulus_p2_4x4x2"]
+TOL = 1e-12
+
+
+def _solve(d, kdata, krow, kcol, rhs):
+    ndof = int(d["nb_dof_tot"])
+    K = sp.coo_matrix((kdata, (krow, kcol)), shape=(ndof, ndof)).tocsc()
+    K = K + K.T
+    idof = d["ind_dof_free"][:int(d["nb_dof_free"])] - 1
+    x = spla.spsolve(K[idof, :][:, idof], rhs[idof])
+    sol = np.zeros(ndof)
+    sol[idof] = x
+    return sol.reshape(-1, 3)
+
+
+# ----------------------------------------------------------------- CPU: oracle
+def test_oracle_dload_beam_known_answer():
+    """benchs/dload/test_dload_beam_dist.py:66-81: tip deflection -1142.857
+    (analytic), rtol 2e-2, for the p=2 refined beam under normal pressure."""
+    d, args = load_fixture("dload_beam_dist")
+    sol = _solve(d, *oracle.sys_linmat_lindef_static(*args))
+    val = sol[int(d["check_cp"]), int(d["check_comp"])]
+    assert np.isclose(val, float(d["check_value"]), rtol=float(d["check_rtol"]))
+
+
+def test_oracle_volume_force_known_answer():
+    """benchs/volume_force/test_volume_force_3d.py:38,74-80: Abaqus
+    displacement at xi=(1,1,0), relative error < 2e-3 (U102 body force)."""
+    d, args = load_fixture("volume_force_3d")
+    sol = _solve(d, *oracle.sys_linmat_lindef_static(*args))
+    v = sol[int(d["check_cp"])]
+    ref = d["check_disp"]
+    assert np.linalg.norm(v - ref) / np.linalg.norm(ref) < float(d["check_rtol"])
+
+
+def test_oracle_cantilever_resultant_and_beam_theory():
+    """Cantilever 10x1x1 (E=210000): the traction resultant is exactly -1 in z
+    and the tip deflection is close to Euler-Bernoulli P L^3 / (3 E I)."""
+    d, args = load_fixture("cantilever_p2_16x4x4")
+    kdata, krow, kcol, F = oracle.sys_linmat_lindef_static(*args)
+    assert int(d["nb_data"]) == 850176
+    Fz = F.reshape(-1, 3)
+    assert np.isclose(Fz[:, 2].sum(), -1.0, rtol=1e-13)
+    assert np.abs(Fz[:, :2]).max() == 0.0
+    sol = _solve(d, kdata, krow, kcol, F)
+    eb = 1.0 * 10.0 ** 3 / (3 * 210000.0 * (1.0 / 12.0))
+    assert np.isclose(sol[:, 2].min(), -eb, rtol=0.05)
+
+
+def test_oracle_stiffness_is_symmetric_psd_with_rigid_modes():
+    """K = Kside + Kside^T annihilates the 6 rigid-body modes of the
+    unconstrained single-element cube."""
+    d, args = load_fixture("grad_unit_cube")
+    kdata, krow, kcol, _ = oracle.sys_linmat_lindef_static(*args)
+    n = int(d["nb_dof_tot"])
+    K = sp.coo_matrix((kdata, (krow, kcol)), shape=(n, n)).toarray()
+    K = K + K.T
+    X = d["COORDS3D"].T
+    modes = []
+    for c in range(3):
+        m = np.zeros((X.shape[0], 3)); m[:, c] = 1.0; modes.append(m.ravel())
+    for (a, b) in ((0, 1), (1, 2), (0, 2)):
+        m = np.zeros((X.shape[0], 3)); m[:, a] = -X[:, b]; m[:, b] = X[:, a]
+        modes.append(m.ravel())
+    scale = np.abs(K).max()
+    for m in modes:
+        assert np.abs(K @ m).max() < 1e-10 * scale
+    assert np.linalg.eigvalsh(K).min() > -1e-9 * scale
+
+
+# ------------------------------------------------------------------ GPU parity
+def _gpu_vs_oracle(name):
+    from yeti_b200.stiffmtrx_elemstorage import sys_linmat_lindef_static
+    d, args = load_fixture(name)
+    ref = oracle.sys_linmat_lindef_static(*args)
+    got = sys_linmat_lindef_static(*args)
+    return d, ref, got
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", FIXTURES)
+def test_gpu_coo_matches_oracle(cuda_ok, name):
+    d, (k0, r0, c0, f0), (k1, r1, c1, f1) = _gpu_vs_oracle(name)
+    assert k1.dtype == np.float64 and r1.dtype == np.int32 and c1.dtype == np.int32
+    assert k1.shape == k0.shape
+    np.testing.assert_array_equal(r1, r0)
+    np.testing.assert_array_equal(c1, c0)
+    assert np.linalg.norm(k1 - k0) <= TOL * np.linalg.norm(k0)
+    assert np.abs(k1 - k0).max() <= TOL * np.abs(k0).max()
+    if np.linalg.norm(f0) > 0:
+        assert np.linalg.norm(f1 - f0) <= TOL * np.linalg.norm(f0)
+    else:
+        assert np.linalg.norm(f1) == 0.0
+    if int(d["nb_dof_free"]) < int(d["nb_dof_tot"]) and np.linalg.norm(f0) > 0:
+        s0 = _solve(d, k0, r0, c0, f0)
+        s1 = _solve(d, k1, r1, c1, f1)
+        assert np.linalg.norm(s1 - s0) <= TOL * np.linalg.norm(s0)
+
+
+@pytest.mark.gpu
+def test_gpu_coo_device_output_and_inactive_elements(cuda_ok):
+    """Device-resident outputs, and slots compacted over active elements."""
+    import torch
+    from yeti_b200.stiffmtrx_elemstorage import sys_linmat_lindef_static
+    d, args = load_fixture("cantilever_p2_16x4x4")
+    active = np.ones(int(d["nb_elem"]), dtype=np.int64)
+    active[::3] = 0
+    nb_data = int(active.sum()) * 3321
+    args = list(args)
+    args[0] = active
+    args[1] = nb_data
+    k0, r0, c0, f0 = oracle.sys_linmat_lindef_static(*args)
+    k1, r1, c1, f1 = sys_linmat_lindef_static(*args, device_out=True)
+    assert k1.is_cuda and k1.numel() == nb_data
+    np.testing.assert_array_equal(r1.cpu().numpy(), r0)
+    np.testing.assert_array_equal(c1.cpu().numpy(), c0)
+    k1 = k1.cpu().numpy()
+    assert np.linalg.norm(k1 - k0) <= TOL * np.linalg.norm(k0)
+    f1 = f1.cpu().numpy()
+    assert np.linalg.norm(f1 - f0) <= TOL * np.linalg.norm(f0)
+    torch.cuda.synchronize()
+
+
+@pytest.mark.gpu
+def test_gpu_rejects_unsupported_element(cuda_ok):
+    from yeti_b200._lib import YetiError
+    from yeti_b200.stiffmtrx_elemstorage import sys_linmat_lindef_static
+    d, args = load_fixture("grad_unit_cube")
+    args = list(args)
+    args[10] = "U3"   # shell patch
+    with pytest.raises(YetiError):
+        sys_linmat_lindef_static(*args)

@@ -1,0 +1,766 @@
+// U1 solid element stiffness and COO assembly on the GPU.
+//
+// Replaces stiffmtrx_elemstorage.sys_linmat_lindef_static
+// (src/yeti_iga/main/build_system_elemStorage.f90:24-315) and the element
+// routine UELMAT_byCP (src/yeti_iga/main/UELMAT.f90:22-225) with its helpers
+// shap (shap.f90:21-180), stiffmatrix_byCP (stiffmatrix.F90:130-225),
+// material_lib (material_lib.f90:75-87) and shapPress (shapPress.f:18-262).
+//
+// Kernel design: one CTA per element.  Stage A: one thread per Gauss point
+// evaluates the rational basis derivatives dR/dx (3 x nnode) and the volume
+// weight into shared memory.  Stage B: one thread per control-point pair
+// (i <= j) accumulates the 3x3 block over the Gauss points and writes its 9
+// (or 6, diagonal) COO entries at the reference's slot positions, so the
+// writes of consecutive threads are contiguous.  Elements whose Gauss data do
+// not fit shared memory are processed in Gauss-point chunks (read-modify-write
+// of the element's own slots).  The load vector is a second kernel over the
+// elements that carry distributed loads.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <memory>
+
+#include "nurbs.cuh"
+#include "u1_model.cuh"
+
+namespace yeti {
+
+// ---------------------------------------------------------------- Gauss rules
+void gauss_legendre_host(int n, double *x, double *w) {
+    for (int i = 0; i < n; i++) {
+        double z = -std::cos(M_PI * (i + 0.75) / (n + 0.5));
+        double pp = 1.0;
+        for (int it = 0; it < 100; it++) {
+            double p1 = 1.0, p2 = 0.0;
+            for (int k = 1; k <= n; k++) {
+                double p3 = p2;
+                p2 = p1;
+                p1 = ((2.0 * k - 1.0) * z * p2 - (k - 1.0) * p3) / k;
+            }
+            pp = n * (z * p1 - p2) / (z * z - 1.0);
+            double dz = p1 / pp;
+            z -= dz;
+            if (std::fabs(dz) < 1e-17) break;
+        }
+        double p1 = 1.0, p2 = 0.0;
+        for (int k = 1; k <= n; k++) {
+            double p3 = p2;
+            p2 = p1;
+            p1 = ((2.0 * k - 1.0) * z * p2 - (k - 1.0) * p3) / k;
+        }
+        pp = n * (z * p1 - p2) / (z * z - 1.0);
+        x[i] = z;
+        w[i] = 2.0 / ((1.0 - z * z) * pp * pp);
+    }
+    for (int i = 0; i < n / 2; i++) {
+        double a = 0.5 * (x[n - 1 - i] - x[i]);
+        double b = 0.5 * (w[n - 1 - i] + w[i]);
+        x[i] = -a;
+        x[n - 1 - i] = a;
+        w[i] = b;
+        w[n - 1 - i] = b;
+    }
+    if (n % 2) x[n / 2] = 0.0;
+}
+
+void gauss_volume_host(int n, std::vector<double> &g) {
+    double x[32], w[32];
+    gauss_legendre_host(n, x, w);
+    g.assign(4 * n * n * n, 0.0);
+    int q = 0;
+    for (int i = 0; i < n; i++)
+        for (int j = 0; j < n; j++)
+            for (int k = 0; k < n; k++, q++) {
+                g[4 * q] = w[i] * w[j] * w[k];
+                g[4 * q + 1] = x[i];
+                g[4 * q + 2] = x[j];
+                g[4 * q + 3] = x[k];
+            }
+}
+
+void gauss_face_host(int n, int face, std::vector<double> &g) {
+    double x[32], w[32];
+    gauss_legendre_host(n, x, w);
+    g.assign(4 * n * n, 0.0);
+    for (int j = 0; j < n; j++)
+        for (int i = 0; i < n; i++) {
+            double *p = &g[4 * (i + n * j)];
+            p[0] = w[i] * w[j];
+            switch (face) {
+                case 1: p[1] = -1.0; p[2] = x[i]; p[3] = x[j]; break;
+                case 2: p[1] = 1.0; p[2] = x[i]; p[3] = x[j]; break;
+                case 3: p[1] = x[i]; p[2] = -1.0; p[3] = x[j]; break;
+                case 4: p[1] = x[i]; p[2] = 1.0; p[3] = x[j]; break;
+                case 5: p[1] = x[j]; p[2] = x[i]; p[3] = -1.0; break;
+                default: p[1] = x[j]; p[2] = x[i]; p[3] = 1.0; break;
+            }
+        }
+}
+
+// ------------------------------------------------------------ model preparing
+int u1_prepare(yeti_ctx *ctx, const yeti_u1_model *m, U1Model &out) {
+    YETI_CHECK(m && m->coords && m->ien && m->nb_elem_patch && m->nkv &&
+                   m->ukv && m->nijk && m->weight && m->jpqr && m->nnode &&
+                   m->nbint && m->matprops && m->active,
+               YETI_EINVAL, "U1 model: a required array is NULL");
+    YETI_CHECK(m->nb_patch > 0 && m->nb_elem >= 0 && m->nb_cp > 0,
+               YETI_EINVAL, "U1 model: bad sizes");
+    out.patches.clear();
+    out.patches.resize(m->nb_patch);
+    out.nb_cp = m->nb_cp;
+    int64_t jelem = 0, ukv_off = 0, ien_off = 0, count = 0;
+    for (int64_t ip = 0; ip < m->nb_patch; ip++) {
+        U1Patch &P = out.patches[ip];
+        for (int d = 0; d < 3; d++) {
+            P.p[d] = (int)m->jpqr[3 * ip + d];
+            P.nkv[d] = (int)m->nkv[3 * ip + d];
+        }
+        P.nelem = m->nb_elem_patch[ip];
+        P.elem_begin = jelem;
+        P.nn = (int)m->nnode[ip];
+        bool any_active = false;
+        for (int64_t e = 0; e < P.nelem; e++)
+            if (m->active[jelem + e] == 1) any_active = true;
+        if (any_active) {
+            YETI_CHECK(!m->is_u1 || m->is_u1[ip], YETI_EUNSUPPORTED,
+                       "patch %lld: only U1/THREED solid elements are on this "
+                       "path", (long long)ip + 1);
+            YETI_CHECK(P.nkv[1] > 0 && P.nkv[2] > 0, YETI_EUNSUPPORTED,
+                       "patch %lld: only 3D patches are supported",
+                       (long long)ip + 1);
+            for (int d = 0; d < 3; d++)
+                YETI_CHECK(P.p[d] >= 1 && P.p[d] <= kMaxDeg &&
+                               P.nkv[d] >= 2 * P.p[d] + 2,
+                           YETI_EINVAL, "patch %lld: degree %d / knots %d",
+                           (long long)ip + 1, P.p[d], P.nkv[d]);
+            YETI_CHECK(P.nn == (P.p[0] + 1) * (P.p[1] + 1) * (P.p[2] + 1),
+                       YETI_EINVAL, "patch %lld: nnode %d does not match the "
+                       "degrees", (long long)ip + 1, P.nn);
+        }
+        P.nq = (int)m->nbint[ip];
+        int ng = (int)std::pow((double)P.nq, 1.0 / 3.0);
+        if (ng < 1) ng = 1;
+        while (ng * ng * ng < P.nq) ng++;
+        P.ng = ng;
+        YETI_CHECK(P.nq >= 1 && ng <= 32, YETI_EINVAL,
+                   "patch %lld: NBINT %d", (long long)ip + 1, P.nq);
+        P.E = m->matprops[2 * ip];
+        P.nu = m->matprops[2 * ip + 1];
+        P.rho = m->rho ? m->rho[ip] : 0.0;
+        P.nb_data_elem = 9LL * P.nn * (P.nn - 1) / 2 + 6LL * P.nn;
+        const int nn = P.nn;
+        std::vector<int32_t> ien, span, gid;
+        std::vector<double> w;
+        for (int64_t e = 0; e < P.nelem; e++, jelem++) {
+            if (m->active[jelem] != 1) continue;
+            P.act.push_back(jelem);
+            P.slot.push_back(count);
+            count += P.nb_data_elem;
+            gid.push_back((int32_t)jelem);
+            for (int a = 0; a < nn; a++) {
+                int64_t cp = m->ien[ien_off + e * nn + a];
+                YETI_CHECK(cp >= 1 && cp <= m->nb_cp, YETI_EINVAL,
+                           "IEN entry %lld of element %lld out of range",
+                           (long long)cp, (long long)jelem + 1);
+                ien.push_back((int32_t)(cp - 1));
+                w.push_back(m->weight[ien_off + e * nn + a]);
+            }
+            for (int d = 0; d < 3; d++) {
+                int64_t ni = m->nijk[3 * jelem + d];
+                YETI_CHECK(ni >= P.p[d] + 1 && ni <= P.nkv[d] - P.p[d] - 1,
+                           YETI_EINVAL, "Nijk of element %lld out of range",
+                           (long long)jelem + 1);
+                span.push_back((int32_t)ni);
+            }
+        }
+        P.nactive = (int64_t)P.act.size();
+        int nk = P.nkv[0] + P.nkv[1] + P.nkv[2];
+        if (P.nactive) {
+            YETI_TRY(upload(ctx, P.knots, m->ukv + ukv_off, nk));
+            std::vector<double> g;
+            gauss_volume_host(P.ng, g);
+            YETI_TRY(upload(ctx, P.gauss, g.data(), g.size()));
+            YETI_TRY(upload(ctx, P.ien, ien.data(), ien.size()));
+            YETI_TRY(upload(ctx, P.w, w.data(), w.size()));
+            YETI_TRY(upload(ctx, P.span, span.data(), span.size()));
+            YETI_TRY(upload(ctx, P.slotd, P.slot.data(), P.slot.size()));
+            YETI_TRY(upload(ctx, P.gid, gid.data(), gid.size()));
+        }
+        ukv_off += nk;
+        ien_off += P.nelem * nn;
+    }
+    YETI_CHECK(jelem == m->nb_elem, YETI_EINVAL,
+               "sum of nb_elem_patch (%lld) != nb_elem (%lld)",
+               (long long)jelem, (long long)m->nb_elem);
+    out.nb_data = count;
+    YETI_TRY(upload(ctx, out.coords, m->coords, (size_t)3 * m->nb_cp));
+    return YETI_OK;
+}
+
+// ---------------------------------------------------------------- kernels
+struct StiffArgs {
+    int p0, p1, p2, nn, nq, qchunk;
+    const double *U0, *U1, *U2;
+    const double *gauss;
+    const double *coords;
+    const int32_t *ien;
+    const double *w;
+    const int32_t *span;
+    const int64_t *slot;
+    double lam, mu;
+    double *kdata;
+    int32_t *krow, *kcol;
+};
+
+// Rational basis at parent point t of an element: dR/dxi into dRdxi_out
+// (3*nn, stride 3 per node), and the 3x3 d x / d xi into J.  Two passes over
+// the nodes (normalisation sums, then values) so no per-thread node arrays
+// are needed.  Follows shap.f90:90-140.
+__device__ inline void rational_derivs(
+    int p0, int p1, int p2, int nn, const double *U0, const double *U1,
+    const double *U2, const int *ni, const double *u1, const double *u2,
+    const double *t, const double *w, const double *xe, double *dRdxi_out,
+    double J[3][3], double *Rsum_inv, double *Fv /* 6*kMaxDeg1 */) {
+    double xi[3];
+    for (int d = 0; d < 3; d++)
+        xi[d] = ((u2[d] - u1[d]) * t[d] + (u2[d] + u1[d])) * 0.5;
+    double *FN = Fv, *dFN = Fv + kMaxDeg1, *FM = Fv + 2 * kMaxDeg1,
+           *dFM = Fv + 3 * kMaxDeg1, *FL = Fv + 4 * kMaxDeg1,
+           *dFL = Fv + 5 * kMaxDeg1;
+    bspline_ders(ni[0], p0, xi[0], U0, FN, dFN);
+    bspline_ders(ni[1], p1, xi[1], U1, FM, dFM);
+    bspline_ders(ni[2], p2, xi[2], U2, FL, dFL);
+    double S = 0.0, sx0 = 0.0, sx1 = 0.0, sx2 = 0.0;
+    int a = 0;
+    for (int k = 0; k <= p2; k++)
+        for (int j = 0; j <= p1; j++)
+            for (int i = 0; i <= p0; i++, a++) {
+                double wa = w[a];
+                S += FN[p0 - i] * FM[p1 - j] * FL[p2 - k] * wa;
+                sx0 += dFN[p0 - i] * FM[p1 - j] * FL[p2 - k] * wa;
+                sx1 += FN[p0 - i] * dFM[p1 - j] * FL[p2 - k] * wa;
+                sx2 += FN[p0 - i] * FM[p1 - j] * dFL[p2 - k] * wa;
+            }
+    double inv = 1.0 / S;
+    *Rsum_inv = inv;
+    for (int r = 0; r < 3; r++)
+        for (int c = 0; c < 3; c++) J[r][c] = 0.0;
+    a = 0;
+    for (int k = 0; k <= p2; k++)
+        for (int j = 0; j <= p1; j++)
+            for (int i = 0; i <= p0; i++, a++) {
+                double wa = w[a];
+                double R = FN[p0 - i] * FM[p1 - j] * FL[p2 - k] * wa * inv;
+                double d0 = (dFN[p0 - i] * FM[p1 - j] * FL[p2 - k] * wa - R * sx0) * inv;
+                double d1 = (FN[p0 - i] * dFM[p1 - j] * FL[p2 - k] * wa - R * sx1) * inv;
+                double d2 = (FN[p0 - i] * FM[p1 - j] * dFL[p2 - k] * wa - R * sx2) * inv;
+                if (dRdxi_out) {
+                    dRdxi_out[3 * a] = d0;
+                    dRdxi_out[3 * a + 1] = d1;
+                    dRdxi_out[3 * a + 2] = d2;
+                }
+                for (int r = 0; r < 3; r++) {
+                    double x = xe[3 * a + r];
+                    J[r][0] += x * d0;
+                    J[r][1] += x * d1;
+                    J[r][2] += x * d2;
+                }
+            }
+}
+
+// MatrixInv for 3x3 (operateurs.f:385-423); returns the determinant.
+__device__ inline double inv3(const double B[3][3], double A[3][3]) {
+    double det = B[0][1] * B[1][2] * B[2][0] - B[0][2] * B[1][1] * B[2][0] +
+                 B[0][2] * B[1][0] * B[2][1] - B[0][0] * B[1][2] * B[2][1] +
+                 B[0][0] * B[1][1] * B[2][2] - B[0][1] * B[1][0] * B[2][2];
+    A[0][0] = (B[1][1] * B[2][2] - B[1][2] * B[2][1]) / det;
+    A[0][1] = (B[0][2] * B[2][1] - B[0][1] * B[2][2]) / det;
+    A[0][2] = (B[0][1] * B[1][2] - B[0][2] * B[1][1]) / det;
+    A[1][0] = (B[1][2] * B[2][0] - B[1][0] * B[2][2]) / det;
+    A[1][1] = (B[0][0] * B[2][2] - B[0][2] * B[2][0]) / det;
+    A[1][2] = (B[0][2] * B[1][0] - B[0][0] * B[1][2]) / det;
+    A[2][0] = (B[1][0] * B[2][1] - B[1][1] * B[2][0]) / det;
+    A[2][1] = (B[0][1] * B[2][0] - B[0][0] * B[2][1]) / det;
+    A[2][2] = (B[0][0] * B[1][1] - B[0][1] * B[1][0]) / det;
+    return det;
+}
+
+// Parent-element Jacobian determinant (shap.f90:155-178).
+__device__ inline double parent_det(const double J[3][3], const double *u1,
+                                    const double *u2) {
+    double A[3][3];
+    for (int r = 0; r < 3; r++)
+        for (int c = 0; c < 3; c++) A[r][c] = J[r][c] * (0.5 * (u2[c] - u1[c]));
+    return A[0][0] * A[1][1] * A[2][2] + A[0][1] * A[1][2] * A[2][0] +
+           A[1][0] * A[2][1] * A[0][2] - A[0][2] * A[1][1] * A[2][0] -
+           A[0][1] * A[1][0] * A[2][2] - A[1][2] * A[2][1] * A[0][0];
+}
+
+__global__ void __launch_bounds__(256)
+k_u1_stiffness(StiffArgs a) {
+    extern __shared__ double smem[];
+    const int nn = a.nn;
+    double *xe = smem;                      // 3*nn element CP coordinates
+    double *we = xe + 3 * nn;               // nn element weights
+    double *dR = we + nn;                   // qchunk * nn * 3
+    double *dv = dR + (size_t)a.qchunk * nn * 3;  // qchunk
+    __shared__ double su1[3], su2[3];
+    __shared__ int sni[3];
+    const int e = blockIdx.x;
+    const int tid = threadIdx.x;
+    const int32_t *ien = a.ien + (size_t)e * nn;
+    for (int i = tid; i < nn; i += blockDim.x) {
+        int cp = ien[i];
+        xe[3 * i] = a.coords[3 * cp];
+        xe[3 * i + 1] = a.coords[3 * cp + 1];
+        xe[3 * i + 2] = a.coords[3 * cp + 2];
+        we[i] = a.w[(size_t)e * nn + i];
+    }
+    if (tid < 3) {
+        const double *U = tid == 0 ? a.U0 : (tid == 1 ? a.U1 : a.U2);
+        int ni = a.span[3 * e + tid];
+        sni[tid] = ni;
+        su1[tid] = U[ni - 1];
+        su2[tid] = U[ni];
+    }
+    const int npairs = nn * (nn + 1) / 2;
+    const int64_t base = a.slot[e];
+    const double lam = a.lam, mu = a.mu, l2m = lam + 2.0 * mu;
+    for (int q0 = 0; q0 < a.nq; q0 += a.qchunk) {
+        const int nqc = min(a.qchunk, a.nq - q0);
+        __syncthreads();
+        // ---- stage A: basis derivatives at the chunk's Gauss points
+        for (int ql = tid; ql < nqc; ql += blockDim.x) {
+            const double *g = a.gauss + 4 * (q0 + ql);
+            double Fv[6 * kMaxDeg1];
+            double J[3][3], Ji[3][3], inv;
+            double *dRq = dR + (size_t)ql * nn * 3;
+            rational_derivs(a.p0, a.p1, a.p2, nn, a.U0, a.U1, a.U2, sni, su1,
+                            su2, g + 1, we, xe, dRq, J, &inv, Fv);
+            inv3(J, Ji);
+            dv[ql] = g[0] * fabs(parent_det(J, su1, su2));
+            for (int n = 0; n < nn; n++) {
+                double d0 = dRq[3 * n], d1 = dRq[3 * n + 1], d2 = dRq[3 * n + 2];
+                for (int c = 0; c < 3; c++)
+                    dRq[3 * n + c] = d0 * Ji[0][c] + d1 * Ji[1][c] + d2 * Ji[2][c];
+            }
+        }
+        __syncthreads();
+        // ---- stage B: one thread per control-point pair (i <= j)
+        for (int t = tid; t < npairs; t += blockDim.x) {
+            int j = (int)((sqrt(8.0 * t + 1.0) - 1.0) * 0.5);
+            while (j * (j + 1) / 2 > t) j--;
+            while ((j + 1) * (j + 2) / 2 <= t) j++;
+            const int i = t - j * (j + 1) / 2;
+            double K[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+            for (int q = 0; q < nqc; q++) {
+                const double *A = dR + ((size_t)q * nn + i) * 3;
+                const double *B = dR + ((size_t)q * nn + j) * 3;
+                const double a0 = A[0], a1 = A[1], a2 = A[2];
+                const double b0 = B[0], b1 = B[1], b2 = B[2];
+                const double d = dv[q];
+                // B_i^T D B_j for isotropic D (stiffmatrix.F90:167-216)
+                K[0][0] += (a0 * (l2m * b0) + a1 * (mu * b1) + a2 * (mu * b2)) * d;
+                K[1][1] += (a1 * (l2m * b1) + a0 * (mu * b0) + a2 * (mu * b2)) * d;
+                K[2][2] += (a2 * (l2m * b2) + a0 * (mu * b0) + a1 * (mu * b1)) * d;
+                K[0][1] += (a0 * (lam * b1) + a1 * (mu * b0)) * d;
+                K[1][0] += (a1 * (lam * b0) + a0 * (mu * b1)) * d;
+                K[0][2] += (a0 * (lam * b2) + a2 * (mu * b0)) * d;
+                K[2][0] += (a2 * (lam * b0) + a0 * (mu * b2)) * d;
+                K[1][2] += (a1 * (lam * b2) + a2 * (mu * b1)) * d;
+                K[2][1] += (a2 * (lam * b1) + a1 * (mu * b2)) * d;
+            }
+            const int64_t jb = base + 9LL * j * (j - 1) / 2 + 6LL * j;
+            const int dofi = 3 * ien[i], dofj = 3 * ien[j];
+            if (i < j) {
+                const int64_t s = jb + 9LL * i;
+                for (int ll = 0; ll < 3; ll++)
+                    for (int kk = 0; kk < 3; kk++) {
+                        const int64_t o = s + 3 * ll + kk;
+                        double v = K[kk][ll];
+                        if (q0 > 0) v += a.kdata[o];
+                        a.kdata[o] = v;
+                        if (q0 == 0) {
+                            a.krow[o] = dofi + kk;
+                            a.kcol[o] = dofj + ll;
+                        }
+                    }
+            } else {
+                const int64_t s = jb + 9LL * j;
+                for (int ll = 0; ll < 3; ll++)
+                    for (int kk = 0; kk <= ll; kk++) {
+                        const int64_t o = s + ll * (ll + 1) / 2 + kk;
+                        double v = (kk == ll) ? K[kk][ll] * 0.5 : K[kk][ll];
+                        if (q0 > 0) v += a.kdata[o];
+                        a.kdata[o] = v;
+                        if (q0 == 0) {
+                            a.krow[o] = dofj + kk;
+                            a.kcol[o] = dofj + ll;
+                        }
+                    }
+            }
+        }
+    }
+}
+
+// Distributed loads of one element: body loads 101 (centrifugal) and 102
+// (volume force) integrated over the volume rule, surface loads 10..99 over
+// the face rule (UELMAT.f90:121-223).
+struct LoadTerm {
+    int kind;        // 0: body 101, 1: body 102, 2: surface
+    int face, type;  // surface: face 1..6, type 0..4
+    int ifield;      // nodal distribution row (type 4), 0-based
+    double mag;      // ADLMAG
+    double info[6];  // additional infos (axis points / direction)
+};
+
+struct RhsArgs {
+    int p0, p1, p2, nn, nq, ng;
+    const double *U0, *U1, *U2;
+    const double *gauss;      // volume rule
+    const double *gface;      // 6 faces x ng^2 x 4
+    const double *coords;
+    const int32_t *ien;       // per active element
+    const double *w;
+    const int32_t *span;
+    const int32_t *elems;     // active-element local indices with loads
+    const int32_t *term_ptr;  // CSR into terms
+    const LoadTerm *terms;
+    double rho;
+    int nb_n_dist;
+    const double *nodal_dist;
+    double *F;
+};
+
+__global__ void __launch_bounds__(128) k_u1_rhs(RhsArgs a) {
+    extern __shared__ double smem[];
+    const int nn = a.nn;
+    const int e = a.elems[blockIdx.x];
+    double *xe = smem;
+    double *we = xe + 3 * nn;
+    double *rhs = we + nn;            // 3*nn
+    double *qR = rhs + 3 * nn;        // per Gauss point: R sum inverse
+    __shared__ double su1[3], su2[3];
+    __shared__ int sni[3];
+    const int tid = threadIdx.x;
+    const int32_t *ien = a.ien + (size_t)e * nn;
+    for (int i = tid; i < nn; i += blockDim.x) {
+        int cp = ien[i];
+        for (int d = 0; d < 3; d++) xe[3 * i + d] = a.coords[3 * cp + d];
+        we[i] = a.w[(size_t)e * nn + i];
+    }
+    for (int i = tid; i < 3 * nn; i += blockDim.x) rhs[i] = 0.0;
+    if (tid < 3) {
+        const double *U = tid == 0 ? a.U0 : (tid == 1 ? a.U1 : a.U2);
+        int ni = a.span[3 * e + tid];
+        sni[tid] = ni;
+        su1[tid] = U[ni - 1];
+        su2[tid] = U[ni];
+    }
+    __syncthreads();
+    (void)qR;
+    for (int ti = a.term_ptr[blockIdx.x]; ti < a.term_ptr[blockIdx.x + 1]; ti++) {
+        const LoadTerm T = a.terms[ti];
+        const int npts = T.kind == 2 ? a.ng * a.ng : a.nq;
+        const double *rule = T.kind == 2 ? a.gface + (size_t)(T.face - 1) * a.ng * a.ng * 4 : a.gauss;
+        for (int q = tid; q < npts; q += blockDim.x) {
+            const double *g = rule + 4 * q;
+            double Fv[6 * kMaxDeg1], J[3][3], inv;
+            rational_derivs(a.p0, a.p1, a.p2, nn, a.U0, a.U1, a.U2, sni, su1,
+                            su2, g + 1, we, xe, nullptr, J, &inv, Fv);
+            double A[3][3];
+            for (int r = 0; r < 3; r++)
+                for (int c = 0; c < 3; c++) A[r][c] = J[r][c] * (0.5 * (su2[c] - su1[c]));
+            double vec[3] = {0, 0, 0}, dvol = 0.0;
+            double xg[3] = {0, 0, 0};
+            double *FN = Fv, *FM = Fv + 2 * kMaxDeg1, *FL = Fv + 4 * kMaxDeg1;
+            if (T.kind == 2 || T.kind == 0 || T.type == 4) {
+                int n = 0;
+                for (int k = 0; k <= a.p2; k++)
+                    for (int j = 0; j <= a.p1; j++)
+                        for (int i = 0; i <= a.p0; i++, n++) {
+                            double R = FN[a.p0 - i] * FM[a.p1 - j] * FL[a.p2 - k] * we[n] * inv;
+                            for (int d = 0; d < 3; d++) xg[d] += R * xe[3 * n + d];
+                        }
+            }
+            double fmag = T.mag;
+            if (T.kind == 2) {
+                double c1[3] = {A[0][0], A[1][0], A[2][0]};
+                double c2[3] = {A[0][1], A[1][1], A[2][1]};
+                double c3[3] = {A[0][2], A[1][2], A[2][2]};
+                const double *P = c2, *Q = c3;   // surface measure pair
+                switch (T.face) {
+                    case 1: case 2: P = c2; Q = c3; break;
+                    case 3: case 4: P = c3; Q = c1; break;
+                    default: P = c1; Q = c2; break;
+                }
+                double nx = P[1] * Q[2] - P[2] * Q[1];
+                double ny = P[2] * Q[0] - P[0] * Q[2];
+                double nz = P[0] * Q[1] - P[1] * Q[0];
+                double detj = sqrt(nx * nx + ny * ny + nz * nz);
+                if (T.type >= 1 && T.type <= 3) {
+                    vec[T.type - 1] = 1.0;
+                } else {   // normal pressure, orientation of shapPress.f:229-258
+                    const double *U = c1, *V = c2;
+                    switch (T.face) {
+                        case 1: U = c2; V = c3; break;
+                        case 2: U = c3; V = c2; break;
+                        case 3: U = c3; V = c1; break;
+                        case 4: U = c1; V = c3; break;
+                        case 5: U = c1; V = c2; break;
+                        default: U = c2; V = c1; break;
+                    }
+                    vec[0] = (U[1] * V[2] - U[2] * V[1]) / detj;
+                    vec[1] = (U[2] * V[0] - U[0] * V[2]) / detj;
+                    vec[2] = (U[0] * V[1] - U[1] * V[0]) / detj;
+                }
+                dvol = g[0] * detj;
+                if (T.type == 4) {
+                    fmag = 0.0;
+                    int n = 0;
+                    for (int k = 0; k <= a.p2; k++)
+                        for (int j = 0; j <= a.p1; j++)
+                            for (int i = 0; i <= a.p0; i++, n++) {
+                                double R = FN[a.p0 - i] * FM[a.p1 - j] * FL[a.p2 - k] * we[n] * inv;
+                                fmag += a.nodal_dist[T.ifield + (size_t)a.nb_n_dist * ien[n]] * R;
+                            }
+                }
+                for (int d = 0; d < 3; d++) vec[d] *= dvol * fmag;
+            } else {
+                dvol = g[0] * fabs(A[0][0] * A[1][1] * A[2][2] + A[0][1] * A[1][2] * A[2][0] +
+                                   A[1][0] * A[2][1] * A[0][2] - A[0][2] * A[1][1] * A[2][0] -
+                                   A[0][1] * A[1][0] * A[2][2] - A[1][2] * A[2][1] * A[0][0]);
+                if (T.kind == 0) {   // centrifugal, UELMAT.f90:125-151
+                    double vd[3], ag[3];
+                    for (int d = 0; d < 3; d++) vd[d] = T.info[3 + d] - T.info[d];
+                    double nr = sqrt(vd[0] * vd[0] + vd[1] * vd[1] + vd[2] * vd[2]);
+                    for (int d = 0; d < 3; d++) {
+                        vd[d] /= nr;
+                        ag[d] = xg[d] - T.info[d];
+                    }
+                    double sc = ag[0] * vd[0] + ag[1] * vd[1] + ag[2] * vd[2];
+                    for (int d = 0; d < 3; d++)
+                        vec[d] = a.rho * (T.mag * T.mag) * (ag[d] - sc * vd[d]) * dvol;
+                } else {             // volume force, UELMAT.f90:153-166
+                    for (int d = 0; d < 3; d++) vec[d] = T.mag * T.info[d] * dvol;
+                }
+            }
+            int n = 0;
+            for (int k = 0; k <= a.p2; k++)
+                for (int j = 0; j <= a.p1; j++)
+                    for (int i = 0; i <= a.p0; i++, n++) {
+                        double R = FN[a.p0 - i] * FM[a.p1 - j] * FL[a.p2 - k] * we[n] * inv;
+                        for (int d = 0; d < 3; d++) atomicAdd(&rhs[3 * n + d], R * vec[d]);
+                    }
+        }
+        __syncthreads();
+    }
+    for (int i = tid; i < 3 * nn; i += blockDim.x)
+        atomicAdd(&a.F[3 * (size_t)ien[i / 3] + (i % 3)], rhs[i]);
+}
+
+static bool in_list(const int64_t *l, int64_t n, int64_t v) {
+    for (int64_t i = 0; i < n; i++)
+        if (l[i] == v) return true;
+    return false;
+}
+
+}  // namespace yeti
+
+using namespace yeti;
+
+YETI_API int yeti_assemble_u1_coo(yeti_ctx *ctx, const yeti_u1_model *m,
+                                  int64_t nb_data, double *kdata,
+                                  int32_t *krow, int32_t *kcol, double *F,
+                                  int mem) {
+    YETI_CHECK(ctx && m && kdata && krow && kcol && F, YETI_EINVAL,
+               "yeti_assemble_u1_coo: NULL argument");
+    YETI_CHECK(mem == YETI_MEM_HOST || mem == YETI_MEM_DEVICE, YETI_EINVAL,
+               "yeti_assemble_u1_coo: bad mem flag %d", mem);
+    DeviceGuard guard(ctx->device);
+    U1Model M;
+    YETI_TRY(u1_prepare(ctx, m, M));
+    YETI_CHECK(M.nb_data <= nb_data, YETI_EINVAL,
+               "nb_data %lld smaller than the %lld slots of the active "
+               "elements", (long long)nb_data, (long long)M.nb_data);
+    const int64_t ndof = 3 * m->nb_cp;
+    // ---- load vector: concentrated loads are assigned (not added) first,
+    // build_system_elemStorage.f90:137-152
+    std::vector<double> F0(ndof, 0.0);
+    int64_t kk = 0;
+    for (int64_t il = 0; il < m->nb_load; il++) {
+        int64_t ty = m->jdltype[il];
+        if (ty / 10 < 1) {
+            YETI_CHECK(ty >= 1 && ty <= 3, YETI_EUNSUPPORTED,
+                       "concentrated load direction %lld", (long long)ty);
+            for (int64_t c = 0; c < m->load_target_nbelem[il]; c++) {
+                int64_t cp = m->inddload[kk + c];
+                YETI_CHECK(cp >= 1 && cp <= m->nb_cp, YETI_EINVAL,
+                           "concentrated load CP %lld", (long long)cp);
+                F0[(cp - 1) * 3 + ty - 1] = m->adlmag[il];
+            }
+        } else if (ty != 101 && ty != 102) {
+            YETI_CHECK(ty > 9 && ty < 100 && (ty % 10) <= 4 &&
+                           ty / 10 >= 1 && ty / 10 <= 6,
+                       YETI_EUNSUPPORTED, "distributed load type U%lld is not "
+                       "on the U1 path", (long long)ty);
+        }
+        kk += m->load_target_nbelem[il];
+    }
+    DevBuf dK, dR, dC, dF;
+    double *k_ = kdata, *f_ = F;
+    int32_t *r_ = krow, *c_ = kcol;
+    if (mem == YETI_MEM_HOST) {
+        YETI_TRY(dK.alloc(ctx, nb_data * sizeof(double)));
+        YETI_TRY(dR.alloc(ctx, nb_data * sizeof(int32_t)));
+        YETI_TRY(dC.alloc(ctx, nb_data * sizeof(int32_t)));
+        YETI_TRY(dF.alloc(ctx, ndof * sizeof(double)));
+        k_ = dK.as<double>();
+        r_ = dR.as<int32_t>();
+        c_ = dC.as<int32_t>();
+        f_ = dF.as<double>();
+    }
+    if (M.nb_data < nb_data) {   // slots beyond the active elements stay 0
+        YETI_CUDA(cudaMemsetAsync(k_ + M.nb_data, 0, (nb_data - M.nb_data) * sizeof(double), ctx->stream));
+        YETI_CUDA(cudaMemsetAsync(r_ + M.nb_data, 0, (nb_data - M.nb_data) * sizeof(int32_t), ctx->stream));
+        YETI_CUDA(cudaMemsetAsync(c_ + M.nb_data, 0, (nb_data - M.nb_data) * sizeof(int32_t), ctx->stream));
+    }
+    YETI_CUDA(cudaMemcpyAsync(f_, F0.data(), ndof * sizeof(double),
+                              cudaMemcpyHostToDevice, ctx->stream));
+    int smem_optin = 0;
+    YETI_CUDA(cudaDeviceGetAttribute(&smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, ctx->device));
+    const size_t smem_cap = std::min<size_t>(smem_optin, 200 * 1024);
+    YETI_CUDA(cudaFuncSetAttribute(k_u1_stiffness, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_cap));
+    std::vector<std::unique_ptr<DevBuf>> keep;
+    auto newbuf = [&keep]() -> DevBuf & {
+        keep.emplace_back(new DevBuf());
+        return *keep.back();
+    };
+    for (size_t ip = 0; ip < M.patches.size(); ip++) {
+        U1Patch &P = M.patches[ip];
+        if (!P.nactive) continue;
+        const size_t fixed = sizeof(double) * 4 * P.nn;
+        const size_t perq = sizeof(double) * (3 * P.nn + 1);
+        YETI_CHECK(fixed + perq <= smem_cap, YETI_EUNSUPPORTED,
+                   "element with %d nodes does not fit shared memory", P.nn);
+        int qchunk = (int)std::min<size_t>(P.nq, (smem_cap - fixed) / perq);
+        StiffArgs a;
+        a.p0 = P.p[0]; a.p1 = P.p[1]; a.p2 = P.p[2];
+        a.nn = P.nn; a.nq = P.nq; a.qchunk = qchunk;
+        a.U0 = P.knots.as<double>();
+        a.U1 = a.U0 + P.nkv[0];
+        a.U2 = a.U1 + P.nkv[1];
+        a.gauss = P.gauss.as<double>();
+        a.coords = M.coords.as<double>();
+        a.ien = P.ien.as<int32_t>();
+        a.w = P.w.as<double>();
+        a.span = P.span.as<int32_t>();
+        a.slot = P.slotd.as<int64_t>();
+        a.lam = (P.E * P.nu) / ((1.0 + P.nu) * (1.0 - 2.0 * P.nu));
+        a.mu = P.E / (2.0 * (1.0 + P.nu));
+        a.kdata = k_; a.krow = r_; a.kcol = c_;
+        const size_t smem = fixed + perq * qchunk;
+        int64_t left = P.nactive, off = 0;
+        while (left > 0) {   // grid.x limit
+            int64_t n = std::min<int64_t>(left, 1 << 30);
+            StiffArgs b = a;
+            b.ien += off * P.nn; b.w += off * P.nn; b.span += off * 3; b.slot += off;
+            k_u1_stiffness<<<(unsigned)n, 256, smem, ctx->stream>>>(b);
+            YETI_CUDA(cudaGetLastError());
+            left -= n; off += n;
+        }
+        // ---- distributed loads of this patch's elements
+        std::vector<int32_t> elems, tptr(1, 0);
+        std::vector<LoadTerm> terms;
+        for (int64_t le = 0; le < P.nactive; le++) {
+            const int64_t jel = P.act[le] + 1;   // 1-based element number
+            int64_t k2 = 0, cinfo = 0;
+            size_t before = terms.size();
+            for (int64_t il = 0; il < m->nb_load; il++) {
+                int64_t nt = m->load_target_nbelem[il], ty = m->jdltype[il];
+                if ((ty == 101 || ty == 102 || (ty > 9 && ty < 100)) &&
+                    in_list(m->inddload + k2, nt, jel)) {
+                    LoadTerm T;
+                    memset(&T, 0, sizeof(T));
+                    T.mag = m->adlmag[il];
+                    if (ty == 101 || ty == 102) {
+                        T.kind = ty == 101 ? 0 : 1;
+                        int nneed = ty == 101 ? 6 : 3;
+                        YETI_CHECK(cinfo + nneed <= m->len_load_addinfos, YETI_EINVAL,
+                                   "load %lld: missing additional infos", (long long)il + 1);
+                        for (int d = 0; d < nneed; d++) T.info[d] = m->load_addinfos[cinfo + d];
+                    } else {
+                        T.kind = 2;
+                        T.face = (int)(ty / 10);
+                        T.type = (int)(ty % 10);
+                        if (T.type == 4) {
+                            YETI_CHECK(cinfo < m->len_load_addinfos && m->nodal_dist, YETI_EINVAL,
+                                       "load %lld: nodal distribution missing", (long long)il + 1);
+                            T.ifield = (int)m->load_addinfos[cinfo] - 1;
+                            YETI_CHECK(T.ifield >= 0 && T.ifield < m->nb_n_dist, YETI_EINVAL,
+                                       "load %lld: nodal field index", (long long)il + 1);
+                        }
+                    }
+                    terms.push_back(T);
+                }
+                k2 += nt;
+                cinfo += m->nb_load_addinfos ? m->nb_load_addinfos[il] : 0;
+            }
+            if (terms.size() > before) {
+                elems.push_back((int32_t)le);
+                tptr.push_back((int32_t)terms.size());
+            }
+        }
+        if (!elems.empty()) {
+            std::vector<double> gf(6 * 4 * P.ng * P.ng), tmp;
+            for (int f = 1; f <= 6; f++) {
+                gauss_face_host(P.ng, f, tmp);
+                std::copy(tmp.begin(), tmp.end(), gf.begin() + (f - 1) * 4 * P.ng * P.ng);
+            }
+            DevBuf &dgf = newbuf();
+            YETI_TRY(upload(ctx, dgf, gf.data(), gf.size()));
+            DevBuf &del = newbuf();
+            YETI_TRY(upload(ctx, del, elems.data(), elems.size()));
+            DevBuf &dtp = newbuf();
+            YETI_TRY(upload(ctx, dtp, tptr.data(), tptr.size()));
+            DevBuf &dtm = newbuf();
+            YETI_TRY(upload(ctx, dtm, terms.data(), terms.size()));
+            DevBuf *dnd = nullptr;
+            if (m->nodal_dist && m->nb_n_dist > 0) {
+                dnd = &newbuf();
+                YETI_TRY(upload(ctx, *dnd, m->nodal_dist, (size_t)m->nb_n_dist * m->nb_cp));
+            }
+            RhsArgs r;
+            r.p0 = P.p[0]; r.p1 = P.p[1]; r.p2 = P.p[2];
+            r.nn = P.nn; r.nq = P.nq; r.ng = P.ng;
+            r.U0 = P.knots.as<double>(); r.U1 = r.U0 + P.nkv[0]; r.U2 = r.U1 + P.nkv[1];
+            r.gauss = P.gauss.as<double>();
+            r.gface = dgf.as<double>();
+            r.coords = M.coords.as<double>();
+            r.ien = P.ien.as<int32_t>();
+            r.w = P.w.as<double>();
+            r.span = P.span.as<int32_t>();
+            r.elems = del.as<int32_t>();
+            r.term_ptr = dtp.as<int32_t>();
+            r.terms = dtm.as<LoadTerm>();
+            r.rho = P.rho;
+            r.nb_n_dist = (int)m->nb_n_dist;
+            r.nodal_dist = dnd ? dnd->as<double>() : nullptr;
+            r.F = f_;
+            size_t smem = sizeof(double) * (4 * P.nn + 3 * P.nn + 8);
+            YETI_CHECK(smem <= smem_cap, YETI_EUNSUPPORTED, "element too large for the load kernel");
+            YETI_CUDA(cudaFuncSetAttribute(k_u1_rhs, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_cap));
+            k_u1_rhs<<<(unsigned)elems.size(), 128, smem, ctx->stream>>>(r);
+            YETI_CUDA(cudaGetLastError());
+        }
+    }
+    if (mem == YETI_MEM_HOST) {
+        YETI_CUDA(cudaMemcpyAsync(kdata, k_, nb_data * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+        YETI_CUDA(cudaMemcpyAsync(krow, r_, nb_data * sizeof(int32_t), cudaMemcpyDeviceToHost, ctx->stream));
+        YETI_CUDA(cudaMemcpyAsync(kcol, c_, nb_data * sizeof(int32_t), cudaMemcpyDeviceToHost, ctx->stream));
+        YETI_CUDA(cudaMemcpyAsync(F, f_, ndof * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    }
+    // the model's device arrays are released on return: wait for the work
+    YETI_CUDA(cudaStreamSynchronize(ctx->stream));
+    return YETI_OK;
+}

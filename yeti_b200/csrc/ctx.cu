@@ -1,0 +1,117 @@
+// Context management, error reporting and device-memory accounting.
+#include <cstdarg>
+#include <cstring>
+
+#include "common.cuh"
+
+namespace yeti {
+
+static thread_local char g_err[1024] = "";
+
+void set_error(const char *fmt, ...) {
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(g_err, sizeof(g_err), fmt, ap);
+    va_end(ap);
+}
+
+int cuda_fail(cudaError_t e, const char *what, const char *file, int line) {
+    set_error("CUDA error %s (%s) in %s at %s:%d", cudaGetErrorName(e),
+              cudaGetErrorString(e), what, file, line);
+    return YETI_ECUDA;
+}
+
+int dev_alloc(yeti_ctx *ctx, void **ptr, size_t bytes) {
+    *ptr = nullptr;
+    if (bytes == 0) bytes = 16;
+    if (ctx->hbm_budget && ctx->bytes_in_use + bytes > ctx->hbm_budget) {
+        set_error("HBM budget exceeded: %zu in use + %zu requested > %zu",
+                  ctx->bytes_in_use, bytes, ctx->hbm_budget);
+        return YETI_ENOMEM;
+    }
+    cudaError_t e = cudaMalloc(ptr, bytes);
+    if (e != cudaSuccess) {
+        (void)cudaGetLastError();
+        set_error("cudaMalloc of %zu bytes failed: %s", bytes,
+                  cudaGetErrorString(e));
+        *ptr = nullptr;
+        return YETI_ENOMEM;
+    }
+    ctx->bytes_in_use += bytes;
+    return YETI_OK;
+}
+
+void dev_free(yeti_ctx *ctx, void *ptr, size_t bytes) {
+    if (!ptr) return;
+    cudaFree(ptr);
+    if (ctx) ctx->bytes_in_use -= (bytes ? bytes : 16);
+}
+
+bool is_device_pointer(const void *p) {
+    cudaPointerAttributes a;
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        (void)cudaGetLastError();
+        return false;
+    }
+    return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+}
+
+}  // namespace yeti
+
+using namespace yeti;
+
+YETI_API const char *yeti_last_error(void) { return g_err; }
+
+YETI_API const char *yeti_version(void) { return "yeti_b200 0.1 (sm_100a)"; }
+
+YETI_API int yeti_ctx_create(int device, size_t hbm_budget_bytes,
+                             yeti_ctx **out) {
+    YETI_CHECK(out, YETI_EINVAL, "yeti_ctx_create: out is NULL");
+    *out = nullptr;
+    int n = 0;
+    YETI_CUDA(cudaGetDeviceCount(&n));
+    YETI_CHECK(device >= 0 && device < n, YETI_EINVAL,
+               "yeti_ctx_create: device %d out of range (%d devices)", device,
+               n);
+    DeviceGuard g(device);
+    yeti_ctx *c = new yeti_ctx();
+    c->device = device;
+    c->hbm_budget = hbm_budget_bytes;
+    cudaError_t e = cudaStreamCreateWithFlags(&c->own_stream,
+                                              cudaStreamNonBlocking);
+    if (e != cudaSuccess) {
+        delete c;
+        return cuda_fail(e, "cudaStreamCreate", __FILE__, __LINE__);
+    }
+    c->stream = c->own_stream;
+    *out = c;
+    return YETI_OK;
+}
+
+YETI_API int yeti_ctx_destroy(yeti_ctx *ctx) {
+    if (!ctx) return YETI_OK;
+    DeviceGuard g(ctx->device);
+    if (ctx->own_stream) {
+        cudaStreamSynchronize(ctx->own_stream);
+        cudaStreamDestroy(ctx->own_stream);
+    }
+    delete ctx;
+    return YETI_OK;
+}
+
+YETI_API int yeti_ctx_set_stream(yeti_ctx *ctx, void *stream) {
+    YETI_CHECK(ctx, YETI_EINVAL, "yeti_ctx_set_stream: ctx is NULL");
+    ctx->stream = stream ? static_cast<cudaStream_t>(stream) : ctx->own_stream;
+    return YETI_OK;
+}
+
+YETI_API int yeti_ctx_synchronize(yeti_ctx *ctx) {
+    YETI_CHECK(ctx, YETI_EINVAL, "yeti_ctx_synchronize: ctx is NULL");
+    DeviceGuard g(ctx->device);
+    YETI_CUDA(cudaStreamSynchronize(ctx->stream));
+    return YETI_OK;
+}
+
+YETI_API size_t yeti_ctx_bytes_in_use(const yeti_ctx *ctx) {
+    return ctx ? ctx->bytes_in_use : 0;
+}
