@@ -169,6 +169,9 @@ def _save_model(name, igap, extra=None):
 
 def main():
     IGAparametrization = _load_igaparam()
+    # the .inp reader writes <part>.save files into the working directory
+    import tempfile
+    os.chdir(tempfile.mkdtemp(prefix="yeti_fixtures_"))
 
     # 1. benchs/omp/test_build_stifmatrix_omp.py:41-73 model
     m = IGAparametrization(filename=os.path.join(REF, "benchs/omp/beam-dist"))
