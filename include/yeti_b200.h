@@ -129,6 +129,17 @@ int yeti_assemble_u1_coo(yeti_ctx *ctx, const yeti_u1_model *model,
  */
 typedef struct yeti_wq_op yeti_wq_op;
 
+/* One-direction WQ rule of degree p on nel uniform elements (host memory,
+ * dense row-major nfun x nqp, nfun = p + nel, nqp = 2(p + nel) - 1):
+ * point positions x, basis values B0 and derivatives B1, and weights Wxy for
+ * test derivative order x and trial derivative order y.  Replaces
+ * basis_weights.wq_get_size_data / wq_get_data
+ * (src/yeti_iga/iga_wq_mf/fsrc/iga_wq_basis_weights.f90:198-260); any output
+ * pointer may be NULL. */
+int yeti_wq_rule_1d_size(int p, int nel, int32_t *nfun, int32_t *nqp);
+int yeti_wq_rule_1d(int p, int nel, double *x, double *B0, double *B1,
+                    double *W00, double *W01, double *W10, double *W11);
+
 typedef struct {
     int32_t iterations;        /* total inner (Krylov) iterations        */
     int32_t outer_iterations;  /* FP64 refinement steps (mixed mode)      */

@@ -103,6 +103,10 @@ def test_gpu_coo_matches_oracle(cuda_ok, name):
     np.testing.assert_array_equal(c1, c0)
     assert np.linalg.norm(k1 - k0) <= TOL * np.linalg.norm(k0)
     assert np.abs(k1 - k0).max() <= TOL * np.abs(k0).max()
+    # the FP64 kernels follow the reference's operation order without FMA
+    # contraction: the COO values and the load vector are bit-identical
+    np.testing.assert_array_equal(k1, k0)
+    np.testing.assert_array_equal(f1, f0)
     if np.linalg.norm(f0) > 0:
         assert np.linalg.norm(f1 - f0) <= TOL * np.linalg.norm(f0)
     else:

@@ -23,6 +23,11 @@ NVCC_FLAGS = ["-O3", "-lineinfo", "-std=c++17", "--expt-relaxed-constexpr",
               "-Xptxas", "-O3", "-DNDEBUG"]
 
 
+# Per-file extra flags.  The Gauss-quadrature assembly mirrors the reference's
+# operation order exactly, which requires no FMA contraction.
+EXTRA_FLAGS = {"assemble_u1.cu": ["-fmad=false"]}
+
+
 def nvcc():
     for cand in (os.environ.get("NVCC"), "/usr/local/cuda/bin/nvcc",
                  shutil.which("nvcc")):
@@ -66,7 +71,8 @@ def build(verbose=False, jobs=None):
         obj = os.path.join(BUILD, os.path.basename(src) + ".o")
         objs.append(obj)
         if _stale(obj, [src] + headers):
-            cmd = base + ["-c", src, "-o", obj]
+            cmd = base + EXTRA_FLAGS.get(os.path.basename(src), []) + [
+                "-c", src, "-o", obj]
             if verbose:
                 print(" ".join(cmd))
             procs.append((src, subprocess.Popen(cmd, stdout=subprocess.PIPE,

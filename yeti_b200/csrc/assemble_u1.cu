@@ -403,9 +403,12 @@ k_u1_stiffness(StiffArgs a) {
     }
 }
 
-// Distributed loads of one element: body loads 101 (centrifugal) and 102
-// (volume force) integrated over the volume rule, surface loads 10..99 over
-// the face rule (UELMAT.f90:121-223).
+// Distributed loads (UELMAT.f90:121-223), deterministic and in the reference's
+// operation order.  Phase 1 (k_u1_elem_rhs) evaluates the RHS of each loaded
+// element into a buffer: per-point data first (one thread per quadrature
+// point), then one thread per element dof accumulates over the points in
+// order.  Phase 2 (k_u1_rhs_gather) adds, for every dof, the element
+// contributions in element order (build_system_elemStorage.f90:295-303).
 struct LoadTerm {
     int kind;        // 0: body 101, 1: body 102, 2: surface
     int face, type;  // surface: face 1..6, type 0..4
@@ -429,17 +432,18 @@ struct RhsArgs {
     double rho;
     int nb_n_dist;
     const double *nodal_dist;
-    double *F;
+    double *erhs;             // (n loaded elements, 3*nn)
 };
 
-__global__ void __launch_bounds__(128) k_u1_rhs(RhsArgs a) {
+__global__ void __launch_bounds__(1024) k_u1_elem_rhs(RhsArgs a) {
     extern __shared__ double smem[];
     const int nn = a.nn;
     const int e = a.elems[blockIdx.x];
-    double *xe = smem;
-    double *we = xe + 3 * nn;
-    double *rhs = we + nn;            // 3*nn
-    double *qR = rhs + 3 * nn;        // per Gauss point: R sum inverse
+    const int n0 = a.p0 + 1, n1 = a.p1 + 1, n2 = a.p2 + 1;
+    const int nb = n0 + n1 + n2;
+    double *xe = smem;                 // 3*nn
+    double *we = xe + 3 * nn;          // nn
+    double *qd = we + nn;              // per-point data
     __shared__ double su1[3], su2[3];
     __shared__ int sni[3];
     const int tid = threadIdx.x;
@@ -449,7 +453,6 @@ __global__ void __launch_bounds__(128) k_u1_rhs(RhsArgs a) {
         for (int d = 0; d < 3; d++) xe[3 * i + d] = a.coords[3 * cp + d];
         we[i] = a.w[(size_t)e * nn + i];
     }
-    for (int i = tid; i < 3 * nn; i += blockDim.x) rhs[i] = 0.0;
     if (tid < 3) {
         const double *U = tid == 0 ? a.U0 : (tid == 1 ? a.U1 : a.U2);
         int ni = a.span[3 * e + tid];
@@ -457,106 +460,155 @@ __global__ void __launch_bounds__(128) k_u1_rhs(RhsArgs a) {
         su1[tid] = U[ni - 1];
         su2[tid] = U[ni];
     }
+    const int t0 = a.term_ptr[blockIdx.x], t1 = a.term_ptr[blockIdx.x + 1];
+    int nbody = 0;
+    for (int t = t0; t < t1; t++) nbody += (a.terms[t].kind != 2);
     __syncthreads();
-    (void)qR;
-    for (int ti = a.term_ptr[blockIdx.x]; ti < a.term_ptr[blockIdx.x + 1]; ti++) {
-        const LoadTerm T = a.terms[ti];
-        const int npts = T.kind == 2 ? a.ng * a.ng : a.nq;
-        const double *rule = T.kind == 2 ? a.gface + (size_t)(T.face - 1) * a.ng * a.ng * 4 : a.gauss;
-        for (int q = tid; q < npts; q += blockDim.x) {
+    // R of node n at a point whose basis values are stored at bv
+    auto Rval = [&](const double *bv, double inv, int n) {
+        int i = n % n0, j = (n / n0) % n1, k = n / (n0 * n1);
+        return bv[a.p0 - i] * bv[n0 + a.p1 - j] * bv[n0 + n1 + a.p2 - k] * we[n] * inv;
+    };
+    double acc = 0.0;   // RHS entry (node tid/3, component tid%3)
+    const int node = tid / 3, comp = tid % 3;
+    const bool mine_ok = tid < 3 * nn;
+    // ---- body loads, volume rule (UELMAT.f90:109-171)
+    if (nbody > 0) {
+        const int stride = nb + 2 + 3 * nbody;
+        for (int q = tid; q < a.nq; q += blockDim.x) {
+            const double *g = a.gauss + 4 * q;
+            double Fv[6 * kMaxDeg1], J[3][3], inv;
+            rational_derivs(a.p0, a.p1, a.p2, nn, a.U0, a.U1, a.U2, sni, su1,
+                            su2, g + 1, we, xe, nullptr, J, &inv, Fv);
+            double *o = qd + (size_t)q * stride;
+            for (int i = 0; i < n0; i++) o[i] = Fv[i];
+            for (int i = 0; i < n1; i++) o[n0 + i] = Fv[2 * kMaxDeg1 + i];
+            for (int i = 0; i < n2; i++) o[n0 + n1 + i] = Fv[4 * kMaxDeg1 + i];
+            o[nb] = inv;
+            double dvol = g[0] * fabs(parent_det(J, su1, su2));
+            o[nb + 1] = dvol;
+            double pg[3] = {0.0, 0.0, 0.0};
+            for (int n = 0; n < nn; n++) {
+                double R = Rval(o, inv, n);
+                for (int d = 0; d < 3; d++) pg[d] = pg[d] + R * xe[3 * n + d];
+            }
+            int bt = 0;
+            for (int t = t0; t < t1; t++) {
+                const LoadTerm &T = a.terms[t];
+                if (T.kind == 2) continue;
+                double *pre = o + nb + 2 + 3 * bt;
+                if (T.kind == 0) {      // centrifugal (UELMAT.f90:125-151)
+                    double vd[3], ag[3];
+                    for (int d = 0; d < 3; d++) vd[d] = T.info[3 + d] - T.info[d];
+                    double nr = sqrt(vd[0] * vd[0] + vd[1] * vd[1] + vd[2] * vd[2]);
+                    for (int d = 0; d < 3; d++) vd[d] = vd[d] / nr;
+                    for (int d = 0; d < 3; d++) ag[d] = pg[d] - T.info[d];
+                    double sc = ag[0] * vd[0] + ag[1] * vd[1] + ag[2] * vd[2];
+                    for (int d = 0; d < 3; d++)
+                        pre[d] = a.rho * (T.mag * T.mag) * (ag[d] - sc * vd[d]);
+                } else {                // volume force (UELMAT.f90:153-166)
+                    for (int d = 0; d < 3; d++) pre[d] = T.mag * T.info[d];
+                }
+                bt++;
+            }
+        }
+        __syncthreads();
+        if (mine_ok) {
+            for (int q = 0; q < a.nq; q++) {
+                const double *o = qd + (size_t)q * stride;
+                const double R = Rval(o, o[nb], node), dvol = o[nb + 1];
+                for (int bt = 0; bt < nbody; bt++)
+                    acc = acc + o[nb + 2 + 3 * bt + comp] * R * dvol;
+            }
+        }
+        __syncthreads();
+    }
+    // ---- surface loads, face rule (UELMAT.f90:173-223, shapPress.f)
+    const int nf = a.ng * a.ng;
+    const int fstride = nb + 6;
+    for (int t = t0; t < t1; t++) {
+        const LoadTerm T = a.terms[t];
+        if (T.kind != 2) continue;
+        const double *rule = a.gface + (size_t)(T.face - 1) * nf * 4;
+        for (int q = tid; q < nf; q += blockDim.x) {
             const double *g = rule + 4 * q;
             double Fv[6 * kMaxDeg1], J[3][3], inv;
             rational_derivs(a.p0, a.p1, a.p2, nn, a.U0, a.U1, a.U2, sni, su1,
                             su2, g + 1, we, xe, nullptr, J, &inv, Fv);
+            double *o = qd + (size_t)q * fstride;
+            for (int i = 0; i < n0; i++) o[i] = Fv[i];
+            for (int i = 0; i < n1; i++) o[n0 + i] = Fv[2 * kMaxDeg1 + i];
+            for (int i = 0; i < n2; i++) o[n0 + n1 + i] = Fv[4 * kMaxDeg1 + i];
+            o[nb] = inv;
             double A[3][3];
             for (int r = 0; r < 3; r++)
                 for (int c = 0; c < 3; c++) A[r][c] = J[r][c] * (0.5 * (su2[c] - su1[c]));
-            double vec[3] = {0, 0, 0}, dvol = 0.0;
-            double xg[3] = {0, 0, 0};
-            double *FN = Fv, *FM = Fv + 2 * kMaxDeg1, *FL = Fv + 4 * kMaxDeg1;
-            if (T.kind == 2 || T.kind == 0 || T.type == 4) {
-                int n = 0;
-                for (int k = 0; k <= a.p2; k++)
-                    for (int j = 0; j <= a.p1; j++)
-                        for (int i = 0; i <= a.p0; i++, n++) {
-                            double R = FN[a.p0 - i] * FM[a.p1 - j] * FL[a.p2 - k] * we[n] * inv;
-                            for (int d = 0; d < 3; d++) xg[d] += R * xe[3 * n + d];
-                        }
+            double c1[3] = {A[0][0], A[1][0], A[2][0]};
+            double c2[3] = {A[0][1], A[1][1], A[2][1]};
+            double c3[3] = {A[0][2], A[1][2], A[2][2]};
+            const double *P = c2, *Q = c3;   // surface measure pair
+            switch (T.face) {
+                case 1: case 2: P = c2; Q = c3; break;
+                case 3: case 4: P = c3; Q = c1; break;
+                default: P = c1; Q = c2; break;
+            }
+            double nx = P[1] * Q[2] - P[2] * Q[1];
+            double ny = P[2] * Q[0] - P[0] * Q[2];
+            double nz = P[0] * Q[1] - P[1] * Q[0];
+            double detj = sqrt(nx * nx + ny * ny + nz * nz);
+            double vec[3] = {0.0, 0.0, 0.0};
+            if (T.type >= 1 && T.type <= 3) {
+                vec[T.type - 1] = 1.0;
+            } else {   // normal pressure, orientation of shapPress.f:229-258
+                const double *U = c1, *V = c2;
+                switch (T.face) {
+                    case 1: U = c2; V = c3; break;
+                    case 2: U = c3; V = c2; break;
+                    case 3: U = c3; V = c1; break;
+                    case 4: U = c1; V = c3; break;
+                    case 5: U = c1; V = c2; break;
+                    default: U = c2; V = c1; break;
+                }
+                vec[0] = (U[1] * V[2] - U[2] * V[1]) / detj;
+                vec[1] = (U[2] * V[0] - U[0] * V[2]) / detj;
+                vec[2] = (U[0] * V[1] - U[1] * V[0]) / detj;
             }
             double fmag = T.mag;
-            if (T.kind == 2) {
-                double c1[3] = {A[0][0], A[1][0], A[2][0]};
-                double c2[3] = {A[0][1], A[1][1], A[2][1]};
-                double c3[3] = {A[0][2], A[1][2], A[2][2]};
-                const double *P = c2, *Q = c3;   // surface measure pair
-                switch (T.face) {
-                    case 1: case 2: P = c2; Q = c3; break;
-                    case 3: case 4: P = c3; Q = c1; break;
-                    default: P = c1; Q = c2; break;
-                }
-                double nx = P[1] * Q[2] - P[2] * Q[1];
-                double ny = P[2] * Q[0] - P[0] * Q[2];
-                double nz = P[0] * Q[1] - P[1] * Q[0];
-                double detj = sqrt(nx * nx + ny * ny + nz * nz);
-                if (T.type >= 1 && T.type <= 3) {
-                    vec[T.type - 1] = 1.0;
-                } else {   // normal pressure, orientation of shapPress.f:229-258
-                    const double *U = c1, *V = c2;
-                    switch (T.face) {
-                        case 1: U = c2; V = c3; break;
-                        case 2: U = c3; V = c2; break;
-                        case 3: U = c3; V = c1; break;
-                        case 4: U = c1; V = c3; break;
-                        case 5: U = c1; V = c2; break;
-                        default: U = c2; V = c1; break;
-                    }
-                    vec[0] = (U[1] * V[2] - U[2] * V[1]) / detj;
-                    vec[1] = (U[2] * V[0] - U[0] * V[2]) / detj;
-                    vec[2] = (U[0] * V[1] - U[1] * V[0]) / detj;
-                }
-                dvol = g[0] * detj;
-                if (T.type == 4) {
-                    fmag = 0.0;
-                    int n = 0;
-                    for (int k = 0; k <= a.p2; k++)
-                        for (int j = 0; j <= a.p1; j++)
-                            for (int i = 0; i <= a.p0; i++, n++) {
-                                double R = FN[a.p0 - i] * FM[a.p1 - j] * FL[a.p2 - k] * we[n] * inv;
-                                fmag += a.nodal_dist[T.ifield + (size_t)a.nb_n_dist * ien[n]] * R;
-                            }
-                }
-                for (int d = 0; d < 3; d++) vec[d] *= dvol * fmag;
-            } else {
-                dvol = g[0] * fabs(A[0][0] * A[1][1] * A[2][2] + A[0][1] * A[1][2] * A[2][0] +
-                                   A[1][0] * A[2][1] * A[0][2] - A[0][2] * A[1][1] * A[2][0] -
-                                   A[0][1] * A[1][0] * A[2][2] - A[1][2] * A[2][1] * A[0][0]);
-                if (T.kind == 0) {   // centrifugal, UELMAT.f90:125-151
-                    double vd[3], ag[3];
-                    for (int d = 0; d < 3; d++) vd[d] = T.info[3 + d] - T.info[d];
-                    double nr = sqrt(vd[0] * vd[0] + vd[1] * vd[1] + vd[2] * vd[2]);
-                    for (int d = 0; d < 3; d++) {
-                        vd[d] /= nr;
-                        ag[d] = xg[d] - T.info[d];
-                    }
-                    double sc = ag[0] * vd[0] + ag[1] * vd[1] + ag[2] * vd[2];
-                    for (int d = 0; d < 3; d++)
-                        vec[d] = a.rho * (T.mag * T.mag) * (ag[d] - sc * vd[d]) * dvol;
-                } else {             // volume force, UELMAT.f90:153-166
-                    for (int d = 0; d < 3; d++) vec[d] = T.mag * T.info[d] * dvol;
-                }
+            if (T.type == 4) {
+                fmag = 0.0;
+                for (int n = 0; n < nn; n++)
+                    fmag = fmag + a.nodal_dist[T.ifield + (size_t)a.nb_n_dist * ien[n]] * Rval(o, inv, n);
             }
-            int n = 0;
-            for (int k = 0; k <= a.p2; k++)
-                for (int j = 0; j <= a.p1; j++)
-                    for (int i = 0; i <= a.p0; i++, n++) {
-                        double R = FN[a.p0 - i] * FM[a.p1 - j] * FL[a.p2 - k] * we[n] * inv;
-                        for (int d = 0; d < 3; d++) atomicAdd(&rhs[3 * n + d], R * vec[d]);
-                    }
+            o[nb + 1] = vec[0];
+            o[nb + 2] = vec[1];
+            o[nb + 3] = vec[2];
+            o[nb + 4] = g[0] * detj;
+            o[nb + 5] = fmag;
+        }
+        __syncthreads();
+        if (mine_ok) {
+            double fbl = 0.0;
+            for (int q = 0; q < nf; q++) {
+                const double *o = qd + (size_t)q * fstride;
+                const double R = Rval(o, o[nb], node);
+                fbl = fbl + R * o[nb + 1 + comp] * o[nb + 4] * o[nb + 5];
+            }
+            acc = acc + fbl;
         }
         __syncthreads();
     }
-    for (int i = tid; i < 3 * nn; i += blockDim.x)
-        atomicAdd(&a.F[3 * (size_t)ien[i / 3] + (i % 3)], rhs[i]);
+    if (mine_ok) a.erhs[(size_t)blockIdx.x * 3 * nn + tid] = acc;
+}
+
+// F[dof] += element contributions in element order.
+__global__ void k_u1_rhs_gather(int64_t ndof, const int64_t *ptr,
+                                const int64_t *idx, const double *erhs,
+                                double *F) {
+    int64_t dof = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (dof >= ndof) return;
+    double acc = F[dof];
+    for (int64_t k = ptr[dof]; k < ptr[dof + 1]; k++) acc = acc + erhs[idx[k]];
+    F[dof] = acc;
 }
 
 static bool in_list(const int64_t *l, int64_t n, int64_t v) {
@@ -636,6 +688,14 @@ YETI_API int yeti_assemble_u1_coo(yeti_ctx *ctx, const yeti_u1_model *m,
         keep.emplace_back(new DevBuf());
         return *keep.back();
     };
+    struct Loaded { int patch; int64_t local; int64_t off; };
+    struct PatchRhs { DevBuf *buf; size_t first; };
+    std::vector<Loaded> loaded;
+    std::vector<PatchRhs> patch_erhs;
+    int64_t erhs_total = 0;
+    std::vector<int64_t> ien_offset(M.patches.size(), 0);
+    for (size_t ip = 1; ip < M.patches.size(); ip++)
+        ien_offset[ip] = ien_offset[ip - 1] + M.patches[ip - 1].nelem * M.patches[ip - 1].nn;
     for (size_t ip = 0; ip < M.patches.size(); ip++) {
         U1Patch &P = M.patches[ip];
         if (!P.nactive) continue;
@@ -672,10 +732,12 @@ YETI_API int yeti_assemble_u1_coo(yeti_ctx *ctx, const yeti_u1_model *m,
         // ---- distributed loads of this patch's elements
         std::vector<int32_t> elems, tptr(1, 0);
         std::vector<LoadTerm> terms;
+        int max_body = 0;
         for (int64_t le = 0; le < P.nactive; le++) {
             const int64_t jel = P.act[le] + 1;   // 1-based element number
             int64_t k2 = 0, cinfo = 0;
             size_t before = terms.size();
+            int nbody = 0;
             for (int64_t il = 0; il < m->nb_load; il++) {
                 int64_t nt = m->load_target_nbelem[il], ty = m->jdltype[il];
                 if ((ty == 101 || ty == 102 || (ty > 9 && ty < 100)) &&
@@ -689,6 +751,7 @@ YETI_API int yeti_assemble_u1_coo(yeti_ctx *ctx, const yeti_u1_model *m,
                         YETI_CHECK(cinfo + nneed <= m->len_load_addinfos, YETI_EINVAL,
                                    "load %lld: missing additional infos", (long long)il + 1);
                         for (int d = 0; d < nneed; d++) T.info[d] = m->load_addinfos[cinfo + d];
+                        nbody++;
                     } else {
                         T.kind = 2;
                         T.face = (int)(ty / 10);
@@ -709,9 +772,15 @@ YETI_API int yeti_assemble_u1_coo(yeti_ctx *ctx, const yeti_u1_model *m,
             if (terms.size() > before) {
                 elems.push_back((int32_t)le);
                 tptr.push_back((int32_t)terms.size());
+                max_body = std::max(max_body, nbody);
+                loaded.push_back({(int)ip, le, erhs_total});
+                erhs_total += 3LL * P.nn;
             }
         }
         if (!elems.empty()) {
+            YETI_CHECK(P.nn * 3 <= 1024, YETI_EUNSUPPORTED,
+                       "distributed loads on elements with more than 341 nodes "
+                       "are not supported");
             std::vector<double> gf(6 * 4 * P.ng * P.ng), tmp;
             for (int f = 1; f <= 6; f++) {
                 gauss_face_host(P.ng, f, tmp);
@@ -730,6 +799,9 @@ YETI_API int yeti_assemble_u1_coo(yeti_ctx *ctx, const yeti_u1_model *m,
                 dnd = &newbuf();
                 YETI_TRY(upload(ctx, *dnd, m->nodal_dist, (size_t)m->nb_n_dist * m->nb_cp));
             }
+            DevBuf &der = newbuf();
+            YETI_TRY(der.alloc(ctx, sizeof(double) * 3 * P.nn * elems.size()));
+            patch_erhs.push_back({&der, loaded.size() - elems.size()});
             RhsArgs r;
             r.p0 = P.p[0]; r.p1 = P.p[1]; r.p2 = P.p[2];
             r.nn = P.nn; r.nq = P.nq; r.ng = P.ng;
@@ -746,13 +818,51 @@ YETI_API int yeti_assemble_u1_coo(yeti_ctx *ctx, const yeti_u1_model *m,
             r.rho = P.rho;
             r.nb_n_dist = (int)m->nb_n_dist;
             r.nodal_dist = dnd ? dnd->as<double>() : nullptr;
-            r.F = f_;
-            size_t smem = sizeof(double) * (4 * P.nn + 3 * P.nn + 8);
+            r.erhs = der.as<double>();
+            const int nb = P.p[0] + P.p[1] + P.p[2] + 3;
+            const size_t per = std::max<size_t>((size_t)P.nq * (nb + 2 + 3 * max_body),
+                                                (size_t)P.ng * P.ng * (nb + 6));
+            size_t smem = sizeof(double) * (4 * P.nn + per);
             YETI_CHECK(smem <= smem_cap, YETI_EUNSUPPORTED, "element too large for the load kernel");
-            YETI_CUDA(cudaFuncSetAttribute(k_u1_rhs, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_cap));
-            k_u1_rhs<<<(unsigned)elems.size(), 128, smem, ctx->stream>>>(r);
+            YETI_CUDA(cudaFuncSetAttribute(k_u1_elem_rhs, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_cap));
+            const int nthr = std::max(128, (3 * P.nn + 31) / 32 * 32);
+            k_u1_elem_rhs<<<(unsigned)elems.size(), nthr, smem, ctx->stream>>>(r);
             YETI_CUDA(cudaGetLastError());
         }
+    }
+    // ---- phase 2: per-dof sums of the element contributions, element order
+    if (!loaded.empty()) {
+        // one contiguous buffer: copy each patch's element RHS slice in order
+        DevBuf &dall = newbuf();
+        YETI_TRY(dall.alloc(ctx, sizeof(double) * erhs_total));
+        int64_t off = 0;
+        for (auto &pe : patch_erhs) {
+            YETI_CUDA(cudaMemcpyAsync(dall.as<double>() + off, pe.buf->ptr, pe.buf->bytes,
+                                      cudaMemcpyDeviceToDevice, ctx->stream));
+            off += (int64_t)(pe.buf->bytes / sizeof(double));
+        }
+        std::vector<int64_t> cnt(ndof + 1, 0), idx;
+        std::vector<std::vector<int64_t>> lists(ndof);
+        for (auto &L : loaded) {
+            const U1Patch &P = M.patches[L.patch];
+            const int64_t jel = P.act[L.local];
+            const int64_t ien_base = ien_offset[L.patch] + (jel - P.elem_begin) * P.nn;
+            for (int n = 0; n < P.nn; n++) {
+                int64_t cp = m->ien[ien_base + n] - 1;
+                for (int d = 0; d < 3; d++) lists[3 * cp + d].push_back(L.off + 3 * n + d);
+            }
+        }
+        for (int64_t i = 0; i < ndof; i++) {
+            cnt[i + 1] = cnt[i] + (int64_t)lists[i].size();
+            idx.insert(idx.end(), lists[i].begin(), lists[i].end());
+        }
+        DevBuf &dptr = newbuf();
+        YETI_TRY(upload(ctx, dptr, cnt.data(), cnt.size()));
+        DevBuf &didx = newbuf();
+        YETI_TRY(upload(ctx, didx, idx.data(), idx.size()));
+        k_u1_rhs_gather<<<(unsigned)((ndof + 255) / 256), 256, 0, ctx->stream>>>(
+            ndof, dptr.as<int64_t>(), didx.as<int64_t>(), dall.as<double>(), f_);
+        YETI_CUDA(cudaGetLastError());
     }
     if (mem == YETI_MEM_HOST) {
         YETI_CUDA(cudaMemcpyAsync(kdata, k_, nb_data * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));

@@ -32,13 +32,21 @@ __host__ __device__ inline void bspline_ders(int ni, int p, double u,
         ndu[j][j] = saved;
     }
     for (int j = 0; j <= p; j++) N[j] = ndu[j][p];
+    // first derivatives in the reciprocal form of the reference's k-loop
+    // (dersbasisfuns.f90:79-124 with nders = 1)
     for (int r = 0; r <= p; r++) {
         double d = 0.0;
         if (p >= 1) {
-            if (r >= 1) d = ndu[r - 1][p - 1] / ndu[p][r - 1];
-            if (r <= p - 1) d -= ndu[r][p - 1] / ndu[p][r];
+            if (r >= 1) {
+                double a = 1.0 / ndu[p][r - 1];
+                d = a * ndu[r - 1][p - 1];
+            }
+            if (r <= p - 1) {
+                double a = -1.0 / ndu[p][r];
+                d = d + a * ndu[r][p - 1];
+            }
         }
-        dN[r] = d * p;
+        dN[r] = d * (double)p;
     }
 }
 
