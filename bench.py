@@ -1,0 +1,372 @@
+"""Benchmark: solved DOF/s of the weighted-quadrature elasticity solve.
+
+Workload (one step = one complete Jacobi-PCG solve): the unit-cube NURBS patch
+of degree 3 with 64 x 64 x 64 elements (67^3 control points, 902,289 dofs),
+interior control points perturbed U(-0.2h, 0.2h), weights U(0.8, 1.2), E=1,
+nu=0.3, clamped at z=0, body force (0, 0, -1), solved with FP32 operator and
+inner PCG plus FP64 residual / iterative refinement.  Synthetic, seeded
+inputs; the operator data (~1.35 GB) is far larger than L2, so no L2 flush
+is needed between steps.
+
+    python bench.py [--gpus N --steps K --warmup W] [--impl reference]
+
+Prints one JSON line (rank 0).  Under torchrun each rank solves its own
+replica (no collective in the data path: replicas only).
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+METRIC = ("solved DOF/s at rel.err<=1e-8 (mixed vs plain FP64, 1 B200); "
+          "serve p50/p99 ms")
+WORKLOAD = {"workload": "WQ elasticity PCG, unit-cube NURBS patch p=3 64^3 "
+                        "elements, perturbed +-0.2h, weights U(0.8,1.2), "
+                        "E=1 nu=0.3, clamped z=0, body force (0,0,-1)",
+            "nel": [64, 64, 64], "p": 3, "seed": 20261203,
+            "l2": "operator data (1.35 GB) larger than L2: no flush needed"}
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--nel", type=int, nargs=3, default=[64, 64, 64])
+    ap.add_argument("--p", type=int, default=3)
+    ap.add_argument("--rtol", type=float, default=1e-8)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def measured_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def profiled_traffic(name):
+    """Bytes per launch read from a committed ncu summary (profiles/), if any:
+    a line 'traffic_bytes_per_launch: <float>'."""
+    path = os.path.join(ROOT, "profiles", name)
+    try:
+        for line in open(path):
+            if line.startswith("traffic_bytes_per_launch:"):
+                return float(line.split(":")[1])
+    except OSError:
+        pass
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi samples of SM clock and throttle reasons during a region."""
+
+    Q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                 "-lms", "200", "-i", str(self.device)],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.t.join(timeout=2)
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 8:
+                continue
+            try:
+                sm.append(float(f[0]))
+                mx = float(f[1])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[4:8]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_init():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if ws > 1:
+        import torch
+        import torch.distributed as dist
+        from datetime import timedelta
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600),
+                                device_id=torch.device("cuda", local))
+    return ws, rank, local
+
+
+def max_over_ranks(x, ws):
+    if ws == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(ws):
+    if ws > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+# ------------------------------------------------------------ CPU baseline
+def cpu_reference_rate(args, iters_fp64, sample_applies=1):
+    """The reference's algorithm on the host cores: the restated
+    mf_wq_get_ku_3d with the rank-one sparse products of
+    tensor3d_sparsedot_vector (oracle/oracle_wq.c, OpenMP over all cores),
+    one apply timed on the full workload; solved DOF/s = n_free /
+    (iterations x time per CG iteration)."""
+    import oracle.wq_cpu as wc
+    from yeti_b200.patches import cube_patch
+    P = cube_patch(tuple(args.nel), args.p, perturb=0.2, wrange=(0.8, 1.2),
+                   seed=WORKLOAD["seed"])
+    res = wc.time_reference_apply(P, 1.0, 0.3, {"w0": (0, 1, 2)},
+                                  n_applies=sample_applies)
+    t_iter = res["seconds_per_apply"] + res["seconds_per_vector_ops"]
+    nfree = res["nfree"]
+    return {"value": nfree / (iters_fp64 * t_iter), "unit": "DOF/s",
+            "cores": res["threads"], "kind": "port",
+            "sample": (f"{sample_applies} operator apply(ies) of the full "
+                       f"{args.nel} p={args.p} workload with the reference's "
+                       f"rank-one sparse products ({res['seconds_per_apply']:.2f} s "
+                       f"each), scaled by the {iters_fp64} Jacobi-PCG iterations "
+                       f"the FP64 solve needs")}
+
+
+def run_reference(args):
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    iters = ITERS_FP64_DEFAULT
+    vals = []
+    base = None
+    for _ in range(args.warmup + args.steps):
+        base = cpu_reference_rate(args, iters)
+        vals.append(base["value"])
+    v = statistics.median(vals[args.warmup:]) if args.steps else vals[-1]
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "DOF/s",
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": dict(WORKLOAD, nel=args.nel, p=args.p),
+            "cpu_baseline": dict(base, value=v),
+            "e2e": {"value": v, "unit": "DOF/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# Iterations of the FP64 Jacobi-PCG on the default workload (measured on a
+# B200 with this code; used only by the CPU reference arm, which cannot run
+# a full CPU solve within the time limit).
+ITERS_FP64_DEFAULT = 900
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    import torch
+
+    from yeti_b200 import _lib
+    from yeti_b200.patches import cube_patch
+    from yeti_b200.wq import WQElasticity
+
+    ws, rank, local = dist_init()
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    ctx = _lib.default_context(local)
+    ctx.set_stream(torch.cuda.current_stream(dev))
+    L = _lib.lib()
+    seed = WORKLOAD["seed"] + rank
+    P = cube_patch(tuple(args.nel), args.p, perturb=0.2, wrange=(0.8, 1.2), seed=seed)
+    t0 = time.perf_counter()
+    op = WQElasticity(P, 1.0, 0.3, {"w0": (0, 1, 2)}, precisions="both", ctx=ctx)
+    setup_s = time.perf_counter() - t0
+    b_host = op.eval_bodyforce_vector([0.0, 0.0, -1.0])
+    b = torch.from_numpy(b_host).to(dev)
+
+    # FP64 reference solution (untimed, tight) and the plain FP64 solve
+    xref, st_ref = op.pcg(b, rtol=1e-12)
+    torch.cuda.synchronize()
+    x64, st64 = op.pcg(b, rtol=args.rtol)
+    err64 = (torch.linalg.norm(x64 - xref) / torch.linalg.norm(xref)).item()
+
+    def step():
+        x, st = op.pcg(b, rtol=args.rtol, mixed=True)
+        return x, st
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    barrier(ws)
+    clocks = ClockSampler(local)
+    clocks.start()
+    l0 = L.yeti_kernel_launches()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record()
+    stats = []
+    for _ in range(args.steps):
+        x, st = step()
+        stats.append(st)
+    e1.record()
+    torch.cuda.synchronize()
+    launches = L.yeti_kernel_launches() - l0
+    ms = e0.elapsed_time(e1)
+    clk = clocks.stop()
+    ms = max_over_ranks(ms, ws)
+    barrier(ws)
+    err = (torch.linalg.norm(x - xref) / torch.linalg.norm(xref)).item()
+    value = ws * op.nfree * args.steps / (ms / 1e3)
+
+    # plain FP64 throughput for the same tolerance (device-resident)
+    e0.record()
+    for _ in range(max(1, args.steps)):
+        op.pcg(b, rtol=args.rtol)
+    e1.record()
+    torch.cuda.synchronize()
+    ms64 = e0.elapsed_time(e1) / max(1, args.steps)
+
+    # end to end through the public API with pinned host buffers
+    bh = torch.empty(op.ndof, dtype=torch.float64, pin_memory=True)
+    bh.copy_(torch.from_numpy(b_host))
+    bh_np = bh.numpy()
+    torch.cuda.synchronize()
+    e0.record()
+    t_wall = time.perf_counter()
+    for _ in range(args.steps):
+        xh, _ = op.pcg(bh_np, rtol=args.rtol, mixed=True)
+    e1.record()
+    torch.cuda.synchronize()
+    ms_e2e = max_over_ranks(e0.elapsed_time(e1), ws)
+    wall_e2e = time.perf_counter() - t_wall
+
+    # roofline of the dominant kernel: the FP32 operator apply
+    u32 = torch.randn(op.ndof, dtype=torch.float32, device=dev)
+    k32 = torch.empty_like(u32)
+    for _ in range(5):
+        op.apply_device(u32, k32, "f32")
+    torch.cuda.synchronize()
+    napp = 30
+    e0.record()
+    for _ in range(napp):
+        op.apply_device(u32, k32, "f32")
+    e1.record()
+    torch.cuda.synchronize()
+    t_app = e0.elapsed_time(e1) / napp / 1e3
+    alg_bytes = op.nqp * 48 * 4 + 2 * op.ndof * 4
+    peak, peak_kind = measured_peaks()
+    achieved = alg_bytes / t_app / 1e9
+    u64 = u32.double()
+    k64 = torch.empty_like(u64)
+    op.apply_device(u64, k64, "f64")
+    e0.record()
+    for _ in range(10):
+        op.apply_device(u64, k64, "f64")
+    e1.record()
+    torch.cuda.synchronize()
+    t_app64 = e0.elapsed_time(e1) / 10 / 1e3
+
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        try:
+            cpu = cpu_reference_rate(args, st64["iterations"])
+        except Exception as exc:  # report, do not hide
+            cpu = {"value": None, "error": repr(exc)[:200]}
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "DOF/s", "n_gpus": ws,
+            "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "precision": "FP32 operator + inner PCG, FP64 residual and refinement",
+            "data": "synthetic",
+            "config": dict(WORKLOAD, nel=args.nel, p=args.p, rtol=args.rtol,
+                           parallelism=f"replicas x{ws}", ndof=op.ndof,
+                           nfree=op.nfree, nqp=op.nqp),
+            "solve": {"iterations": stats[-1]["iterations"],
+                      "outer_iterations": stats[-1]["outer_iterations"],
+                      "fp64_applies": stats[-1]["fp64_applies"],
+                      "rel_residual": stats[-1]["rel_residual"],
+                      "rel_residual_inf": stats[-1]["rel_residual_inf"],
+                      "rel_error_vs_fp64_ref": err,
+                      "ref_rel_residual": st_ref["rel_residual"]},
+            "fp64": {"value": ws * op.nfree / (ms64 / 1e3), "ms_per_step": ms64,
+                     "iterations": st64["iterations"], "rel_error_vs_fp64_ref": err64},
+            "mixed_over_fp64": (value / ws) / (op.nfree / (ms64 / 1e3)),
+            "setup_s": setup_s,
+            "e2e": {"value": ws * op.nfree * args.steps / (ms_e2e / 1e3), "unit": "DOF/s",
+                    "h2d_bytes_per_step": 2 * op.ndof * 8,
+                    "d2h_bytes_per_step": op.ndof * 8,
+                    "wall_s": wall_e2e},
+            "gpu_launches": int(launches),
+            "roofline": {"bound": "hbm", "kernel": "k_wq_apply<float>",
+                         "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "peak_kind": peak_kind,
+                         "traffic": profiled_traffic("wq_apply_f32_p3_64cube.txt"),
+                         "alg_bytes_per_launch": alg_bytes,
+                         "apply_us": t_app * 1e6, "apply_f64_us": t_app64 * 1e6,
+                         "f64_frac": (op.nqp * 48 * 8 + 2 * op.ndof * 8) / t_app64 / 1e9 / peak},
+            "cpu_baseline": cpu,
+            "clocks": clk,
+            "serve": None,
+        }
+        print(json.dumps(line), flush=True)
+    if ws > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -55,6 +55,9 @@ typedef struct yeti_ctx yeti_ctx;
 const char *yeti_last_error(void);
 /* Library version string. */
 const char *yeti_version(void);
+/* Number of CUDA kernels the library has launched in this process (no
+ * counterpart in the reference: evidence that the device path ran). */
+uint64_t yeti_kernel_launches(void);
 
 /* Create a context on CUDA device `device`.  The context owns a stream
  * (non-blocking) unless yeti_ctx_set_stream() supplies one.  hbm_budget_bytes

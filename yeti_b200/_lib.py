@@ -62,6 +62,7 @@ def _declare(lib):
     sig = {
         "yeti_last_error": (ctypes.c_char_p, []),
         "yeti_version": (ctypes.c_char_p, []),
+        "yeti_kernel_launches": (ctypes.c_uint64, []),
         "yeti_ctx_create": (i32, [i32, ctypes.c_size_t, ctypes.POINTER(vp)]),
         "yeti_ctx_destroy": (i32, [vp]),
         "yeti_ctx_set_stream": (i32, [vp, vp]),

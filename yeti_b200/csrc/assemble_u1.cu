@@ -726,6 +726,7 @@ YETI_API int yeti_assemble_u1_coo(yeti_ctx *ctx, const yeti_u1_model *m,
             StiffArgs b = a;
             b.ien += off * P.nn; b.w += off * P.nn; b.span += off * 3; b.slot += off;
             k_u1_stiffness<<<(unsigned)n, 256, smem, ctx->stream>>>(b);
+            count_launches(1);
             YETI_CUDA(cudaGetLastError());
             left -= n; off += n;
         }
@@ -827,6 +828,7 @@ YETI_API int yeti_assemble_u1_coo(yeti_ctx *ctx, const yeti_u1_model *m,
             YETI_CUDA(cudaFuncSetAttribute(k_u1_elem_rhs, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_cap));
             const int nthr = std::max(128, (3 * P.nn + 31) / 32 * 32);
             k_u1_elem_rhs<<<(unsigned)elems.size(), nthr, smem, ctx->stream>>>(r);
+            count_launches(1);
             YETI_CUDA(cudaGetLastError());
         }
     }
@@ -862,6 +864,7 @@ YETI_API int yeti_assemble_u1_coo(yeti_ctx *ctx, const yeti_u1_model *m,
         YETI_TRY(upload(ctx, didx, idx.data(), idx.size()));
         k_u1_rhs_gather<<<(unsigned)((ndof + 255) / 256), 256, 0, ctx->stream>>>(
             ndof, dptr.as<int64_t>(), didx.as<int64_t>(), dall.as<double>(), f_);
+        count_launches(1);
         YETI_CUDA(cudaGetLastError());
     }
     if (mem == YETI_MEM_HOST) {

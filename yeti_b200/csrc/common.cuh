@@ -123,4 +123,8 @@ struct DeviceGuard {
 // Is `p` device-accessible memory (device or managed)?
 bool is_device_pointer(const void *p);
 
+// Process-wide count of kernel launches issued by the library (reported by
+// yeti_kernel_launches(); lets callers verify the device path ran).
+void count_launches(uint64_t n);
+
 }  // namespace yeti

@@ -1,4 +1,5 @@
 // Context management, error reporting and device-memory accounting.
+#include <atomic>
 #include <cstdarg>
 #include <cstring>
 
@@ -47,6 +48,10 @@ void dev_free(yeti_ctx *ctx, void *ptr, size_t bytes) {
     if (ctx) ctx->bytes_in_use -= (bytes ? bytes : 16);
 }
 
+static std::atomic<uint64_t> g_launches{0};
+
+void count_launches(uint64_t n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+
 bool is_device_pointer(const void *p) {
     cudaPointerAttributes a;
     if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
@@ -63,6 +68,10 @@ using namespace yeti;
 YETI_API const char *yeti_last_error(void) { return g_err; }
 
 YETI_API const char *yeti_version(void) { return "yeti_b200 0.1 (sm_100a)"; }
+
+YETI_API uint64_t yeti_kernel_launches(void) {
+    return g_launches.load(std::memory_order_relaxed);
+}
 
 YETI_API int yeti_ctx_create(int device, size_t hbm_budget_bytes,
                              yeti_ctx **out) {

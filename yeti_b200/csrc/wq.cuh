@@ -1,0 +1,90 @@
+// Weighted-quadrature (WQ) elasticity on one NURBS patch: shared definitions
+// of the host setup and the device kernels.
+//
+// Data layout in HBM
+// ------------------
+// The patch's tensor grid of WQ points is cut into element blocks
+// (blk_u x blk_v x blk_w).  Every point belongs to exactly one element (the
+// element whose half-open knot span holds it; the last element also owns
+// the end point), hence to exactly one block.  Per-point operator data are
+// stored block by block, entry-major inside a block:
+//     coef[(qoff[b] * 48) + e * nq_b + local_point]
+// so one CTA streams one contiguous chunk and consecutive threads read
+// consecutive addresses.  The 48 entries are the upper triangle of the
+// symmetric 9x9 S^ = S / W^2 (45, row-major, index sym9) and g = grad W / W.
+// Vectors are component-major [c][iw][iv][iu].
+#pragma once
+#include <vector>
+
+#include "common.cuh"
+#include "wq_rule.h"
+
+namespace yeti {
+
+constexpr int kWQCoef = 48;
+constexpr int kWQThreads = 256;
+
+__host__ __device__ constexpr int sym9(int I, int J) {
+    return I <= J ? I * 9 - I * (I - 1) / 2 + (J - I)
+                  : J * 9 - J * (J - 1) / 2 + (I - J);
+}
+
+// Per block position along one direction: first element, element count,
+// first owned point, owned point count.
+struct BlkInfo {
+    int e0, ne, q0, nq;
+};
+
+// One direction as seen by the kernels.
+struct WQAxis {
+    int p, nfun, nqp, nb;   // degree, functions, points, blocks
+    int NF, NQ;             // max functions / points of a block (tile dims)
+    const BlkInfo *blk;     // nb entries
+};
+
+// Everything a kernel needs about the patch (passed by value).
+template <class T>
+struct WQView {
+    WQAxis ax[3];
+    const T *tiles[3];      // [nb][6][NF][NQ]: B0 B1 W00 W01 W10 W11
+    const int64_t *qoff;    // first point (block-tiled numbering) of a block
+    const T *coef;          // [nqp_total * 48] block-tiled, entry-major
+    const T *wcp;           // CP weights (ncp)
+    int cmask[3];           // clamped faces per component (bit f)
+    int64_t ncp;
+};
+
+}  // namespace yeti
+
+struct yeti_wq_op;
+namespace yeti {
+// Enqueue Ku += K u (Ku must be zeroed by the caller) on stream s; prec
+// YETI_PREC_F64 / F32 selects the operator data and the vector type.  done:
+// optional device flag, the kernel returns at once when it is set.
+int wq_apply_dev(yeti_wq_op *op, const void *u, void *Ku, int prec,
+                 const int *done, cudaStream_t s);
+}  // namespace yeti
+
+// The operator object behind the opaque yeti_wq_op handle.
+struct yeti_wq_op {
+    yeti_ctx *ctx = nullptr;
+    int p[3] = {0, 0, 0}, nel[3] = {0, 0, 0}, n[3] = {0, 0, 0};
+    int nqp[3] = {0, 0, 0};
+    int64_t ncp = 0, ndof = 0, nfree = 0, nqp_total = 0, nblocks = 0;
+    int prec_mask = 0;
+    int cmask[3] = {0, 0, 0};
+    double E = 0, nu = 0;
+    std::vector<yeti::BlkInfo> blk[3];
+    int NF[3] = {0, 0, 0}, NQ[3] = {0, 0, 0};
+    yeti::DevBuf blkd[3];
+    yeti::DevBuf tiles64[3], tiles32[3], dtiles[3];
+    yeti::DevBuf qoff;
+    yeti::DevBuf coef64, coef32;
+    yeti::DevBuf w64, w32;
+    yeti::DevBuf jw;        // |detJ| / W per point (FP64, block-tiled)
+    yeti::DevBuf diag;      // diagonal (FP64, clamped dofs = 1)
+    yeti::DevBuf dinv64, dinv32;
+    yeti::DevBuf ws64, ws32, scal, parts;   // PCG workspaces
+    double setup_ms = 0.0;
+    int64_t bytes_data = 0;
+};

@@ -1,0 +1,137 @@
+"""Weighted-quadrature matrix-free elasticity on the GPU.
+
+``WQElasticity`` mirrors the reference's WQ driver
+``iga_wq_mf/ThermoMechaIGA/pysrc/lib/fortran_mf_wq.py`` for the mechanical
+problem: ``eval_Ku`` (``:404-419``), ``eval_bodyforce_vector`` (``:493-513``)
+and ``mf_conj_grad`` (``:545-560``), on one NURBS patch with uniform open knot
+vectors.  Everything runs in libyeti_b200.so (``yeti_wq_*``).
+
+Vectors are component-major ``[c][iw][iv][iu]`` of length 3*ncp, clamped
+dofs included and held at zero.
+"""
+import ctypes
+
+import numpy as np
+
+from . import _lib
+from ._lib import CGStats, MEM_DEVICE, MEM_HOST, PREC_F32, PREC_F64, check, lib, ptr
+from .patches import face_mask, free_mask
+
+WQ_F64, WQ_F32 = 1, 2
+
+
+class WQElasticity:
+    """WQ operator of a patch (see ``yeti_b200.patches.cube_patch``).
+
+    clamp_faces: {'u0'|'u1'|'v0'|'v1'|'w0'|'w1': components} clamps those
+    displacement components on the face (the reference erases the matching
+    rows of its 1-D matrices, fortran_mf_wq.py:240-267).
+    precisions: 'f64', 'f32' or 'both' operator data to keep on the device.
+    """
+
+    def __init__(self, patch, E, nu, clamp_faces=None, precisions="both",
+                 ctx=None):
+        self.ctx = ctx or _lib.default_context()
+        self.patch = patch
+        self.clamp_faces = clamp_faces or {}
+        mask = {"f64": WQ_F64, "f32": WQ_F32, "both": WQ_F64 | WQ_F32}[precisions]
+        p = np.ascontiguousarray(patch["p"], dtype=np.int32)
+        nel = np.ascontiguousarray(patch["nel"], dtype=np.int32)
+        cps = np.ascontiguousarray(patch["cps"], dtype=np.float64)
+        w = np.ascontiguousarray(patch["weights"], dtype=np.float64)
+        dm = face_mask(self.clamp_faces)
+        h = ctypes.c_void_p()
+        check(lib().yeti_wq_setup(self.ctx.handle, ptr(p), ptr(nel), ptr(cps),
+                                  ptr(w), float(E), float(nu), ptr(dm), mask,
+                                  ctypes.byref(h)), "yeti_wq_setup")
+        self.handle = h
+        vals = [ctypes.c_int64() for _ in range(5)]
+        check(lib().yeti_wq_info(h, *[ctypes.byref(v) for v in vals]),
+              "yeti_wq_info")
+        self.ncp, self.ndof, self.nfree, self.nqp, self.bytes = (v.value for v in vals)
+        self.free_mask = free_mask(patch, self.clamp_faces)
+
+    # ------------------------------------------------------------- operator
+    def eval_Ku(self, u, precision="f64"):
+        """K u.  u: numpy array (host) or torch CUDA tensor (device, result
+        returned as a tensor of the same dtype)."""
+        prec = PREC_F64 if precision == "f64" else PREC_F32
+        if isinstance(u, np.ndarray):
+            dt = np.float64 if prec == PREC_F64 else np.float32
+            uu = np.ascontiguousarray(u, dtype=dt)
+            out = np.empty_like(uu)
+            check(lib().yeti_wq_apply(self.handle, ptr(uu), ptr(out), prec,
+                                      MEM_HOST), "yeti_wq_apply")
+            return out
+        import torch
+        uu = u.contiguous()
+        out = torch.empty_like(uu)
+        check(lib().yeti_wq_apply(self.handle, ptr(uu), ptr(out), prec,
+                                  MEM_DEVICE), "yeti_wq_apply")
+        return out
+
+    def apply_device(self, u, out, precision="f64"):
+        """out = K u for device tensors (no allocation, no host sync)."""
+        prec = PREC_F64 if precision == "f64" else PREC_F32
+        check(lib().yeti_wq_apply(self.handle, ptr(u), ptr(out), prec,
+                                  MEM_DEVICE), "yeti_wq_apply")
+
+    def diag(self):
+        d = np.empty(self.ndof)
+        check(lib().yeti_wq_diag(self.handle, ptr(d), MEM_HOST), "yeti_wq_diag")
+        return d
+
+    def eval_bodyforce_vector(self, f):
+        """Load vector of a constant body-force density f = (fx, fy, fz)."""
+        ff = np.ascontiguousarray(f, dtype=np.float64)
+        out = np.empty(self.ndof)
+        check(lib().yeti_wq_body_force(self.handle, ptr(ff), ptr(out),
+                                       MEM_HOST), "yeti_wq_body_force")
+        return out
+
+    # --------------------------------------------------------------- solver
+    def pcg(self, b, rtol=1e-8, maxit=20000, mixed=False, x0=None):
+        """Jacobi PCG.  b, x0: numpy (host) or torch CUDA float64 tensors.
+        Returns (x, stats dict)."""
+        st = CGStats()
+        mode = 1 if mixed else 0
+        if isinstance(b, np.ndarray):
+            bb = np.ascontiguousarray(b, dtype=np.float64)
+            x = np.zeros_like(bb) if x0 is None else np.array(x0, dtype=np.float64)
+            mem = MEM_HOST
+        else:
+            import torch
+            bb = b.contiguous()
+            x = torch.zeros_like(bb) if x0 is None else x0.clone()
+            mem = MEM_DEVICE
+        rc = lib().yeti_wq_pcg(self.handle, ptr(bb), ptr(x), float(rtol),
+                               int(maxit), mode, ctypes.byref(st), mem)
+        check(rc, "yeti_wq_pcg")
+        return x, st.as_dict()
+
+    def mf_conj_grad(self, bi, nbIterations, epsilon, method="WP",
+                     directsol=None, isCG=True, mixed=False):
+        """Twin of fortran_mf_wq.mf_conj_grad (fortran_mf_wq.py:545-560):
+        returns (sol, residue, error) with residue/error the reference's
+        inf-norm measures at the start and the end of the solve."""
+        if method != "WP" or not isCG:
+            raise NotImplementedError("Jacobi-preconditioned CG only")
+        x, st = self.pcg(bi, rtol=epsilon, maxit=nbIterations, mixed=mixed)
+        residue = np.array([1.0, st["rel_residual_inf"]])
+        error = np.array([1.0, 0.0])
+        if directsol is not None:
+            ds = np.asarray(directsol)
+            error[1] = np.abs(ds - x).max() / np.abs(ds).max()
+        self.last_stats = st
+        return x, residue, error
+
+    def close(self):
+        if getattr(self, "handle", None):
+            lib().yeti_wq_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
