@@ -174,9 +174,11 @@ int yeti_wq_diag(yeti_wq_op *op, double *d, int mem);
 /* Body-force load vector for a constant force density f[3]
  * (wq_get_force_3d, wq_assembly.f90:1193-1251). */
 int yeti_wq_body_force(yeti_wq_op *op, const double f[3], double *F, int mem);
-/* Jacobi-preconditioned CG on K x = b (x holds the initial guess).
- * mode 0: plain FP64.  mode 1: FP32 operator and inner PCG with FP64
- * residual and iterative-refinement correction.  Stops when the FP64 true
+/* Jacobi-preconditioned Krylov solve of K x = b (x holds the initial guess;
+ * replaces wq_mf_cg_3d / wq_mf_bicgstab_3d, mf_wq_solver.f90:642,958).
+ * mode bit 0: mixed precision (FP32 operator and Krylov vectors, FP64 true
+ * residual and solution: reliable updates for CG, iterative refinement for
+ * BiCGSTAB); bit 1: BiCGSTAB instead of CG.  Stops when the FP64 true
  * residual satisfies ||r||_2 <= rtol ||b||_2. */
 int yeti_wq_pcg(yeti_wq_op *op, const double *b, double *x, double rtol,
                 int maxit, int mode, yeti_cg_stats *stats, int mem);

@@ -110,3 +110,52 @@ def sys_linmat_lindef_static(activeElement, nb_data, COORDS3D, IEN,
     if rc != 0:
         raise RuntimeError(f"oracle assembly failed with code {rc}")
     return kdata, krow, kcol, F
+
+
+def grad_lin_elast_work(args, sol, adj, compute_int=True, compute_ext=True,
+                        include_surface=False):
+    """Oracle twin of gradadjointwork.gradlinelastwork_an
+    (src/yeti_iga/optim/gradtotalwork_fullAN.f90:17-300) for U1 patches.
+
+    args: the positional list of get_inputs4system_elemStorage (the model);
+    sol: (3, nb_cp); adj: (nadj, 3, nb_cp).  Returns (gradWint, gradWext),
+    each (nadj, 3, nb_cp).  include_surface adds the surface-load sensitivity
+    the reference leaves out (gradUELMAT_solid.f90:463-477)."""
+    (activeElement, nb_data, COORDS3D, IEN, nb_elem_patch, Nkv, Ukv, Nijk,
+     weight, Jpqr, ELT_TYPE, PROPS, JPROPS, MATERIAL_PROPERTIES, n_mat_props,
+     RHO, TENSOR, indDLoad, JDLType, ADLMAG, load_target_nbelem,
+     load_additionalInfos, nb_load_additionalInfos, bc_values, bc_target,
+     bc_target_nbelem, ind_dof_free, nb_dof_free, MCRD, NBINT, NNODE,
+     nodal_dist) = args[:32]
+    coords = np.asarray(COORDS3D, dtype=np.float64)
+    nb_cp = coords.shape[1]
+    nb_patch = len(np.atleast_1d(nb_elem_patch))
+    _check_u1(ELT_TYPE, TENSOR, nb_patch)
+    adj = np.asarray(adj, dtype=np.float64)
+    nadj = adj.shape[0]
+    nodal = np.asarray(nodal_dist, dtype=np.float64)
+    if nodal.ndim == 1:
+        nodal = nodal.reshape(1, -1)
+    mat = np.asarray(MATERIAL_PROPERTIES, dtype=np.float64).reshape(-1, nb_patch, order="F")[:2]
+    jdl = _i64(JDLType)
+    keep = [_f64(coords), _i64(IEN), _i64(nb_elem_patch), _i64(Nkv), _f64(Ukv),
+            _i64(Nijk), _f64(weight), _i64(Jpqr), _i64(NNODE), _i64(NBINT),
+            _f64(mat), _f64(np.atleast_1d(RHO)), _i64(activeElement),
+            _i64(indDLoad), jdl, _f64(ADLMAG), _i64(load_target_nbelem),
+            _f64(load_additionalInfos), _f64(nodal), _f64(sol), _f64(adj)]
+    gi = np.zeros((nadj, 3, nb_cp), order="F")
+    ge = np.zeros((nadj, 3, nb_cp), order="F")
+    f = lib().oracle_grad_lin_elast_work
+    f.restype = ctypes.c_int
+    i64 = ctypes.c_int64
+    rc = f(i64(nb_patch), i64(len(keep[12])), i64(nb_cp), _p(keep[0]), _p(keep[1]),
+           _p(keep[2]), _p(keep[3]), _p(keep[4]), _p(keep[5]), _p(keep[6]),
+           _p(keep[7]), _p(keep[8]), _p(keep[9]), _p(keep[10]), _p(keep[11]),
+           _p(keep[12]), i64(len(jdl)), _p(keep[13]), _p(keep[14]), _p(keep[15]),
+           _p(keep[16]), _p(keep[17]), i64(nodal.shape[0]), _p(keep[18]),
+           _p(keep[19]), _p(keep[20]), i64(nadj), ctypes.c_int(int(compute_int)),
+           ctypes.c_int(int(compute_ext)), ctypes.c_int(int(include_surface)),
+           gi.ctypes.data_as(ctypes.c_void_p), ge.ctypes.data_as(ctypes.c_void_p))
+    if rc != 0:
+        raise RuntimeError(f"oracle gradient failed with code {rc}")
+    return gi, ge

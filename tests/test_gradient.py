@@ -1,0 +1,131 @@
+"""Adjoint compliance shape gradient: oracle vs finite differences (CPU) and
+GPU kernel vs oracle (bit-identical) and vs finite differences.
+
+The reference's own pin (benchs/grad_solid/test_grad_solid_unit_cube_centrif.py)
+asserts AN == FD within rtol 1e-5 on the p=1 unit cube under a centrifugal
+load; the north-star bar is 1e-6 relative to central FD (h = 1e-6).
+"""
+import numpy as np
+import pytest
+import scipy.sparse as sp
+import scipy.sparse.linalg as spla
+
+import oracle
+from conftest import load_fixture
+
+
+def _oracle_compliance(d, args, coords):
+    a = list(args)
+    a[2] = coords
+    k, r, c, F = oracle.sys_linmat_lindef_static(*a)
+    n = int(d["nb_dof_tot"])
+    K = sp.coo_matrix((k, (r, c)), shape=(n, n)).tocsc()
+    K = K + K.T
+    idof = d["ind_dof_free"][:int(d["nb_dof_free"])] - 1
+    U = np.zeros(n)
+    U[idof] = spla.spsolve(K[idof, :][:, idof], F[idof])
+    return 0.5 * U @ F, U
+
+
+def _fd(fun, X0, sel, h=1e-6):
+    out = []
+    for cp in sel:
+        for c in range(3):
+            Xp, Xm = X0.copy(), X0.copy()
+            Xp[c, cp] += h
+            Xm[c, cp] -= h
+            out.append((fun(Xp) - fun(Xm)) / (2 * h))
+    return np.array(out)
+
+
+# ---------------------------------------------------------------------- CPU
+def test_oracle_gradient_unit_cube_centrifugal_vs_fd():
+    """The reference's own gradient case (centrifugal body load, U101)."""
+    d, args = load_fixture("grad_unit_cube")
+    X0 = np.array(d["COORDS3D"], dtype=float)
+    C0, U = _oracle_compliance(d, args, X0)
+    sol = U.reshape(-1, 3).T
+    gi, ge = oracle.grad_lin_elast_work(args, sol, 0.5 * sol[None])
+    g = gi[0] + 2 * ge[0]
+    sel = np.arange(X0.shape[1])
+    fd = _fd(lambda X: _oracle_compliance(d, args, X)[0], X0, sel)
+    an = np.array([g[c, cp] for cp in sel for c in range(3)])
+    np.testing.assert_allclose(an, fd, rtol=1e-5, atol=1e-8 * np.abs(fd).max())
+
+
+def test_oracle_gradient_with_traction_term_vs_fd():
+    """Outward pressure on the annulus: the surface-load sensitivity (absent
+    from the reference) makes AN agree with FD; without it, it does not."""
+    d, args = load_fixture("quarter_annulus_p2_4x4x2")
+    X0 = np.array(d["COORDS3D"], dtype=float)
+    C0, U = _oracle_compliance(d, args, X0)
+    sol = U.reshape(-1, 3).T
+    rng = np.random.default_rng(0)
+    sel = rng.choice(X0.shape[1], size=8, replace=False)
+    fd = _fd(lambda X: _oracle_compliance(d, args, X)[0], X0, sel)
+    gi, ge = oracle.grad_lin_elast_work(args, sol, 0.5 * sol[None], include_surface=True)
+    g = gi[0] + 2 * ge[0]
+    an = np.array([g[c, cp] for cp in sel for c in range(3)])
+    assert np.linalg.norm(an - fd) / np.linalg.norm(fd) < 1e-6
+    gi, ge = oracle.grad_lin_elast_work(args, sol, 0.5 * sol[None], include_surface=False)
+    g = gi[0] + 2 * ge[0]
+    an = np.array([g[c, cp] for cp in sel for c in range(3)])
+    assert np.linalg.norm(an - fd) / np.linalg.norm(fd) > 0.1
+
+
+# ---------------------------------------------------------------------- GPU
+GRAD_CASES = ["grad_unit_cube", "quarter_annulus_p2_4x4x2", "dload_beam_dist",
+              "cantilever_p2_16x4x4", "volume_force_3d"]
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", GRAD_CASES)
+@pytest.mark.parametrize("surface", [False, True])
+def test_gpu_gradient_matches_oracle(cuda_ok, name, surface):
+    from yeti_b200.gradient import grad_from_system_args
+    d, args = load_fixture(name)
+    X0 = np.array(d["COORDS3D"], dtype=float)
+    rng = np.random.default_rng(1)
+    sol = rng.standard_normal((3, X0.shape[1]))
+    adj = rng.standard_normal((2, 3, X0.shape[1]))
+    gi0, ge0 = oracle.grad_lin_elast_work(args, sol, adj, include_surface=surface)
+    gi1, ge1 = grad_from_system_args(args, sol, adj, True, True, surface)
+    # same operation order, no FMA contraction: bit-identical
+    np.testing.assert_array_equal(gi1, gi0)
+    np.testing.assert_array_equal(ge1, ge0)
+
+
+@pytest.mark.gpu
+def test_gpu_autograd_compliance_backward(cuda_ok):
+    import torch
+    from yeti_b200.gradient import Compliance, compliance_and_gradient
+    d, args = load_fixture("quarter_annulus_p2_4x4x2")
+    X = torch.tensor(np.array(d["COORDS3D"], dtype=float), requires_grad=True)
+    C = Compliance.apply(X, args)
+    C.backward()
+    C0, g0 = compliance_and_gradient(args)
+    assert abs(C.item() - C0) <= 1e-14 * abs(C0)
+    np.testing.assert_array_equal(X.grad.numpy(), g0)
+
+
+@pytest.mark.gpu
+def test_gpu_gradient_annulus_32x32x2_vs_fd(cuda_ok):
+    """Quarter annulus (R 1 -> 4, t 0.1, exact arcs), p=2, 32x32x2 elements,
+    outward unit pressure on the outer face: AN (GPU, with the traction term)
+    vs central FD (h=1e-6) on 20 seeded control points x 3 coordinates."""
+    from yeti_b200.gradient import compliance_and_gradient
+    d, args = load_fixture("quarter_annulus_p2_32x32x2")
+    X0 = np.array(d["COORDS3D"], dtype=float)
+    C0, g = compliance_and_gradient(args)
+    rng = np.random.default_rng(20)
+    sel = rng.choice(X0.shape[1], size=20, replace=False)
+    fd = _fd(lambda X: compliance_and_gradient(args, X, include_surface=True)[0]
+             if False else _gpu_compliance(args, X), X0, sel)
+    an = np.array([g[c, cp] for cp in sel for c in range(3)])
+    assert np.linalg.norm(an - fd) / np.linalg.norm(fd) < 1e-6
+
+
+def _gpu_compliance(args, X):
+    from yeti_b200.gradient import _solve
+    U, F = _solve(args, X)
+    return 0.5 * U @ F

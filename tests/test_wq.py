@@ -111,6 +111,10 @@ def test_gpu_pcg_fp64_and_mixed_match_direct(cuda_ok):
     assert st32["status"] == 0 and st32["rel_residual"] <= 1e-8
     assert st32["fp32_applies"] > 0 and st32["outer_iterations"] >= 1
     assert _rel(x32, xd) < 1e-7
+    for mixed in (False, True):
+        xb, stb = op.pcg(b, rtol=1e-10, mixed=mixed, method="bicgstab")
+        assert stb["status"] == 0 and stb["rel_residual"] <= 1e-10
+        assert _rel(xb, xd) < 1e-8
 
 
 @pytest.mark.gpu

@@ -23,9 +23,10 @@ NVCC_FLAGS = ["-O3", "-lineinfo", "-std=c++17", "--expt-relaxed-constexpr",
               "-Xptxas", "-O3", "-DNDEBUG"]
 
 
-# Per-file extra flags.  The Gauss-quadrature assembly mirrors the reference's
-# operation order exactly, which requires no FMA contraction.
-EXTRA_FLAGS = {"assemble_u1.cu": ["-fmad=false"]}
+# Per-file extra flags.  The Gauss-quadrature assembly and shape gradient
+# mirror the reference's operation order exactly, which requires no FMA
+# contraction.
+EXTRA_FLAGS = {"assemble_u1.cu": ["-fmad=false"], "grad_u1.cu": ["-fmad=false"]}
 
 
 def nvcc():

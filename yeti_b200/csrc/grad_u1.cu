@@ -1,0 +1,724 @@
+// Adjoint shape gradient of the linear-elastic work for U1 solids.
+//
+// Replaces gradadjointwork.gradlinelastwork_an: gradLinElastWork_AN
+// (src/yeti_iga/optim/gradtotalwork_fullAN.f90:17-300) and gradUELMAT1adj
+// (src/yeti_iga/optim/gradUELMAT_solid.f90:18-479), with evalnurbs
+// (src/yeti_iga/main/evaluatenurbsfcts.f:94-209).  The quadrature-point
+// geometry is recomputed from the control points (nothing is stored between
+// the solve and the gradient).  Optionally adds the surface-load sensitivity
+// the reference leaves out (gradUELMAT_solid.f90:463-477): for a load of
+// magnitude f on a face, W_ext = f sum_q w_q UA(xi_q).v(xi_q) with
+// v = P x Q (normal pressure, shapPress.f face ordering) or e_t |A x B|
+// (fixed direction), differentiated through the face tangents.
+//
+// Kernel design: one CTA per active element.  Stage A: one thread per
+// quadrature point computes the basis, covariant frame, metrics, strains and
+// stresses of the state and adjoint fields into shared memory.  Stage B: one
+// thread per control point accumulates its (nadj x 3) derivative over the
+// points in order.  A second kernel sums element contributions per control
+// point in element order (deterministic).  Compiled without FMA contraction
+// and following the reference's operation order.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <memory>
+
+#include "nurbs.cuh"
+#include "u1_model.cuh"
+
+namespace yeti {
+
+constexpr int kGradMaxAdj = 4;
+
+__device__ __constant__ int c_vi[6] = {0, 1, 2, 0, 0, 1};
+__device__ __constant__ int c_vj[6] = {0, 1, 2, 1, 2, 2};
+
+struct GradArgs {
+    int p0, p1, p2, nn, nq, ng, nadj;
+    int compute_int, compute_ext, include_surface;
+    const double *U0, *U1, *U2;
+    const double *gauss;      // volume rule (4 * nq)
+    const double *gface;      // 6 faces x ng^2 x 4
+    const double *coords;
+    const int32_t *ien;       // per active element
+    const double *w;
+    const int32_t *span;
+    const int32_t *elems;     // elements of this launch (active-local index)
+    const int32_t *term_ptr;  // loads of each element (CSR)
+    const int32_t *terms;     // load indices
+    const int32_t *jdltype;
+    const double *adlmag;
+    const double *addinfos;
+    const double *nodal_dist;
+    int nb_n_dist;
+    const double *sol;        // (3, nb_cp)
+    const double *adj;        // (nadj, 3, nb_cp)
+    double E, nu, rho;
+    double *egi, *ege;        // (n elements, nadj*3*nn)
+};
+
+// evalnurbs at parametric xi: R[nn], dR[3*a+i]
+__device__ void eval_nurbs(const GradArgs &a, const int *ni, const double *xi,
+                           const double *we, double *R, double *dR) {
+    double FN[kMaxDeg1], dFN[kMaxDeg1], FM[kMaxDeg1], dFM[kMaxDeg1],
+        FL[kMaxDeg1], dFL[kMaxDeg1];
+    bspline_ders(ni[0], a.p0, xi[0], a.U0, FN, dFN);
+    bspline_ders(ni[1], a.p1, xi[1], a.U1, FM, dFM);
+    bspline_ders(ni[2], a.p2, xi[2], a.U2, FL, dFL);
+    int n = 0;
+    double S = 0.0, sx0 = 0.0, sx1 = 0.0, sx2 = 0.0;
+    for (int k = 0; k <= a.p2; k++)
+        for (int j = 0; j <= a.p1; j++)
+            for (int i = 0; i <= a.p0; i++, n++) {
+                R[n] = FN[a.p0 - i] * FM[a.p1 - j] * FL[a.p2 - k] * we[n];
+                S = S + R[n];
+                dR[3 * n] = dFN[a.p0 - i] * FM[a.p1 - j] * FL[a.p2 - k] * we[n];
+                sx0 = sx0 + dR[3 * n];
+                dR[3 * n + 1] = FN[a.p0 - i] * dFM[a.p1 - j] * FL[a.p2 - k] * we[n];
+                sx1 = sx1 + dR[3 * n + 1];
+                dR[3 * n + 2] = FN[a.p0 - i] * FM[a.p1 - j] * dFL[a.p2 - k] * we[n];
+                sx2 = sx2 + dR[3 * n + 2];
+            }
+    const double inv = 1.0 / S;
+    const double sx[3] = {sx0, sx1, sx2};
+    for (int q = 0; q < a.nn; q++) {
+        R[q] = R[q] * inv;
+        for (int i = 0; i < 3; i++) dR[3 * q + i] = (dR[3 * q + i] - R[q] * sx[i]) * inv;
+    }
+}
+
+__device__ __forceinline__ void gcross(const double *u, const double *v, double *w) {
+    w[0] = u[1] * v[2] - u[2] * v[1];
+    w[1] = u[2] * v[0] - u[0] * v[2];
+    w[2] = u[0] * v[1] - u[1] * v[0];
+}
+
+__device__ __forceinline__ double gdot(const double *u, const double *v) {
+    return u[0] * v[0] + u[1] * v[1] + u[2] * v[2];
+}
+
+__device__ void ginv3(const double B[3][3], double A[3][3]) {
+    double det = B[0][1] * B[1][2] * B[2][0] - B[0][2] * B[1][1] * B[2][0] +
+                 B[0][2] * B[1][0] * B[2][1] - B[0][0] * B[1][2] * B[2][1] +
+                 B[0][0] * B[1][1] * B[2][2] - B[0][1] * B[1][0] * B[2][2];
+    A[0][0] = (B[1][1] * B[2][2] - B[1][2] * B[2][1]) / det;
+    A[0][1] = (B[0][2] * B[2][1] - B[0][1] * B[2][2]) / det;
+    A[0][2] = (B[0][1] * B[1][2] - B[0][2] * B[1][1]) / det;
+    A[1][0] = (B[1][2] * B[2][0] - B[1][0] * B[2][2]) / det;
+    A[1][1] = (B[0][0] * B[2][2] - B[0][2] * B[2][0]) / det;
+    A[1][2] = (B[0][2] * B[1][0] - B[0][0] * B[1][2]) / det;
+    A[2][0] = (B[1][0] * B[2][1] - B[1][1] * B[2][0]) / det;
+    A[2][1] = (B[0][1] * B[2][0] - B[0][0] * B[2][1]) / det;
+    A[2][2] = (B[0][0] * B[1][1] - B[0][1] * B[1][0]) / det;
+}
+
+// Per-point record layout in shared memory (doubles).
+struct PtLayout {
+    int R, dR, AI, AxA, area, dj, AAE, strain, stress, dU, dUA, sA, tA, work,
+        vA, body, size;
+};
+
+__host__ __device__ inline PtLayout pt_layout(int nn, int nadj, int nbody) {
+    PtLayout L;
+    int o = 0;
+    L.R = o; o += nn;
+    L.dR = o; o += 3 * nn;
+    L.AI = o; o += 9;
+    L.AxA = o; o += 9;
+    L.area = o; o += 1;
+    L.dj = o; o += 1;
+    L.AAE = o; o += 9;
+    L.strain = o; o += 6;
+    L.stress = o; o += 6;
+    L.dU = o; o += 9;
+    L.dUA = o; o += 9 * nadj;
+    L.sA = o; o += 6 * nadj;    // adjoint strain
+    L.tA = o; o += 6 * nadj;    // adjoint stress
+    L.work = o; o += nadj;
+    L.vA = o; o += 3 * nadj;    // adjoint displacement at the point
+    L.body = o; o += 6 * nbody; // (loadF, vectD) of each centrifugal load
+    L.size = o;
+    return L;
+}
+
+__global__ void __launch_bounds__(256) k_u1_grad(GradArgs a) {
+    extern __shared__ double sm[];
+    const int nn = a.nn, nadj = a.nadj;
+    const int e = a.elems[blockIdx.x];
+    double *xe = sm;                    // 3*nn coords
+    double *ue = xe + 3 * nn;           // 3*nn state
+    double *uae = ue + 3 * nn;          // 3*nn*nadj adjoint
+    double *we = uae + 3 * nn * nadj;   // nn weights
+    double *pts = we + nn;
+    __shared__ double su1[3], su2[3];
+    __shared__ int sni[3];
+    __shared__ int s_body[8], s_nbody;
+    const int tid = threadIdx.x;
+    const int32_t *ien = a.ien + (size_t)e * nn;
+    for (int i = tid; i < nn; i += blockDim.x) {
+        const int cp = ien[i];
+        for (int c = 0; c < 3; c++) {
+            xe[3 * i + c] = a.coords[3 * cp + c];
+            ue[3 * i + c] = a.sol[3 * cp + c];
+            for (int k = 0; k < nadj; k++)
+                uae[3 * i + c + 3 * nn * k] = a.adj[k + nadj * (c + 3 * cp)];
+        }
+        we[i] = a.w[(size_t)e * nn + i];
+    }
+    if (tid < 3) {
+        const double *U = tid == 0 ? a.U0 : (tid == 1 ? a.U1 : a.U2);
+        const int ni = a.span[3 * e + tid];
+        sni[tid] = ni;
+        su1[tid] = U[ni - 1];
+        su2[tid] = U[ni];
+    }
+    if (tid == 0) {
+        int nb = 0;
+        if (a.compute_ext)
+            for (int t = a.term_ptr[blockIdx.x]; t < a.term_ptr[blockIdx.x + 1]; t++)
+                if (a.jdltype[a.terms[t]] == 101 && nb < 8) s_body[nb++] = a.terms[t];
+        s_nbody = nb;
+    }
+    __syncthreads();
+    const int nbody = s_nbody;
+    const PtLayout L = pt_layout(nn, nadj, nbody);
+    const double lambda = a.E * a.nu / (1.0 + a.nu) / (1.0 - 2.0 * a.nu);
+    const double mu = a.E / 2.0 / (1.0 + a.nu);
+    // ---------------- stage A: per volume point
+    for (int q = tid; q < a.nq; q += blockDim.x) {
+        double *P = pts + (size_t)q * L.size;
+        const double *g = a.gauss + 4 * q;
+        double xi[3], detJac = g[0];
+        for (int i = 0; i < 3; i++) {
+            xi[i] = ((su2[i] - su1[i]) * g[1 + i] + (su2[i] + su1[i])) * 0.5;
+            detJac = detJac * 0.5 * (su2[i] - su1[i]);
+        }
+        double *R = P + L.R, *dR = P + L.dR;
+        eval_nurbs(a, sni, xi, we, R, dR);
+        double AI[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+        for (int i = 0; i < 3; i++)
+            for (int cp = 0; cp < nn; cp++)
+                for (int c = 0; c < 3; c++) AI[i][c] = AI[i][c] + dR[3 * cp + i] * xe[3 * cp + c];
+        double AxA[3][3];
+        gcross(AI[0], AI[1], AxA[2]);
+        const double Area = gdot(AxA[2], AI[2]);
+        gcross(AI[1], AI[2], AxA[0]);
+        gcross(AI[2], AI[0], AxA[1]);
+        for (int i = 0; i < 3; i++)
+            for (int c = 0; c < 3; c++) {
+                P[L.AI + 3 * i + c] = AI[i][c];
+                P[L.AxA + 3 * i + c] = AxA[i][c];
+            }
+        P[L.area] = Area;
+        P[L.dj] = detJac;
+        if (a.compute_int) {
+            double AAI[3][3], AAE[3][3];
+            for (int i = 0; i < 3; i++)
+                for (int j = 0; j < 3; j++) AAI[i][j] = gdot(AI[i], AI[j]);
+            ginv3(AAI, AAE);
+            double H[6][6];
+            for (int kl = 0; kl < 6; kl++) {
+                const int k = c_vi[kl], l = c_vj[kl];
+                for (int ij = 0; ij <= kl; ij++) {
+                    const int i = c_vi[ij], j = c_vj[ij];
+                    H[ij][kl] = lambda * AAE[i][j] * AAE[k][l] +
+                                mu * (AAE[i][k] * AAE[j][l] + AAE[i][l] * AAE[j][k]);
+                }
+            }
+            for (int kl = 1; kl < 6; kl++)
+                for (int r = kl; r < 6; r++) H[r][kl - 1] = H[kl - 1][r];
+            double dU[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+            for (int i = 0; i < 3; i++)
+                for (int cp = 0; cp < nn; cp++)
+                    for (int c = 0; c < 3; c++) dU[i][c] = dU[i][c] + dR[3 * cp + i] * ue[3 * cp + c];
+            double strain[6], stress[6];
+            for (int ij = 0; ij < 6; ij++) {
+                const int i = c_vi[ij], j = c_vj[ij];
+                if (i == j) strain[ij] = gdot(AI[i], dU[i]);
+                else strain[ij] = gdot(AI[i], dU[j]) + gdot(AI[j], dU[i]);
+            }
+            for (int ii = 0; ii < 6; ii++) {
+                double s = 0.0;
+                for (int jj = 0; jj < 6; jj++) s = s + H[ii][jj] * strain[jj];
+                stress[ii] = s;
+            }
+            for (int i = 0; i < 3; i++)
+                for (int c = 0; c < 3; c++) {
+                    P[L.AAE + 3 * i + c] = AAE[i][c];
+                    P[L.dU + 3 * i + c] = dU[i][c];
+                }
+            for (int ij = 0; ij < 6; ij++) {
+                P[L.strain + ij] = strain[ij];
+                P[L.stress + ij] = stress[ij];
+            }
+            for (int k = 0; k < nadj; k++) {
+                double dA[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+                for (int i = 0; i < 3; i++)
+                    for (int cp = 0; cp < nn; cp++)
+                        for (int c = 0; c < 3; c++)
+                            dA[i][c] = dA[i][c] + dR[3 * cp + i] * uae[3 * cp + c + 3 * nn * k];
+                double sA[6], tA[6];
+                for (int ij = 0; ij < 6; ij++) {
+                    const int i = c_vi[ij], j = c_vj[ij];
+                    if (i == j) sA[ij] = gdot(AI[i], dA[i]);
+                    else sA[ij] = gdot(AI[i], dA[j]) + gdot(AI[j], dA[i]);
+                }
+                for (int ii = 0; ii < 6; ii++) {
+                    double s = 0.0;
+                    for (int jj = 0; jj < 6; jj++) s = s + H[ii][jj] * sA[jj];
+                    tA[ii] = s;
+                }
+                for (int i = 0; i < 3; i++)
+                    for (int c = 0; c < 3; c++) P[L.dUA + 9 * k + 3 * i + c] = dA[i][c];
+                for (int ij = 0; ij < 6; ij++) {
+                    P[L.sA + 6 * k + ij] = sA[ij];
+                    P[L.tA + 6 * k + ij] = tA[ij];
+                }
+            }
+            for (int k = 0; k < nadj; k++) P[L.work + k] = 0.0;
+            for (int ij = 0; ij < 6; ij++)
+                for (int k = 0; k < nadj; k++)
+                    P[L.work + k] = P[L.work + k] + P[L.sA + 6 * k + ij] * stress[ij];
+        }
+        if (a.compute_ext && nbody > 0) {
+            for (int k = 0; k < nadj; k++)
+                for (int c = 0; c < 3; c++) {
+                    double s = 0.0;
+                    for (int cp = 0; cp < nn; cp++) s = s + R[cp] * uae[3 * cp + c + 3 * nn * k];
+                    P[L.vA + 3 * k + c] = s;
+                }
+            // centrifugal loads: the reference advances its info cursor by
+            // 2*MCRD for every centrifugal load acting on the element
+            int loadcount = 0;
+            for (int b = 0; b < nbody; b++) {
+                const int nl = s_body[b];
+                double pg[3] = {0, 0, 0}, A[3], B[3], vd[3], ag[3];
+                for (int cp = 0; cp < nn; cp++)
+                    for (int c = 0; c < 3; c++) pg[c] = pg[c] + R[cp] * xe[3 * cp + c];
+                for (int c = 0; c < 3; c++) A[c] = a.addinfos[loadcount + c];
+                loadcount += 3;
+                for (int c = 0; c < 3; c++) B[c] = a.addinfos[loadcount + c];
+                loadcount += 3;
+                for (int c = 0; c < 3; c++) vd[c] = B[c] - A[c];
+                const double nr = sqrt(vd[0] * vd[0] + vd[1] * vd[1] + vd[2] * vd[2]);
+                for (int c = 0; c < 3; c++) vd[c] = vd[c] / nr;
+                for (int c = 0; c < 3; c++) ag[c] = pg[c] - A[c];
+                const double sc = gdot(ag, vd);
+                for (int c = 0; c < 3; c++) {
+                    P[L.body + 6 * b + c] = a.rho * (a.adlmag[nl] * a.adlmag[nl]) * (ag[c] - sc * vd[c]);
+                    P[L.body + 6 * b + 3 + c] = vd[c];
+                }
+            }
+        }
+    }
+    __syncthreads();
+    // ---------------- stage B: one thread per control point
+    double gi[3 * kGradMaxAdj], ge[3 * kGradMaxAdj];
+    const int cp = tid;
+    const bool mine = cp < nn;
+    for (int i = 0; i < 3 * kGradMaxAdj; i++) gi[i] = ge[i] = 0.0;
+    if (mine) {
+        for (int q = 0; q < a.nq; q++) {
+            const double *P = pts + (size_t)q * L.size;
+            const double *dr = P + L.dR + 3 * cp;
+            const double Area = P[L.area], detJac = P[L.dj];
+            const double *AxA = P + L.AxA;
+            if (a.compute_int) {
+                const double *AI = P + L.AI, *AAE = P + L.AAE;
+                const double *stress = P + L.stress, *strain = P + L.strain, *dU = P + L.dU;
+                double dJ[3] = {0, 0, 0};
+                for (int i = 0; i < 3; i++)
+                    for (int c = 0; c < 3; c++) dJ[c] = dJ[c] + AxA[3 * i + c] * dr[i];
+                for (int k = 0; k < nadj; k++)
+                    for (int c = 0; c < 3; c++) gi[3 * k + c] = gi[3 * k + c] - P[L.work + k] * dJ[c] * detJac;
+                for (int k = 0; k < nadj; k++) {
+                    const double *d = P + L.dUA + 9 * k;
+                    double ev[3] = {0, 0, 0};
+                    for (int ij = 0; ij < 6; ij++) {
+                        const int i = c_vi[ij], j = c_vj[ij];
+                        for (int c = 0; c < 3; c++) {
+                            if (i == j) ev[c] = ev[c] + stress[ij] * d[3 * i + c] * dr[i];
+                            else ev[c] = ev[c] + stress[ij] * d[3 * i + c] * dr[j] + stress[ij] * d[3 * j + c] * dr[i];
+                        }
+                    }
+                    for (int c = 0; c < 3; c++) gi[3 * k + c] = gi[3 * k + c] - ev[c] * Area * detJac;
+                }
+                double dAAI[3][3][3], dAAE[3][3][3];
+                for (int j = 0; j < 3; j++)
+                    for (int i = 0; i < 3; i++)
+                        for (int c = 0; c < 3; c++)
+                            dAAI[i][j][c] = dr[i] * AI[3 * j + c] + AI[3 * i + c] * dr[j];
+                for (int i = 0; i < 3; i++)
+                    for (int j = 0; j < 3; j++)
+                        for (int c = 0; c < 3; c++) dAAE[i][j][c] = 0.0;
+                for (int j = 0; j < 3; j++)
+                    for (int i = 0; i < 3; i++)
+                        for (int l = 0; l < 3; l++)
+                            for (int k = 0; k < 3; k++)
+                                for (int c = 0; c < 3; c++)
+                                    dAAE[i][j][c] = dAAE[i][j][c] - AAE[3 * i + k] * AAE[3 * l + j] * dAAI[k][l][c];
+                double vA[3 * kGradMaxAdj];
+                for (int k = 0; k < nadj; k++) {
+                    const double *tA = P + L.tA + 6 * k;
+                    double ev[3] = {0, 0, 0};
+                    for (int ij = 0; ij < 6; ij++) {
+                        const int i = c_vi[ij], j = c_vj[ij];
+                        for (int c = 0; c < 3; c++) {
+                            if (i == j) ev[c] = ev[c] + tA[ij] * dU[3 * i + c] * dr[i];
+                            else ev[c] = ev[c] + tA[ij] * dU[3 * i + c] * dr[j] + tA[ij] * dU[3 * j + c] * dr[i];
+                        }
+                    }
+                    for (int c = 0; c < 3; c++) vA[3 * k + c] = ev[c];
+                }
+                for (int kl = 0; kl < 6; kl++) {
+                    const int k = c_vi[kl], l = c_vj[kl];
+                    for (int ij = 0; ij < 6; ij++) {
+                        const int i = c_vi[ij], j = c_vj[ij];
+                        double dC[3];
+                        for (int c = 0; c < 3; c++)
+                            dC[c] = lambda * dAAE[i][j][c] * AAE[3 * k + l] + lambda * AAE[3 * i + j] * dAAE[k][l][c] +
+                                    mu * dAAE[i][k][c] * AAE[3 * j + l] + mu * AAE[3 * i + k] * dAAE[j][l][c] +
+                                    mu * dAAE[i][l][c] * AAE[3 * j + k] + mu * AAE[3 * i + l] * dAAE[j][k][c];
+                        for (int kk = 0; kk < nadj; kk++)
+                            for (int c = 0; c < 3; c++)
+                                vA[3 * kk + c] = vA[3 * kk + c] + dC[c] * strain[ij] * P[L.sA + 6 * kk + kl];
+                    }
+                }
+                for (int k = 0; k < nadj; k++)
+                    for (int c = 0; c < 3; c++) gi[3 * k + c] = gi[3 * k + c] - vA[3 * k + c] * Area * detJac;
+            }
+            if (a.compute_ext) {
+                for (int b = 0; b < nbody; b++) {
+                    const double *lf = P + L.body + 6 * b, *vd = lf + 3;
+                    const int nl = s_body[b];
+                    double dJ[3] = {0, 0, 0};
+                    for (int i = 0; i < 3; i++)
+                        for (int c = 0; c < 3; c++) dJ[c] = dJ[c] + AxA[3 * i + c] * dr[i];
+                    for (int k = 0; k < nadj; k++) {
+                        const double sf = gdot(lf, P + L.vA + 3 * k);
+                        for (int c = 0; c < 3; c++) ge[3 * k + c] = ge[3 * k + c] + sf * dJ[c] * detJac;
+                    }
+                    for (int k = 0; k < nadj; k++) {
+                        const double *ua = P + L.vA + 3 * k;
+                        double df[3] = {0, 0, 0};
+                        for (int id = 0; id < 3; id++)
+                            for (int jd = 0; jd < 3; jd++) {
+                                if (id == jd) df[jd] = df[jd] + ua[id] * (1.0 - vd[id] * vd[jd]);
+                                else df[jd] = df[jd] - ua[id] * (vd[id] * vd[jd]);
+                            }
+                        for (int c = 0; c < 3; c++) {
+                            df[c] = df[c] * (a.rho * (a.adlmag[nl] * a.adlmag[nl]) * P[L.R + cp]);
+                            ge[3 * k + c] = ge[3 * k + c] + df[c] * Area * detJac;
+                        }
+                    }
+                }
+            }
+        }
+    }
+    // ---------------- surface loads (not in the reference)
+    if (a.compute_ext && a.include_surface) {
+        const int nf = a.ng * a.ng;
+        for (int t = a.term_ptr[blockIdx.x]; t < a.term_ptr[blockIdx.x + 1]; t++) {
+            const int nl = a.terms[t];
+            const int ty = a.jdltype[nl];
+            if (!(ty > 9 && ty < 100)) continue;
+            const int face = ty / 10, type = ty % 10;
+            // per face point: R (nn), dR (3nn), AJ (9), fmag, w, vA (3nadj)
+            const int fs = 4 * nn + 11 + 3 * nadj;
+            __syncthreads();
+            for (int q = tid; q < nf; q += blockDim.x) {
+                double *P = pts + (size_t)q * fs;
+                const double *g = a.gface + ((size_t)(face - 1) * nf + q) * 4;
+                double xi[3], h[3];
+                for (int i = 0; i < 3; i++) {
+                    xi[i] = ((su2[i] - su1[i]) * g[1 + i] + (su2[i] + su1[i])) * 0.5;
+                    h[i] = 0.5 * (su2[i] - su1[i]);
+                }
+                double *R = P, *dR = P + nn;
+                eval_nurbs(a, sni, xi, we, R, dR);
+                double AJ[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+                for (int cq = 0; cq < nn; cq++)
+                    for (int b = 0; b < 3; b++)
+                        for (int c = 0; c < 3; c++) AJ[b][c] = AJ[b][c] + xe[3 * cq + c] * dR[3 * cq + b];
+                for (int b = 0; b < 3; b++)
+                    for (int c = 0; c < 3; c++) P[4 * nn + 3 * b + c] = AJ[b][c] * h[b];
+                double fmag = a.adlmag[nl];
+                if (type == 4) {
+                    const int ifield = (int)a.addinfos[0] - 1;
+                    fmag = 0.0;
+                    for (int cq = 0; cq < nn; cq++)
+                        fmag = fmag + a.nodal_dist[ifield + (size_t)a.nb_n_dist * ien[cq]] * R[cq];
+                }
+                P[4 * nn + 9] = fmag;
+                P[4 * nn + 10] = g[0];
+                for (int k = 0; k < nadj; k++)
+                    for (int c = 0; c < 3; c++) {
+                        double s = 0.0;
+                        for (int cq = 0; cq < nn; cq++) s = s + R[cq] * uae[3 * cq + c + 3 * nn * k];
+                        P[4 * nn + 11 + 3 * k + c] = s;
+                    }
+            }
+            __syncthreads();
+            if (mine) {
+                int ia, ib, ip, iq;
+                switch (face) { case 1: case 2: ia = 1; ib = 2; break; case 3: case 4: ia = 2; ib = 0; break; default: ia = 0; ib = 1; }
+                switch (face) {
+                    case 1: ip = 1; iq = 2; break; case 2: ip = 2; iq = 1; break;
+                    case 3: ip = 2; iq = 0; break; case 4: ip = 0; iq = 2; break;
+                    case 5: ip = 0; iq = 1; break; default: ip = 1; iq = 0; break;
+                }
+                double h[3];
+                for (int i = 0; i < 3; i++) h[i] = 0.5 * (su2[i] - su1[i]);
+                for (int q = 0; q < nf; q++) {
+                    const double *P = pts + (size_t)q * fs;
+                    const double *dR = P + nn;
+                    const double *AJ = P + 4 * nn;
+                    const double fmag = P[4 * nn + 9], wq = P[4 * nn + 10];
+                    for (int k = 0; k < nadj; k++) {
+                        const double *ua = P + 4 * nn + 11 + 3 * k;
+                        double gg[3];
+                        if (type == 0 || type == 4) {
+                            const double cP = dR[3 * cp + ip] * h[ip], cQ = dR[3 * cp + iq] * h[iq];
+                            double QxU[3], UxP[3];
+                            gcross(AJ + 3 * iq, ua, QxU);
+                            gcross(ua, AJ + 3 * ip, UxP);
+                            for (int c = 0; c < 3; c++) gg[c] = cP * QxU[c] + cQ * UxP[c];
+                        } else {
+                            double n[3];
+                            gcross(AJ + 3 * ia, AJ + 3 * ib, n);
+                            const double nr = sqrt(n[0] * n[0] + n[1] * n[1] + n[2] * n[2]);
+                            for (int c = 0; c < 3; c++) n[c] = n[c] / nr;
+                            const double cA = dR[3 * cp + ia] * h[ia], cB = dR[3 * cp + ib] * h[ib];
+                            double Bxn[3], nxA[3];
+                            gcross(AJ + 3 * ib, n, Bxn);
+                            gcross(n, AJ + 3 * ia, nxA);
+                            for (int c = 0; c < 3; c++) gg[c] = ua[type - 1] * (cA * Bxn[c] + cB * nxA[c]);
+                        }
+                        for (int c = 0; c < 3; c++) ge[3 * k + c] = ge[3 * k + c] + gg[c] * wq * fmag;
+                    }
+                }
+            }
+        }
+    }
+    if (mine) {
+        double *oi = a.egi + (size_t)blockIdx.x * nadj * 3 * nn;
+        double *oe = a.ege + (size_t)blockIdx.x * nadj * 3 * nn;
+        for (int k = 0; k < nadj; k++)
+            for (int c = 0; c < 3; c++) {
+                oi[k + nadj * (c + 3 * cp)] = gi[3 * k + c];
+                oe[k + nadj * (c + 3 * cp)] = ge[3 * k + c];
+            }
+    }
+}
+
+// g[k + nadj*(c + 3*cp)] = sum over elements (in order) of their entries
+__global__ void k_grad_gather(int64_t n, const int64_t *ptr, const int64_t *idx,
+                              const double *egi, const double *ege, double *gi,
+                              double *ge) {
+    const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    double ai = 0.0, ae = 0.0;
+    for (int64_t k = ptr[t]; k < ptr[t + 1]; k++) {
+        ai = ai + egi[idx[k]];
+        ae = ae + ege[idx[k]];
+    }
+    gi[t] = ai;
+    ge[t] = ae;
+}
+
+static bool in_list_g(const int64_t *l, int64_t n, int64_t v) {
+    for (int64_t i = 0; i < n; i++)
+        if (l[i] == v) return true;
+    return false;
+}
+
+}  // namespace yeti
+
+using namespace yeti;
+
+YETI_API int yeti_grad_lin_elast_work(yeti_ctx *ctx, const yeti_u1_model *m,
+                                      const double *sol, const double *adj,
+                                      int64_t nadj, int compute_wint,
+                                      int compute_wext, int include_surface,
+                                      double *gwint, double *gwext, int mem) {
+    YETI_CHECK(ctx && m && sol && adj && gwint && gwext, YETI_EINVAL,
+               "yeti_grad_lin_elast_work: NULL argument");
+    YETI_CHECK(nadj >= 1 && nadj <= kGradMaxAdj, YETI_EINVAL,
+               "yeti_grad_lin_elast_work: nadj %lld outside 1..%d", (long long)nadj, kGradMaxAdj);
+    DeviceGuard guard(ctx->device);
+    U1Model M;
+    YETI_TRY(u1_prepare(ctx, m, M));
+    cudaStream_t s = ctx->stream;
+    const int64_t ncp = m->nb_cp;
+    const int64_t nout = nadj * 3 * ncp;
+    DevBuf dsol, dadj, dgi, dge;
+    const double *sol_d = sol, *adj_d = adj;
+    double *gi_d = gwint, *ge_d = gwext;
+    if (mem == YETI_MEM_HOST) {
+        YETI_TRY(upload(ctx, dsol, sol, (size_t)3 * ncp));
+        YETI_TRY(upload(ctx, dadj, adj, (size_t)nout));
+        YETI_TRY(dgi.alloc(ctx, nout * sizeof(double)));
+        YETI_TRY(dge.alloc(ctx, nout * sizeof(double)));
+        sol_d = dsol.as<double>();
+        adj_d = dadj.as<double>();
+        gi_d = dgi.as<double>();
+        ge_d = dge.as<double>();
+    }
+    int smem_optin = 0;
+    YETI_CUDA(cudaDeviceGetAttribute(&smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, ctx->device));
+    YETI_CUDA(cudaFuncSetAttribute(k_u1_grad, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_optin));
+    std::vector<std::unique_ptr<DevBuf>> keep;
+    auto newbuf = [&keep]() -> DevBuf & {
+        keep.emplace_back(new DevBuf());
+        return *keep.back();
+    };
+    DevBuf dj, da, dinfo, dnd;
+    std::vector<int32_t> jdl(m->nb_load > 0 ? m->nb_load : 1, 0);
+    for (int64_t i = 0; i < m->nb_load; i++) jdl[i] = (int32_t)m->jdltype[i];
+    YETI_TRY(upload(ctx, dj, jdl.data(), jdl.size()));
+    std::vector<double> adl(m->nb_load > 0 ? m->nb_load : 1, 0.0);
+    for (int64_t i = 0; i < m->nb_load; i++) adl[i] = m->adlmag[i];
+    YETI_TRY(upload(ctx, da, adl.data(), adl.size()));
+    std::vector<double> inf(m->len_load_addinfos > 0 ? m->len_load_addinfos : 1, 0.0);
+    for (int64_t i = 0; i < m->len_load_addinfos; i++) inf[i] = m->load_addinfos[i];
+    YETI_TRY(upload(ctx, dinfo, inf.data(), inf.size()));
+    if (m->nodal_dist && m->nb_n_dist > 0)
+        YETI_TRY(upload(ctx, dnd, m->nodal_dist, (size_t)m->nb_n_dist * m->nb_cp));
+    // element contributions, in global element order
+    struct Done { int patch; int64_t local; int64_t off; };
+    std::vector<Done> done;
+    std::vector<DevBuf *> ebufs_i, ebufs_e;
+    std::vector<int64_t> ien_offset(M.patches.size(), 0);
+    for (size_t ip = 1; ip < M.patches.size(); ip++)
+        ien_offset[ip] = ien_offset[ip - 1] + M.patches[ip - 1].nelem * M.patches[ip - 1].nn;
+    int64_t etotal = 0;
+    for (size_t ip = 0; ip < M.patches.size(); ip++) {
+        U1Patch &P = M.patches[ip];
+        if (!P.nactive) continue;
+        YETI_CHECK(P.nn <= 256, YETI_EUNSUPPORTED,
+                   "shape gradient: elements with more than 256 nodes are not supported");
+        std::vector<int32_t> elems, tptr(1, 0), terms;
+        int max_body = 0;
+        for (int64_t le = 0; le < P.nactive; le++) {
+            const int64_t jel = P.act[le] + 1;
+            int64_t k2 = 0;
+            int nb = 0;
+            for (int64_t il = 0; il < m->nb_load; il++) {
+                const int64_t nt = m->load_target_nbelem[il], ty = m->jdltype[il];
+                if ((ty == 101 || (ty > 9 && ty < 100)) && in_list_g(m->inddload + k2, nt, jel)) {
+                    terms.push_back((int32_t)il);
+                    nb += ty == 101;
+                    if (ty == 4 % 10 && 0) {}
+                }
+                k2 += nt;
+            }
+            YETI_CHECK(nb <= 8, YETI_EUNSUPPORTED, "more than 8 centrifugal loads on one element");
+            max_body = std::max(max_body, nb);
+            elems.push_back((int32_t)le);
+            tptr.push_back((int32_t)terms.size());
+            done.push_back({(int)ip, le, etotal});
+            etotal += nadj * 3 * P.nn;
+        }
+        std::vector<double> gf(6 * 4 * P.ng * P.ng), tmp;
+        for (int f = 1; f <= 6; f++) {
+            gauss_face_host(P.ng, f, tmp);
+            std::copy(tmp.begin(), tmp.end(), gf.begin() + (f - 1) * 4 * P.ng * P.ng);
+        }
+        DevBuf &dgf = newbuf();
+        YETI_TRY(upload(ctx, dgf, gf.data(), gf.size()));
+        DevBuf &del = newbuf();
+        YETI_TRY(upload(ctx, del, elems.data(), elems.size()));
+        DevBuf &dtp = newbuf();
+        YETI_TRY(upload(ctx, dtp, tptr.data(), tptr.size()));
+        DevBuf &dtm = newbuf();
+        if (terms.empty()) terms.push_back(0);
+        YETI_TRY(upload(ctx, dtm, terms.data(), terms.size()));
+        DevBuf &bi = newbuf();
+        DevBuf &be = newbuf();
+        YETI_TRY(bi.alloc(ctx, sizeof(double) * nadj * 3 * P.nn * elems.size()));
+        YETI_TRY(be.alloc(ctx, sizeof(double) * nadj * 3 * P.nn * elems.size()));
+        ebufs_i.push_back(&bi);
+        ebufs_e.push_back(&be);
+        GradArgs g;
+        g.p0 = P.p[0]; g.p1 = P.p[1]; g.p2 = P.p[2];
+        g.nn = P.nn; g.nq = P.nq; g.ng = P.ng; g.nadj = (int)nadj;
+        g.compute_int = compute_wint; g.compute_ext = compute_wext;
+        g.include_surface = include_surface;
+        g.U0 = P.knots.as<double>(); g.U1 = g.U0 + P.nkv[0]; g.U2 = g.U1 + P.nkv[1];
+        g.gauss = P.gauss.as<double>();
+        g.gface = dgf.as<double>();
+        g.coords = M.coords.as<double>();
+        g.ien = P.ien.as<int32_t>();
+        g.w = P.w.as<double>();
+        g.span = P.span.as<int32_t>();
+        g.elems = del.as<int32_t>();
+        g.term_ptr = dtp.as<int32_t>();
+        g.terms = dtm.as<int32_t>();
+        g.jdltype = dj.as<int32_t>();
+        g.adlmag = da.as<double>();
+        g.addinfos = dinfo.as<double>();
+        g.nodal_dist = dnd.ptr ? dnd.as<double>() : nullptr;
+        g.nb_n_dist = (int)m->nb_n_dist;
+        g.sol = sol_d;
+        g.adj = adj_d;
+        g.E = P.E; g.nu = P.nu; g.rho = P.rho;
+        g.egi = bi.as<double>();
+        g.ege = be.as<double>();
+        const PtLayout L = pt_layout(P.nn, (int)nadj, max_body);
+        const size_t vol = (size_t)P.nq * L.size;
+        const size_t face = (size_t)P.ng * P.ng * (4 * P.nn + 11 + 3 * nadj);
+        const size_t smem = sizeof(double) * ((size_t)(6 + 3 * nadj) * P.nn + P.nn + std::max(vol, face));
+        YETI_CHECK(smem <= (size_t)smem_optin, YETI_EUNSUPPORTED,
+                   "shape gradient: element needs %zu bytes of shared memory", smem);
+        k_u1_grad<<<(unsigned)elems.size(), 256, smem, s>>>(g);
+        count_launches(1);
+        YETI_CUDA(cudaGetLastError());
+    }
+    // gather per (adjoint, component, control point) in element order
+    DevBuf &ai = newbuf();
+    DevBuf &ae = newbuf();
+    YETI_TRY(ai.alloc(ctx, sizeof(double) * std::max<int64_t>(etotal, 1)));
+    YETI_TRY(ae.alloc(ctx, sizeof(double) * std::max<int64_t>(etotal, 1)));
+    {
+        int64_t off = 0;
+        for (size_t i = 0; i < ebufs_i.size(); i++) {
+            YETI_CUDA(cudaMemcpyAsync(ai.as<double>() + off, ebufs_i[i]->ptr, ebufs_i[i]->bytes, cudaMemcpyDeviceToDevice, s));
+            YETI_CUDA(cudaMemcpyAsync(ae.as<double>() + off, ebufs_e[i]->ptr, ebufs_e[i]->bytes, cudaMemcpyDeviceToDevice, s));
+            off += (int64_t)(ebufs_i[i]->bytes / sizeof(double));
+        }
+    }
+    std::vector<std::vector<int64_t>> lists(nout);
+    for (auto &D : done) {
+        const U1Patch &P = M.patches[D.patch];
+        const int64_t jel = P.act[D.local];
+        const int64_t base = ien_offset[D.patch] + (jel - P.elem_begin) * P.nn;
+        for (int a = 0; a < P.nn; a++) {
+            const int64_t cp = m->ien[base + a] - 1;
+            for (int c = 0; c < 3; c++)
+                for (int k = 0; k < nadj; k++)
+                    lists[k + nadj * (c + 3 * cp)].push_back(D.off + k + nadj * (c + 3 * a));
+        }
+    }
+    std::vector<int64_t> ptr(nout + 1, 0), idx;
+    for (int64_t i = 0; i < nout; i++) {
+        ptr[i + 1] = ptr[i] + (int64_t)lists[i].size();
+        idx.insert(idx.end(), lists[i].begin(), lists[i].end());
+    }
+    if (idx.empty()) idx.push_back(0);
+    DevBuf &dptr = newbuf();
+    DevBuf &didx = newbuf();
+    YETI_TRY(upload(ctx, dptr, ptr.data(), ptr.size()));
+    YETI_TRY(upload(ctx, didx, idx.data(), idx.size()));
+    k_grad_gather<<<(unsigned)((nout + 255) / 256), 256, 0, s>>>(
+        nout, dptr.as<int64_t>(), didx.as<int64_t>(), ai.as<double>(), ae.as<double>(), gi_d, ge_d);
+    count_launches(1);
+    YETI_CUDA(cudaGetLastError());
+    if (!compute_wint) YETI_CUDA(cudaMemsetAsync(gi_d, 0, nout * sizeof(double), s));
+    if (!compute_wext) YETI_CUDA(cudaMemsetAsync(ge_d, 0, nout * sizeof(double), s));
+    if (mem == YETI_MEM_HOST) {
+        YETI_CUDA(cudaMemcpyAsync(gwint, gi_d, nout * sizeof(double), cudaMemcpyDeviceToHost, s));
+        YETI_CUDA(cudaMemcpyAsync(gwext, ge_d, nout * sizeof(double), cudaMemcpyDeviceToHost, s));
+    }
+    YETI_CUDA(cudaStreamSynchronize(s));
+    return YETI_OK;
+}

@@ -232,6 +232,224 @@ __global__ void k_refine(double *x, const float *d32, int64_t n, double inv) {
         x[i] += (double)d32[i] * inv;
 }
 
+// Reliable update, part 1: x64 += scale * d32, d32 = 0
+__global__ void k_ru_accum(double *x, float *d32, int64_t n, double scale) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        x[i] += scale * (double)d32[i];
+        d32[i] = 0.0f;
+    }
+}
+
+// Reliable update, part 2: r32 = r64 / s_new, z32 = dinv r32, p32 *= factor
+// (or p32 = z32 to restart), partials of r.z and r.r
+__global__ void __launch_bounds__(kRedThreads)
+k_ru_replace(const double *r64, float *r32, float *z32, float *p32,
+             const float *dinv, int64_t n, double inv_s, float factor,
+             int restart, double *parts) {
+    __shared__ double sh[32];
+    double rz = 0.0, rr = 0.0;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        const float ri = (float)(r64[i] * inv_s);
+        const float zi = dinv[i] * ri;
+        r32[i] = ri;
+        z32[i] = zi;
+        p32[i] = restart ? zi : p32[i] * factor;
+        rz += (double)ri * (double)zi;
+        rr += (double)ri * (double)ri;
+    }
+    rz = block_sum(rz, sh);
+    rr = block_sum(rr, sh);
+    if (threadIdx.x == 0) {
+        parts[2 * blockIdx.x] = rz;
+        parts[2 * blockIdx.x + 1] = rr;
+    }
+}
+
+__global__ void k_ru_scal(const double *parts, int nparts, CGScal *s,
+                          double tol2, int maxit) {
+    __shared__ double sh[32];
+    const double rz = sum_parts(parts, nparts, 2, 0, sh);
+    const double rr = sum_parts(parts, nparts, 2, 1, sh);
+    if (threadIdx.x == 0) {
+        s->rz = rz;
+        s->rr = rr;
+        s->tol2 = tol2;
+        s->maxit = maxit;
+        s->done = 0;
+    }
+}
+
+// ---------------------------------------------------------------- BiCGSTAB
+// Right-preconditioned BiCGSTAB (the reference's wq_mf_bicgstab_3d,
+// mf_wq_solver.f90:958-1308, with a Jacobi preconditioner).
+struct BiScal {
+    double rho, alpha, omega, beta, rr, tol2, ts, tt;
+    int done, iter, breakdown, maxit;
+};
+
+template <class T>
+__global__ void __launch_bounds__(kRedThreads)
+k_bi_alpha_s(const double *parts, int nparts, BiScal *s) {
+    __shared__ double sh[32];
+    if (s->done) return;
+    const double rv = sum_parts(parts, nparts, 1, 0, sh);
+    if (threadIdx.x == 0) {
+        if (!(rv != 0.0) || !isfinite(rv)) {
+            s->breakdown = 1;
+            s->done = 1;
+        } else {
+            s->alpha = s->rho / rv;
+        }
+    }
+}
+
+// s = r - alpha v; sh = dinv s; t = 0
+template <class T>
+__global__ void __launch_bounds__(kRedThreads)
+k_bi_s(const T *r, const T *v, const T *dinv, T *sv, T *shat, T *t, int64_t n,
+       const BiScal *s) {
+    if (s->done) return;
+    const T a = (T)s->alpha;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        const T si = r[i] - a * v[i];
+        sv[i] = si;
+        shat[i] = dinv[i] * si;
+        t[i] = T(0);
+    }
+}
+
+// partials of t.s and t.t
+template <class T>
+__global__ void __launch_bounds__(kRedThreads)
+k_bi_ts(const T *t, const T *sv, int64_t n, double *parts, const BiScal *s) {
+    __shared__ double sh[32];
+    if (s->done) return;
+    double ts = 0.0, tt = 0.0;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        ts += (double)t[i] * (double)sv[i];
+        tt += (double)t[i] * (double)t[i];
+    }
+    ts = block_sum(ts, sh);
+    tt = block_sum(tt, sh);
+    if (threadIdx.x == 0) {
+        parts[2 * blockIdx.x] = ts;
+        parts[2 * blockIdx.x + 1] = tt;
+    }
+}
+
+__global__ void k_bi_omega(const double *parts, int nparts, BiScal *s) {
+    __shared__ double sh[32];
+    if (s->done) return;
+    const double ts = sum_parts(parts, nparts, 2, 0, sh);
+    const double tt = sum_parts(parts, nparts, 2, 1, sh);
+    if (threadIdx.x == 0) {
+        if (!(tt > 0.0) || !isfinite(ts)) {
+            s->breakdown = 1;
+            s->done = 1;
+        } else {
+            s->omega = ts / tt;
+        }
+    }
+}
+
+// x += alpha ph + omega sh; r = s - omega t; partials of rhat.r and r.r
+template <class T>
+__global__ void __launch_bounds__(kRedThreads)
+k_bi_update(T *x, T *r, const T *rhat, const T *ph, const T *shat, const T *sv,
+            const T *t, int64_t n, double *parts, const BiScal *s) {
+    __shared__ double sh[32];
+    if (s->done) return;
+    const T a = (T)s->alpha, w = (T)s->omega;
+    double rho = 0.0, rr = 0.0;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        x[i] += a * ph[i] + w * shat[i];
+        const T ri = sv[i] - w * t[i];
+        r[i] = ri;
+        rho += (double)rhat[i] * (double)ri;
+        rr += (double)ri * (double)ri;
+    }
+    rho = block_sum(rho, sh);
+    rr = block_sum(rr, sh);
+    if (threadIdx.x == 0) {
+        parts[2 * blockIdx.x] = rho;
+        parts[2 * blockIdx.x + 1] = rr;
+    }
+}
+
+__global__ void k_bi_beta(const double *parts, int nparts, BiScal *s) {
+    __shared__ double sh[32];
+    if (s->done) return;
+    const double rho = sum_parts(parts, nparts, 2, 0, sh);
+    const double rr = sum_parts(parts, nparts, 2, 1, sh);
+    if (threadIdx.x == 0) {
+        s->iter += 1;
+        s->rr = rr;
+        s->beta = (rho / s->rho) * (s->alpha / s->omega);
+        s->rho = rho;
+        if (!isfinite(rr) || rho == 0.0) {
+            s->breakdown = !isfinite(rr);
+            s->done = 1;
+        } else if (rr <= s->tol2 || s->iter >= s->maxit) {
+            s->done = 1;
+        }
+    }
+}
+
+// p = r + beta (p - omega v); ph = dinv p; v = 0
+template <class T>
+__global__ void __launch_bounds__(kRedThreads)
+k_bi_p(T *p, T *ph, const T *r, T *v, const T *dinv, int64_t n,
+       const BiScal *s) {
+    if (s->done) return;
+    const T b = (T)s->beta, w = (T)s->omega;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        const T pi = r[i] + b * (p[i] - w * v[i]);
+        p[i] = pi;
+        ph[i] = dinv[i] * pi;
+        v[i] = T(0);
+    }
+}
+
+// start: rhat = r, p = r, ph = dinv r, v = 0, partials of r.r
+template <class T>
+__global__ void __launch_bounds__(kRedThreads)
+k_bi_start(const T *r, T *rhat, T *p, T *ph, T *v, const T *dinv, int64_t n,
+           double *parts) {
+    __shared__ double sh[32];
+    double rr = 0.0;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        rhat[i] = r[i];
+        p[i] = r[i];
+        ph[i] = dinv[i] * r[i];
+        v[i] = T(0);
+        rr += (double)r[i] * (double)r[i];
+    }
+    rr = block_sum(rr, sh);
+    if (threadIdx.x == 0) parts[blockIdx.x] = rr;
+}
+
+__global__ void k_bi_start_scal(const double *parts, int nparts, BiScal *s,
+                                double tol2, int maxit) {
+    __shared__ double sh[32];
+    const double rr = sum_parts(parts, nparts, 1, 0, sh);
+    if (threadIdx.x == 0) {
+        s->rho = rr;
+        s->rr = rr;
+        s->iter = 0;
+        s->breakdown = 0;
+        s->maxit = maxit;
+        s->tol2 = tol2;
+        s->done = (rr <= tol2) || maxit <= 0 || !(rr == rr);
+    }
+}
+
 // dinv = 1/diag on free dofs, 0 on clamped ones; b masked likewise
 template <class T>
 __global__ void k_dinv(const double *diag, T *dinv, int64_t ncp, int3 n,
@@ -258,9 +476,9 @@ __global__ void k_mask(double *b, const double *dinv, int64_t n) {
 
 static int ensure_workspace(yeti_wq_op *op, bool f32) {
     const int64_t n = op->ndof;
-    if (!op->ws64.ptr) YETI_TRY(op->ws64.alloc(op->ctx, 7 * n * sizeof(double)));
-    if (f32 && !op->ws32.ptr) YETI_TRY(op->ws32.alloc(op->ctx, 5 * n * sizeof(float)));
-    if (!op->scal.ptr) YETI_TRY(op->scal.alloc(op->ctx, 2 * sizeof(CGScal)));
+    if (!op->ws64.ptr) YETI_TRY(op->ws64.alloc(op->ctx, 12 * n * sizeof(double)));
+    if (f32 && !op->ws32.ptr) YETI_TRY(op->ws32.alloc(op->ctx, 10 * n * sizeof(float)));
+    if (!op->scal.ptr) YETI_TRY(op->scal.alloc(op->ctx, 4 * sizeof(CGScal)));
     if (!op->parts.ptr) YETI_TRY(op->parts.alloc(op->ctx, 2 * kRedBlocks * sizeof(double)));
     cudaStream_t s = op->ctx->stream;
     if (!op->dinv64.ptr) {
@@ -282,34 +500,80 @@ static int ensure_workspace(yeti_wq_op *op, bool f32) {
     return YETI_OK;
 }
 
-// Run preconditioned CG on A d = r (vectors of type T) until the device flag
-// is set; the start kernels must have been enqueued.  Returns the iteration
-// count and breakdown flag through the host copy of the scalars.
+// Enqueue up to kChunk CG iterations (every kernel exits at once when the
+// device flag is set).
+template <class T>
+static int cg_chunk(yeti_wq_op *op, int prec, T *x, T *r, T *z, T *p, T *Ap,
+                    const T *dinv, CGScal *ds) {
+    cudaStream_t s = op->ctx->stream;
+    const int64_t n = op->ndof;
+    double *parts = op->parts.as<double>();
+    for (int k = 0; k < kChunk; k++) {
+        YETI_TRY(wq_apply_dev(op, p, Ap, prec, &ds->done, s));
+        k_dot<T, T><<<kRedBlocks, kRedThreads, 0, s>>>(p, Ap, n, parts, &ds->done);
+        k_alpha<<<1, kRedThreads, 0, s>>>(parts, kRedBlocks, ds);
+        k_update<T><<<kRedBlocks, kRedThreads, 0, s>>>(x, r, p, Ap, dinv, z, n, parts, ds);
+        k_beta<<<1, kRedThreads, 0, s>>>(parts, kRedBlocks, ds);
+        k_pupdate<T><<<kRedBlocks, kRedThreads, 0, s>>>(p, z, Ap, n, ds);
+        count_launches(5);
+    }
+    YETI_CUDA(cudaGetLastError());
+    return YETI_OK;
+}
+
 template <class T>
 static int cg_loop(yeti_wq_op *op, int prec, T *x, T *r, T *z, T *p, T *Ap,
                    const T *dinv, CGScal *ds, CGScal *hs) {
+    cudaStream_t s = op->ctx->stream;
+    for (;;) {
+        YETI_TRY(cg_chunk<T>(op, prec, x, r, z, p, Ap, dinv, ds));
+        YETI_CUDA(cudaMemcpyAsync(hs, ds, sizeof(CGScal), cudaMemcpyDeviceToHost, s));
+        YETI_CUDA(cudaStreamSynchronize(s));
+        if (hs->done) break;
+    }
+    return YETI_OK;
+}
+
+template <class T>
+static int bi_loop(yeti_wq_op *op, int prec, T *x, T *r, T *rhat, T *p, T *ph,
+                   T *v, T *sv, T *shat, T *t, const T *dinv, BiScal *ds,
+                   BiScal *hs) {
     cudaStream_t s = op->ctx->stream;
     const int64_t n = op->ndof;
     double *parts = op->parts.as<double>();
     for (;;) {
         for (int k = 0; k < kChunk; k++) {
-            YETI_TRY(wq_apply_dev(op, p, Ap, prec, &ds->done, s));
-            k_dot<T, T><<<kRedBlocks, kRedThreads, 0, s>>>(p, Ap, n, parts, &ds->done);
-            count_launches(1);
-            k_alpha<<<1, kRedThreads, 0, s>>>(parts, kRedBlocks, ds);
-            count_launches(1);
-            k_update<T><<<kRedBlocks, kRedThreads, 0, s>>>(x, r, p, Ap, dinv, z, n, parts, ds);
-            count_launches(1);
-            k_beta<<<1, kRedThreads, 0, s>>>(parts, kRedBlocks, ds);
-            count_launches(1);
-            k_pupdate<T><<<kRedBlocks, kRedThreads, 0, s>>>(p, z, Ap, n, ds);
-            count_launches(1);
+            YETI_TRY(wq_apply_dev(op, ph, v, prec, &ds->done, s));
+            k_dot<T, T><<<kRedBlocks, kRedThreads, 0, s>>>(rhat, v, n, parts, &ds->done);
+            k_bi_alpha_s<T><<<1, kRedThreads, 0, s>>>(parts, kRedBlocks, ds);
+            k_bi_s<T><<<kRedBlocks, kRedThreads, 0, s>>>(r, v, dinv, sv, shat, t, n, ds);
+            YETI_TRY(wq_apply_dev(op, shat, t, prec, &ds->done, s));
+            k_bi_ts<T><<<kRedBlocks, kRedThreads, 0, s>>>(t, sv, n, parts, ds);
+            k_bi_omega<<<1, kRedThreads, 0, s>>>(parts, kRedBlocks, ds);
+            k_bi_update<T><<<kRedBlocks, kRedThreads, 0, s>>>(x, r, rhat, ph, shat, sv, t, n, parts, ds);
+            k_bi_beta<<<1, kRedThreads, 0, s>>>(parts, kRedBlocks, ds);
+            k_bi_p<T><<<kRedBlocks, kRedThreads, 0, s>>>(p, ph, r, v, dinv, n, ds);
+            count_launches(8);
         }
         YETI_CUDA(cudaGetLastError());
-        YETI_CUDA(cudaMemcpyAsync(hs, ds, sizeof(CGScal), cudaMemcpyDeviceToHost, s));
+        YETI_CUDA(cudaMemcpyAsync(hs, ds, sizeof(BiScal), cudaMemcpyDeviceToHost, s));
         YETI_CUDA(cudaStreamSynchronize(s));
         if (hs->done) break;
     }
+    return YETI_OK;
+}
+
+// Host sum of device partials (fixed order).
+static int host_sum(yeti_wq_op *op, const double *parts, int n, int stride,
+                    int off, double *out, bool take_max = false) {
+    std::vector<double> hp((size_t)n * stride);
+    YETI_CUDA(cudaMemcpyAsync(hp.data(), parts, hp.size() * sizeof(double),
+                              cudaMemcpyDeviceToHost, op->ctx->stream));
+    YETI_CUDA(cudaStreamSynchronize(op->ctx->stream));
+    double acc = 0.0;
+    for (int i = 0; i < n; i++)
+        acc = take_max ? std::max(acc, hp[(size_t)i * stride + off]) : acc + hp[(size_t)i * stride + off];
+    *out = acc;
     return YETI_OK;
 }
 
@@ -321,23 +585,28 @@ YETI_API int yeti_wq_pcg(yeti_wq_op *op, const double *b, double *x,
                          double rtol, int maxit, int mode,
                          yeti_cg_stats *stats, int mem) {
     YETI_CHECK(op && b && x, YETI_EINVAL, "yeti_wq_pcg: NULL argument");
-    YETI_CHECK(mode == 0 || mode == 1, YETI_EINVAL, "yeti_wq_pcg: mode %d", mode);
+    YETI_CHECK(mode >= 0 && mode <= 3, YETI_EINVAL, "yeti_wq_pcg: mode %d", mode);
     YETI_CHECK(rtol > 0 && maxit > 0, YETI_EINVAL, "yeti_wq_pcg: rtol %g maxit %d", rtol, maxit);
     YETI_CHECK(op->coef64.ptr, YETI_EINVAL,
                "yeti_wq_pcg: the FP64 operator is required (true residual)");
-    YETI_CHECK(mode == 0 || op->coef32.ptr, YETI_EINVAL,
-               "yeti_wq_pcg: mode 1 needs the FP32 operator (YETI_WQ_F32)");
+    const bool mixed = (mode & 1) != 0, bicg = (mode & 2) != 0;
+    YETI_CHECK(!mixed || op->coef32.ptr, YETI_EINVAL,
+               "yeti_wq_pcg: mixed precision needs the FP32 operator (YETI_WQ_F32)");
     DeviceGuard guard(op->ctx->device);
-    YETI_TRY(ensure_workspace(op, mode == 1));
+    YETI_TRY(ensure_workspace(op, mixed));
     cudaStream_t s = op->ctx->stream;
     const int64_t n = op->ndof;
     double *W = op->ws64.as<double>();
     double *dx = W, *dr = W + n, *dz = W + 2 * n, *dp = W + 3 * n, *dAp = W + 4 * n,
-           *db = W + 5 * n, *dt = W + 6 * n;
+           *db = W + 5 * n, *dt = W + 6 * n, *drh = W + 7 * n, *dph = W + 8 * n,
+           *dsv = W + 9 * n, *dsh = W + 10 * n, *dtt = W + 11 * n;
     double *parts = op->parts.as<double>();
     CGScal *ds = op->scal.as<CGScal>();
+    BiScal *bs = reinterpret_cast<BiScal *>(ds + 2);
     CGScal hs;
+    BiScal hb;
     memset(&hs, 0, sizeof(hs));
+    memset(&hb, 0, sizeof(hb));
     cudaEvent_t e0, e1;
     YETI_CUDA(cudaEventCreate(&e0));
     YETI_CUDA(cudaEventCreate(&e1));
@@ -347,13 +616,11 @@ YETI_API int yeti_wq_pcg(yeti_wq_op *op, const double *b, double *x,
     YETI_CUDA(cudaMemcpyAsync(dx, x, n * sizeof(double), h2d, s));
     const double *dinv = op->dinv64.as<double>();
     k_mask<<<kRedBlocks, kRedThreads, 0, s>>>(db, dinv, n);
-    count_launches(1);
     k_mask<<<kRedBlocks, kRedThreads, 0, s>>>(dx, dinv, n);
-    count_launches(1);
     k_dot<double, double><<<kRedBlocks, kRedThreads, 0, s>>>(db, db, n, parts, nullptr);
-    count_launches(1);
-    k_set_bb<<<1, kRedThreads, 0, s>>>(parts, kRedBlocks, ds);
-    count_launches(1);
+    count_launches(3);
+    double bb = 0.0;
+    YETI_TRY(host_sum(op, parts, kRedBlocks, 1, 0, &bb));
     // r = b - A x
     YETI_CUDA(cudaMemsetAsync(dt, 0, n * sizeof(double), s));
     YETI_TRY(wq_apply_dev(op, dx, dt, YETI_PREC_F64, nullptr, s));
@@ -361,96 +628,139 @@ YETI_API int yeti_wq_pcg(yeti_wq_op *op, const double *b, double *x,
     count_launches(1);
     YETI_CUDA(cudaGetLastError());
     int iters = 0, outer = 0, f64 = 1, f32 = 0, status = YETI_OK;
-    if (mode == 0) {
+    const double tol2 = rtol * rtol * bb;
+    if (!mixed && !bicg) {
+        CGScal init;
+        memset(&init, 0, sizeof(init));
+        init.bb = bb;
+        YETI_CUDA(cudaMemcpyAsync(ds, &init, sizeof(CGScal), cudaMemcpyHostToDevice, s));
         k_start<double><<<kRedBlocks, kRedThreads, 0, s>>>(dr, dinv, dz, dp, dAp, n, parts);
-        count_launches(1);
         k_start_scal<<<1, kRedThreads, 0, s>>>(parts, kRedBlocks, ds, rtol * rtol, maxit);
-        count_launches(1);
+        count_launches(2);
         YETI_CUDA(cudaGetLastError());
         YETI_TRY(cg_loop<double>(op, YETI_PREC_F64, dx, dr, dz, dp, dAp, dinv, ds, &hs));
         iters = hs.iter;
         f64 += hs.iter;
         if (hs.breakdown) status = YETI_EBREAKDOWN;
         outer = 1;
-    } else {
+    } else if (!mixed && bicg) {
+        k_bi_start<double><<<kRedBlocks, kRedThreads, 0, s>>>(dr, drh, dp, dph, dAp, dinv, n, parts);
+        k_bi_start_scal<<<1, kRedThreads, 0, s>>>(parts, kRedBlocks, bs, tol2, maxit);
+        count_launches(2);
+        YETI_CUDA(cudaGetLastError());
+        YETI_TRY(bi_loop<double>(op, YETI_PREC_F64, dx, dr, drh, dp, dph, dAp, dsv, dsh, dtt, dinv, bs, &hb));
+        iters = hb.iter;
+        f64 += 2 * hb.iter;
+        if (hb.breakdown) status = YETI_EBREAKDOWN;
+        outer = 1;
+    } else if (mixed && !bicg) {
+        // FP32 CG with reliable updates: the Krylov iteration runs in FP32
+        // and is never restarted; whenever its recursive residual has
+        // dropped 10x (or reached the tolerance), the solution correction is
+        // folded into the FP64 solution, the true residual is recomputed with
+        // the FP64 operator and replaces the FP32 one (search direction kept,
+        // rescaled).
         float *V = op->ws32.as<float>();
         float *r32 = V, *z32 = V + n, *p32 = V + 2 * n, *Ap32 = V + 3 * n, *d32 = V + 4 * n;
         const float *dinv32 = op->dinv32.as<float>();
-        const double eta = 1e-4;   // inner relative tolerance
-        CGScal hb;
-        YETI_CUDA(cudaMemcpyAsync(&hb, ds, sizeof(CGScal), cudaMemcpyDeviceToHost, s));
-        YETI_CUDA(cudaStreamSynchronize(s));
-        const double bb = hb.bb;
-        for (outer = 0; outer < 50; outer++) {
-            // rr of the FP64 true residual (scratch scalars ds[1])
-            k_dot<double, double><<<kRedBlocks, kRedThreads, 0, s>>>(dr, dr, n, parts, nullptr);
-            count_launches(1);
-            k_set_bb<<<1, kRedThreads, 0, s>>>(parts, kRedBlocks, ds + 1);
-            count_launches(1);
-            YETI_CUDA(cudaMemcpyAsync(&hs, ds + 1, sizeof(CGScal), cudaMemcpyDeviceToHost, s));
-            YETI_CUDA(cudaStreamSynchronize(s));
-            const double rr = hs.bb;
-            if (!(rr == rr)) { status = YETI_EBREAKDOWN; break; }
-            if (rr <= rtol * rtol * bb || iters >= maxit) break;
-            const double scale = 1.0 / std::sqrt(rr);
-            k_to_f32<<<kRedBlocks, kRedThreads, 0, s>>>(dr, r32, d32, n, scale);
-            count_launches(1);
+        const double delta2 = 1e-2;   // replace when ||r|| fell by 10x
+        double rr64 = 0.0;
+        k_dot<double, double><<<kRedBlocks, kRedThreads, 0, s>>>(dr, dr, n, parts, nullptr);
+        count_launches(1);
+        YETI_TRY(host_sum(op, parts, kRedBlocks, 1, 0, &rr64));
+        double sc = std::sqrt(rr64);
+        if (rr64 > tol2 && rr64 == rr64) {
+            k_to_f32<<<kRedBlocks, kRedThreads, 0, s>>>(dr, r32, d32, n, 1.0 / sc);
             k_start<float><<<kRedBlocks, kRedThreads, 0, s>>>(r32, dinv32, z32, p32, Ap32, n, parts);
-            count_launches(1);
-            // inner tolerance relative to ||r32|| = 1
             CGScal init;
             memset(&init, 0, sizeof(init));
             init.bb = 1.0;
             YETI_CUDA(cudaMemcpyAsync(ds, &init, sizeof(CGScal), cudaMemcpyHostToDevice, s));
-            k_start_scal<<<1, kRedThreads, 0, s>>>(parts, kRedBlocks, ds, eta * eta, maxit - iters);
-            count_launches(1);
+            k_start_scal<<<1, kRedThreads, 0, s>>>(parts, kRedBlocks, ds, tol2 / rr64, maxit);
+            count_launches(3);
             YETI_CUDA(cudaGetLastError());
-            YETI_TRY(cg_loop<float>(op, YETI_PREC_F32, d32, r32, z32, p32, Ap32, dinv32, ds, &hs));
-            iters += hs.iter;
-            f32 += hs.iter;
-            k_refine<<<kRedBlocks, kRedThreads, 0, s>>>(dx, d32, n, 1.0 / scale);
+            double rr_ref = 1.0;
+            for (;;) {
+                YETI_TRY(cg_chunk<float>(op, YETI_PREC_F32, d32, r32, z32, p32, Ap32, dinv32, ds));
+                YETI_CUDA(cudaMemcpyAsync(&hs, ds, sizeof(CGScal), cudaMemcpyDeviceToHost, s));
+                YETI_CUDA(cudaStreamSynchronize(s));
+                const int it = hs.iter;
+                if (hs.breakdown) { iters = it; status = YETI_EBREAKDOWN; break; }
+                if (!(hs.done || hs.rr <= delta2 * rr_ref)) continue;
+                // reliable update
+                k_ru_accum<<<kRedBlocks, kRedThreads, 0, s>>>(dx, d32, n, sc);
+                YETI_CUDA(cudaMemsetAsync(dt, 0, n * sizeof(double), s));
+                YETI_TRY(wq_apply_dev(op, dx, dt, YETI_PREC_F64, nullptr, s));
+                k_residual<<<kRedBlocks, kRedThreads, 0, s>>>(db, dt, dinv, dr, n);
+                k_dot<double, double><<<kRedBlocks, kRedThreads, 0, s>>>(dr, dr, n, parts, nullptr);
+                count_launches(3);
+                f64++;
+                outer++;
+                YETI_TRY(host_sum(op, parts, kRedBlocks, 1, 0, &rr64));
+                iters = it;
+                if (!(rr64 == rr64)) { status = YETI_EBREAKDOWN; break; }
+                if (rr64 <= tol2 || it >= maxit) break;
+                const double sc_new = std::sqrt(rr64);
+                // a replacement after the FP32 recursion met the tolerance
+                // restarts the direction (its last update was skipped)
+                k_ru_replace<<<kRedBlocks, kRedThreads, 0, s>>>(dr, r32, z32, p32, dinv32, n,
+                                                                1.0 / sc_new, (float)(sc / sc_new),
+                                                                hs.done ? 1 : 0, parts);
+                k_ru_scal<<<1, kRedThreads, 0, s>>>(parts, kRedBlocks, ds, tol2 / rr64, maxit);
+                count_launches(2);
+                YETI_CUDA(cudaGetLastError());
+                sc = sc_new;
+                rr_ref = 1.0;
+            }
+            f32 = iters;
+        }
+    } else {
+        // mixed BiCGSTAB: FP32 inner solves, FP64 residual and refinement
+        float *V = op->ws32.as<float>();
+        float *r32 = V, *rh = V + n, *p32 = V + 2 * n, *ph = V + 3 * n, *v32 = V + 4 * n,
+              *sv = V + 5 * n, *shh = V + 6 * n, *t32 = V + 7 * n, *d32 = V + 8 * n;
+        const float *dinv32 = op->dinv32.as<float>();
+        const double eta2 = 1e-8;   // inner relative tolerance 1e-4
+        for (outer = 0; outer < 50; outer++) {
+            double rr64 = 0.0;
+            k_dot<double, double><<<kRedBlocks, kRedThreads, 0, s>>>(dr, dr, n, parts, nullptr);
             count_launches(1);
+            YETI_TRY(host_sum(op, parts, kRedBlocks, 1, 0, &rr64));
+            if (!(rr64 == rr64)) { status = YETI_EBREAKDOWN; break; }
+            if (rr64 <= tol2 || iters >= maxit) break;
+            const double sc = 1.0 / std::sqrt(rr64);
+            k_to_f32<<<kRedBlocks, kRedThreads, 0, s>>>(dr, r32, d32, n, sc);
+            k_bi_start<float><<<kRedBlocks, kRedThreads, 0, s>>>(r32, rh, p32, ph, v32, dinv32, n, parts);
+            k_bi_start_scal<<<1, kRedThreads, 0, s>>>(parts, kRedBlocks, bs, eta2, maxit - iters);
+            count_launches(3);
+            YETI_TRY(bi_loop<float>(op, YETI_PREC_F32, d32, r32, rh, p32, ph, v32, sv, shh, t32, dinv32, bs, &hb));
+            iters += hb.iter;
+            f32 += 2 * hb.iter;
+            k_refine<<<kRedBlocks, kRedThreads, 0, s>>>(dx, d32, n, 1.0 / sc);
             YETI_CUDA(cudaMemsetAsync(dt, 0, n * sizeof(double), s));
             YETI_TRY(wq_apply_dev(op, dx, dt, YETI_PREC_F64, nullptr, s));
             k_residual<<<kRedBlocks, kRedThreads, 0, s>>>(db, dt, dinv, dr, n);
-            count_launches(1);
+            count_launches(2);
             YETI_CUDA(cudaGetLastError());
             f64++;
-            if (hs.breakdown && hs.iter == 0) { status = YETI_EBREAKDOWN; break; }
+            if (hb.breakdown && hb.iter == 0) { status = YETI_EBREAKDOWN; break; }
         }
     }
     YETI_CUDA(cudaEventRecord(e1, s));
-    // true FP64 residual (mode 0: recompute; mode 1: dr already holds it)
-    if (mode == 0) {
-        YETI_CUDA(cudaMemsetAsync(dt, 0, n * sizeof(double), s));
-        YETI_TRY(wq_apply_dev(op, dx, dt, YETI_PREC_F64, nullptr, s));
-        k_residual<<<kRedBlocks, kRedThreads, 0, s>>>(db, dt, dinv, dr, n);
-        count_launches(1);
-    }
-    double h[4];
+    // true FP64 residual of the returned solution
+    YETI_CUDA(cudaMemsetAsync(dt, 0, n * sizeof(double), s));
+    YETI_TRY(wq_apply_dev(op, dx, dt, YETI_PREC_F64, nullptr, s));
+    k_residual<<<kRedBlocks, kRedThreads, 0, s>>>(db, dt, dinv, dr, n);
     k_dot<double, double><<<kRedBlocks, kRedThreads, 0, s>>>(dr, dr, n, parts, nullptr);
-    count_launches(1);
-    k_dot<double, double><<<kRedBlocks, kRedThreads, 0, s>>>(db, db, n, parts + kRedBlocks, nullptr);
-    count_launches(1);
-    std::vector<double> hp(2 * kRedBlocks);
-    YETI_CUDA(cudaMemcpyAsync(hp.data(), parts, 2 * kRedBlocks * sizeof(double), cudaMemcpyDeviceToHost, s));
-    YETI_CUDA(cudaStreamSynchronize(s));
-    h[0] = h[1] = 0.0;
-    for (int i = 0; i < kRedBlocks; i++) {
-        h[0] += hp[i];
-        h[1] += hp[kRedBlocks + i];
-    }
+    count_launches(2);
+    double rr = 0.0, rmax = 0.0, bmax = 0.0;
+    YETI_TRY(host_sum(op, parts, kRedBlocks, 1, 0, &rr));
     k_absmax<double><<<kRedBlocks, kRedThreads, 0, s>>>(dr, n, parts);
     count_launches(1);
-    k_absmax<double><<<kRedBlocks, kRedThreads, 0, s>>>(db, n, parts + kRedBlocks);
+    YETI_TRY(host_sum(op, parts, kRedBlocks, 1, 0, &rmax, true));
+    k_absmax<double><<<kRedBlocks, kRedThreads, 0, s>>>(db, n, parts);
     count_launches(1);
-    YETI_CUDA(cudaMemcpyAsync(hp.data(), parts, 2 * kRedBlocks * sizeof(double), cudaMemcpyDeviceToHost, s));
-    YETI_CUDA(cudaStreamSynchronize(s));
-    h[2] = h[3] = 0.0;
-    for (int i = 0; i < kRedBlocks; i++) {
-        h[2] = std::max(h[2], hp[i]);
-        h[3] = std::max(h[3], hp[kRedBlocks + i]);
-    }
+    YETI_TRY(host_sum(op, parts, kRedBlocks, 1, 0, &bmax, true));
     float ms = 0.f;
     YETI_CUDA(cudaEventElapsedTime(&ms, e0, e1));
     cudaEventDestroy(e0);
@@ -458,7 +768,7 @@ YETI_API int yeti_wq_pcg(yeti_wq_op *op, const double *b, double *x,
     const cudaMemcpyKind d2h = mem == YETI_MEM_HOST ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice;
     YETI_CUDA(cudaMemcpyAsync(x, dx, n * sizeof(double), d2h, s));
     YETI_CUDA(cudaStreamSynchronize(s));
-    const double rel = h[1] > 0 ? std::sqrt(h[0] / h[1]) : 0.0;
+    const double rel = bb > 0 ? std::sqrt(rr / bb) : 0.0;
     if (status == YETI_OK && !(rel <= rtol)) status = YETI_ENOTCONV;
     if (stats) {
         stats->iterations = iters;
@@ -466,7 +776,7 @@ YETI_API int yeti_wq_pcg(yeti_wq_op *op, const double *b, double *x,
         stats->fp64_applies = f64;
         stats->fp32_applies = f32;
         stats->rel_residual = rel;
-        stats->rel_residual_inf = h[3] > 0 ? h[2] / h[3] : 0.0;
+        stats->rel_residual_inf = bmax > 0 ? rmax / bmax : 0.0;
         stats->solve_ms = ms;
         stats->status = status;
     }

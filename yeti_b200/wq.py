@@ -37,7 +37,8 @@ class WQElasticity:
         mask = {"f64": WQ_F64, "f32": WQ_F32, "both": WQ_F64 | WQ_F32}[precisions]
         p = np.ascontiguousarray(patch["p"], dtype=np.int32)
         nel = np.ascontiguousarray(patch["nel"], dtype=np.int32)
-        cps = np.ascontiguousarray(patch["cps"], dtype=np.float64)
+        # (3, ncp) in Fortran order: x, y, z of each control point together
+        cps = np.ascontiguousarray(np.asarray(patch["cps"], dtype=np.float64).T)
         w = np.ascontiguousarray(patch["weights"], dtype=np.float64)
         dm = face_mask(self.clamp_faces)
         h = ctypes.c_void_p()
@@ -90,11 +91,17 @@ class WQElasticity:
         return out
 
     # --------------------------------------------------------------- solver
-    def pcg(self, b, rtol=1e-8, maxit=20000, mixed=False, x0=None):
-        """Jacobi PCG.  b, x0: numpy (host) or torch CUDA float64 tensors.
-        Returns (x, stats dict)."""
+    def pcg(self, b, rtol=1e-8, maxit=20000, mixed=False, x0=None,
+            method="cg"):
+        """Jacobi-preconditioned Krylov solve of K x = b.
+
+        method 'cg' (mf_wq_solver.f90:764-802) or 'bicgstab'
+        (mf_wq_solver.f90:958-1308).  mixed=True: FP32 operator and Krylov
+        vectors with the FP64 true residual (CG: reliable updates; BiCGSTAB:
+        iterative refinement).  b, x0: numpy (host) or torch CUDA float64
+        tensors.  Returns (x, stats dict)."""
         st = CGStats()
-        mode = 1 if mixed else 0
+        mode = (1 if mixed else 0) | (2 if method == "bicgstab" else 0)
         if isinstance(b, np.ndarray):
             bb = np.ascontiguousarray(b, dtype=np.float64)
             x = np.zeros_like(bb) if x0 is None else np.array(x0, dtype=np.float64)
@@ -114,9 +121,10 @@ class WQElasticity:
         """Twin of fortran_mf_wq.mf_conj_grad (fortran_mf_wq.py:545-560):
         returns (sol, residue, error) with residue/error the reference's
         inf-norm measures at the start and the end of the solve."""
-        if method != "WP" or not isCG:
-            raise NotImplementedError("Jacobi-preconditioned CG only")
-        x, st = self.pcg(bi, rtol=epsilon, maxit=nbIterations, mixed=mixed)
+        if method != "WP":
+            raise NotImplementedError("Jacobi preconditioning only ('WP')")
+        x, st = self.pcg(bi, rtol=epsilon, maxit=nbIterations, mixed=mixed,
+                         method="cg" if isCG else "bicgstab")
         residue = np.array([1.0, st["rel_residual_inf"]])
         error = np.array([1.0, 0.0])
         if directsol is not None:
