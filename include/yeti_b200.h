@@ -65,7 +65,8 @@ uint64_t yeti_kernel_launches(void);
 int yeti_ctx_create(int device, size_t hbm_budget_bytes, yeti_ctx **out);
 int yeti_ctx_destroy(yeti_ctx *ctx);
 /* Use an existing cudaStream_t (passed as void*) for all work of the
- * context; NULL restores the context's own stream. */
+ * context; NULL restores the context's own stream (pass cudaStreamLegacy,
+ * (void*)0x1, for the legacy default stream). */
 int yeti_ctx_set_stream(yeti_ctx *ctx, void *stream);
 int yeti_ctx_synchronize(yeti_ctx *ctx);
 /* Bytes of device memory currently held by the context's objects. */

@@ -10,10 +10,12 @@
  * it once per trial derivative (forward, with B^T) and once per
  * (test, trial) pair (backward, with W), scaling by the pointwise
  * coefficients in between.  This file restates that structure for the
- * elastic rational operator defined in oracle/wq_ops.py (12 forward and 48
- * backward products per apply), and restates jacobien_physicalposition_3d /
+ * elastic operator defined in oracle/wq_ops.py (B-spline test and trial
+ * functions on the exact NURBS geometry: 9 forward and 27 backward products
+ * per apply), and restates jacobien_physicalposition_3d /
  * eval_mech_coefficient (wq_assembly.f90:233-473, 52-138) for the
- * coefficients, with the geometric orientation of the inverse Jacobian.
+ * coefficients, with the NURBS weights in the geometry map and the geometric
+ * orientation of the inverse Jacobian.
  */
 #include <math.h>
 #include <omp.h>
@@ -32,8 +34,7 @@ typedef struct {
     int64_t ncp, nqp;
     csr_t BT[3][2];   /* B0^T, B1^T: (nqp_d x nfun_d) */
     csr_t W[3][4];    /* W00 W01 W10 W11: (nfun_d x nqp_d) */
-    double *w;        /* CP weights */
-    double *coef;     /* nqp * 48: S^ upper triangle (45), g (3) */
+    double *coef;     /* nqp * 45: upper triangle of S */
     unsigned char *mask;   /* 3*ncp: 1 free, 0 clamped */
 } wq_t;
 
@@ -125,11 +126,9 @@ void *oracle_wq_create(const int *n, const int *q, const double *const *rules,
     }
     op->ncp = (int64_t)n[0] * n[1] * n[2];
     op->nqp = (int64_t)q[0] * q[1] * q[2];
-    op->w = (double *)malloc(sizeof(double) * op->ncp);
-    memcpy(op->w, w, sizeof(double) * op->ncp);
     op->mask = (unsigned char *)malloc(3 * op->ncp);
     memcpy(op->mask, mask, 3 * op->ncp);
-    op->coef = (double *)malloc(sizeof(double) * 48 * op->nqp);
+    op->coef = (double *)malloc(sizeof(double) * 45 * op->nqp);
     /* geometry: forward products of (w x, w y, w z, w) with B0/B1 */
     const int64_t NQ = op->nqp;
     double *F = (double *)calloc((size_t)16 * NQ, sizeof(double));
@@ -181,8 +180,8 @@ void *oracle_wq_create(const int *n, const int *q, const double *const *rules,
         iJ[2][0] = (J[1][0] * J[2][1] - J[1][1] * J[2][0]) * id;
         iJ[2][1] = (J[0][1] * J[2][0] - J[0][0] * J[2][1]) * id;
         iJ[2][2] = (J[0][0] * J[1][1] - J[0][1] * J[1][0]) * id;
-        double scale = fabs(det) / (W * W);
-        double *co = op->coef + 48 * qq;
+        double scale = fabs(det);
+        double *co = op->coef + 45 * qq;
         for (int I = 0; I < 9; I++)
             for (int Jn = I; Jn < 9; Jn++) {
                 int i = I / 3, k = I % 3, j = Jn / 3, l = Jn % 3;
@@ -192,7 +191,6 @@ void *oracle_wq_create(const int *n, const int *q, const double *const *rules,
                         s += iJ[k][d] * MDM[3 * i + d][3 * j + ff] * iJ[l][ff];
                 co[sym9(I, Jn)] = s * scale;
             }
-        for (int l = 0; l < 3; l++) co[45 + l] = f[l + 1][3] / W;
     }
     free(F);
     return op;
@@ -207,7 +205,6 @@ void oracle_wq_free(void *h)
         csr_free(&op->BT[d][1]);
         for (int t = 0; t < 4; t++) csr_free(&op->W[d][t]);
     }
-    free(op->w);
     free(op->coef);
     free(op->mask);
     free(op);
@@ -219,48 +216,38 @@ int oracle_wq_apply(void *h, const double *u, double *Ku)
     wq_t *op = (wq_t *)h;
     const int64_t NC = op->ncp, NQ = op->nqp;
     double *v = (double *)malloc(sizeof(double) * NC);
-    double *F = (double *)calloc((size_t)12 * NQ, sizeof(double));
+    double *F = (double *)calloc((size_t)9 * NQ, sizeof(double));
+    /* F[(3*l + j)] = d u_j / d xi_(l+1) at the points */
     for (int j = 0; j < 3; j++) {
-        for (int64_t a = 0; a < NC; a++) v[a] = op->mask[j * NC + a] ? op->w[a] * u[j * NC + a] : 0.0;
-        for (int l = 0; l < 4; l++)
-            sparsedot3(&op->BT[0][l == 1], &op->BT[1][l == 2], &op->BT[2][l == 3], v,
+        for (int64_t a = 0; a < NC; a++) v[a] = op->mask[j * NC + a] ? u[j * NC + a] : 0.0;
+        for (int l = 0; l < 3; l++)
+            sparsedot3(&op->BT[0][l == 0], &op->BT[1][l == 1], &op->BT[2][l == 2], v,
                        F + (size_t)(3 * l + j) * NQ);
     }
-    double *H = (double *)malloc(sizeof(double) * 16 * NQ);
+    double *H = (double *)malloc(sizeof(double) * 9 * NQ);
     double *out = (double *)malloc(sizeof(double) * NC);
     for (int i = 0; i < 3; i++) {
         #pragma omp parallel for schedule(static)
         for (int64_t qq = 0; qq < NQ; qq++) {
-            const double *co = op->coef + 48 * qq;
-            double f[4][3], g[3] = {co[45], co[46], co[47]}, hh[16];
-            for (int l = 0; l < 4; l++)
+            const double *co = op->coef + 45 * qq;
+            double f[3][3];
+            for (int l = 0; l < 3; l++)
                 for (int j = 0; j < 3; j++) f[l][j] = F[(size_t)(3 * l + j) * NQ + qq];
-            for (int k = 0; k < 3; k++) {
-                double S[9];
-                for (int Jn = 0; Jn < 9; Jn++) S[Jn] = co[sym9(3 * i + k, Jn)];
+            for (int k = 0; k < 3; k++)
                 for (int l = 0; l < 3; l++) {
                     double a = 0.0;
-                    for (int j = 0; j < 3; j++) a += S[3 * j + l] * f[l + 1][j];
-                    hh[(k + 1) * 4 + l + 1] = a;
+                    for (int j = 0; j < 3; j++) a += co[sym9(3 * i + k, 3 * j + l)] * f[l][j];
+                    H[(size_t)(3 * k + l) * NQ + qq] = a;
                 }
-                double h0 = 0.0;
-                for (int j = 0; j < 3; j++)
-                    h0 -= (S[3 * j] * g[0] + S[3 * j + 1] * g[1] + S[3 * j + 2] * g[2]) * f[0][j];
-                hh[(k + 1) * 4] = h0;
-            }
-            for (int lam = 0; lam < 4; lam++)
-                hh[lam] = -(g[0] * hh[4 + lam] + g[1] * hh[8 + lam] + g[2] * hh[12 + lam]);
-            for (int ch = 0; ch < 16; ch++) H[(size_t)ch * NQ + qq] = hh[ch];
         }
         memset(out, 0, sizeof(double) * NC);
-        for (int ch = 0; ch < 16; ch++) {
-            int kap = ch / 4, lam = ch % 4;
-            sparsedot3(&op->W[0][2 * (kap == 1) + (lam == 1)],
-                       &op->W[1][2 * (kap == 2) + (lam == 2)],
-                       &op->W[2][2 * (kap == 3) + (lam == 3)], H + (size_t)ch * NQ, out);
+        for (int ch = 0; ch < 9; ch++) {
+            int kap = ch / 3, lam = ch % 3;
+            sparsedot3(&op->W[0][2 * (kap == 0) + (lam == 0)],
+                       &op->W[1][2 * (kap == 1) + (lam == 1)],
+                       &op->W[2][2 * (kap == 2) + (lam == 2)], H + (size_t)ch * NQ, out);
         }
-        for (int64_t a = 0; a < NC; a++)
-            Ku[i * NC + a] = op->mask[i * NC + a] ? op->w[a] * out[a] : 0.0;
+        for (int64_t a = 0; a < NC; a++) Ku[i * NC + a] = op->mask[i * NC + a] ? out[a] : 0.0;
     }
     free(v);
     free(F);

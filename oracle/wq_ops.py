@@ -7,33 +7,29 @@ The reference ships the WQ matrix-free operator for the scalar (thermal)
 problem only, with B-spline geometry:
   * K u = sum_{k,l} W^{(k,l)} (coef_kl * (B^{(l)})^T u)
     (mf_wq_get_ku_3d, src/yeti_iga/iga_wq_mf/fsrc/mf_wq_solver.f90:284-544),
-    W^{(k,l)} the Kronecker product of the 1-D weights W^{[d==k][d==l]};
+    W^{(k,l)} the Kronecker product of the 1-D weights W^{[d==k][d==l]} and
+    B^{(l)} that of B^{[d==l]};
   * the elastic coefficient S = ext(invJ)^T (MM^T DD MM) ext(invJ) detJ
-    (eval_mech_coefficient, wq_assembly.f90:52-138) used per 3x3 component
+    (eval_mech_coefficient, wq_assembly.f90:52-138), used per 3x3 component
     block (wq_get_stiffness_3d, wq_assembly.f90:1020-1054);
   * the Jacobian from B-spline sums (jacobien_physicalposition_3d,
     wq_assembly.f90:233-473).
-This oracle composes them into the elastic operator and extends it to NURBS:
+This oracle composes them into the elastic operator
 
-  u_j = v_j / W with v_j = sum_a N_a (w_a U_aj), W = sum_a N_a w_a, and the
-  test function R_a = w_a N_a / W, so that with S^ = S / W^2, g = grad W / W
+    (K U)_{a,i} = sum_{k,l} sum_q W^{(k,l)}_a(q) sum_j S[(i,k),(j,l)](q) (B^{(l)} U_j)(q)
 
-      (K U)_ai = w_a sum_{kappa,lambda} sum_q W^{kappa,lambda}_a(q) H^{kappa,lambda}_i(q)
-
-  over test kinds kappa (0: value, 1..3: derivative direction) and trial
-  kinds lambda (same), with, at each point,
-      H^{k,l}_i = sum_j S^[(i,k),(j,l)] dv_j/dxi_l
-      H^{k,0}_i = -sum_j (sum_l S^[(i,k),(j,l)] g_l) v_j
-      H^{0,lambda}_i = -sum_k g_k H^{k,lambda}_i .
-  The 1-D weight of direction d is W^{[d==kappa][d==lambda]} (test order,
-  trial order), as in the reference.  With all weights 1, g = 0 and this is
-  exactly the reference's operator per component block.
+with the reference's B-spline test and trial functions, on the exact NURBS
+geometry: the Jacobian J = dx/dxi of x = sum w_a N_a P_a / sum w_a N_a.
 
 Two deliberate differences from the reference's code, both documented in
 DESIGN.md: the coefficient uses the geometric orientation
 S = ext(invJ) MDM ext(invJ)^T |detJ| with invJ = (dx/dxi)^{-1} (the
 reference's product is transposed, which only agrees for symmetric
-Jacobians), and the Jacobian includes the NURBS weights.
+Jacobians), and the Jacobian includes the NURBS weights.  Rational
+(NURBS) test and trial functions were tried and rejected: under weighted
+quadrature their value/derivative coupling terms make the operator lose
+coercivity on the randomly weighted patches of the benchmark (CG and BiCGSTAB
+fail from 32^3 elements up), while the B-spline space stays solvable.
 """
 import numpy as np
 
@@ -85,7 +81,7 @@ class WQOracle:
         self.n = [self.p[d] + self.nel[d] for d in range(3)]
         self.rules = [wq_rules.wq_rule(self.p[d], self.nel[d]) for d in range(3)]
         nu_, nv_, nw_ = self.n
-        self.w = patch["weights"].reshape(nw_, nv_, nu_)
+        self.w = patch["weights"].reshape(nw_, nv_, nu_)   # geometry weights
         X = patch["cps"].reshape(3, nw_, nv_, nu_)
         self.mask = free_mask(patch, clamp_faces).reshape(3, nw_, nv_, nu_)
         self.ndof = 3 * nu_ * nv_ * nw_
@@ -126,73 +122,46 @@ class WQOracle:
         P = np.zeros(Jq.shape[:-2] + (9, 9))
         for c in range(3):
             P[..., 3 * c:3 * c + 3, 3 * c:3 * c + 3] = invJ
-        S = P @ MDM @ np.swapaxes(P, -1, -2) * np.abs(self.detJ)[..., None, None]
-        self.Shat = S / (W ** 2)[..., None, None]  # (..., 9, 9)
-        self.g = np.moveaxis(gW / W, 0, -1)         # (..., 3)
+        self.S = P @ MDM @ np.swapaxes(P, -1, -2) * np.abs(self.detJ)[..., None, None]
         self.W = W
         self.x = x
 
     # ------------------------------------------------------------ operator
-    def _H(self, F, i):
-        """The 16 point fields H^{kappa,lambda}_i, keyed (kappa, lambda)."""
-        Sh, g = self.Shat, self.g
-        H = {}
-        for k in (1, 2, 3):
-            for l in (1, 2, 3):
-                H[k, l] = sum(Sh[..., 3 * i + k - 1, 3 * j + l - 1] * F[l][j]
-                              for j in range(3))
-            A = [sum(Sh[..., 3 * i + k - 1, 3 * j + l - 1] * g[..., l - 1]
-                     for l in (1, 2, 3)) for j in range(3)]
-            H[k, 0] = -sum(A[j] * F[0][j] for j in range(3))
-        for lam in range(4):
-            H[0, lam] = -sum(g[..., k - 1] * H[k, lam] for k in (1, 2, 3))
-        return H
-
     def apply(self, u):
         u = np.asarray(u, dtype=np.float64).reshape(self.mask.shape) * self.mask
-        v = [self.w * u[j] for j in range(3)]
-        F = [[self.fwd(v[j], lam) for j in range(3)] for lam in range(4)]
+        F = [[self.fwd(u[j], l) for j in range(3)] for l in (1, 2, 3)]
+        S = self.S
         out = np.zeros_like(u)
         for i in range(3):
-            H = self._H(F, i)
             acc = 0.0
-            for (kap, lam), h in H.items():
-                acc = acc + self.bwd(h, kap, lam)
-            out[i] = self.w * acc
+            for k in (1, 2, 3):
+                for l in (1, 2, 3):
+                    h = sum(S[..., 3 * i + k - 1, 3 * j + l - 1] * F[l - 1][j]
+                            for j in range(3))
+                    acc = acc + self.bwd(h, k, l)
+            out[i] = acc
         return (out * self.mask).ravel()
 
     def diag(self):
-        Sh, g = self.Shat, self.g
+        S = self.S
         out = np.zeros(self.mask.shape)
         for i in range(3):
             acc = 0.0
-            for kap in range(4):
-                for lam in range(4):
-                    if kap and lam:
-                        C = Sh[..., 3 * i + kap - 1, 3 * i + lam - 1]
-                    elif kap:
-                        C = -sum(Sh[..., 3 * i + kap - 1, 3 * i + l - 1] * g[..., l - 1]
-                                 for l in (1, 2, 3))
-                    elif lam:
-                        C = -sum(g[..., k - 1] * Sh[..., 3 * i + k - 1, 3 * i + lam - 1]
-                                 for k in (1, 2, 3))
-                    else:
-                        C = sum(g[..., k - 1] * Sh[..., 3 * i + k - 1, 3 * i + l - 1] * g[..., l - 1]
-                                for k in (1, 2, 3) for l in (1, 2, 3))
-                    mats = [self._W(d, kap == d + 1, lam == d + 1) *
-                            self._B(d, lam == d + 1) for d in range(3)]
-                    acc = acc + _bwd(C, *mats)
-            out[i] = self.w ** 2 * acc
+            for k in (1, 2, 3):
+                for l in (1, 2, 3):
+                    mats = [self._W(d, k == d + 1, l == d + 1) *
+                            self._B(d, l == d + 1) for d in range(3)]
+                    acc = acc + _bwd(S[..., 3 * i + k - 1, 3 * i + l - 1], *mats)
+            out[i] = acc
         out = np.where(self.mask > 0, out, 1.0)
         return out.ravel()
 
     def body_force(self, f):
         """Load vector of a constant force density f (wq_get_force_3d,
-        wq_assembly.f90:1193-1251, with the rational test functions)."""
+        wq_assembly.f90:1193-1251)."""
         out = np.zeros(self.mask.shape)
         for i in range(3):
-            h = f[i] * np.abs(self.detJ) / self.W
-            out[i] = self.w * self.bwd(h, 0, 0)
+            out[i] = self.bwd(f[i] * np.abs(self.detJ), 0, 0)
         return (out * self.mask).ravel()
 
     def matrix(self):

@@ -19,6 +19,14 @@ CASES = [
     ((9, 8, 6), (3, 2, 4), 0.15, (0.9, 1.1), {"u0": (0,), "v1": (1, 2)}),
     ((5, 11, 3), (4, 3, 2), 0.1, (0.8, 1.2), {"w0": (0, 1, 2), "w1": (2,)}),
 ]
+# One degree in all directions (2..5) runs the streaming apply kernel: cases
+# with several (u, v) tiles and element ranges.
+STREAM_CASES = [
+    ((17, 12, 6), (3, 3, 3), 0.2, (0.8, 1.2), {"w0": (0, 1, 2)}),
+    ((20, 9, 5), (2, 2, 2), 0.1, (0.9, 1.1), {"w1": (0, 1, 2)}),
+    ((12, 11, 5), (4, 4, 4), 0.15, (0.8, 1.2), {"u0": (0,), "v1": (1, 2)}),
+    ((6, 18, 9), (5, 5, 5), 0.1, None, None),
+]
 
 
 def _rel(a, b):
@@ -74,7 +82,7 @@ def _pair(case, E=1.0, nu=0.3, seed=7):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("case", CASES)
+@pytest.mark.parametrize("case", CASES + STREAM_CASES)
 def test_gpu_apply_diag_force_match_oracle(cuda_ok, case):
     op, ref = _pair(case)
     rng = np.random.default_rng(11)

@@ -128,6 +128,11 @@ def ptr(a):
     return a.data_ptr()
 
 
+# cudaStreamLegacy: the handle of the legacy default stream (a NULL stream
+# argument to yeti_ctx_set_stream selects the context's own stream instead).
+CUDA_STREAM_LEGACY = 0x1
+
+
 class Context:
     """A yeti_ctx on one CUDA device (owns a stream unless one is set)."""
 
@@ -143,6 +148,8 @@ class Context:
         raw = None
         if stream is not None:
             raw = getattr(stream, "cuda_stream", stream)
+            if not raw:
+                raw = CUDA_STREAM_LEGACY   # torch's default stream has handle 0
         check(lib().yeti_ctx_set_stream(self.handle, raw), "yeti_ctx_set_stream")
 
     def synchronize(self):

@@ -566,7 +566,9 @@ YETI_API int yeti_grad_lin_elast_work(yeti_ctx *ctx, const yeti_u1_model *m,
     }
     int smem_optin = 0;
     YETI_CUDA(cudaDeviceGetAttribute(&smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, ctx->device));
-    YETI_CUDA(cudaFuncSetAttribute(k_u1_grad, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_optin));
+    cudaFuncAttributes fattr;
+    YETI_CUDA(cudaFuncGetAttributes(&fattr, k_u1_grad));
+    smem_optin -= (int)fattr.sharedSizeBytes;   // the kernel's static shared memory
     std::vector<std::unique_ptr<DevBuf>> keep;
     auto newbuf = [&keep]() -> DevBuf & {
         keep.emplace_back(new DevBuf());
@@ -670,6 +672,7 @@ YETI_API int yeti_grad_lin_elast_work(yeti_ctx *ctx, const yeti_u1_model *m,
         const size_t smem = sizeof(double) * ((size_t)(6 + 3 * nadj) * P.nn + P.nn + std::max(vol, face));
         YETI_CHECK(smem <= (size_t)smem_optin, YETI_EUNSUPPORTED,
                    "shape gradient: element needs %zu bytes of shared memory", smem);
+        YETI_CUDA(cudaFuncSetAttribute(k_u1_grad, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         k_u1_grad<<<(unsigned)elems.size(), 256, smem, s>>>(g);
         count_launches(1);
         YETI_CUDA(cudaGetLastError());

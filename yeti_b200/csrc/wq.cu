@@ -8,16 +8,18 @@
 //     (mf_wq_solver.f90:6-164, tensor_algebra.f90:1484-1596) -> k_wq_diag
 //   wq_get_force_3d (wq_assembly.f90:1193-1251)           -> k_wq_force
 //   wq_mf_cg_3d 'WP' (mf_wq_solver.f90:764-802)           -> yeti_wq_pcg
-// generalised from the scalar operator to 3x3 elastic blocks and to rational
-// (NURBS) patches; the math is stated in oracle/wq_ops.py and DESIGN.md.
+// generalised from the scalar operator to 3x3 elastic blocks, with B-spline
+// test and trial functions on the exact NURBS geometry (the Jacobian uses
+// the control-point weights); the math is stated in oracle/wq_ops.py.
 //
 // Kernel design (one CTA per element block, all stages in shared memory):
 //   load    the block's dense 1-D tiles (functions x owned points) for the
 //           three directions and the block's control-point values;
 //   forward sum factorisation w -> v -> u: 4 trial kinds (value, d/du,
 //           d/dv, d/dw) per component at the block's points;
-//   point   per component i, the 16 channels H^{kappa,lambda}_i from the
-//           streamed 48 coefficients (the HBM stream of the operator);
+//   point   per component i, the channels H^{kappa,lambda}_i from the
+//           streamed 45 coefficients (the HBM stream of the operator);
+//           the value channels (kappa or lambda = 0) are zero;
 //   backward sum factorisation u -> v -> w with the 1-D weights
 //           W^{[d==kappa][d==lambda]}, channels merged as soon as their
 //           remaining weights coincide (16 -> 9 -> 4 -> 1);
@@ -270,11 +272,11 @@ __device__ inline void copy_tiles(const WQAxis *ax, const T *const *tiles,
 struct SetupArgs {
     WQView<double> v;          // tiles64 + axes (coef unused)
     const double *cps;         // (3, ncp)
-    const double *wts;         // ncp
+    const double *wts;         // ncp: geometry weights
     double mdm[81];
     double *coef64;            // may be null
     float *coef32;             // may be null
-    double *jw;                // |detJ| / W
+    double *jw;                // |detJ|
     int *flags;                // bit0: detJ > 0 seen, bit1: < 0, bit2: bad
 };
 
@@ -335,9 +337,9 @@ __global__ void __launch_bounds__(kWQThreads) k_wq_setup(SetupArgs a) {
         iJ[2][0] = (J[1][0] * J[2][1] - J[1][1] * J[2][0]) * id;
         iJ[2][1] = (J[0][1] * J[2][0] - J[0][0] * J[2][1]) * id;
         iJ[2][2] = (J[0][0] * J[1][1] - J[0][1] * J[1][0]) * id;
-        const double scale = fabs(det) / (W * W);
+        const double scale = fabs(det);
         const int64_t base = c.qoff * kWQCoef;
-        // S^[(i,k),(j,l)] = sum_{d,f} iJ[k][d] MDM[(i,d),(j,f)] iJ[l][f] |det| / W^2
+        // S[(i,k),(j,l)] = sum_{d,f} iJ[k][d] MDM[(i,d),(j,f)] iJ[l][f] |det|
         for (int I = 0; I < 9; I++) {
             const int i = I / 3, k = I % 3;
             for (int Jn = I; Jn < 9; Jn++) {
@@ -354,12 +356,7 @@ __global__ void __launch_bounds__(kWQThreads) k_wq_setup(SetupArgs a) {
                 if (a.coef32) a.coef32[base + (int64_t)e * nqb + q] = (float)s;
             }
         }
-        for (int l = 0; l < 3; l++) {
-            const double g = f[l + 1][3] / W;
-            if (a.coef64) a.coef64[base + (int64_t)(45 + l) * nqb + q] = g;
-            if (a.coef32) a.coef32[base + (int64_t)(45 + l) * nqb + q] = (float)g;
-        }
-        a.jw[c.qoff + q] = fabs(det) / W;
+        a.jw[c.qoff + q] = fabs(det);
     }
     if (flags) atomicOr(a.flags, flags);
 }
@@ -373,34 +370,27 @@ struct ApplyArgs {
     const int *done;   // optional early-exit flag (PCG)
 };
 
-// Pointwise map of component i: 16 channels from the 12 trial values.
+// Pointwise map of component i: the 16 channels from the 9 derivative
+// trial values (value channels are zero).
 template <class T>
 __device__ __forceinline__ void point_channels(const T *coef, int64_t base,
                                                int nqb, int q, int i,
                                                const T *F, T *H) {
-    T f[4][3];
-    for (int l = 0; l < 4; l++)
-        for (int j = 0; j < 3; j++) f[l][j] = F[(l * 3 + j) * nqb + q];
-    T g[3];
-    for (int l = 0; l < 3; l++) g[l] = coef[base + (int64_t)(45 + l) * nqb + q];
+    T f[3][3];
+    for (int l = 0; l < 3; l++)
+        for (int j = 0; j < 3; j++) f[l][j] = F[((l + 1) * 3 + j) * nqb + q];
     T h[16];
+    for (int ch = 0; ch < 4; ch++) h[ch] = 0;
     for (int k = 0; k < 3; k++) {
         T S[9];
         for (int Jn = 0; Jn < 9; Jn++) S[Jn] = coef[base + (int64_t)sym9(3 * i + k, Jn) * nqb + q];
-        T h0 = 0;
+        h[(k + 1) * 4] = 0;
         for (int l = 0; l < 3; l++) {
             T acc = 0;
-            for (int j = 0; j < 3; j++) acc += S[3 * j + l] * f[l + 1][j];
+            for (int j = 0; j < 3; j++) acc += S[3 * j + l] * f[l][j];
             h[(k + 1) * 4 + (l + 1)] = acc;
         }
-        for (int j = 0; j < 3; j++) {
-            T a = S[3 * j] * g[0] + S[3 * j + 1] * g[1] + S[3 * j + 2] * g[2];
-            h0 -= a * f[0][j];
-        }
-        h[(k + 1) * 4] = h0;
     }
-    for (int lam = 0; lam < 4; lam++)
-        h[lam] = -(g[0] * h[4 + lam] + g[1] * h[8 + lam] + g[2] * h[12 + lam]);
     for (int ch = 0; ch < 16; ch++) H[ch * nqb + q] = h[ch];
 }
 
@@ -425,9 +415,8 @@ __global__ void __launch_bounds__(kWQThreads) k_wq_apply(ApplyArgs<T> a) {
         const int fu = o % nfu, fv = (o / nfu) % nfv, fw = o / (nfu * nfv);
         const int gu = c.b[0].e0 + fu, gv = c.b[1].e0 + fv, gw = c.b[2].e0 + fw;
         const int64_t cp = gu + (int64_t)ax[0].nfun * (gv + (int64_t)ax[1].nfun * gw);
-        const T w = a.v.wcp[cp];
         for (int cc = 0; cc < 3; cc++)
-            X[cc * nx + o] = clamped(a.v.cmask[cc], ax, gu, gv, gw) ? T(0) : w * a.u[cc * a.v.ncp + cp];
+            X[cc * nx + o] = clamped(a.v.cmask[cc], ax, gu, gv, gw) ? T(0) : a.u[cc * a.v.ncp + cp];
     }
     __syncthreads();
     T *F = sm + P.F;
@@ -452,15 +441,15 @@ __global__ void __launch_bounds__(kWQThreads) k_wq_apply(ApplyArgs<T> a) {
             const int gu = c.b[0].e0 + fu, gv = c.b[1].e0 + fv, gw = c.b[2].e0 + fw;
             if (clamped(a.v.cmask[i], ax, gu, gv, gw)) continue;
             const int64_t cp = gu + (int64_t)ax[0].nfun * (gv + (int64_t)ax[1].nfun * gw);
-            atomicAdd(&a.Ku[i * a.v.ncp + cp], a.v.wcp[cp] * out[o]);
+            atomicAdd(&a.Ku[i * a.v.ncp + cp], out[o]);
         }
         __syncthreads();
     }
 }
 
 // ------------------------------------------------------------------- diag
-// diag_(a,i) = w_a^2 sum_{kappa,lambda} sum_q (W^{kappa,lambda} .* B^lambda)_a(q)
-//              C^{kappa,lambda}_ii(q)
+// diag_(a,i) = sum_{kappa,lambda >= 1} sum_q (W^{kappa,lambda} .* B^lambda)_a(q)
+//              S[(i,kappa),(i,lambda)](q)
 template <class T>
 struct DiagArgs {
     WQView<T> v;
@@ -493,22 +482,11 @@ __global__ void __launch_bounds__(kWQThreads) k_wq_diag(DiagArgs<T> a) {
     const T *coef = a.v.coef;
     for (int i = 0; i < 3; i++) {
         for (int q = threadIdx.x; q < nqb; q += blockDim.x) {
-            T g[3], S[3][3];
-            for (int l = 0; l < 3; l++) g[l] = coef[base + (int64_t)(45 + l) * nqb + q];
-            for (int k = 0; k < 3; k++)
-                for (int l = 0; l < 3; l++)
-                    S[k][l] = coef[base + (int64_t)sym9(3 * i + k, 3 * i + l) * nqb + q];
             for (int kap = 0; kap < 4; kap++)
-                for (int lam = 0; lam < 4; lam++) {
-                    T C = 0;
-                    if (kap && lam) C = S[kap - 1][lam - 1];
-                    else if (kap) for (int l = 0; l < 3; l++) C -= S[kap - 1][l] * g[l];
-                    else if (lam) for (int k = 0; k < 3; k++) C -= g[k] * S[k][lam - 1];
-                    else
-                        for (int k = 0; k < 3; k++)
-                            for (int l = 0; l < 3; l++) C += g[k] * S[k][l] * g[l];
-                    H[(kap * 4 + lam) * nqb + q] = C;
-                }
+                for (int lam = 0; lam < 4; lam++)
+                    H[(kap * 4 + lam) * nqb + q] =
+                        (kap && lam) ? coef[base + (int64_t)sym9(3 * i + kap - 1, 3 * i + lam - 1) * nqb + q]
+                                     : T(0);
         }
         __syncthreads();
         backward<T>(sm + P.tile[0], sm + P.tile[1], sm + P.tile[2], 2, NF, NQ, c,
@@ -517,8 +495,7 @@ __global__ void __launch_bounds__(kWQThreads) k_wq_diag(DiagArgs<T> a) {
             const int fu = o % nfu, fv = (o / nfu) % nfv, fw = o / (nfu * nfv);
             const int gu = c.b[0].e0 + fu, gv = c.b[1].e0 + fv, gw = c.b[2].e0 + fw;
             const int64_t cp = gu + (int64_t)ax[0].nfun * (gv + (int64_t)ax[1].nfun * gw);
-            const double w = (double)a.v.wcp[cp];
-            atomicAdd(&a.diag[i * a.v.ncp + cp], w * w * (double)out[o]);
+            atomicAdd(&a.diag[i * a.v.ncp + cp], (double)out[o]);
         }
         __syncthreads();
     }
@@ -565,7 +542,7 @@ __global__ void __launch_bounds__(kWQThreads) k_wq_force(ForceArgs a) {
             const int gu = c.b[0].e0 + fu, gv = c.b[1].e0 + fv, gw = c.b[2].e0 + fw;
             if (clamped(a.v.cmask[i], ax, gu, gv, gw)) continue;
             const int64_t cp = gu + (int64_t)ax[0].nfun * (gv + (int64_t)ax[1].nfun * gw);
-            atomicAdd(&a.F[i * a.v.ncp + cp], a.v.wcp[cp] * out[o]);
+            atomicAdd(&a.F[i * a.v.ncp + cp], out[o]);
         }
         __syncthreads();
     }
@@ -621,7 +598,7 @@ static void build_tiles(const WQRule1D &R, const std::vector<BlkInfo> &blk,
 
 template <class T>
 static WQView<T> make_view(const yeti_wq_op *op, const DevBuf *tiles,
-                           const DevBuf &coef, const DevBuf &w) {
+                           const DevBuf &coef) {
     WQView<T> v;
     for (int d = 0; d < 3; d++) {
         v.ax[d].p = op->p[d];
@@ -636,7 +613,6 @@ static WQView<T> make_view(const yeti_wq_op *op, const DevBuf *tiles,
     }
     v.qoff = op->qoff.as<int64_t>();
     v.coef = coef.as<T>();
-    v.wcp = w.as<T>();
     v.ncp = op->ncp;
     return v;
 }
@@ -659,8 +635,7 @@ static int launch_apply(yeti_wq_op *op, const T *u, T *Ku, const int *done,
                         cudaStream_t s) {
     const bool f64 = sizeof(T) == 8;
     ApplyArgs<T> a;
-    a.v = make_view<T>(op, f64 ? op->tiles64 : op->tiles32, f64 ? op->coef64 : op->coef32,
-                       f64 ? op->w64 : op->w32);
+    a.v = make_view<T>(op, f64 ? op->tiles64 : op->tiles32, f64 ? op->coef64 : op->coef32);
     a.u = u;
     a.Ku = Ku;
     a.done = done;
@@ -675,6 +650,11 @@ static int launch_apply(yeti_wq_op *op, const T *u, T *Ku, const int *done,
 
 int wq_apply_dev(yeti_wq_op *op, const void *u, void *Ku, int prec,
                  const int *done, cudaStream_t s) {
+    if (op->st.active) {
+        if (prec == YETI_PREC_F64)
+            return wq_stream_apply<double>(op, (const double *)u, (double *)Ku, done, s);
+        return wq_stream_apply<float>(op, (const float *)u, (float *)Ku, done, s);
+    }
     if (prec == YETI_PREC_F64)
         return launch_apply<double>(op, (const double *)u, (double *)Ku, done, s);
     return launch_apply<float>(op, (const float *)u, (float *)Ku, done, s);
@@ -707,7 +687,7 @@ YETI_API int yeti_wq_setup(yeti_ctx *ctx, const int32_t p[3],
     const int QB[3] = {8, 8, 4};
     int64_t ncp = 1;
     for (int d = 0; d < 3; d++) {
-        YETI_CHECK(p[d] >= 1 && p[d] <= 8 && nel[d] >= 2 && nel[d] <= 100000,
+        YETI_CHECK(p[d] >= 2 && p[d] <= 8 && nel[d] >= 2 && nel[d] <= 100000,
                    YETI_EINVAL, "yeti_wq_setup: p[%d]=%d nel[%d]=%d", d, p[d], d,
                    nel[d]);
         op->p[d] = p[d];
@@ -778,11 +758,7 @@ YETI_API int yeti_wq_setup(yeti_ctx *ctx, const int32_t p[3],
     // geometry -> coefficients
     DevBuf dcps, dw, flags;
     YETI_TRY(upload(ctx, dcps, cps, (size_t)3 * ncp));
-    YETI_TRY(upload(ctx, op->w64, weights, (size_t)ncp));
-    {
-        std::vector<float> wf(weights, weights + ncp);
-        YETI_TRY(upload(ctx, op->w32, wf.data(), wf.size()));
-    }
+    YETI_TRY(upload(ctx, dw, weights, (size_t)ncp));
     const int64_t ncoef = op->nqp_total * kWQCoef;
     if (prec_mask & YETI_WQ_F64) YETI_TRY(op->coef64.alloc(ctx, ncoef * sizeof(double)));
     if (prec_mask & YETI_WQ_F32) YETI_TRY(op->coef32.alloc(ctx, ncoef * sizeof(float)));
@@ -790,9 +766,9 @@ YETI_API int yeti_wq_setup(yeti_ctx *ctx, const int32_t p[3],
     YETI_TRY(flags.alloc(ctx, sizeof(int)));
     YETI_CUDA(cudaMemsetAsync(flags.ptr, 0, sizeof(int), ctx->stream));
     SetupArgs sa;
-    sa.v = make_view<double>(op.get(), op->tiles64, op->coef64, op->w64);
+    sa.v = make_view<double>(op.get(), op->tiles64, op->coef64);
     sa.cps = dcps.as<double>();
-    sa.wts = op->w64.as<double>();
+    sa.wts = dw.as<double>();
     {
         // MDM = MM^T DD MM (wq_assembly.f90:92-109)
         const double lam = (E * nu) / ((1.0 + nu) * (1.0 - 2.0 * nu));
@@ -839,7 +815,7 @@ YETI_API int yeti_wq_setup(yeti_ctx *ctx, const int32_t p[3],
         YETI_TRY(wq_smem_limit(ctx, smem));
         if (prec_mask & YETI_WQ_F64) {
             DiagArgs<double> da;
-            da.v = make_view<double>(op.get(), op->tiles64, op->coef64, op->w64);
+            da.v = make_view<double>(op.get(), op->tiles64, op->coef64);
             for (int d = 0; d < 3; d++) da.dtiles[d] = op->dtiles[d].as<double>();
             da.diag = op->diag.as<double>();
             YETI_CUDA(cudaFuncSetAttribute(k_wq_diag<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
@@ -856,7 +832,7 @@ YETI_API int yeti_wq_setup(yeti_ctx *ctx, const int32_t p[3],
                 YETI_TRY(upload(ctx, dt[d], t4f[d].data(), t4f[d].size()));
             }
             DiagArgs<float> da;
-            da.v = make_view<float>(op.get(), op->tiles32, op->coef32, op->w32);
+            da.v = make_view<float>(op.get(), op->tiles32, op->coef32);
             for (int d = 0; d < 3; d++) da.dtiles[d] = dt[d].as<float>();
             da.diag = op->diag.as<double>();
             YETI_CUDA(cudaFuncSetAttribute(k_wq_diag<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
@@ -867,6 +843,11 @@ YETI_API int yeti_wq_setup(yeti_ctx *ctx, const int32_t p[3],
         YETI_CUDA(cudaGetLastError());
     }
     YETI_CUDA(cudaStreamSynchronize(ctx->stream));
+    // the streaming apply (degrees 2..5) takes the coefficients in its own layout
+    if (wq_stream_supported(op.get())) {
+        YETI_TRY(wq_stream_setup(op.get(), R));
+        YETI_TRY(wq_stream_permute(op.get()));
+    }
     op->setup_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
     op->bytes_data = (op->coef64.bytes + op->coef32.bytes);
     *out = op.release();
@@ -964,7 +945,7 @@ YETI_API int yeti_wq_body_force(yeti_wq_op *op, const double f[3], double *F,
     }
     YETI_CUDA(cudaMemsetAsync(FF, 0, op->ndof * sizeof(double), s));
     ForceArgs a;
-    a.v = make_view<double>(op, op->tiles64, op->coef64, op->w64);
+    a.v = make_view<double>(op, op->tiles64, op->coef64);
     a.jw = op->jw.as<double>();
     for (int d = 0; d < 3; d++) a.f[d] = f[d];
     a.F = FF;

@@ -10,8 +10,8 @@
 // stored block by block, entry-major inside a block:
 //     coef[(qoff[b] * 48) + e * nq_b + local_point]
 // so one CTA streams one contiguous chunk and consecutive threads read
-// consecutive addresses.  The 48 entries are the upper triangle of the
-// symmetric 9x9 S^ = S / W^2 (45, row-major, index sym9) and g = grad W / W.
+// consecutive addresses.  The 45 entries are the upper triangle of the
+// symmetric 9x9 coefficient S (row-major, index sym9).
 // Vectors are component-major [c][iw][iv][iu].
 #pragma once
 #include <vector>
@@ -21,7 +21,7 @@
 
 namespace yeti {
 
-constexpr int kWQCoef = 48;
+constexpr int kWQCoef = 45;
 constexpr int kWQThreads = 256;
 
 __host__ __device__ constexpr int sym9(int I, int J) {
@@ -48,8 +48,7 @@ struct WQView {
     WQAxis ax[3];
     const T *tiles[3];      // [nb][6][NF][NQ]: B0 B1 W00 W01 W10 W11
     const int64_t *qoff;    // first point (block-tiled numbering) of a block
-    const T *coef;          // [nqp_total * 48] block-tiled, entry-major
-    const T *wcp;           // CP weights (ncp)
+    const T *coef;          // [nqp_total * 45] block-tiled, entry-major
     int cmask[3];           // clamped faces per component (bit f)
     int64_t ncp;
 };
@@ -58,6 +57,29 @@ struct WQView {
 
 struct yeti_wq_op;
 namespace yeti {
+
+// Tables of the streaming apply kernel (degrees 2..5, wq_stream.cu); index
+// [0] / [1] of grid, smem, seg: FP64 / FP32 kernel.
+struct WQStreamPlan {
+    bool active = false;     // coefficients are in the streaming layout
+    int ntile[2] = {0, 0};   // (u, v) tiles
+    int grid[2] = {0, 0};
+    int per_sm[2] = {0, 0};
+    size_t smem[2] = {0, 0};
+    int64_t ncoef = 0;
+    DevBuf elem[3], band64[3], band32[3], wq0, tq0[2], tnq[2];
+    DevBuf tile_off, tile_pstride, seg[2], cta_seg[2];
+};
+
+bool wq_stream_supported(const yeti_wq_op *op);
+// Build the tile tables and work segments (after the 1-D rules).
+int wq_stream_setup(yeti_wq_op *op, const WQRule1D R[3]);
+// Move coef64 / coef32 from the element-block layout into the streaming
+// layout (after every kernel that reads the element-block layout).
+int wq_stream_permute(yeti_wq_op *op);
+template <class T>
+int wq_stream_apply(yeti_wq_op *op, const T *u, T *Ku, const int *done, cudaStream_t s);
+
 // Enqueue Ku += K u (Ku must be zeroed by the caller) on stream s; prec
 // YETI_PREC_F64 / F32 selects the operator data and the vector type.  done:
 // optional device flag, the kernel returns at once when it is set.
@@ -80,11 +102,11 @@ struct yeti_wq_op {
     yeti::DevBuf tiles64[3], tiles32[3], dtiles[3];
     yeti::DevBuf qoff;
     yeti::DevBuf coef64, coef32;
-    yeti::DevBuf w64, w32;
-    yeti::DevBuf jw;        // |detJ| / W per point (FP64, block-tiled)
+    yeti::DevBuf jw;        // |detJ| per point (FP64, block-tiled)
     yeti::DevBuf diag;      // diagonal (FP64, clamped dofs = 1)
     yeti::DevBuf dinv64, dinv32;
     yeti::DevBuf ws64, ws32, scal, parts;   // PCG workspaces
+    yeti::WQStreamPlan st;
     double setup_ms = 0.0;
     int64_t bytes_data = 0;
 };
