@@ -170,6 +170,18 @@ int yeti_wq_info(const yeti_wq_op *op, int64_t *ncp, int64_t *ndof,
                  int64_t *nfree, int64_t *nqp, int64_t *bytes);
 /* Ku = K u.  prec YETI_PREC_F64: u, Ku are double; YETI_PREC_F32: float. */
 int yeti_wq_apply(yeti_wq_op *op, const void *u, void *Ku, int prec, int mem);
+/* K u with HOST buffers u and Ku (as yeti_wq_apply with YETI_MEM_HOST) that
+ * allocates no device memory.  No counterpart in the reference.  For callers
+ * that cannot allocate device memory at this point -- a process whose device
+ * memory is all reserved by another allocator, or a latency-critical loop that
+ * must not pay cudaMalloc/cudaFree's implicit synchronisation -- the two
+ * vectors are staged in one file-scope device array of at most 2,097,152 dofs
+ * per vector (32 MiB, held by every GPU that loads the library until exit);
+ * larger operators return YETI_EINVAL.  The first call on a device looks the
+ * array's device address up (cudaGetSymbolAddress); make that first call
+ * before any stream capture.  All calls share the array: calls that overlap on
+ * the GPU race. */
+int yeti_wq_apply_static(yeti_wq_op *op, const void *u, void *Ku, int prec);
 /* Diagonal of K (3*ncp doubles; clamped dofs hold 1). */
 int yeti_wq_diag(yeti_wq_op *op, double *d, int mem);
 /* Body-force load vector for a constant force density f[3]
