@@ -26,6 +26,7 @@ STREAM_CASES = [
     ((20, 9, 5), (2, 2, 2), 0.1, (0.9, 1.1), {"w1": (0, 1, 2)}),
     ((12, 11, 5), (4, 4, 4), 0.15, (0.8, 1.2), {"u0": (0,), "v1": (1, 2)}),
     ((6, 18, 9), (5, 5, 5), 0.1, None, None),
+    ((10, 24, 4), (3, 3, 3), 0.2, (0.8, 1.2), {"v0": (0, 1, 2)}),
 ]
 
 

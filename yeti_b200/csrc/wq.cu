@@ -899,6 +899,7 @@ YETI_API int yeti_wq_apply(yeti_wq_op *op, const void *u, void *Ku, int prec,
     if (mem == YETI_MEM_HOST) {
         YETI_CUDA(cudaMemcpyAsync(Ku, kk, nb, cudaMemcpyDeviceToHost, s));
         YETI_CUDA(cudaStreamSynchronize(s));
+        YETI_TRY(wq_stream_check(op));
     }
     return YETI_OK;
 }

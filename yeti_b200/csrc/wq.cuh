@@ -67,8 +67,9 @@ struct WQStreamPlan {
     int per_sm[2] = {0, 0};
     size_t smem[2] = {0, 0};
     int64_t ncoef = 0;
-    DevBuf elem[3], band64[3], band32[3], wq0, tq0[2], tnq[2];
+    DevBuf elem[3], band64[3], band32[3], wq0, tq0[2], tnq[2], treg[2];
     DevBuf tile_off, tile_pstride, seg[2], cta_seg[2];
+    DevBuf err;              // int: a kernel's bounded wait gave up
 };
 
 bool wq_stream_supported(const yeti_wq_op *op);
@@ -79,6 +80,9 @@ int wq_stream_setup(yeti_wq_op *op, const WQRule1D R[3]);
 int wq_stream_permute(yeti_wq_op *op);
 template <class T>
 int wq_stream_apply(yeti_wq_op *op, const T *u, T *Ku, const int *done, cudaStream_t s);
+// YETI_ETIMEDOUT (and clears the flag) if a streaming kernel reported a
+// bounded wait that gave up since the last check; synchronises the stream.
+int wq_stream_check(yeti_wq_op *op);
 
 // Enqueue Ku += K u (Ku must be zeroed by the caller) on stream s; prec
 // YETI_PREC_F64 / F32 selects the operator data and the vector type.  done:

@@ -768,6 +768,7 @@ YETI_API int yeti_wq_pcg(yeti_wq_op *op, const double *b, double *x,
     const cudaMemcpyKind d2h = mem == YETI_MEM_HOST ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice;
     YETI_CUDA(cudaMemcpyAsync(x, dx, n * sizeof(double), d2h, s));
     YETI_CUDA(cudaStreamSynchronize(s));
+    YETI_TRY(wq_stream_check(op));
     const double rel = bb > 0 ? std::sqrt(rr / bb) : 0.0;
     if (status == YETI_OK && !(rel <= rtol)) status = YETI_ENOTCONV;
     if (stats) {

@@ -9,28 +9,35 @@
 // marches through the w point planes of that range.  Every WQ point belongs
 // to one element and, in each direction, its B0/B1/W** rows are non-zero for
 // the p+1 functions elem(q)..elem(q)+p only (checked on the host), so every
-// 1-D contraction is a band of width p+1:
+// 1-D contraction is a band of width p+1.  Per plane:
 //
 //   A  forward w : Y_t[c][fv][fu] = sum_m Bt_w(qw,m) X[c][fv][fu][e+m]
 //                  (one thread per (c, fv, fu) column; X for functions
 //                  e..e+p lives in a register ring that advances with e)
-//   B  forward v : Z_s[c][qv][fu]  (s: B0v.Y0, B1v.Y0, B0v.Y1)
-//   C1 forward u : F[l][j][qv][qu] = d u_j / d xi_l   (one thread per row,
-//                  register ring of p+1 Z values along u)
-//   C2 point     : h[i][k][l] = sum_j S[(i,k),(j,l)] F[l][j] with the 45
-//                  streamed coefficients of the point (the HBM stream)
-//   C3 backward u: G[i][k][l][qv][fu] with weights W^{[k==u][l==u]}
-//                  (one thread per (row, i, k), rings along u)
-//   D  backward v: K[i][k][lw][fv][fu], channels merged on (l == w)
+//   -- barrier --
+//   each warp owns two point rows qv of the tile and runs, with warp
+//   synchronisation only:
+//   B  forward v : Z_s[c][row][fu]  (s: B0v.Y0, B1v.Y0, B0v.Y1)
+//   C  forward u + pointwise, one lane per point: F[l][j] = d u_j / d xi_l,
+//                  then h[i][k][l] = sum_j S[(i,k),(j,l)] F[l][j] with the
+//                  45 streamed coefficients of the point (the HBM stream)
+//   G  backward u: one lane per (row, channel (i,k,l)) walks the row,
+//                  weights W^{[k==u][l==u]}
+//   -- barrier --
+//   D  backward v: one thread per (i, k, fu) walks the column over the tile's
+//                  rows; channels merged on (l == w): K[i][k][fv][fu][lw]
+//   -- barrier --
 //   E  backward w: accumulation into a register ring of output planes
 //                  e..e+p; plane e is complete after element e and is added
 //                  to Ku (atomics: tiles overlap on the p halo functions,
 //                  element ranges overlap on p planes)
 //
-// Shared memory holds one plane's intermediates in two regions whose
-// lifetimes alternate (R1: Y, F, G; R2: Z, h, K), so every stage reads one
-// region and writes the other.  While a plane is processed, the next plane's
-// coefficient block (contiguous, 256-byte aligned) is prefetched into L2.
+// The walks keep the p+1 functions of the current element in registers.  In
+// a regular tile (every element owns two points: all but the first and last
+// element of a direction) the walk is unrolled at compile time and the ring
+// is register renaming; the first and last tiles take a run-time walk.
+// While a plane is processed, the next plane's coefficient block
+// (contiguous, 256-byte aligned) is prefetched into L2.
 #include <algorithm>
 #include <numeric>
 
@@ -41,29 +48,48 @@ namespace yeti {
 namespace {
 
 constexpr int kTQ = 16;          // max points of a tile per direction
+constexpr int kNE = kTQ / 2;     // max elements of a regular tile
 constexpr int kThreads = 256;    // one thread per point of a plane tile
-constexpr int kQP = 17;          // padded pitch of point-indexed rows
+constexpr int kWarps = kThreads / 32;
+constexpr int kHS = 2 * kTQ + 1; // channel stride of a warp's h block
 
 constexpr int cmax(int a, int b) { return a > b ? a : b; }
+constexpr int round4(int a) { return (a + 3) / 4 * 4; }
+
+// Channel stride of a warp's G block: at least two rows of NFM, and chosen
+// so that stage D's threads ((i,k)-major, fu fastest) of consecutive (i,k)
+// fall on disjoint banks.
+constexpr int gstride(int nfm) {
+    int g = 2 * nfm;
+    while (!((3 * g) % 32 >= nfm && (3 * g) % 32 <= 32 - nfm)) g++;
+    return g;
+}
 
 template <int P>
 struct Dims {
     static constexpr int PB = P + 1;
-    static constexpr int NFM = kTQ / 2 + P;   // max functions of a tile
-    static constexpr int Y = 2 * 3 * NFM * NFM;
-    static constexpr int F = 9 * kTQ * kQP;
-    static constexpr int G = 27 * kTQ * NFM;
-    static constexpr int Z = 9 * kTQ * NFM;
-    static constexpr int H = 27 * kTQ * kQP;
-    static constexpr int K = 18 * NFM * NFM;
-    static constexpr int R1 = cmax(Y, cmax(F, G));
-    static constexpr int R2 = cmax(Z, cmax(H, K));
-    static constexpr int TAB = kTQ * 6 * PB;
+    static constexpr int PBP = round4(PB);     // padded band row
+    static constexpr int NFM = kNE + P;        // max functions of a tile
+    static constexpr int GS = gstride(NFM);
+    static constexpr int Y = round4(2 * 3 * NFM * NFM);
+    static constexpr int ZHP = round4(cmax(9 * 2 * NFM, 27 * kHS));   // Z, then h
+    static constexpr int GP = round4(27 * GS);                        // G
+    static constexpr int K = 9 * NFM * NFM * 2;                       // aliases the Z/h parts
+    static constexpr int TAB = kTQ * 6 * PBP;
+    static constexpr int OFF_ZH = Y;
+    static constexpr int OFF_G = OFF_ZH + kWarps * ZHP;
+    static constexpr int OFF_TAB = OFF_G + kWarps * GP;
+    static constexpr int TOTAL = OFF_TAB + 2 * TAB;
     static constexpr int NCOL = 3 * NFM * NFM;
     static constexpr int CPT = (NCOL + kThreads - 1) / kThreads;
+    static constexpr int CB = kTQ * kTQ * 45;   // one plane's coefficients (staged kernels)
+    static_assert(K <= kWarps * ZHP, "K must fit in the Z/h parts");
+    // values, then the staged coefficient block (FP32), the two rel tables
+    // and the mbarrier
     template <class T>
     static constexpr size_t smem_bytes() {
-        return (size_t)(R1 + R2 + 2 * TAB) * sizeof(T) + 2 * kTQ * sizeof(int);
+        return (size_t)(TOTAL + (sizeof(T) == 4 ? CB : 0)) * sizeof(T) + 2 * kTQ * sizeof(int) +
+               sizeof(uint64_t);
     }
 };
 
@@ -71,8 +97,246 @@ __device__ __forceinline__ void prefetch_l2(const void *p) {
     asm volatile("prefetch.global.L2 [%0];" ::"l"(p));
 }
 
-__device__ __forceinline__ float ld_stream(const float *p) { return __ldcs(p); }
-__device__ __forceinline__ double ld_stream(const double *p) { return __ldcs(p); }
+// The p+1 band values of one row of a band table (rows padded to a multiple
+// of 4 values, 16-byte aligned), with vector loads.
+template <int P>
+__device__ __forceinline__ void load_band(const float *p, float (&w)[P + 1]) {
+    constexpr int NV = round4(P + 1) / 4;
+    float t[4 * NV];
+#pragma unroll
+    for (int i = 0; i < NV; i++) {
+        const float4 v = reinterpret_cast<const float4 *>(p)[i];
+        t[4 * i] = v.x;
+        t[4 * i + 1] = v.y;
+        t[4 * i + 2] = v.z;
+        t[4 * i + 3] = v.w;
+    }
+#pragma unroll
+    for (int m = 0; m <= P; m++) w[m] = t[m];
+}
+
+template <int P>
+__device__ __forceinline__ void load_band(const double *p, double (&w)[P + 1]) {
+    constexpr int NV = round4(P + 1) / 2;
+    double t[2 * NV];
+#pragma unroll
+    for (int i = 0; i < NV; i++) {
+        const double2 v = reinterpret_cast<const double2 *>(p)[i];
+        t[2 * i] = v.x;
+        t[2 * i + 1] = v.y;
+    }
+#pragma unroll
+    for (int m = 0; m <= P; m++) w[m] = t[m];
+}
+
+__device__ __forceinline__ void store_pair(float *p, float a, float b) {
+    *reinterpret_cast<float2 *>(p) = make_float2(a, b);
+}
+__device__ __forceinline__ void store_pair(double *p, double a, double b) {
+    *reinterpret_cast<double2 *>(p) = make_double2(a, b);
+}
+__device__ __forceinline__ void load_pair(const float *p, float &a, float &b) {
+    const float2 v = *reinterpret_cast<const float2 *>(p);
+    a = v.x;
+    b = v.y;
+}
+__device__ __forceinline__ void load_pair(const double *p, double &a, double &b) {
+    const double2 v = *reinterpret_cast<const double2 *>(p);
+    a = v.x;
+    b = v.y;
+}
+
+// ------------------------------------------------ bulk copies (TMA engine)
+constexpr int kWaitTries = 1 << 16;   // bound of every mbarrier wait
+
+__device__ __forceinline__ uint32_t smem_addr(const void *p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void mbar_init(uint64_t *bar) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(bar)) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+// One bulk copy global -> shared that completes the barrier's current phase.
+// dst and src 16-byte aligned, bytes a multiple of 16.
+__device__ __forceinline__ void bulk_load(void *dst, const void *src, uint32_t bytes, uint64_t *bar) {
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)),
+                 "r"(bytes)
+                 : "memory");
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+            smem_addr(dst)),
+        "l"(src), "r"(bytes), "r"(smem_addr(bar))
+        : "memory");
+}
+// Wait for the phase with the given parity, at most kWaitTries polls.
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity) {
+    for (int i = 0; i < kWaitTries; i++) {
+        uint32_t ok;
+        asm volatile(
+            "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+            " selp.u32 %0, 1, 0, p;\n}"
+            : "=r"(ok)
+            : "r"(smem_addr(bar)), "r"(parity)
+            : "memory");
+        if (ok) return true;
+    }
+    return false;
+}
+
+// ---------------------------------------------------------------- walks
+// Tile patterns of one direction (host flag): 1 every element owns two
+// points; 2 the first element owns p+1 points, the others two (the first
+// tile); 3 the last element owns p+2 points, the others two (the last tile);
+// 0 anything else (run-time walk).
+__host__ __device__ constexpr int pat_nemax(int P, int pat) {
+    return pat == 1 ? kNE : pat == 2 ? 1 + (kTQ - (P + 1)) / 2 : 1 + (kTQ - (P + 2)) / 2;
+}
+// first point of element e in a tile of pattern pat
+__host__ __device__ constexpr int pat_q0(int P, int pat, int e) {
+    return pat == 2 ? (e == 0 ? 0 : P + 1 + 2 * (e - 1)) : 2 * e;
+}
+
+// Backward u of one channel of one row: g[f] = sum_q W_kind(q, f - rel(q)) h[q],
+// walked element by element with the accumulators of the element's p+1
+// functions named at compile time.
+template <class T, int P, int PAT>
+__device__ __forceinline__ void walk_u(const T *h, T *g, const T *tab, int kind, int ne) {
+    constexpr int PBP = round4(P + 1), NEM = pat_nemax(P, PAT), NF = NEM + P;
+    T a[NF];
+#pragma unroll
+    for (int f = 0; f < NF; f++) a[f] = T(0);
+#pragma unroll
+    for (int e = 0; e < NEM; e++) {
+        if (e < ne) {
+            const int q0 = pat_q0(P, PAT, e);
+            const int np = PAT == 2 ? (e == 0 ? P + 1 : 2) : (PAT == 3 && e == ne - 1 ? P + 2 : 2);
+#pragma unroll
+            for (int pt = 0; pt < P + 2; pt++) {
+                if (pt < np) {
+                    const int q = q0 + pt;
+                    T w[P + 1];
+                    load_band<P>(tab + (q * 6 + kind) * PBP, w);
+                    const T x = h[q];
+#pragma unroll
+                    for (int m = 0; m <= P; m++) a[e + m] += w[m] * x;
+                }
+            }
+            g[e] = a[e];
+        }
+    }
+#pragma unroll
+    for (int f = 1; f < NF; f++)
+        if (f >= ne && f < ne + P) g[f] = a[f];
+}
+
+template <class T, int P>
+__device__ __forceinline__ void walk_u_generic(const T *h, T *g, const T *tab, int kind,
+                                               const int *rel, int nq) {
+    constexpr int PBP = round4(P + 1);
+    T a[P + 1];
+#pragma unroll
+    for (int m = 0; m <= P; m++) a[m] = T(0);
+    int cur = 0;
+    for (int q = 0; q < nq; q++) {
+        const int r = rel[q];
+        if (r != cur) {
+            g[cur] = a[0];
+#pragma unroll
+            for (int m = 0; m < P; m++) a[m] = a[m + 1];
+            a[P] = T(0);
+            cur = r;
+        }
+        T w[P + 1];
+        load_band<P>(tab + (q * 6 + kind) * PBP, w);
+        const T x = h[q];
+#pragma unroll
+        for (int m = 0; m <= P; m++) a[m] += w[m] * x;
+    }
+#pragma unroll
+    for (int m = 0; m <= P; m++) g[cur + m] = a[m];
+}
+
+// Backward v of the three channels (i,k,l=0..2) of one fu column, merged on
+// the w key: kp[fv] = (sum wa g0 + wb g1, sum wa g2), wa at table row ka
+// (trial l != v), wb at ka+1 (trial l == v).  G of row qv of the tile lives
+// in the block of warp qv/2: gb + (qv/2)*GP + (qv%2)*NFM + l*GS.
+template <class T, int P, int PAT>
+__device__ __forceinline__ void walk_v(const T *gb, T *kp, const T *tab, int ka, int ne) {
+    using D = Dims<P>;
+    constexpr int PBP = D::PBP, NEM = pat_nemax(P, PAT), NF = NEM + P, NFM = D::NFM;
+    constexpr int GS = D::GS, GP = D::GP;
+    T A0[NF], A1[NF];
+#pragma unroll
+    for (int f = 0; f < NF; f++) A0[f] = A1[f] = T(0);
+#pragma unroll
+    for (int e = 0; e < NEM; e++) {
+        if (e < ne) {
+            const int q0 = pat_q0(P, PAT, e);
+            const int np = PAT == 2 ? (e == 0 ? P + 1 : 2) : (PAT == 3 && e == ne - 1 ? P + 2 : 2);
+#pragma unroll
+            for (int pt = 0; pt < P + 2; pt++) {
+                if (pt < np) {
+                    const int q = q0 + pt;
+                    T wa[P + 1], wb[P + 1];
+                    load_band<P>(tab + (q * 6 + ka) * PBP, wa);
+                    load_band<P>(tab + (q * 6 + ka + 1) * PBP, wb);
+                    const T *g = gb + (q >> 1) * GP + (q & 1) * NFM;
+                    const T x0 = g[0], x1 = g[GS], x2 = g[2 * GS];
+#pragma unroll
+                    for (int m = 0; m <= P; m++) {
+                        A0[e + m] += wa[m] * x0 + wb[m] * x1;
+                        A1[e + m] += wa[m] * x2;
+                    }
+                }
+            }
+            store_pair(kp + e * (2 * NFM), A0[e], A1[e]);
+        }
+    }
+#pragma unroll
+    for (int f = 1; f < NF; f++)
+        if (f >= ne && f < ne + P) store_pair(kp + f * (2 * NFM), A0[f], A1[f]);
+}
+
+template <class T, int P>
+__device__ __forceinline__ void walk_v_generic(const T *gb, T *kp, const T *tab, int ka,
+                                               const int *rel, int nq) {
+    using D = Dims<P>;
+    constexpr int PBP = D::PBP, NFM = D::NFM, GS = D::GS, GP = D::GP;
+    T A0[P + 1], A1[P + 1];
+#pragma unroll
+    for (int m = 0; m <= P; m++) A0[m] = A1[m] = T(0);
+    int cur = 0;
+    for (int q = 0; q < nq; q++) {
+        const int r = rel[q];
+        if (r != cur) {
+            store_pair(kp + cur * (2 * NFM), A0[0], A1[0]);
+#pragma unroll
+            for (int m = 0; m < P; m++) {
+                A0[m] = A0[m + 1];
+                A1[m] = A1[m + 1];
+            }
+            A0[P] = A1[P] = T(0);
+            cur = r;
+        }
+        T wa[P + 1], wb[P + 1];
+        load_band<P>(tab + (q * 6 + ka) * PBP, wa);
+        load_band<P>(tab + (q * 6 + ka + 1) * PBP, wb);
+        const T *g = gb + (q >> 1) * GP + (q & 1) * NFM;
+        const T x0 = g[0], x1 = g[GS], x2 = g[2 * GS];
+#pragma unroll
+        for (int m = 0; m <= P; m++) {
+            A0[m] += wa[m] * x0 + wb[m] * x1;
+            A1[m] += wa[m] * x2;
+        }
+    }
+#pragma unroll
+    for (int m = 0; m <= P; m++) store_pair(kp + (cur + m) * (2 * NFM), A0[m], A1[m]);
+}
+
+__device__ __forceinline__ int relu_last_plus1(const int *elem, int q0, int nq, int f0) {
+    return elem[q0 + nq - 1] - f0 + 1;
+}
 
 }  // namespace
 
@@ -86,9 +350,10 @@ struct StreamArgs {
     const int *tile_pstride;   // coefficients per w plane of a tile (padded)
     const int *tq0[2];         // first point of a u / v tile
     const int *tnq[2];         // points of a u / v tile
+    const int *treg[2];        // tile pattern (walk_u): 1 regular, 2 first, 3 last, 0 other
     int ntile[2];
     const int *elem[3];        // element owning each point
-    const T *band[3];          // [nqp][6][p+1]: B0 B1 W00 W01 W10 W11
+    const T *band[3];          // [nqp][6][round4(p+1)]: B0 B1 W00 W01 W10 W11
     const int *wq0;            // first w point of each element (nel_w + 1)
     int nqw;                   // w points
     const int4 *seg;           // (tile, e_begin, e_end, -)
@@ -96,21 +361,35 @@ struct StreamArgs {
     int nfun[3];
     int64_t ncp;
     int cmask[3];
+    int *err;                  // set to 1 when a bounded wait gave up
 };
 
 template <class T, int P>
 __global__ void __launch_bounds__(kThreads, 2) k_wq_apply_stream(StreamArgs<T> a) {
     using D = Dims<P>;
-    constexpr int PB = D::PB, NFM = D::NFM, CPT = D::CPT;
+    constexpr int PB = D::PB, PBP = D::PBP, NFM = D::NFM, CPT = D::CPT;
+    constexpr int GS = D::GS, GP = D::GP, ZHP = D::ZHP;
+    // FP32: each plane's coefficient block is brought into shared memory by a
+    // bulk copy issued one plane ahead; FP64 reads it from HBM directly
+    constexpr bool kStaged = sizeof(T) == 4;
     if (a.done && *a.done) return;
     extern __shared__ __align__(16) unsigned char smraw[];
-    T *R1 = reinterpret_cast<T *>(smraw);
-    T *R2 = R1 + D::R1;
-    T *tabu = R2 + D::R2;
-    T *tabv = tabu + D::TAB;
-    int *relu = reinterpret_cast<int *>(tabv + D::TAB);
-    int *relv = relu + kTQ;
-    const int tid = threadIdx.x;
+    T *const sm = reinterpret_cast<T *>(smraw);
+    T *const RY = sm;
+    T *const RZH = sm + D::OFF_ZH;   // per warp: Z, then h; K (all warps) after G
+    T *const RG = sm + D::OFF_G;     // per warp: G
+    T *const tabu = sm + D::OFF_TAB;
+    T *const tabv = tabu + D::TAB;
+    T *const cbuf = sm + D::TOTAL;
+    int *const relu = reinterpret_cast<int *>(sm + D::TOTAL + (kStaged ? D::CB : 0));
+    int *const relv = relu + kTQ;
+    uint64_t *const bar = reinterpret_cast<uint64_t *>(relv + kTQ);
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    uint32_t phase = 0;
+    if constexpr (kStaged) {
+        if (tid == 0) mbar_init(bar);
+        __syncthreads();
+    }
     const int64_t plane = (int64_t)a.nfun[0] * a.nfun[1];
 
     for (int si = a.cta_seg[blockIdx.x]; si < a.cta_seg[blockIdx.x + 1]; si++) {
@@ -118,24 +397,36 @@ __global__ void __launch_bounds__(kThreads, 2) k_wq_apply_stream(StreamArgs<T> a
         const int tu = sg.x % a.ntile[0], tv = sg.x / a.ntile[0];
         const int qu0 = a.tq0[0][tu], nqu = a.tnq[0][tu];
         const int qv0 = a.tq0[1][tv], nqv = a.tnq[1][tv];
+        const int patu = a.treg[0][tu], patv = a.treg[1][tv];
+        const bool regu = patu == 1, regv = patv == 1;
         const int fu0 = a.elem[0][qu0], fv0 = a.elem[1][qv0];
         const int nfu = a.elem[0][qu0 + nqu - 1] + PB - fu0;
         const int nfv = a.elem[1][qv0 + nqv - 1] + PB - fv0;
+        const int neu = relu_last_plus1(a.elem[0], qu0, nqu, fu0);   // elements of the tile
+        const int nev = relu_last_plus1(a.elem[1], qv0, nqv, fv0);
         const int npts = nqu * nqv;
         const T *coef_t = a.coef + a.tile_off[sg.x];
         const int pstride = a.tile_pstride[sg.x];
         const int pbytes = npts * kWQCoef * (int)sizeof(T);
+        const int nrow = min(2, nqv - 2 * warp);   // rows of this warp (may be <= 0)
 
         __syncthreads();   // the previous segment is done with the tables
-        for (int i = tid; i < kTQ * 6 * PB; i += kThreads) {
-            const int q = i / (6 * PB), r = i - q * (6 * PB);
-            tabu[i] = q < nqu ? a.band[0][(size_t)(qu0 + q) * 6 * PB + r] : T(0);
-            tabv[i] = q < nqv ? a.band[1][(size_t)(qv0 + q) * 6 * PB + r] : T(0);
+        for (int i = tid; i < kTQ * 6 * PBP; i += kThreads) {
+            const int q = i / (6 * PBP), r = i - q * (6 * PBP);
+            tabu[i] = q < nqu ? a.band[0][(size_t)(qu0 + q) * 6 * PBP + r] : T(0);
+            tabv[i] = q < nqv ? a.band[1][(size_t)(qv0 + q) * 6 * PBP + r] : T(0);
         }
         if (tid < kTQ) {
             relu[tid] = tid < nqu ? a.elem[0][qu0 + tid] - fu0 : 0;
             relv[tid] = tid < nqv ? a.elem[1][qv0 + tid] - fv0 : 0;
         }
+        const uint32_t cbytes = (uint32_t)((npts * kWQCoef * (int)sizeof(T) + 15) & ~15);
+        if constexpr (kStaged) {
+            if (tid == 0) bulk_load(cbuf, coef_t + (int64_t)a.wq0[sg.y] * pstride, cbytes, bar);
+        }
+        // stage D thread: (ik, fu)
+        const bool d_act = tid < 9 * nfu;
+        const int d_ik = d_act ? tid / nfu : 0, d_fu = d_act ? tid - d_ik * nfu : 0;
 
         // columns (c, fv, fu) of this thread: stages A and E
         const int ncol = 3 * nfv * nfu;
@@ -194,7 +485,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_wq_apply_stream(StreamArgs<T> a
             }
             const int qw_end = a.wq0[e + 1];
             for (int qw = a.wq0[e]; qw < qw_end; qw++) {
-                const T *bw = a.band[2] + (size_t)qw * 6 * PB;
+                const T *bw = a.band[2] + (size_t)qw * 6 * PBP;
                 if (qw + 1 < a.nqw) {
                     const char *pn = reinterpret_cast<const char *>(coef_t + (int64_t)(qw + 1) * pstride);
                     for (int off = tid * 128; off < pbytes; off += kThreads * 128) prefetch_l2(pn + off);
@@ -202,11 +493,8 @@ __global__ void __launch_bounds__(kThreads, 2) k_wq_apply_stream(StreamArgs<T> a
                 // ---- A: forward w
                 {
                     T b0[PB], b1[PB];
-#pragma unroll
-                    for (int m = 0; m < PB; m++) {
-                        b0[m] = bw[m];
-                        b1[m] = bw[PB + m];
-                    }
+                    load_band<P>(bw, b0);
+                    load_band<P>(bw + PBP, b1);
 #pragma unroll
                     for (int cc = 0; cc < CPT; cc++) {
                         if (!(cinfo[cc] & 4)) continue;
@@ -217,218 +505,184 @@ __global__ void __launch_bounds__(kThreads, 2) k_wq_apply_stream(StreamArgs<T> a
                             y1 += b1[m] * x[cc][m];
                         }
                         const int c = cinfo[cc] & 3, k = cinfo[cc] >> 3;
-                        R1[c * NFM * NFM + k] = y0;
-                        R1[(3 + c) * NFM * NFM + k] = y1;
+                        RY[c * NFM * NFM + k] = y0;
+                        RY[(3 + c) * NFM * NFM + k] = y1;
                     }
                 }
-                __syncthreads();
-                // ---- B: forward v, thread (qv, fu)
-                {
-                    const int qv = tid >> 4, fu = tid & 15;
-                    if (qv < nqv && fu < nfu) {
-                        const int rv = relv[qv];
-                        const T *w0 = tabv + (qv * 6 + 0) * PB;
-                        const T *w1 = tabv + (qv * 6 + 1) * PB;
-                        T b0[PB], b1[PB];
+                if constexpr (kStaged) {
+                    // this plane's coefficient block has landed in shared memory
+                    const bool ok = mbar_wait(bar, phase);
+                    if (__syncthreads_or(!ok)) {
+                        if (tid == 0) atomicOr(a.err, 1);
+                        mbar_wait(bar, phase);   // let a copy still in flight land
+                        return;
+                    }
+                    phase ^= 1;
+                } else {
+                    __syncthreads();
+                }
+                if (nrow > 0) {
+                    T *const zh = RZH + warp * ZHP;
+                    T *const gp = RG + warp * GP;
+                    // ---- B: forward v of this warp's rows, lane (row, fu)
+                    {
+                        const int row = lane >> 4, fu = lane & 15;
+                        if (row < nrow && fu < nfu) {
+                            const int qv = 2 * warp + row;
+                            const int rv = regv ? (qv >> 1) : relv[qv];
+                            T b0[PB], b1[PB];
+                            load_band<P>(tabv + (qv * 6 + 0) * PBP, b0);
+                            load_band<P>(tabv + (qv * 6 + 1) * PBP, b1);
 #pragma unroll
-                        for (int m = 0; m < PB; m++) {
-                            b0[m] = w0[m];
-                            b1[m] = w1[m];
-                        }
+                            for (int c = 0; c < 3; c++) {
+                                const T *y0 = RY + (c * NFM + rv) * NFM + fu;
+                                const T *y1 = RY + ((3 + c) * NFM + rv) * NFM + fu;
+                                T z0 = 0, z1 = 0, z2 = 0;
 #pragma unroll
-                        for (int c = 0; c < 3; c++) {
-                            const T *y0 = R1 + (c * NFM + rv) * NFM + fu;
-                            const T *y1 = R1 + ((3 + c) * NFM + rv) * NFM + fu;
-                            T z0 = 0, z1 = 0, z2 = 0;
-#pragma unroll
-                            for (int m = 0; m < PB; m++) {
-                                const T a0 = y0[m * NFM], a1 = y1[m * NFM];
-                                z0 += b0[m] * a0;
-                                z1 += b1[m] * a0;
-                                z2 += b0[m] * a1;
+                                for (int m = 0; m < PB; m++) {
+                                    const T a0 = y0[m * NFM], a1 = y1[m * NFM];
+                                    z0 += b0[m] * a0;
+                                    z1 += b1[m] * a0;
+                                    z2 += b0[m] * a1;
+                                }
+                                zh[(0 * 3 + c) * (2 * NFM) + row * NFM + fu] = z0;
+                                zh[(1 * 3 + c) * (2 * NFM) + row * NFM + fu] = z1;
+                                zh[(2 * 3 + c) * (2 * NFM) + row * NFM + fu] = z2;
                             }
-                            R2[((0 * 3 + c) * kTQ + qv) * NFM + fu] = z0;
-                            R2[((1 * 3 + c) * kTQ + qv) * NFM + fu] = z1;
-                            R2[((2 * 3 + c) * kTQ + qv) * NFM + fu] = z2;
                         }
                     }
-                }
-                __syncthreads();
-                // ---- C1: forward u, thread (row qv, s, j), ring along u
-                if (tid < 9 * kTQ) {
-                    const int qv = tid & 15, sj = tid >> 4;
-                    if (qv < nqv) {
-                        const int kind = sj < 3 ? 1 : 0;   // s = 0 takes d/du
-                        const T *zr = R2 + (sj * kTQ + qv) * NFM;
-                        T *fr = R1 + (sj * kTQ + qv) * kQP;
-                        T z[PB];
-#pragma unroll
-                        for (int m = 0; m < PB; m++) z[m] = zr[m];
-                        int cur = 0;
-                        for (int qu = 0; qu < nqu; qu++) {
-                            const int r = relu[qu];
-                            if (r != cur) {
-#pragma unroll
-                                for (int m = 0; m < P; m++) z[m] = z[m + 1];
-                                z[P] = zr[r + P];
-                                cur = r;
-                            }
-                            const T *w = tabu + (qu * 6 + kind) * PB;
-                            T v = 0;
-#pragma unroll
-                            for (int m = 0; m < PB; m++) v += w[m] * z[m];
-                            fr[qu] = v;
-                        }
-                    }
-                }
-                __syncthreads();
-                // ---- C2: pointwise coefficients, thread (qv, qu)
-                {
-                    const int qv = tid >> 4, qu = tid & 15;
-                    if (qv < nqv && qu < nqu) {
+                    __syncwarp();
+                    // ---- C: forward u and the pointwise coefficients, lane (row, qu)
+                    {
+                        const int row = lane >> 4, qu = lane & 15;
+                        const bool act = row < nrow && qu < nqu;
                         T f[3][3];
+                        if (act) {
+                            const int ru = regu ? (qu >> 1) : relu[qu];
+                            T b0[PB], b1[PB];
+                            load_band<P>(tabu + (qu * 6 + 0) * PBP, b0);
+                            load_band<P>(tabu + (qu * 6 + 1) * PBP, b1);
 #pragma unroll
-                        for (int l = 0; l < 3; l++)
+                            for (int l = 0; l < 3; l++)
 #pragma unroll
-                            for (int j = 0; j < 3; j++) f[l][j] = R1[((l * 3 + j) * kTQ + qv) * kQP + qu];
-                        const T *cp = coef_t + (int64_t)qw * pstride + qv * nqu + qu;
-                        T h[27];
+                                for (int j = 0; j < 3; j++) {
+                                    const T *zr = zh + (l * 3 + j) * (2 * NFM) + row * NFM + ru;
+                                    T v = 0;
 #pragma unroll
-                        for (int ch = 0; ch < 27; ch++) h[ch] = T(0);
+                                    for (int m = 0; m < PB; m++) v += (l == 0 ? b1[m] : b0[m]) * zr[m];
+                                    f[l][j] = v;
+                                }
+                        }
+                        __syncwarp();   // the warp's Z is read; h takes its place
+                        if (act) {
+                            const int pt = (2 * warp + row) * nqu + qu;
+                            if constexpr (kStaged) {
+                                // point-major block in shared memory: 45 values per point
+                                const T *cp = cbuf + pt * kWQCoef;
+                                T h[27];
 #pragma unroll
-                        for (int I = 0; I < 9; I++) {
+                                for (int ch = 0; ch < 27; ch++) h[ch] = T(0);
 #pragma unroll
-                            for (int J = I; J < 9; J++) {
-                                const T s = ld_stream(cp + sym9(I, J) * npts);
-                                const int i = I / 3, k = I % 3, j = J / 3, l = J % 3;
-                                h[(i * 3 + k) * 3 + l] += s * f[l][j];
-                                if (I != J) h[(j * 3 + l) * 3 + k] += s * f[k][i];
+                                for (int I = 0; I < 9; I++) {
+#pragma unroll
+                                    for (int J = I; J < 9; J++) {
+                                        const T sv = cp[sym9(I, J)];
+                                        const int i = I / 3, k = I % 3, j = J / 3, l = J % 3;
+                                        h[(i * 3 + k) * 3 + l] += sv * f[l][j];
+                                        if (I != J) h[(j * 3 + l) * 3 + k] += sv * f[k][i];
+                                    }
+                                }
+#pragma unroll
+                                for (int ch = 0; ch < 27; ch++) zh[ch * kHS + row * kTQ + qu] = h[ch];
+                            } else {
+                                // entry-major block in HBM, one output component at a
+                                // time (the symmetric partner entries hit L1)
+                                const T *cp = coef_t + (int64_t)qw * pstride + pt;
+#pragma unroll
+                                for (int i = 0; i < 3; i++) {
+#pragma unroll
+                                    for (int k = 0; k < 3; k++) {
+                                        T h0 = 0, h1 = 0, h2 = 0;
+#pragma unroll
+                                        for (int J = 0; J < 9; J++) {
+                                            const T sv = __ldg(cp + sym9(3 * i + k, J) * npts);
+                                            const int j = J / 3, l = J % 3;
+                                            if (l == 0) h0 += sv * f[0][j];
+                                            else if (l == 1) h1 += sv * f[1][j];
+                                            else h2 += sv * f[2][j];
+                                        }
+                                        const int ch = (i * 3 + k) * 3;
+                                        zh[(ch + 0) * kHS + row * kTQ + qu] = h0;
+                                        zh[(ch + 1) * kHS + row * kTQ + qu] = h1;
+                                        zh[(ch + 2) * kHS + row * kTQ + qu] = h2;
+                                    }
+                                }
                             }
                         }
-#pragma unroll
-                        for (int ch = 0; ch < 27; ch++) R2[(ch * kTQ + qv) * kQP + qu] = h[ch];
+                    }
+                    __syncwarp();
+                    // ---- G: backward u, lane (row, channel), 54 walks per warp
+                    for (int wk = lane; wk < 54; wk += 32) {
+                        const int row = wk & 1, ch = wk >> 1;
+                        if (row < nrow) {
+                            const int k = (ch / 3) % 3, l = ch % 3;
+                            const int kind = 2 + 2 * (k == 0) + (l == 0);   // W_{[k==u][l==u]}
+                            const T *hr = zh + ch * kHS + row * kTQ;
+                            T *gr = gp + ch * GS + row * NFM;
+                            switch (patu) {
+                                case 1: walk_u<T, P, 1>(hr, gr, tabu, kind, neu); break;
+                                case 2: walk_u<T, P, 2>(hr, gr, tabu, kind, neu); break;
+                                case 3: walk_u<T, P, 3>(hr, gr, tabu, kind, neu); break;
+                                default: walk_u_generic<T, P>(hr, gr, tabu, kind, relu, nqu);
+                            }
+                        }
                     }
                 }
                 __syncthreads();
-                // ---- C3: backward u, thread (row qv, i, k), rings along u
-                if (tid < 9 * kTQ) {
-                    const int qv = tid & 15, ik = tid >> 4;
-                    if (qv < nqv) {
-                        const int ka = 2 + 2 * (ik % 3 == 0);   // W_{[k==u], 0}
-                        const T *h0 = R2 + ((ik * 3 + 0) * kTQ + qv) * kQP;
-                        const T *h1 = R2 + ((ik * 3 + 1) * kTQ + qv) * kQP;
-                        const T *h2 = R2 + ((ik * 3 + 2) * kTQ + qv) * kQP;
-                        T *g0 = R1 + ((ik * 3 + 0) * kTQ + qv) * NFM;
-                        T *g1 = R1 + ((ik * 3 + 1) * kTQ + qv) * NFM;
-                        T *g2 = R1 + ((ik * 3 + 2) * kTQ + qv) * NFM;
-                        T a0[PB], a1[PB], a2[PB];
-#pragma unroll
-                        for (int m = 0; m < PB; m++) a0[m] = a1[m] = a2[m] = T(0);
-                        int cur = 0;
-                        for (int qu = 0; qu < nqu; qu++) {
-                            const int r = relu[qu];
-                            if (r != cur) {
-                                g0[cur] = a0[0];
-                                g1[cur] = a1[0];
-                                g2[cur] = a2[0];
-#pragma unroll
-                                for (int m = 0; m < P; m++) {
-                                    a0[m] = a0[m + 1];
-                                    a1[m] = a1[m + 1];
-                                    a2[m] = a2[m + 1];
-                                }
-                                a0[P] = a1[P] = a2[P] = T(0);
-                                cur = r;
-                            }
-                            const T *wa = tabu + (qu * 6 + ka + 1) * PB;   // trial d/du
-                            const T *wb = tabu + (qu * 6 + ka) * PB;       // trial d/dv, d/dw
-                            const T x0 = h0[qu], x1 = h1[qu], x2 = h2[qu];
-#pragma unroll
-                            for (int m = 0; m < PB; m++) {
-                                a0[m] += wa[m] * x0;
-                                a1[m] += wb[m] * x1;
-                                a2[m] += wb[m] * x2;
-                            }
-                        }
-#pragma unroll
-                        for (int m = 0; m < PB; m++) {
-                            g0[cur + m] = a0[m];
-                            g1[cur + m] = a1[m];
-                            g2[cur + m] = a2[m];
-                        }
-                    }
+                if constexpr (kStaged) {
+                    // every warp is done with the block: bring in the next plane's
+                    if (tid == 0 && qw + 1 < a.wq0[sg.z])
+                        bulk_load(cbuf, coef_t + (int64_t)(qw + 1) * pstride, cbytes, bar);
                 }
-                __syncthreads();
-                // ---- D: backward v, thread (fu, i, k), rings along v
-                if (tid < 9 * kTQ) {
-                    const int fu = tid & 15, ik = tid >> 4;
-                    if (fu < nfu) {
-                        const int ka = 2 + 2 * (ik % 3 == 1);   // W_{[k==v], 0}
-                        const T *g0 = R1 + ((ik * 3 + 0) * kTQ) * NFM + fu;
-                        const T *g1 = R1 + ((ik * 3 + 1) * kTQ) * NFM + fu;
-                        const T *g2 = R1 + ((ik * 3 + 2) * kTQ) * NFM + fu;
-                        T *k0 = R2 + ((ik * 2 + 0) * NFM) * NFM + fu;
-                        T *k1 = R2 + ((ik * 2 + 1) * NFM) * NFM + fu;
-                        T A0[PB], A1[PB];
-#pragma unroll
-                        for (int m = 0; m < PB; m++) A0[m] = A1[m] = T(0);
-                        int cur = 0;
-                        for (int qv = 0; qv < nqv; qv++) {
-                            const int r = relv[qv];
-                            if (r != cur) {
-                                k0[cur * NFM] = A0[0];
-                                k1[cur * NFM] = A1[0];
-#pragma unroll
-                                for (int m = 0; m < P; m++) {
-                                    A0[m] = A0[m + 1];
-                                    A1[m] = A1[m + 1];
-                                }
-                                A0[P] = A1[P] = T(0);
-                                cur = r;
-                            }
-                            const T *wa = tabv + (qv * 6 + ka) * PB;       // trial d/du, d/dw
-                            const T *wb = tabv + (qv * 6 + ka + 1) * PB;   // trial d/dv
-                            const T x0 = g0[qv * NFM], x1 = g1[qv * NFM], x2 = g2[qv * NFM];
-#pragma unroll
-                            for (int m = 0; m < PB; m++) {
-                                A0[m] += wa[m] * x0 + wb[m] * x1;
-                                A1[m] += wa[m] * x2;
-                            }
-                        }
-#pragma unroll
-                        for (int m = 0; m < PB; m++) {
-                            k0[(cur + m) * NFM] = A0[m];
-                            k1[(cur + m) * NFM] = A1[m];
-                        }
+                // ---- D: backward v, thread (i, k, fu); K aliases the Z/h parts
+                if (d_act) {
+                    const int ik = d_ik, fu = d_fu;
+                    const int ka = 2 + 2 * (ik % 3 == 1);   // W_{[k==v], 0}
+                    const T *gb = RG + (ik * 3) * GS + fu;
+                    T *kp = RZH + (ik * NFM * NFM + fu) * 2;
+                    switch (patv) {
+                        case 1: walk_v<T, P, 1>(gb, kp, tabv, ka, nev); break;
+                        case 2: walk_v<T, P, 2>(gb, kp, tabv, ka, nev); break;
+                        case 3: walk_v<T, P, 3>(gb, kp, tabv, ka, nev); break;
+                        default: walk_v_generic<T, P>(gb, kp, tabv, ka, relv, nqv);
                     }
                 }
                 __syncthreads();
                 // ---- E: backward w into the register ring of output planes
                 {
                     T w00[PB], w01[PB], w10[PB], w11[PB];
-#pragma unroll
-                    for (int m = 0; m < PB; m++) {
-                        w00[m] = bw[2 * PB + m];
-                        w01[m] = bw[3 * PB + m];
-                        w10[m] = bw[4 * PB + m];
-                        w11[m] = bw[5 * PB + m];
-                    }
+                    load_band<P>(bw + 2 * PBP, w00);
+                    load_band<P>(bw + 3 * PBP, w01);
+                    load_band<P>(bw + 4 * PBP, w10);
+                    load_band<P>(bw + 5 * PBP, w11);
 #pragma unroll
                     for (int cc = 0; cc < CPT; cc++) {
                         if (!(cinfo[cc] & 4)) continue;
                         const int i = cinfo[cc] & 3, kidx = cinfo[cc] >> 3;
-                        const T *kb = R2 + (i * 6) * NFM * NFM + kidx;
-                        const T s00 = kb[0 * NFM * NFM] + kb[2 * NFM * NFM];
-                        const T s01 = kb[1 * NFM * NFM] + kb[3 * NFM * NFM];
-                        const T s10 = kb[4 * NFM * NFM];
-                        const T s11 = kb[5 * NFM * NFM];
+                        const T *kb = RZH + ((i * 3) * NFM * NFM + kidx) * 2;
+                        T k00, k01, k10, k11, k20, k21;
+                        load_pair(kb, k00, k01);
+                        load_pair(kb + 2 * NFM * NFM, k10, k11);
+                        load_pair(kb + 4 * NFM * NFM, k20, k21);
+                        const T s00 = k00 + k10, s01 = k01 + k11;
 #pragma unroll
                         for (int m = 0; m < PB; m++)
-                            acc[cc][m] += w00[m] * s00 + w01[m] * s01 + w10[m] * s10 + w11[m] * s11;
+                            acc[cc][m] += w00[m] * s00 + w01[m] * s01 + w10[m] * k20 + w11[m] * k21;
                     }
                 }
-                // no barrier: the next plane's stage A writes R1, last read
-                // by stage D before the barrier above
+                // no barrier: the next plane's stage A writes only RY, and
+                // the next B writes the Z/h parts after the barrier that
+                // follows A
             }
             // output plane e is complete for this element range
 #pragma unroll
@@ -450,28 +704,46 @@ __global__ void __launch_bounds__(kThreads, 2) k_wq_apply_stream(StreamArgs<T> a
 }
 
 // ------------------------------------------------------------------ host
-// Tiles of whole elements with at most kTQ points, balanced in size.
+// Tiles of whole elements with at most kTQ points: the first and last tiles
+// take the boundary elements (which own more than two points) and as many
+// neighbours as fit; the elements between (two points each) are split into
+// balanced regular tiles of at most kNE elements.
 static void make_tiles(const std::vector<int> &elem_q0, int nel, std::vector<int> &q0,
-                       std::vector<int> &nq) {
-    const int nqp = elem_q0[nel];
-    const int nt0 = (nqp + kTQ - 1) / kTQ;
+                       std::vector<int> &nq, std::vector<int> &reg) {
     q0.clear();
     nq.clear();
-    int e = 0, t = 0;
-    while (e < nel) {
-        const int start = elem_q0[e];
-        // aim for an even split of the remaining points over the remaining tiles
-        const int left_tiles = std::max(1, nt0 - t);
-        const int target = (nqp - start + left_tiles - 1) / left_tiles;
-        int end = e;
-        while (end < nel && elem_q0[end + 1] - start <= kTQ &&
-               (end == e || elem_q0[end] - start < target))
-            end++;
-        q0.push_back(start);
-        nq.push_back(elem_q0[end] - start);
-        e = end;
-        t++;
+    reg.clear();
+    auto pts = [&](int a, int b) { return elem_q0[b] - elem_q0[a]; };   // elements [a, b)
+    int first_end = 1;
+    while (first_end < nel && pts(0, first_end + 1) <= kTQ) first_end++;
+    int last_begin = nel;
+    if (first_end < nel) {
+        last_begin = nel - 1;
+        while (last_begin - 1 >= first_end && pts(last_begin - 1, nel) <= kTQ) last_begin--;
     }
+    // walk pattern of a tile (see walk_u): 1 all elements own two points,
+    // 2 only the first element of the patch differs, 3 only the last
+    auto add = [&](int a, int b) {
+        bool inner2 = true;   // elements other than the patch's first / last own 2
+        for (int e = a; e < b; e++)
+            if (e != 0 && e != nel - 1) inner2 = inner2 && (pts(e, e + 1) == 2);
+        const bool has_first = a == 0, has_last = b == nel;
+        int pat = 0;
+        if (inner2 && !has_first && !has_last) pat = 1;
+        else if (inner2 && has_first && !has_last) pat = 2;
+        else if (inner2 && has_last && !has_first) pat = 3;
+        q0.push_back(elem_q0[a]);
+        nq.push_back(pts(a, b));
+        reg.push_back(pat);
+    };
+    add(0, first_end);
+    const int nmid = last_begin - first_end;
+    if (nmid > 0) {
+        const int t = (nmid + kNE - 1) / kNE;
+        for (int k = 0; k < t; k++)
+            add(first_end + (int)((int64_t)nmid * k / t), first_end + (int)((int64_t)nmid * (k + 1) / t));
+    }
+    if (last_begin < nel) add(last_begin, nel);
 }
 
 template <class T>
@@ -508,9 +780,14 @@ __global__ void k_wq_stream_permute(const T *src, T *dst, const int64_t *qoff1,
         while (tq0v[tv] + tnqv[tv] <= qv) tv++;
         const int t = tu + ntu * tv;
         const int nqt = tnqu[tu] * tnqv[tv];
-        const int64_t dbase = tile_off[t] + (int64_t)qw * tile_pstride[t] +
-                              (qv - tq0v[tv]) * tnqu[tu] + (qu - tq0u[tu]);
-        for (int e = 0; e < kWQCoef; e++) dst[dbase + (int64_t)e * nqt] = src[sbase + e * nqb];
+        const int pt = (qv - tq0v[tv]) * tnqu[tu] + (qu - tq0u[tu]);
+        const int64_t pbase = tile_off[t] + (int64_t)qw * tile_pstride[t];
+        // FP32 blocks point-major (staged whole into shared memory), FP64
+        // blocks entry-major (read straight from HBM, coalesced per entry)
+        if (sizeof(T) == 4)
+            for (int e = 0; e < kWQCoef; e++) dst[pbase + (int64_t)pt * kWQCoef + e] = src[sbase + e * nqb];
+        else
+            for (int e = 0; e < kWQCoef; e++) dst[pbase + (int64_t)e * nqt + pt] = src[sbase + e * nqb];
     }
 }
 
@@ -555,7 +832,7 @@ bool wq_stream_supported(const yeti_wq_op *op) {
 int wq_stream_setup(yeti_wq_op *op, const WQRule1D R[3]) {
     yeti_ctx *ctx = op->ctx;
     WQStreamPlan &st = op->st;
-    const int P = op->p[0], PB = P + 1;
+    const int P = op->p[0], PBP = (P + 1 + 3) / 4 * 4;
     std::vector<int> elem_q0[3];
     for (int d = 0; d < 3; d++) {
         const int nel = op->nel[d], nq = op->nqp[d];
@@ -573,13 +850,13 @@ int wq_stream_setup(yeti_wq_op *op, const WQRule1D R[3]) {
         // banded 1-D tables; every non-zero must lie in the band
         const std::vector<double> *M[6] = {&R[d].B0, &R[d].B1, &R[d].W00,
                                            &R[d].W01, &R[d].W10, &R[d].W11};
-        std::vector<double> band((size_t)nq * 6 * PB, 0.0);
+        std::vector<double> band((size_t)nq * 6 * PBP, 0.0);
         for (int q = 0; q < nq; q++)
             for (int k = 0; k < 6; k++)
                 for (int f = 0; f < R[d].nfun; f++) {
                     const double v = (*M[k])[(size_t)f * nq + q];
                     const int m = f - elem[q];
-                    if (m >= 0 && m <= P) band[((size_t)q * 6 + k) * PB + m] = v;
+                    if (m >= 0 && m <= P) band[((size_t)q * 6 + k) * PBP + m] = v;
                     else YETI_CHECK(v == 0.0, YETI_EUNSUPPORTED,
                                     "WQ streaming: rule entry outside the band (dir %d, f %d, q %d)",
                                     d, f, q);
@@ -590,9 +867,10 @@ int wq_stream_setup(yeti_wq_op *op, const WQRule1D R[3]) {
         YETI_TRY(upload_vec(ctx, st.band32[d], bandf));
     }
     YETI_TRY(upload_vec(ctx, st.wq0, elem_q0[2]));
-    std::vector<int> tq0[2], tnq[2];
+    std::vector<int> tq0[2], tnq[2], treg[2];
     for (int d = 0; d < 2; d++) {
-        make_tiles(elem_q0[d], op->nel[d], tq0[d], tnq[d]);
+        make_tiles(elem_q0[d], op->nel[d], tq0[d], tnq[d], treg[d]);
+        YETI_TRY(upload_vec(ctx, st.treg[d], treg[d]));
         st.ntile[d] = (int)tq0[d].size();
         YETI_TRY(upload_vec(ctx, st.tq0[d], tq0[d]));
         YETI_TRY(upload_vec(ctx, st.tnq[d], tnq[d]));
@@ -611,6 +889,8 @@ int wq_stream_setup(yeti_wq_op *op, const WQRule1D R[3]) {
     st.ncoef = toff[ntiles];
     YETI_TRY(upload_vec(ctx, st.tile_off, toff));
     YETI_TRY(upload_vec(ctx, st.tile_pstride, pstride));
+    YETI_TRY(st.err.alloc(ctx, sizeof(int)));
+    YETI_CUDA(cudaMemsetAsync(st.err.ptr, 0, sizeof(int), ctx->stream));
 
     // kernels and grid
     YETI_TRY(stream_prepare_kernels(op));
@@ -728,6 +1008,7 @@ static int launch_stream(yeti_wq_op *op, const T *u, T *Ku, const int *done, cud
     for (int d = 0; d < 2; d++) {
         a.tq0[d] = st.tq0[d].as<int>();
         a.tnq[d] = st.tnq[d].as<int>();
+        a.treg[d] = st.treg[d].as<int>();
         a.ntile[d] = st.ntile[d];
     }
     for (int d = 0; d < 3; d++) {
@@ -737,6 +1018,7 @@ static int launch_stream(yeti_wq_op *op, const T *u, T *Ku, const int *done, cud
         a.cmask[d] = op->cmask[d];
     }
     a.wq0 = st.wq0.as<int>();
+    a.err = st.err.as<int>();
     a.nqw = op->nqp[2];
     a.seg = st.seg[which].as<int4>();
     a.cta_seg = st.cta_seg[which].as<int>();
@@ -758,6 +1040,19 @@ int wq_stream_apply(yeti_wq_op *op, const T *u, T *Ku, const int *done, cudaStre
             set_error("WQ streaming: degree %d", op->p[0]);
             return YETI_EUNSUPPORTED;
     }
+}
+
+int wq_stream_check(yeti_wq_op *op) {
+    if (!op->st.active) return YETI_OK;
+    int h = 0;
+    YETI_CUDA(cudaMemcpyAsync(&h, op->st.err.ptr, sizeof(int), cudaMemcpyDeviceToHost, op->ctx->stream));
+    YETI_CUDA(cudaStreamSynchronize(op->ctx->stream));
+    if (h) {
+        YETI_CUDA(cudaMemsetAsync(op->st.err.ptr, 0, sizeof(int), op->ctx->stream));
+        set_error("WQ apply: a bounded wait for a coefficient copy gave up; results are invalid");
+        return YETI_ETIMEDOUT;
+    }
+    return YETI_OK;
 }
 
 template int wq_stream_apply<float>(yeti_wq_op *, const float *, float *, const int *, cudaStream_t);
