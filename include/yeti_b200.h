@@ -212,6 +212,63 @@ int yeti_grad_lin_elast_work(yeti_ctx *ctx, const yeti_u1_model *model,
                              int include_surface_loads, double *gwint,
                              double *gwext, int mem);
 
+/* ------------------------------------------------------------------------
+ * Serving: persistent request loop (no counterpart in the reference)
+ * ------------------------------------------------------------------------
+ * A server owns an engine thread and a private context on `device`.
+ * Submitted requests wait in arrival order and are admitted while fewer than
+ * max_active are active and their estimated device bytes fit in
+ * hbm_budget_bytes (0: no bound) beside the active ones.  An admitted request
+ * gets its WQ operator (FP64 data) and one Jacobi-PCG per right-hand side;
+ * the solves of all active requests run concurrently on the device (CUDA
+ * graphs of 16 iterations on a pool of streams) with operators and Krylov
+ * state resident in HBM.  Submit, poll and wait may be called from any host
+ * thread.
+ */
+typedef struct yeti_server yeti_server;
+
+typedef struct {
+    int32_t p[3], nel[3];         /* degrees 2..8, elements per direction  */
+    const double *cps;            /* (3, ncp) host, as yeti_wq_setup       */
+    const double *weights;        /* (ncp) host                            */
+    double E, nu;
+    uint8_t dirichlet[18];        /* as yeti_wq_setup                      */
+    int32_t nrhs;                 /* 1..8                                  */
+    const double *rhs;            /* nrhs x 3*ncp host, component-major    */
+    double rtol;                  /* ||r||_2 <= rtol ||b||_2               */
+    int32_t maxit;
+} yeti_serve_request;
+
+typedef struct {
+    int32_t status;               /* YETI_OK or the error code             */
+    int32_t nrhs;
+    int64_t ndof;
+    int32_t iterations[8];
+    double rel_residual[8];       /* true FP64 residual of each solution   */
+    double queue_ms;              /* submit -> admission                   */
+    double solve_ms;              /* admission -> last solution            */
+    double total_ms;              /* submit -> last solution               */
+} yeti_serve_result;
+
+int yeti_serve_open(int device, size_t hbm_budget_bytes, int max_active,
+                    yeti_server **out);
+/* Copies the request's arrays; returns at once with a ticket.  A request
+ * whose estimated device bytes exceed the budget is refused (YETI_ENOMEM). */
+int yeti_serve_submit(yeti_server *srv, const yeti_serve_request *req,
+                      int64_t *ticket);
+/* 1: done (x gets nrhs x ndof doubles, res filled, ticket released),
+ * 0: pending, < 0: the request failed (error code; ticket released). */
+int yeti_serve_poll(yeti_server *srv, int64_t ticket, double *x,
+                    yeti_serve_result *res);
+/* As poll, blocking up to timeout_ms (< 0: no limit; YETI_ETIMEDOUT). */
+int yeti_serve_wait(yeti_server *srv, int64_t ticket, double timeout_ms,
+                    double *x, yeti_serve_result *res);
+int yeti_serve_stats(yeti_server *srv, int64_t *done, int64_t *queued,
+                     int32_t *active, int32_t *peak_active,
+                     size_t *committed_bytes);
+/* Finishes the active requests, fails the queued ones, joins the thread. */
+int yeti_serve_close(yeti_server *srv);
+
 #ifdef __cplusplus
 }
 #endif

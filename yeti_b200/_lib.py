@@ -57,6 +57,33 @@ class CGStats(ctypes.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
+class ServeRequest(ctypes.Structure):
+    _fields_ = [
+        ("p", ctypes.c_int32 * 3), ("nel", ctypes.c_int32 * 3),
+        ("cps", c_p), ("weights", c_p), ("E", ctypes.c_double),
+        ("nu", ctypes.c_double), ("dirichlet", ctypes.c_uint8 * 18),
+        ("nrhs", ctypes.c_int32), ("rhs", c_p), ("rtol", ctypes.c_double),
+        ("maxit", ctypes.c_int32),
+    ]
+
+
+class ServeResult(ctypes.Structure):
+    _fields_ = [
+        ("status", ctypes.c_int32), ("nrhs", ctypes.c_int32),
+        ("ndof", c_i64), ("iterations", ctypes.c_int32 * 8),
+        ("rel_residual", ctypes.c_double * 8), ("queue_ms", ctypes.c_double),
+        ("solve_ms", ctypes.c_double), ("total_ms", ctypes.c_double),
+    ]
+
+    def as_dict(self):
+        n = self.nrhs
+        return {"status": self.status, "ndof": self.ndof,
+                "iterations": list(self.iterations[:n]),
+                "rel_residual": list(self.rel_residual[:n]),
+                "queue_ms": self.queue_ms, "solve_ms": self.solve_ms,
+                "total_ms": self.total_ms}
+
+
 def _declare(lib):
     vp, i32, i64, dbl = c_p, ctypes.c_int, c_i64, ctypes.c_double
     sig = {
@@ -68,6 +95,12 @@ def _declare(lib):
         "yeti_ctx_set_stream": (i32, [vp, vp]),
         "yeti_ctx_synchronize": (i32, [vp]),
         "yeti_ctx_bytes_in_use": (ctypes.c_size_t, [vp]),
+        "yeti_serve_open": (i32, [i32, ctypes.c_size_t, i32, ctypes.POINTER(vp)]),
+        "yeti_serve_submit": (i32, [vp, ctypes.POINTER(ServeRequest), ctypes.POINTER(i64)]),
+        "yeti_serve_poll": (i32, [vp, i64, vp, ctypes.POINTER(ServeResult)]),
+        "yeti_serve_wait": (i32, [vp, i64, dbl, vp, ctypes.POINTER(ServeResult)]),
+        "yeti_serve_stats": (i32, [vp, vp, vp, vp, vp, vp]),
+        "yeti_serve_close": (i32, [vp]),
         "yeti_assemble_u1_coo": (i32, [vp, ctypes.POINTER(U1Model), i64, vp,
                                        vp, vp, vp, i32]),
         "yeti_wq_setup": (i32, [vp, vp, vp, vp, vp, dbl, dbl, vp, i32,

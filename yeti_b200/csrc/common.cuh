@@ -49,6 +49,9 @@ struct yeti_ctx {
     cudaStream_t own_stream = nullptr;  // stream created by the context
     size_t hbm_budget = 0;              // 0: unbounded
     size_t bytes_in_use = 0;
+    // allocate with cudaMallocAsync / cudaFreeAsync on `stream` (no implicit
+    // device synchronisation; for contexts driven by the serving loop)
+    bool stream_ordered = false;
 };
 
 namespace yeti {

@@ -30,7 +30,8 @@ int dev_alloc(yeti_ctx *ctx, void **ptr, size_t bytes) {
                   ctx->bytes_in_use, bytes, ctx->hbm_budget);
         return YETI_ENOMEM;
     }
-    cudaError_t e = cudaMalloc(ptr, bytes);
+    cudaError_t e = ctx->stream_ordered ? cudaMallocAsync(ptr, bytes, ctx->stream)
+                                        : cudaMalloc(ptr, bytes);
     if (e != cudaSuccess) {
         (void)cudaGetLastError();
         set_error("cudaMalloc of %zu bytes failed: %s", bytes,
@@ -44,7 +45,8 @@ int dev_alloc(yeti_ctx *ctx, void **ptr, size_t bytes) {
 
 void dev_free(yeti_ctx *ctx, void *ptr, size_t bytes) {
     if (!ptr) return;
-    cudaFree(ptr);
+    if (ctx && ctx->stream_ordered) cudaFreeAsync(ptr, ctx->stream);
+    else cudaFree(ptr);
     if (ctx) ctx->bytes_in_use -= (bytes ? bytes : 16);
 }
 

@@ -80,6 +80,37 @@ int wq_stream_setup(yeti_wq_op *op, const WQRule1D R[3]);
 int wq_stream_permute(yeti_wq_op *op);
 template <class T>
 int wq_stream_apply(yeti_wq_op *op, const T *u, T *Ku, const int *done, cudaStream_t s);
+// One FP64 Jacobi-PCG solve of a WQ operator (x0 = 0) that advances in
+// chunks of iterations captured once in a CUDA graph, on its own stream and
+// without host synchronisation: the serving loop launches a chunk, polls its
+// event, and launches the next until the device-side scalars say done.  The
+// workspace is allocated stream-ordered on that stream.
+struct CgSolve {
+    yeti_wq_op *op = nullptr;
+    cudaStream_t stream = nullptr;
+    void *dmem = nullptr;        // b x r z p Ap (6n doubles), partials, scalars
+    void *host_scal = nullptr;   // pinned copy of the scalars (owned by the caller)
+    cudaGraphExec_t chunk = nullptr;
+    cudaEvent_t ev = nullptr;
+    int nblk = 0;
+    bool in_flight = false;
+    int iterations = 0;
+    double rel_residual = 0.0;   // true FP64 residual of the returned x
+    void release();
+    ~CgSolve() { release(); }
+};
+// Bytes of host memory the caller provides as host_scal (pinned).
+size_t cgsolve_scal_bytes();
+int cgsolve_begin(CgSolve &cs, yeti_wq_op *op, cudaStream_t s, void *host_scal,
+                  const double *b_host, double rtol, int maxit);
+// Enqueue the next chunk (graph launch + event).
+int cgsolve_launch(CgSolve &cs);
+// *state: 0 a chunk is in flight, 1 chunk done and more iterations needed,
+// 2 converged or iteration limit, 3 breakdown.
+int cgsolve_poll(CgSolve &cs, int *state);
+// Copy x to the host, compute the true residual, free the workspace.
+int cgsolve_finish(CgSolve &cs, double *x_host);
+
 // YETI_ETIMEDOUT (and clears the flag) if a streaming kernel reported a
 // bounded wait that gave up since the last check; synchronises the stream.
 int wq_stream_check(yeti_wq_op *op);

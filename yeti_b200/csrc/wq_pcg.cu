@@ -563,6 +563,152 @@ static int bi_loop(yeti_wq_op *op, int prec, T *x, T *r, T *rhat, T *p, T *ph,
     return YETI_OK;
 }
 
+// ------------------------------------------- resumable solves (serving loop)
+static int ensure_dinv64(yeti_wq_op *op) {
+    if (op->dinv64.ptr) return YETI_OK;
+    YETI_TRY(op->dinv64.alloc(op->ctx, op->ndof * sizeof(double)));
+    k_dinv<double><<<kRedBlocks, kRedThreads, 0, op->ctx->stream>>>(
+        op->diag.as<double>(), op->dinv64.as<double>(), op->ncp,
+        make_int3(op->n[0], op->n[1], op->n[2]), op->cmask[0], op->cmask[1], op->cmask[2]);
+    count_launches(1);
+    YETI_CUDA(cudaGetLastError());
+    YETI_CUDA(cudaStreamSynchronize(op->ctx->stream));
+    return YETI_OK;
+}
+
+size_t cgsolve_scal_bytes() { return sizeof(CGScal); }
+
+void CgSolve::release() {
+    if (chunk) cudaGraphExecDestroy(chunk);
+    if (ev) cudaEventDestroy(ev);
+    if (dmem) cudaFreeAsync(dmem, stream);
+    chunk = nullptr;
+    ev = nullptr;
+    dmem = nullptr;
+    in_flight = false;
+}
+
+struct SolveView {
+    double *b, *x, *r, *z, *p, *Ap, *parts;
+    CGScal *s;
+};
+
+static SolveView solve_view(const CgSolve &cs) {
+    const int64_t n = cs.op->ndof;
+    double *W = static_cast<double *>(cs.dmem);
+    SolveView v;
+    v.b = W;
+    v.x = W + n;
+    v.r = W + 2 * n;
+    v.z = W + 3 * n;
+    v.p = W + 4 * n;
+    v.Ap = W + 5 * n;
+    v.parts = W + 6 * n;
+    v.s = reinterpret_cast<CGScal *>(W + 6 * n + 2 * cs.nblk);
+    return v;
+}
+
+int cgsolve_begin(CgSolve &cs, yeti_wq_op *op, cudaStream_t st, void *host_scal,
+                  const double *b_host, double rtol, int maxit) {
+    YETI_CHECK(op && host_scal && b_host && op->coef64.ptr, YETI_EINVAL,
+               "cgsolve_begin: missing operator data");
+    YETI_TRY(ensure_dinv64(op));
+    cs.release();
+    cs.op = op;
+    cs.stream = st;
+    cs.host_scal = host_scal;
+    const int64_t n = op->ndof;
+    cs.nblk = (int)std::max<int64_t>(1, std::min<int64_t>(kRedBlocks, (n + kRedThreads - 1) / kRedThreads));
+    const size_t bytes = (6 * n + 2 * (size_t)cs.nblk) * sizeof(double) + 2 * sizeof(CGScal);
+    YETI_CUDA(cudaMallocAsync(&cs.dmem, bytes, st));
+    const SolveView v = solve_view(cs);
+    const double *dinv = op->dinv64.as<double>();
+    const int nb = cs.nblk;
+    YETI_CUDA(cudaMemcpyAsync(v.b, b_host, n * sizeof(double), cudaMemcpyHostToDevice, st));
+    YETI_CUDA(cudaMemsetAsync(v.x, 0, n * sizeof(double), st));
+    YETI_CUDA(cudaMemsetAsync(v.s, 0, sizeof(CGScal), st));
+    k_mask<<<nb, kRedThreads, 0, st>>>(v.b, dinv, n);
+    YETI_CUDA(cudaMemcpyAsync(v.r, v.b, n * sizeof(double), cudaMemcpyDeviceToDevice, st));
+    k_dot<double, double><<<nb, kRedThreads, 0, st>>>(v.b, v.b, n, v.parts, nullptr);
+    k_set_bb<<<1, kRedThreads, 0, st>>>(v.parts, nb, v.s);
+    k_start<double><<<nb, kRedThreads, 0, st>>>(v.r, dinv, v.z, v.p, v.Ap, n, v.parts);
+    k_start_scal<<<1, kRedThreads, 0, st>>>(v.parts, nb, v.s, rtol * rtol, maxit);
+    count_launches(5);
+    YETI_CUDA(cudaGetLastError());
+    // one chunk of iterations, captured once
+    cudaGraph_t g = nullptr;
+    YETI_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+    int rc = YETI_OK;
+    for (int k = 0; k < kChunk && rc == YETI_OK; k++) {
+        rc = wq_apply_dev(op, v.p, v.Ap, YETI_PREC_F64, &v.s->done, st);
+        k_dot<double, double><<<nb, kRedThreads, 0, st>>>(v.p, v.Ap, n, v.parts, &v.s->done);
+        k_alpha<<<1, kRedThreads, 0, st>>>(v.parts, nb, v.s);
+        k_update<double><<<nb, kRedThreads, 0, st>>>(v.x, v.r, v.p, v.Ap, dinv, v.z, n, v.parts, v.s);
+        k_beta<<<1, kRedThreads, 0, st>>>(v.parts, nb, v.s);
+        k_pupdate<double><<<nb, kRedThreads, 0, st>>>(v.p, v.z, v.Ap, n, v.s);
+    }
+    cudaMemcpyAsync(cs.host_scal, v.s, sizeof(CGScal), cudaMemcpyDeviceToHost, st);
+    const cudaError_t ce = cudaStreamEndCapture(st, &g);
+    YETI_TRY(rc);
+    YETI_CUDA(ce);
+    const cudaError_t ie = cudaGraphInstantiate(&cs.chunk, g, 0);
+    cudaGraphDestroy(g);
+    YETI_CUDA(ie);
+    YETI_CUDA(cudaEventCreateWithFlags(&cs.ev, cudaEventDisableTiming));
+    return YETI_OK;
+}
+
+int cgsolve_launch(CgSolve &cs) {
+    YETI_CUDA(cudaGraphLaunch(cs.chunk, cs.stream));
+    YETI_CUDA(cudaEventRecord(cs.ev, cs.stream));
+    count_launches(6 * kChunk);
+    cs.in_flight = true;
+    return YETI_OK;
+}
+
+int cgsolve_poll(CgSolve &cs, int *state) {
+    if (cs.in_flight) {
+        const cudaError_t q = cudaEventQuery(cs.ev);
+        if (q == cudaErrorNotReady) {
+            *state = 0;
+            return YETI_OK;
+        }
+        YETI_CUDA(q);
+        cs.in_flight = false;
+    }
+    const CGScal *h = static_cast<const CGScal *>(cs.host_scal);
+    cs.iterations = h->iter;
+    *state = h->breakdown ? 3 : (h->done ? 2 : 1);
+    return YETI_OK;
+}
+
+int cgsolve_finish(CgSolve &cs, double *x_host) {
+    const SolveView v = solve_view(cs);
+    yeti_wq_op *op = cs.op;
+    const int64_t n = op->ndof;
+    const int nb = cs.nblk;
+    cudaStream_t st = cs.stream;
+    // true residual with the FP64 operator (Ap is free now)
+    YETI_CUDA(cudaMemsetAsync(v.Ap, 0, n * sizeof(double), st));
+    YETI_TRY(wq_apply_dev(op, v.x, v.Ap, YETI_PREC_F64, nullptr, st));
+    k_residual<<<nb, kRedThreads, 0, st>>>(v.b, v.Ap, op->dinv64.as<double>(), v.r, n);
+    k_dot<double, double><<<nb, kRedThreads, 0, st>>>(v.r, v.r, n, v.parts, nullptr);
+    k_dot<double, double><<<nb, kRedThreads, 0, st>>>(v.b, v.b, n, v.parts + nb, nullptr);
+    count_launches(3);
+    std::vector<double> hp(2 * (size_t)nb);
+    YETI_CUDA(cudaMemcpyAsync(hp.data(), v.parts, hp.size() * sizeof(double), cudaMemcpyDeviceToHost, st));
+    YETI_CUDA(cudaMemcpyAsync(x_host, v.x, n * sizeof(double), cudaMemcpyDeviceToHost, st));
+    YETI_CUDA(cudaStreamSynchronize(st));
+    double rr = 0.0, bb = 0.0;
+    for (int i = 0; i < nb; i++) {
+        rr += hp[i];
+        bb += hp[nb + i];
+    }
+    cs.rel_residual = bb > 0 ? std::sqrt(rr / bb) : 0.0;
+    cs.release();
+    return YETI_OK;
+}
+
 // Host sum of device partials (fixed order).
 static int host_sum(yeti_wq_op *op, const double *parts, int n, int stride,
                     int off, double *out, bool take_max = false) {
