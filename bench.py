@@ -50,10 +50,12 @@ def parse():
     ap.add_argument("--rtol", type=float, default=1e-9)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--serve-requests", type=int, default=2000)
-    ap.add_argument("--serve-rate", type=float, default=100.0,
+    ap.add_argument("--serve-rate", type=float, default=25.0,
                     help="Poisson arrival rate of the serving stream (requests/s)")
     ap.add_argument("--serve-budget-gb", type=float, default=32.0)
     ap.add_argument("--no-serve", action="store_true")
+    ap.add_argument("--no-extra", action="store_true",
+                    help="skip the assembly, gradient and p=4 block measurements")
     return ap.parse_args()
 
 
@@ -220,7 +222,7 @@ def serve_stream(args, device):
     from yeti_b200.serve import Server, run_stream, synthetic_requests
     reqs = synthetic_requests(args.serve_requests, seed=WORKLOAD["seed"] + 7)
     budget = int(args.serve_budget_gb * (1 << 30))
-    with Server(device=device, hbm_budget_bytes=budget, max_active=64) as srv:
+    with Server(device=device, hbm_budget_bytes=budget, max_active=128) as srv:
         out = run_stream(srv, reqs, args.serve_rate, seed=WORKLOAD["seed"] + 8, rtol=1e-8)
         st = srv.stats()
     lat = out["latency_ms"]
@@ -232,8 +234,107 @@ def serve_stream(args, device):
             "p99_ms": float(np.percentile(lat, 99)) if len(lat) else None,
             "solved_dof_per_s": out["solved_dofs"] / out["wall_s"],
             "cg_iterations_total": int(sum(its)), "peak_active": st["peak_active"],
-            "max_active": 64, "hbm_budget_bytes": budget, "rtol": 1e-8,
+            "max_active": 128, "hbm_budget_bytes": budget, "rtol": 1e-8,
             "precision": "FP64 operator and Krylov vectors"}
+
+
+def _median_ms(fn, reps, sync):
+    ts = []
+    for _ in range(reps):
+        sync()
+        t0 = time.perf_counter()
+        fn()
+        sync()
+        ts.append((time.perf_counter() - t0) * 1e3)
+    return float(np.median(ts))
+
+
+def _system_args(name):
+    from yeti_b200.stiffmtrx_elemstorage import SYSTEM_ARG_NAMES
+    d = np.load(os.path.join(ROOT, "tests", "golden", f"{name}.npz"))
+    return [d[k] if d[k].ndim else d[k][()] for k in SYSTEM_ARG_NAMES]
+
+
+def extra_configs(args, device):
+    """The other configurations of the path, each beside its CPU oracle:
+    U1 Gauss assembly of the p=2 16x4x4 cantilever (COO), the compliance
+    shape gradient of the p=2 32x32x2 quarter annulus, and the p=4
+    128x128x32 WQ block (200 FP32 applies and a mixed solve)."""
+    import torch
+    import oracle
+    from yeti_b200.gradient import grad_from_system_args, _solve
+    from yeti_b200.patches import cube_patch
+    from yeti_b200.stiffmtrx_elemstorage import sys_linmat_lindef_static
+    from yeti_b200.wq import WQElasticity
+    sync = torch.cuda.synchronize
+    out = {}
+    # C1: assembly (parity: bit-identical COO and F)
+    a1 = _system_args("cantilever_p2_16x4x4")
+    sys_linmat_lindef_static(*a1, device_out=True)
+    t_gpu = _median_ms(lambda: sys_linmat_lindef_static(*a1, device_out=True), 20, sync)
+    t_gpu_host = _median_ms(lambda: sys_linmat_lindef_static(*a1), 10, sync)
+    kd, kr, kc, F = sys_linmat_lindef_static(*a1)
+    t0 = time.perf_counter()
+    ko, _, _, Fo = oracle.sys_linmat_lindef_static(*a1)
+    t_cpu = (time.perf_counter() - t0) * 1e3
+    out["assembly_p2_16x4x4"] = {
+        "nb_data": int(kd.size), "gpu_ms_device_out": t_gpu, "gpu_ms_host_buffers": t_gpu_host,
+        "cpu_oracle_ms": t_cpu, "cpu_cores": 1,
+        "bit_identical": bool(np.array_equal(kd, ko) and np.array_equal(F, Fo))}
+    # C3: shape gradient (adjoint kernel; parity vs the CPU oracle)
+    a3 = _system_args("quarter_annulus_p2_32x32x2")
+    U, _ = _solve(a3, np.asarray(a3[2], dtype=np.float64))
+    sol = U.reshape(-1, 3).T
+    adj = 0.5 * sol[None]
+    grad_from_system_args(a3, sol, adj)
+    t_g = _median_ms(lambda: grad_from_system_args(a3, sol, adj), 5, sync)
+    gi, ge = grad_from_system_args(a3, sol, adj)
+    t0 = time.perf_counter()
+    oi, oe = oracle.grad_lin_elast_work(a3, sol, adj)
+    t_go = (time.perf_counter() - t0) * 1e3
+    ref = np.concatenate([oi.ravel(), oe.ravel()])
+    got = np.concatenate([gi.ravel(), ge.ravel()])
+    out["gradient_p2_32x32x2"] = {
+        "nb_cp": int(sol.shape[1]), "gpu_ms_host_buffers": t_g, "cpu_oracle_ms": t_go,
+        "cpu_cores": 1, "max_rel_diff_vs_oracle": float(np.abs(got - ref).max() / np.abs(ref).max())}
+    # C5: p=4 128x128x32 WQ block
+    P = cube_patch((128, 128, 32), 4, size=(4.0, 4.0, 1.0), perturb=0.1, wrange=(0.8, 1.2),
+                   seed=WORKLOAD["seed"] + 5)
+    op = WQElasticity(P, 1.0, 0.3, {"w0": (0, 1, 2)}, precisions="both")
+    dev = torch.device("cuda", device)
+    u32 = torch.randn(op.ndof, dtype=torch.float32, device=dev)
+    k32 = torch.empty_like(u32)
+    for _ in range(3):
+        op.apply_device(u32, k32, "f32")
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(200):
+        op.apply_device(u32, k32, "f32")
+    e1.record()
+    sync()
+    t_app = e0.elapsed_time(e1) / 200 / 1e3
+    alg = op.nqp * 45 * 4 + 2 * op.ndof * 4
+    peak, kind = measured_peaks()
+    b = torch.from_numpy(op.eval_bodyforce_vector([0.0, 0.0, -1.0])).to(dev)
+    xref, st_ref = op.pcg(b, rtol=1e-12, maxit=50000)
+    sync()
+    t0 = time.perf_counter()
+    x, st = op.pcg(b, rtol=1e-8, mixed=True, maxit=50000)
+    sync()
+    t_solve = time.perf_counter() - t0
+    err = (torch.linalg.norm(x - xref) / torch.linalg.norm(xref)).item()
+    out["wq_p4_128x128x32"] = {
+        "ndof": op.ndof, "nqp": op.nqp, "apply_f32_us": t_app * 1e6,
+        "achieved_gbs": alg / t_app / 1e9, "peak_gbs": peak, "frac": alg / t_app / 1e9 / peak,
+        "peak_kind": peak_kind_note(kind), "mixed_solve_s": t_solve,
+        "iterations": st["iterations"], "rel_residual": st["rel_residual"],
+        "rel_error_vs_fp64": err, "fp64_ref_rel_residual": st_ref["rel_residual"]}
+    del op
+    return out
+
+
+def peak_kind_note(kind):
+    return "of measured" if kind == "measured" else "of fallback"
 
 
 # Iterations of the FP64 Jacobi-PCG on the default workload (measured on a
@@ -356,6 +457,9 @@ def main():
     serve = None
     if not args.no_serve and args.serve_requests > 0:
         serve = serve_stream(args, local)
+    extra = None
+    if rank == 0 and ws == 1 and not args.no_extra:
+        extra = extra_configs(args, local)
 
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
@@ -401,6 +505,7 @@ def main():
             "cpu_baseline": cpu,
             "clocks": clk,
             "serve": serve,
+            "other_configs": extra,
         }
         print(json.dumps(line), flush=True)
     if ws > 1:

@@ -9,15 +9,7 @@ if ROOT not in sys.path:
     sys.path.insert(0, ROOT)
 GOLDEN = os.path.join(ROOT, "tests", "golden")
 
-SYSTEM_ARG_NAMES = [
-    "activeElement", "nb_data", "COORDS3D", "IEN", "nb_elem_patch", "Nkv",
-    "Ukv", "Nijk", "weight", "Jpqr", "ELT_TYPE", "PROPS", "JPROPS",
-    "MATERIAL_PROPERTIES", "n_mat_props", "RHO", "TENSOR", "indDLoad",
-    "JDLType", "ADLMAG", "load_target_nbelem", "load_additionalInfos",
-    "nb_load_additionalInfos", "bc_values", "bc_target", "bc_target_nbelem",
-    "ind_dof_free", "nb_dof_free", "MCRD", "NBINT", "NNODE", "nodal_dist",
-    "nb_bc", "nb_load", "nb_patch", "nb_elem", "nb_cp", "nb_dof_tot",
-]
+from yeti_b200.stiffmtrx_elemstorage import SYSTEM_ARG_NAMES  # noqa: E402
 
 
 def pytest_configure(config):

@@ -36,7 +36,7 @@ namespace yeti {
 namespace {
 
 constexpr int kMaxRhs = 8;
-constexpr int kStreams = 32;
+constexpr int kStreams = 64;
 
 double now_ms() {
     using namespace std::chrono;

@@ -13,7 +13,20 @@ import numpy as np
 from . import _lib
 from ._lib import MEM_DEVICE, MEM_HOST, U1Model, check, lib, ptr
 
-__all__ = ["sys_linmat_lindef_static", "pack_u1_model"]
+__all__ = ["sys_linmat_lindef_static", "pack_u1_model", "SYSTEM_ARG_NAMES"]
+
+# The 38 positional arguments, in the order of
+# IGAparametrization.get_inputs4system_elemStorage()
+# (IGA_parametrization.py:1705-1716).
+SYSTEM_ARG_NAMES = [
+    "activeElement", "nb_data", "COORDS3D", "IEN", "nb_elem_patch", "Nkv",
+    "Ukv", "Nijk", "weight", "Jpqr", "ELT_TYPE", "PROPS", "JPROPS",
+    "MATERIAL_PROPERTIES", "n_mat_props", "RHO", "TENSOR", "indDLoad",
+    "JDLType", "ADLMAG", "load_target_nbelem", "load_additionalInfos",
+    "nb_load_additionalInfos", "bc_values", "bc_target", "bc_target_nbelem",
+    "ind_dof_free", "nb_dof_free", "MCRD", "NBINT", "NNODE", "nodal_dist",
+    "nb_bc", "nb_load", "nb_patch", "nb_elem", "nb_cp", "nb_dof_tot",
+]
 
 
 def _i64(a):
