@@ -3,6 +3,12 @@ single NURBS patch.
 
 TEST INFRASTRUCTURE ONLY (see oracle/__init__.py).
 
+Parity unpinned: the reference has no elastic WQ operator to compare with;
+the 1-D rules used here are pinned to the reference's Python twin
+(tests/golden/wq_rules.npz), and the operator is checked for exactness on
+affine patches, against a dense direct solve and against the reference's
+rank-one algorithm (oracle/oracle_wq.c) in tests/test_wq.py.
+
 The reference ships the WQ matrix-free operator for the scalar (thermal)
 problem only, with B-spline geometry:
   * K u = sum_{k,l} W^{(k,l)} (coef_kl * (B^{(l)})^T u)
