@@ -24,7 +24,22 @@ constexpr int kChunk = 16;          // iterations enqueued per host check
 struct CGScal {
     double rz, pAp, alpha, beta, rr, bb, tol2, scale;
     int done, iter, breakdown, maxit;
+    unsigned int ticket;   // blocks of a fused reduction that have finished
 };
+
+// Last-block-done: every block publishes its partials, then takes a ticket;
+// the block that takes the last one sees all partials (fixed summation
+// order, so the result does not depend on block timing) and resets the
+// ticket for the next reduction.
+__device__ __forceinline__ bool last_block(unsigned int *ticket) {
+    __shared__ bool last;
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) last = atomicAdd(ticket, 1u) == gridDim.x - 1;
+    __syncthreads();
+    if (last) __threadfence();
+    return last;
+}
 
 __device__ __forceinline__ double block_sum(double v, double *sh) {
     for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
@@ -87,11 +102,37 @@ k_absmax(const A *a, int64_t n, double *parts) {
     if (threadIdx.x == 0) parts[blockIdx.x] = v;
 }
 
-__global__ void k_alpha(const double *parts, int nparts, CGScal *s) {
+// p = z + beta p; Ap = 0
+template <class T>
+__global__ void __launch_bounds__(kRedThreads)
+k_pupdate(T *p, const T *z, T *Ap, int64_t n, const CGScal *s) {
+    if (s->done) return;
+    const T b = (T)s->beta;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        p[i] = z[i] + b * p[i];
+        Ap[i] = T(0);
+    }
+}
+
+// p.Ap partials, then (last block) alpha = rz / p.Ap
+template <class T>
+__global__ void __launch_bounds__(kRedThreads)
+k_dot_alpha(const T *p, const T *Ap, int64_t n, double *parts, CGScal *s) {
     __shared__ double sh[32];
     if (s->done) return;
-    const double pAp = sum_parts(parts, nparts, 1, 0, sh);
+    double v = 0.0;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x)
+        v += (double)p[i] * (double)Ap[i];
+    v = block_sum(v, sh);
+    if (threadIdx.x == 0) __stcg(&parts[blockIdx.x], v);
+    if (!last_block(&s->ticket)) return;
+    double pAp = 0.0;
+    for (int i = threadIdx.x; i < (int)gridDim.x; i += blockDim.x) pAp += __ldcg(&parts[i]);
+    pAp = block_sum(pAp, sh);
     if (threadIdx.x == 0) {
+        s->ticket = 0;
         s->pAp = pAp;
         if (!(pAp > 0.0) || !isfinite(pAp)) {
             s->breakdown = 1;
@@ -102,11 +143,11 @@ __global__ void k_alpha(const double *parts, int nparts, CGScal *s) {
     }
 }
 
-// x += a p; r -= a Ap; z = dinv r; partials of r.z and r.r
+// x += a p; r -= a Ap; z = dinv r; then (last block) beta, rz, rr, stop test
 template <class T>
 __global__ void __launch_bounds__(kRedThreads)
-k_update(T *x, T *r, const T *p, const T *Ap, const T *dinv, T *z, int64_t n,
-         double *parts, const CGScal *s) {
+k_update_beta(T *x, T *r, const T *p, const T *Ap, const T *dinv, T *z, int64_t n,
+              double *parts, CGScal *s) {
     __shared__ double sh[32];
     if (s->done) return;
     const T a = (T)s->alpha;
@@ -124,40 +165,29 @@ k_update(T *x, T *r, const T *p, const T *Ap, const T *dinv, T *z, int64_t n,
     rz = block_sum(rz, sh);
     rr = block_sum(rr, sh);
     if (threadIdx.x == 0) {
-        parts[2 * blockIdx.x] = rz;
-        parts[2 * blockIdx.x + 1] = rr;
+        __stcg(&parts[2 * blockIdx.x], rz);
+        __stcg(&parts[2 * blockIdx.x + 1], rr);
     }
-}
-
-__global__ void k_beta(const double *parts, int nparts, CGScal *s) {
-    __shared__ double sh[32];
-    if (s->done) return;
-    const double rz = sum_parts(parts, nparts, 2, 0, sh);
-    const double rr = sum_parts(parts, nparts, 2, 1, sh);
+    if (!last_block(&s->ticket)) return;
+    double srz = 0.0, srr = 0.0;
+    for (int i = threadIdx.x; i < (int)gridDim.x; i += blockDim.x) {
+        srz += __ldcg(&parts[2 * i]);
+        srr += __ldcg(&parts[2 * i + 1]);
+    }
+    srz = block_sum(srz, sh);
+    srr = block_sum(srr, sh);
     if (threadIdx.x == 0) {
+        s->ticket = 0;
         s->iter += 1;
-        s->rr = rr;
-        s->beta = rz / s->rz;
-        s->rz = rz;
-        if (!isfinite(rr)) {
+        s->rr = srr;
+        s->beta = srz / s->rz;
+        s->rz = srz;
+        if (!isfinite(srr)) {
             s->breakdown = 1;
             s->done = 1;
-        } else if (rr <= s->tol2 || s->iter >= s->maxit) {
+        } else if (srr <= s->tol2 || s->iter >= s->maxit) {
             s->done = 1;
         }
-    }
-}
-
-// p = z + beta p; Ap = 0
-template <class T>
-__global__ void __launch_bounds__(kRedThreads)
-k_pupdate(T *p, const T *z, T *Ap, int64_t n, const CGScal *s) {
-    if (s->done) return;
-    const T b = (T)s->beta;
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
-         i += (int64_t)gridDim.x * blockDim.x) {
-        p[i] = z[i] + b * p[i];
-        Ap[i] = T(0);
     }
 }
 
@@ -510,12 +540,10 @@ static int cg_chunk(yeti_wq_op *op, int prec, T *x, T *r, T *z, T *p, T *Ap,
     double *parts = op->parts.as<double>();
     for (int k = 0; k < kChunk; k++) {
         YETI_TRY(wq_apply_dev(op, p, Ap, prec, &ds->done, s));
-        k_dot<T, T><<<kRedBlocks, kRedThreads, 0, s>>>(p, Ap, n, parts, &ds->done);
-        k_alpha<<<1, kRedThreads, 0, s>>>(parts, kRedBlocks, ds);
-        k_update<T><<<kRedBlocks, kRedThreads, 0, s>>>(x, r, p, Ap, dinv, z, n, parts, ds);
-        k_beta<<<1, kRedThreads, 0, s>>>(parts, kRedBlocks, ds);
+        k_dot_alpha<T><<<kRedBlocks, kRedThreads, 0, s>>>(p, Ap, n, parts, ds);
+        k_update_beta<T><<<kRedBlocks, kRedThreads, 0, s>>>(x, r, p, Ap, dinv, z, n, parts, ds);
         k_pupdate<T><<<kRedBlocks, kRedThreads, 0, s>>>(p, z, Ap, n, ds);
-        count_launches(5);
+        count_launches(3);
     }
     YETI_CUDA(cudaGetLastError());
     return YETI_OK;
@@ -641,10 +669,9 @@ int cgsolve_begin(CgSolve &cs, yeti_wq_op *op, cudaStream_t st, void *host_scal,
     int rc = YETI_OK;
     for (int k = 0; k < kChunk && rc == YETI_OK; k++) {
         rc = wq_apply_dev(op, v.p, v.Ap, YETI_PREC_F64, &v.s->done, st);
-        k_dot<double, double><<<nb, kRedThreads, 0, st>>>(v.p, v.Ap, n, v.parts, &v.s->done);
-        k_alpha<<<1, kRedThreads, 0, st>>>(v.parts, nb, v.s);
-        k_update<double><<<nb, kRedThreads, 0, st>>>(v.x, v.r, v.p, v.Ap, dinv, v.z, n, v.parts, v.s);
-        k_beta<<<1, kRedThreads, 0, st>>>(v.parts, nb, v.s);
+        k_dot_alpha<double><<<nb, kRedThreads, 0, st>>>(v.p, v.Ap, n, v.parts, v.s);
+        k_update_beta<double><<<nb, kRedThreads, 0, st>>>(v.x, v.r, v.p, v.Ap, dinv, v.z, n,
+                                                          v.parts, v.s);
         k_pupdate<double><<<nb, kRedThreads, 0, st>>>(v.p, v.z, v.Ap, n, v.s);
     }
     cudaMemcpyAsync(cs.host_scal, v.s, sizeof(CGScal), cudaMemcpyDeviceToHost, st);
@@ -661,7 +688,7 @@ int cgsolve_begin(CgSolve &cs, yeti_wq_op *op, cudaStream_t st, void *host_scal,
 int cgsolve_launch(CgSolve &cs) {
     YETI_CUDA(cudaGraphLaunch(cs.chunk, cs.stream));
     YETI_CUDA(cudaEventRecord(cs.ev, cs.stream));
-    count_launches(6 * kChunk);
+    count_launches(4 * kChunk);
     cs.in_flight = true;
     return YETI_OK;
 }
