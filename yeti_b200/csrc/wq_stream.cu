@@ -472,7 +472,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_wq_apply_stream(StreamArgs<T> a
         for (int cc = 0; cc < CPT; cc++)
 #pragma unroll
             for (int m = 0; m < P; m++) x[cc][m] = load_x(cc, sg.y + m);
-        {
+        if (!kStaged) {
             const char *p0 = reinterpret_cast<const char *>(coef_t + (int64_t)a.wq0[sg.y] * pstride);
             for (int off = tid * 128; off < pbytes; off += kThreads * 128) prefetch_l2(p0 + off);
         }
@@ -486,7 +486,9 @@ __global__ void __launch_bounds__(kThreads, 2) k_wq_apply_stream(StreamArgs<T> a
             const int qw_end = a.wq0[e + 1];
             for (int qw = a.wq0[e]; qw < qw_end; qw++) {
                 const T *bw = a.band[2] + (size_t)qw * 6 * PBP;
-                if (qw + 1 < a.nqw) {
+                if (!kStaged && qw + 1 < a.nqw) {
+                    // FP64 reads the coefficients straight from HBM: prefetch
+                    // the next plane into L2 (FP32 stages it with a bulk copy)
                     const char *pn = reinterpret_cast<const char *>(coef_t + (int64_t)(qw + 1) * pstride);
                     for (int off = tid * 128; off < pbytes; off += kThreads * 128) prefetch_l2(pn + off);
                 }
