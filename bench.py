@@ -234,6 +234,8 @@ def serve_stream(args, device):
             "p99_ms": float(np.percentile(lat, 99)) if len(lat) else None,
             "solved_dof_per_s": out["solved_dofs"] / out["wall_s"],
             "cg_iterations_total": int(sum(its)), "peak_active": st["peak_active"],
+            "thread_ms": {"setup": st["setup_ms"], "retire": st["retire_ms"],
+                          "poll": st["poll_ms"]},
             "max_active": 128, "hbm_budget_bytes": budget, "rtol": 1e-8,
             "precision": "FP64 operator and Krylov vectors"}
 

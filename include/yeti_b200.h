@@ -266,7 +266,12 @@ int yeti_serve_wait(yeti_server *srv, int64_t ticket, double timeout_ms,
 int yeti_serve_stats(yeti_server *srv, int64_t *done, int64_t *queued,
                      int32_t *active, int32_t *peak_active,
                      size_t *committed_bytes);
-/* Finishes the active requests, fails the queued ones, joins the thread. */
+/* Cumulative thread time (ms): worker threads in operator setups and solve
+ * starts, worker threads in retirements (solution copies, frees), the engine
+ * thread in polling and relaunching chunks. */
+int yeti_serve_times(yeti_server *srv, double *setup_ms, double *retire_ms,
+                     double *poll_ms);
+/* Finishes the active requests, fails the queued ones, joins the threads. */
 int yeti_serve_close(yeti_server *srv);
 
 #ifdef __cplusplus

@@ -100,6 +100,7 @@ def _declare(lib):
         "yeti_serve_poll": (i32, [vp, i64, vp, ctypes.POINTER(ServeResult)]),
         "yeti_serve_wait": (i32, [vp, i64, dbl, vp, ctypes.POINTER(ServeResult)]),
         "yeti_serve_stats": (i32, [vp, vp, vp, vp, vp, vp]),
+        "yeti_serve_times": (i32, [vp, vp, vp, vp]),
         "yeti_serve_close": (i32, [vp]),
         "yeti_assemble_u1_coo": (i32, [vp, ctypes.POINTER(U1Model), i64, vp,
                                        vp, vp, vp, i32]),

@@ -1,6 +1,7 @@
 // Shared definitions of the yeti_b200 library (host + device).
 #pragma once
 #include <cuda_runtime.h>
+#include <atomic>
 #include <cstdint>
 #include <cstdio>
 #include <string>
@@ -48,7 +49,7 @@ struct yeti_ctx {
     cudaStream_t stream = nullptr;      // stream all work goes to
     cudaStream_t own_stream = nullptr;  // stream created by the context
     size_t hbm_budget = 0;              // 0: unbounded
-    size_t bytes_in_use = 0;
+    std::atomic<size_t> bytes_in_use{0};
     // allocate with cudaMallocAsync / cudaFreeAsync on `stream` (no implicit
     // device synchronisation; for contexts driven by the serving loop)
     bool stream_ordered = false;

@@ -27,7 +27,7 @@ int dev_alloc(yeti_ctx *ctx, void **ptr, size_t bytes) {
     if (bytes == 0) bytes = 16;
     if (ctx->hbm_budget && ctx->bytes_in_use + bytes > ctx->hbm_budget) {
         set_error("HBM budget exceeded: %zu in use + %zu requested > %zu",
-                  ctx->bytes_in_use, bytes, ctx->hbm_budget);
+                  ctx->bytes_in_use.load(), bytes, ctx->hbm_budget);
         return YETI_ENOMEM;
     }
     cudaError_t e = ctx->stream_ordered ? cudaMallocAsync(ptr, bytes, ctx->stream)
@@ -124,5 +124,5 @@ YETI_API int yeti_ctx_synchronize(yeti_ctx *ctx) {
 }
 
 YETI_API size_t yeti_ctx_bytes_in_use(const yeti_ctx *ctx) {
-    return ctx ? ctx->bytes_in_use : 0;
+    return ctx ? ctx->bytes_in_use.load() : 0;
 }

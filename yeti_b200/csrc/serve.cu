@@ -2,22 +2,28 @@
 //
 // No counterpart in the reference (YETI solves one model per Python call).
 // Requests (a patch of any degree 2..5 and element counts, material, clamps,
-// 1..8 right-hand sides) are queued by yeti_serve_submit and taken by one
-// engine thread that owns a private context:
-//   admission  in arrival order, while the number of active requests is
-//              below the slot count and the estimated device bytes of the
-//              request fit in the HBM budget next to the active ones;
-//   setup      the WQ operator on the device (yeti_wq_setup, FP64 data);
-//   solve      one resumable FP64 Jacobi-PCG per right-hand side
-//              (CgSolve), each on a stream of the pool, advancing in chunks
-//              of iterations captured in a CUDA graph, so that the solves of
-//              all active requests overlap on the device; the engine polls
-//              chunk events and relaunches until converged;
-//   retire     results copied to the request, operator and workspaces
-//              freed (stream-ordered, no device-wide synchronisation),
-//              budget released, waiters notified.
-// Operators, Krylov vectors and scalars stay on the device for the life of a
-// request; the host only sees one small scalar copy per chunk.
+// 1..8 right-hand sides) are queued by yeti_serve_submit.  One engine thread
+// and a pool of worker threads serve them:
+//   admission  (engine) in arrival order, while the number of active
+//              requests is below the slot count and the estimated device
+//              bytes of the request fit in the HBM budget next to the active
+//              ones;
+//   setup      (worker) the WQ operator on the device (yeti_wq_setup, FP64
+//              data) and the start of one resumable FP64 Jacobi-PCG per
+//              right-hand side (CgSolve) on a stream of the pool;
+//   solve      (engine) the solves advance in chunks of iterations captured
+//              in a CUDA graph, so that the solves of all active requests
+//              overlap on the device; the engine polls chunk events and
+//              relaunches until converged;
+//   retire     (worker) solutions and true residuals copied out, operator
+//              and workspaces freed (stream-ordered, no device-wide
+//              synchronisation), budget released, waiters notified.
+// Setups and retirements wait for host copies; on the engine thread they
+// stalled the relaunch of every other request's chunks (measured: 30 ms per
+// setup under load against 2 ms alone), so they run on the workers, each with
+// its own context and a high-priority stream; the solve streams have the low
+// priority.  Operators, Krylov vectors and scalars stay on the device for the
+// life of a request; the host only sees one small scalar copy per chunk.
 #include <algorithm>
 #include <chrono>
 #include <condition_variable>
@@ -54,7 +60,8 @@ struct Request {
     size_t est = 0;
     yeti_wq_op *op = nullptr;
     std::vector<std::unique_ptr<CgSolve>> solves;
-    std::vector<int> finished;
+    std::vector<int> finished;   // per right-hand side: 0 running, 2 done, 3 breakdown
+    int fail = YETI_OK;          // an error of the engine's polls
     std::vector<double> x;
     int iters[kMaxRhs] = {};
     double rel[kMaxRhs] = {};
@@ -83,43 +90,53 @@ size_t estimate_bytes(const Request &r) {
 using namespace yeti;
 
 struct yeti_server {
-    yeti_ctx *ctx = nullptr;
+    yeti_ctx *ctx = nullptr;           // the engine's context
     size_t budget = 0;
     int max_active = 0;
-    std::mutex mu;
-    std::condition_variable cv_work;   // new requests / stop
-    std::condition_variable cv_done;   // finished requests
-    std::deque<Request *> queue;
+    std::mutex mu;                     // everything below except `active`
+    std::condition_variable cv_work;   // engine: new requests, ready solves, stop
+    std::condition_variable cv_task;   // workers: new tasks, stop
+    std::condition_variable cv_done;   // callers: finished requests
+    std::deque<Request *> queue;       // submitted, not admitted
+    std::deque<std::pair<int, Request *>> tasks;   // (0 setup | 1 retire, request)
+    std::vector<Request *> ready;      // set up, first chunks launched
     std::map<int64_t, std::unique_ptr<Request>> reqs;
     std::vector<Request *> active;     // engine thread only
-    std::vector<cudaStream_t> streams;
+    std::vector<cudaStream_t> streams; // solve streams (low priority)
     void *pinned = nullptr;            // scalar slots of the CG solves
     std::vector<void *> free_slots;
+    std::vector<yeti_ctx *> wctx;      // one context per worker (high-priority stream)
+    // one stream per worker that only its worker uses, and only to capture
+    // chunk graphs: no other thread enqueues into it (work enqueued into a
+    // capturing stream would join the capture)
+    std::vector<cudaStream_t> wcap;
+    std::vector<std::thread> workers;
     int64_t next_ticket = 1;
     size_t committed = 0;
     int64_t n_done = 0;
     int n_active = 0, peak_active = 0;
     int rr = 0;
-    bool stop = false;
+    // worker time in setups and retirements, engine time in polls (ms)
+    double t_setup_ms = 0, t_retire_ms = 0, t_poll_ms = 0;
+    bool stop = false, stop_workers = false;
     std::thread engine;
 
+    // Release everything a request holds and publish its result (workers).
     void finish(Request *r, int status, const std::string &err) {
-        for (size_t k = 0; k < r->solves.size(); k++) {
-            CgSolve *s = r->solves[k].get();
-            if (!s) continue;
-            // a failed request may still have chunks in flight: let them
-            // end before the operator they read is freed
-            if (s->in_flight) cudaEventSynchronize(s->ev);
-            if (s->host_scal) free_slots.push_back(s->host_scal);
-            s->host_scal = nullptr;
-            s->release();
+        for (auto &cs : r->solves) {
+            // a failed request may still have chunks in flight: let them end
+            // before the operator they read is freed
+            if (cs->in_flight) cudaEventSynchronize(cs->ev);
+            cs->release();
         }
-        r->solves.clear();
         if (r->op) {
             yeti_wq_destroy(r->op);
             r->op = nullptr;
         }
         std::lock_guard<std::mutex> lk(mu);
+        for (auto &cs : r->solves)
+            if (cs->host_scal) free_slots.push_back(cs->host_scal);
+        r->solves.clear();
         r->status = status;
         r->err = err;
         r->t_done = now_ms();
@@ -127,18 +144,19 @@ struct yeti_server {
         n_active--;
         n_done++;
         cv_done.notify_all();
+        cv_work.notify_one();   // a slot and budget are free again
     }
 
-    // setup of the operator and start of the solves; false on failure
-    // (the request is finished with an error)
-    bool start(Request *r) {
+    // Worker: operator setup and start of the solves; the request then goes
+    // to the engine through `ready`.
+    void setup(Request *r, yeti_ctx *wc, cudaStream_t cap) {
         r->t_admit = now_ms();
         yeti_wq_op *op = nullptr;
-        int rc = yeti_wq_setup(ctx, r->p, r->nel, r->cps.data(), r->weights.data(), r->E, r->nu,
+        int rc = yeti_wq_setup(wc, r->p, r->nel, r->cps.data(), r->weights.data(), r->E, r->nu,
                                r->dir, YETI_WQ_F64, &op);
         if (rc != YETI_OK) {
             finish(r, rc, yeti_last_error());
-            return false;
+            return;
         }
         r->op = op;
         r->ndof = op->ndof;
@@ -146,24 +164,68 @@ struct yeti_server {
         r->finished.assign(r->nrhs, 0);
         for (int k = 0; k < r->nrhs; k++) {
             std::unique_ptr<CgSolve> cs(new CgSolve());
-            void *slot = free_slots.back();
-            free_slots.pop_back();
-            cudaStream_t st = streams[rr++ % kStreams];
-            rc = cgsolve_begin(*cs, op, st, slot, r->rhs.data() + (size_t)k * r->ndof, r->rtol,
-                               r->maxit);
-            if (rc == YETI_OK) rc = cgsolve_launch(*cs);
-            if (rc != YETI_OK) {
-                free_slots.push_back(slot);
-                cs->release();
-                finish(r, rc, yeti_last_error());
-                return false;
+            void *slot;
+            cudaStream_t st;
+            {
+                std::lock_guard<std::mutex> lk(mu);
+                slot = free_slots.back();
+                free_slots.pop_back();
+                st = streams[rr++ % (int)streams.size()];
             }
+            rc = cgsolve_begin(*cs, op, st, slot, r->rhs.data() + (size_t)k * r->ndof, r->rtol,
+                               r->maxit, cap);
+            cs->host_scal = slot;   // returned by finish whatever happened
+            if (rc == YETI_OK) rc = cgsolve_launch(*cs);
             r->solves.push_back(std::move(cs));
+            if (rc != YETI_OK) {
+                finish(r, rc, yeti_last_error());
+                return;
+            }
         }
-        return true;
+        std::lock_guard<std::mutex> lk(mu);
+        ready.push_back(r);
+        cv_work.notify_one();
     }
 
-    // poll the solves of a request; true when all are finished
+    // Worker: copy the solutions out and retire the request.
+    void retire(Request *r, yeti_ctx *wc) {
+        int rc = r->fail;
+        bool broke = false;
+        for (int k = 0; k < r->nrhs && rc == YETI_OK; k++) {
+            CgSolve &cs = *r->solves[k];
+            r->iters[k] = cs.iterations;
+            rc = cgsolve_finish(cs, r->x.data() + (size_t)k * r->ndof, wc->stream);
+            r->rel[k] = cs.rel_residual;
+            broke = broke || r->finished[k] == 3;
+        }
+        if (rc == YETI_OK && broke) {
+            rc = YETI_EBREAKDOWN;
+            set_error("serving: Krylov breakdown");
+        }
+        finish(r, rc, rc == YETI_OK ? std::string() : std::string(yeti_last_error()));
+    }
+
+    void work(int w) {
+        cudaSetDevice(ctx->device);
+        for (;;) {
+            std::pair<int, Request *> t;
+            {
+                std::unique_lock<std::mutex> lk(mu);
+                cv_task.wait(lk, [&] { return stop_workers || !tasks.empty(); });
+                if (tasks.empty()) return;
+                t = tasks.front();
+                tasks.pop_front();
+            }
+            const double t0 = now_ms();
+            if (t.first == 0) setup(t.second, wctx[w], wcap[w]);
+            else retire(t.second, wctx[w]);
+            std::lock_guard<std::mutex> lk(mu);
+            (t.first == 0 ? t_setup_ms : t_retire_ms) += now_ms() - t0;
+        }
+    }
+
+    // Engine: poll the solves of a request, relaunch chunks; true when every
+    // right-hand side is finished (or an error occurred).
     bool progress(Request *r, bool &moved) {
         int left = 0;
         for (int k = 0; k < r->nrhs; k++) {
@@ -175,48 +237,39 @@ struct yeti_server {
                 rc = cgsolve_launch(cs);
                 moved = true;
             } else if (rc == YETI_OK && state >= 2) {
-                r->iters[k] = cs.iterations;
-                rc = cgsolve_finish(cs, r->x.data() + (size_t)k * r->ndof);
-                r->rel[k] = cs.rel_residual;
-                free_slots.push_back(cs.host_scal);
-                cs.host_scal = nullptr;
-                r->finished[k] = 1;
+                r->finished[k] = state;
                 moved = true;
-                if (rc == YETI_OK && state == 3) {
-                    rc = YETI_EBREAKDOWN;
-                    set_error("serving: Krylov breakdown after %d iterations", cs.iterations);
-                }
             }
             if (rc != YETI_OK) {
-                finish(r, rc, yeti_last_error());
+                r->fail = rc;
                 return true;
             }
             left += !r->finished[k];
         }
-        if (left == 0) {
-            r->solves.clear();
-            finish(r, YETI_OK, "");
-            return true;
-        }
-        return false;
+        return left == 0;
     }
 
+    // Engine: admission, chunk relaunches, hand-over of finished requests.
     void run() {
         cudaSetDevice(ctx->device);
         for (;;) {
-            std::vector<Request *> admit;
             {
                 std::unique_lock<std::mutex> lk(mu);
-                if (active.empty() && queue.empty()) {
-                    cv_work.wait(lk, [&] { return stop || !queue.empty(); });
-                }
-                if (stop && active.empty()) {
+                if (active.empty() && ready.empty())
+                    cv_work.wait_for(lk, std::chrono::milliseconds(2), [&] {
+                        return stop || !ready.empty() ||
+                               (!queue.empty() && n_active < max_active &&
+                                (!budget || committed + queue.front()->est <= budget));
+                    });
+                if (stop && active.empty() && ready.empty() && n_active == 0) {
                     for (Request *q : queue) {
                         q->status = YETI_EINVAL;
                         q->err = "serving: server closed before the request was admitted";
                         q->t_done = now_ms();
                     }
                     queue.clear();
+                    stop_workers = true;
+                    cv_task.notify_all();
                     cv_done.notify_all();
                     return;
                 }
@@ -227,15 +280,29 @@ struct yeti_server {
                     committed += q->est;
                     n_active++;
                     peak_active = std::max(peak_active, n_active);
-                    admit.push_back(q);
+                    tasks.emplace_back(0, q);
+                    cv_task.notify_one();
                 }
+                for (Request *q : ready) active.push_back(q);
+                ready.clear();
             }
-            for (Request *q : admit)
-                if (start(q)) active.push_back(q);
-            bool moved = !admit.empty();
+            const double t1 = now_ms();
+            bool moved = false;
             for (size_t i = 0; i < active.size();) {
-                if (progress(active[i], moved)) active.erase(active.begin() + i);
-                else i++;
+                Request *r = active[i];
+                if (!progress(r, moved)) {
+                    i++;
+                    continue;
+                }
+                moved = true;
+                active.erase(active.begin() + i);
+                std::lock_guard<std::mutex> lk(mu);
+                tasks.emplace_back(1, r);
+                cv_task.notify_one();
+            }
+            {
+                std::lock_guard<std::mutex> lk(mu);
+                t_poll_ms += now_ms() - t1;
             }
             if (!moved && !active.empty()) std::this_thread::sleep_for(std::chrono::microseconds(20));
         }
@@ -255,10 +322,37 @@ YETI_API int yeti_serve_open(int device, size_t hbm_budget_bytes, int max_active
     s->budget = hbm_budget_bytes;
     s->max_active = max_active;
     DeviceGuard g(device);
+    int prio_low = 0, prio_high = 0;
+    YETI_CUDA(cudaDeviceGetStreamPriorityRange(&prio_low, &prio_high));
     for (int i = 0; i < kStreams; i++) {
         cudaStream_t st;
-        YETI_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+        YETI_CUDA(cudaStreamCreateWithPriority(&st, cudaStreamNonBlocking, prio_low));
         s->streams.push_back(st);
+    }
+    // keep the memory that retired requests free in the device's
+    // stream-ordered pool instead of returning it to the driver at every
+    // synchronisation
+    {
+        cudaMemPool_t pool;
+        YETI_CUDA(cudaDeviceGetDefaultMemPool(&pool, device));
+        uint64_t keep = hbm_budget_bytes ? (uint64_t)hbm_budget_bytes : UINT64_MAX, cur = 0;
+        YETI_CUDA(cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &cur));
+        if (cur < keep) YETI_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep));
+    }
+    constexpr int kWorkers = 4;
+    for (int w = 0; w < kWorkers; w++) {
+        yeti_ctx *wc = nullptr;
+        YETI_TRY(yeti_ctx_create(device, 0, &wc));
+        wc->stream_ordered = true;
+        cudaStream_t hs;
+        YETI_CUDA(cudaStreamCreateWithPriority(&hs, cudaStreamNonBlocking, prio_high));
+        cudaStreamDestroy(wc->own_stream);
+        wc->own_stream = hs;
+        wc->stream = hs;
+        s->wctx.push_back(wc);
+        cudaStream_t cs;
+        YETI_CUDA(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+        s->wcap.push_back(cs);
     }
     const size_t slot = (cgsolve_scal_bytes() + 127) / 128 * 128;
     const int nslots = max_active * kMaxRhs;
@@ -266,6 +360,7 @@ YETI_API int yeti_serve_open(int device, size_t hbm_budget_bytes, int max_active
     for (int i = nslots - 1; i >= 0; i--)
         s->free_slots.push_back(static_cast<char *>(s->pinned) + slot * i);
     yeti_server *raw = s.get();
+    for (int w = 0; w < kWorkers; w++) s->workers.emplace_back([raw, w] { raw->work(w); });
     s->engine = std::thread([raw] { raw->run(); });
     *out = s.release();
     return YETI_OK;
@@ -363,6 +458,16 @@ YETI_API int yeti_serve_wait(yeti_server *srv, int64_t ticket, double timeout_ms
     return take_result(srv, it, x, res);
 }
 
+YETI_API int yeti_serve_times(yeti_server *srv, double *setup_ms, double *retire_ms,
+                              double *poll_ms) {
+    YETI_CHECK(srv, YETI_EINVAL, "yeti_serve_times: NULL server");
+    std::lock_guard<std::mutex> lk(srv->mu);
+    if (setup_ms) *setup_ms = srv->t_setup_ms;
+    if (retire_ms) *retire_ms = srv->t_retire_ms;
+    if (poll_ms) *poll_ms = srv->t_poll_ms;
+    return YETI_OK;
+}
+
 YETI_API int yeti_serve_stats(yeti_server *srv, int64_t *done, int64_t *queued, int32_t *active,
                               int32_t *peak_active, size_t *committed_bytes) {
     YETI_CHECK(srv, YETI_EINVAL, "yeti_serve_stats: NULL server");
@@ -383,6 +488,10 @@ YETI_API int yeti_serve_close(yeti_server *srv) {
         srv->cv_work.notify_all();
     }
     if (srv->engine.joinable()) srv->engine.join();
+    for (auto &w : srv->workers)
+        if (w.joinable()) w.join();
+    for (yeti_ctx *wc : srv->wctx) yeti_ctx_destroy(wc);
+    for (cudaStream_t cs : srv->wcap) cudaStreamDestroy(cs);
     {
         DeviceGuard g(srv->ctx->device);
         for (cudaStream_t st : srv->streams) {

@@ -101,15 +101,20 @@ struct CgSolve {
 };
 // Bytes of host memory the caller provides as host_scal (pinned).
 size_t cgsolve_scal_bytes();
+// The chunk graph is captured on `capture` when given (a stream no other
+// thread enqueues into while it is captured), else on s.
 int cgsolve_begin(CgSolve &cs, yeti_wq_op *op, cudaStream_t s, void *host_scal,
-                  const double *b_host, double rtol, int maxit);
+                  const double *b_host, double rtol, int maxit,
+                  cudaStream_t capture = nullptr);
 // Enqueue the next chunk (graph launch + event).
 int cgsolve_launch(CgSolve &cs);
 // *state: 0 a chunk is in flight, 1 chunk done and more iterations needed,
 // 2 converged or iteration limit, 3 breakdown.
 int cgsolve_poll(CgSolve &cs, int *state);
 // Copy x to the host, compute the true residual, free the workspace.
-int cgsolve_finish(CgSolve &cs, double *x_host);
+// The work runs on `on` (after the solve's last chunk) when given, else on
+// the solve's stream.
+int cgsolve_finish(CgSolve &cs, double *x_host, cudaStream_t on = nullptr);
 
 // YETI_ETIMEDOUT (and clears the flag) if a streaming kernel reported a
 // bounded wait that gave up since the last check; synchronises the stream.

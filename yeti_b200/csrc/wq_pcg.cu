@@ -637,7 +637,7 @@ static SolveView solve_view(const CgSolve &cs) {
 }
 
 int cgsolve_begin(CgSolve &cs, yeti_wq_op *op, cudaStream_t st, void *host_scal,
-                  const double *b_host, double rtol, int maxit) {
+                  const double *b_host, double rtol, int maxit, cudaStream_t capture) {
     YETI_CHECK(op && host_scal && b_host && op->coef64.ptr, YETI_EINVAL,
                "cgsolve_begin: missing operator data");
     YETI_TRY(ensure_dinv64(op));
@@ -665,17 +665,18 @@ int cgsolve_begin(CgSolve &cs, yeti_wq_op *op, cudaStream_t st, void *host_scal,
     YETI_CUDA(cudaGetLastError());
     // one chunk of iterations, captured once
     cudaGraph_t g = nullptr;
-    YETI_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+    cudaStream_t cap = capture ? capture : st;
+    YETI_CUDA(cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal));
     int rc = YETI_OK;
     for (int k = 0; k < kChunk && rc == YETI_OK; k++) {
-        rc = wq_apply_dev(op, v.p, v.Ap, YETI_PREC_F64, &v.s->done, st);
-        k_dot_alpha<double><<<nb, kRedThreads, 0, st>>>(v.p, v.Ap, n, v.parts, v.s);
-        k_update_beta<double><<<nb, kRedThreads, 0, st>>>(v.x, v.r, v.p, v.Ap, dinv, v.z, n,
+        rc = wq_apply_dev(op, v.p, v.Ap, YETI_PREC_F64, &v.s->done, cap);
+        k_dot_alpha<double><<<nb, kRedThreads, 0, cap>>>(v.p, v.Ap, n, v.parts, v.s);
+        k_update_beta<double><<<nb, kRedThreads, 0, cap>>>(v.x, v.r, v.p, v.Ap, dinv, v.z, n,
                                                           v.parts, v.s);
-        k_pupdate<double><<<nb, kRedThreads, 0, st>>>(v.p, v.z, v.Ap, n, v.s);
+        k_pupdate<double><<<nb, kRedThreads, 0, cap>>>(v.p, v.z, v.Ap, n, v.s);
     }
-    cudaMemcpyAsync(cs.host_scal, v.s, sizeof(CGScal), cudaMemcpyDeviceToHost, st);
-    const cudaError_t ce = cudaStreamEndCapture(st, &g);
+    cudaMemcpyAsync(cs.host_scal, v.s, sizeof(CGScal), cudaMemcpyDeviceToHost, cap);
+    const cudaError_t ce = cudaStreamEndCapture(cap, &g);
     YETI_TRY(rc);
     YETI_CUDA(ce);
     const cudaError_t ie = cudaGraphInstantiate(&cs.chunk, g, 0);
@@ -709,12 +710,13 @@ int cgsolve_poll(CgSolve &cs, int *state) {
     return YETI_OK;
 }
 
-int cgsolve_finish(CgSolve &cs, double *x_host) {
+int cgsolve_finish(CgSolve &cs, double *x_host, cudaStream_t on) {
     const SolveView v = solve_view(cs);
     yeti_wq_op *op = cs.op;
     const int64_t n = op->ndof;
     const int nb = cs.nblk;
-    cudaStream_t st = cs.stream;
+    cudaStream_t st = on ? on : cs.stream;
+    if (on) YETI_CUDA(cudaStreamWaitEvent(on, cs.ev, 0));
     // true residual with the FP64 operator (Ap is free now)
     YETI_CUDA(cudaMemsetAsync(v.Ap, 0, n * sizeof(double), st));
     YETI_TRY(wq_apply_dev(op, v.x, v.Ap, YETI_PREC_F64, nullptr, st));

@@ -92,8 +92,12 @@ class Server:
         check(lib().yeti_serve_stats(self.handle, ctypes.byref(done), ctypes.byref(queued),
                                      ctypes.byref(active), ctypes.byref(peak),
                                      ctypes.byref(committed)), "yeti_serve_stats")
+        t = [ctypes.c_double() for _ in range(3)]
+        check(lib().yeti_serve_times(self.handle, *[ctypes.byref(v) for v in t]),
+              "yeti_serve_times")
         return {"done": done.value, "queued": queued.value, "active": active.value,
-                "peak_active": peak.value, "committed_bytes": committed.value}
+                "peak_active": peak.value, "committed_bytes": committed.value,
+                "setup_ms": t[0].value, "retire_ms": t[1].value, "poll_ms": t[2].value}
 
     def close(self):
         if getattr(self, "handle", None):
