@@ -155,9 +155,22 @@ def max_over_ranks(x, ws):
         return x
     import torch
     import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
+
+
+def replica_seed(rank):
+    """Each rank solves its own replica of the workload (replicas only: no
+    collective in the data path), seeded by its rank."""
+    return WORKLOAD["seed"] + rank
+
+
+def aggregate_rate(units_per_rank, ms_max, ws, steps=1):
+    """Whole-job throughput: the units all ranks processed divided by the
+    slowest rank's time (max over ranks)."""
+    return ws * units_per_rank * steps / (ms_max / 1e3)
 
 
 def barrier(ws):
@@ -361,7 +374,7 @@ def main():
     ctx = _lib.default_context(local)
     ctx.set_stream(torch.cuda.current_stream(dev))
     L = _lib.lib()
-    seed = WORKLOAD["seed"] + rank
+    seed = replica_seed(rank)
     P = cube_patch(tuple(args.nel), args.p, perturb=0.2, wrange=(0.8, 1.2), seed=seed)
     t0 = time.perf_counter()
     op = WQElasticity(P, 1.0, 0.3, {"w0": (0, 1, 2)}, precisions="both", ctx=ctx)
@@ -432,7 +445,7 @@ def main():
     ms = max_over_ranks(ms, ws)
     barrier(ws)
     err = (torch.linalg.norm(x - xref) / torch.linalg.norm(xref)).item()
-    value = ws * op.nfree * args.steps / (ms / 1e3)
+    value = aggregate_rate(op.nfree, ms, ws, args.steps)
 
     # plain FP64 throughput for the same tolerance (device-resident)
     e0.record()
