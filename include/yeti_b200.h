@@ -187,14 +187,33 @@ int yeti_wq_diag(yeti_wq_op *op, double *d, int mem);
 /* Body-force load vector for a constant force density f[3]
  * (wq_get_force_3d, wq_assembly.f90:1193-1251). */
 int yeti_wq_body_force(yeti_wq_op *op, const double f[3], double *F, int mem);
-/* Jacobi-preconditioned Krylov solve of K x = b (x holds the initial guess;
+/* Mode bits of yeti_wq_pcg. */
+#define YETI_PCG_MIXED 1       /* FP32 operator and Krylov vectors          */
+#define YETI_PCG_BICGSTAB 2    /* BiCGSTAB instead of CG                    */
+#define YETI_PCG_FD 4          /* fast-diagonalisation preconditioner
+                                  (mf_wq_solver.f90:803-953) instead of
+                                  Jacobi; a[c][d] = mean of S[(c,d),(c,d)]
+                                  (the reference's 'JM')                    */
+#define YETI_PCG_FD_SCALED 8   /* with YETI_PCG_FD: diagonal scaling
+                                  sqrt(diag(P)/diag(K)) ('JMS', 'TDS')      */
+#define YETI_PCG_FD_UNIT 16    /* with YETI_PCG_FD: a[c][d] = 1 ('C')       */
+
+/* Preconditioned Krylov solve of K x = b (x holds the initial guess;
  * replaces wq_mf_cg_3d / wq_mf_bicgstab_3d, mf_wq_solver.f90:642,958).
  * mode bit 0: mixed precision (FP32 operator and Krylov vectors, FP64 true
  * residual and solution: reliable updates for CG, iterative refinement for
- * BiCGSTAB); bit 1: BiCGSTAB instead of CG.  Stops when the FP64 true
- * residual satisfies ||r||_2 <= rtol ||b||_2. */
+ * BiCGSTAB); bit 1: BiCGSTAB instead of CG; bits 2-4: the fast-diagonalisation
+ * preconditioner (YETI_PCG_FD*), Jacobi when clear.  Stops when the FP64
+ * true residual satisfies ||r||_2 <= rtol ||b||_2. */
 int yeti_wq_pcg(yeti_wq_op *op, const double *b, double *x, double rtol,
                 int maxit, int mode, yeti_cg_stats *stats, int mem);
+/* z = P^{-1} r for the fast-diagonalisation preconditioner selected by the
+ * YETI_PCG_FD* bits of `variant` (fast_diagonalization_3d,
+ * tensor_algebra.f90:1107-1161, per displacement component, with
+ * scaling_FastDiag :1598-1625 when YETI_PCG_FD_SCALED).  prec YETI_PREC_F64 /
+ * F32: r and z are double / float; z is zero on clamped dofs. */
+int yeti_wq_fd_apply(yeti_wq_op *op, const void *r, void *z, int prec,
+                     int variant, int mem);
 
 /* ------------------------------------------------------------------------
  * Adjoint shape gradient of the linear-elastic work (U1, 3D)

@@ -181,15 +181,88 @@ class WQOracle:
             e[c] = 0.0
         return K
 
-    def pcg(self, b, rtol=1e-8, maxit=10000, x0=None):
-        """Jacobi-preconditioned CG (the 'WP' loop of wq_mf_cg_3d,
-        mf_wq_solver.f90:764-802, with a Jacobi preconditioner), stopping on
-        ||r||_2 <= rtol ||b||_2.  Returns (x, iterations, rel. residual)."""
+    # ------------------------------------------ fast diagonalisation
+    def fd_box(self, c):
+        """Free function range [lo, hi) along u, v, w of component c."""
+        m = self.mask[c] > 0                       # (nw, nv, nu)
+        out = []
+        for axes in ((0, 1), (0, 2), (1, 2)):      # reduce to u, v, w
+            idx = np.nonzero(m.any(axis=axes))[0]
+            out.append((int(idx[0]), int(idx[-1]) + 1))
+        return out
+
+    def fd_1d(self, d, lo, hi):
+        """Restricted, symmetrised 1-D WQ matrices (K, M) = (W11 B1^T,
+        W00 B0^T) of direction d (eigen_decomposition's KK and MM,
+        tensor_algebra.f90:1038-1063)."""
+        R = self.rules[d]
+        M = (R["W00"] @ R["B0"].T)[lo:hi, lo:hi]
+        K = (R["W11"] @ R["B1"].T)[lo:hi, lo:hi]
+        return 0.5 * (K + K.T), 0.5 * (M + M.T)
+
+    def fd_setup(self, scaled=False, unit=False):
+        """Per component: box, eigenpairs of K_d U = M_d U lam (scipy's
+        generalised symmetric solver, U^T M U = I), coefficients a[c][d]
+        (1, or the mean over the points of S[(c,d),(c,d)]) and, when scaled,
+        s = sqrt(diag(P) / diag(K)) (find_parametric_diag_3d and
+        scaling_FastDiag, tensor_algebra.f90:1452-1482, 1598-1625)."""
+        from scipy.linalg import eigh
+        dK = self.diag().reshape(self.mask.shape)
+        plan = []
+        for c in range(3):
+            box = self.fd_box(c)
+            a = [1.0 if unit else float(self.S[..., 3 * c + d, 3 * c + d].mean())
+                 for d in range(3)]
+            eig, dg = [], []
+            for d, (lo, hi) in enumerate(box):
+                K, M = self.fd_1d(d, lo, hi)
+                lam, U = eigh(K, M)
+                eig.append((lam, U))
+                dg.append((np.diag(K).copy(), np.diag(M).copy()))
+            lam3 = (a[2] * eig[2][0][:, None, None] + a[1] * eig[1][0][None, :, None]
+                    + a[0] * eig[0][0][None, None, :])
+            s = None
+            if scaled:
+                (ku, mu), (kv, mv), (kw, mw) = dg
+                dp = (a[0] * mw[:, None, None] * mv[None, :, None] * ku[None, None, :]
+                      + a[1] * mw[:, None, None] * kv[None, :, None] * mu[None, None, :]
+                      + a[2] * kw[:, None, None] * mv[None, :, None] * mu[None, None, :])
+                sl = tuple(slice(*box[d]) for d in (2, 1, 0))
+                s = np.sqrt(dp / dK[c][sl])
+            plan.append(dict(box=box, a=a, U=[e[1] for e in eig], lam3=lam3, s=s))
+        return plan
+
+    def fd_apply(self, r, plan):
+        """z = P^{-1} r (fast_diagonalization_3d, tensor_algebra.f90:1107-1161,
+        per component on its free box; zero on clamped dofs)."""
+        r = np.asarray(r, dtype=np.float64).reshape(self.mask.shape)
+        z = np.zeros_like(r)
+        for c, pc in enumerate(plan):
+            sl = tuple(slice(*pc["box"][d]) for d in (2, 1, 0))
+            x = r[c][sl]
+            if pc["s"] is not None:
+                x = x * pc["s"]
+            Uu, Uv, Uw = pc["U"]
+            y = np.einsum("wvu,ua,vb,wc->cba", x, Uu, Uv, Uw, optimize=True)
+            y = y / pc["lam3"]
+            x = np.einsum("cba,ua,vb,wc->wvu", y, Uu, Uv, Uw, optimize=True)
+            if pc["s"] is not None:
+                x = x * pc["s"]
+            z[c][sl] = x
+        return z.ravel()
+
+    def pcg(self, b, rtol=1e-8, maxit=10000, x0=None, precond=None):
+        """Preconditioned CG (the loop of wq_mf_cg_3d, mf_wq_solver.f90:
+        764-802 and 897-953), stopping on ||r||_2 <= rtol ||b||_2; Jacobi
+        unless precond (a callable r -> z) is given.  Returns (x,
+        iterations, rel. residual)."""
         m = self.mask.ravel()
         dinv = m / self.diag()
+        if precond is None:
+            precond = lambda v: dinv * v   # noqa: E731
         x = np.zeros_like(b) if x0 is None else x0.copy()
         r = (b - self.apply(x)) * m
-        z = dinv * r
+        z = precond(r)
         p = z.copy()
         rz = r @ z
         bn = np.linalg.norm(b * m)
@@ -201,7 +274,7 @@ class WQOracle:
             r -= alpha * Ap
             if np.linalg.norm(r) <= rtol * bn:
                 break
-            z = dinv * r
+            z = precond(r)
             rz_new = r @ z
             p = z + (rz_new / rz) * p
             rz = rz_new

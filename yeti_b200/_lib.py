@@ -114,6 +114,7 @@ def _declare(lib):
         "yeti_wq_body_force": (i32, [vp, vp, vp, i32]),
         "yeti_wq_pcg": (i32, [vp, vp, vp, dbl, i32, i32,
                               ctypes.POINTER(CGStats), i32]),
+        "yeti_wq_fd_apply": (i32, [vp, vp, vp, i32, i32, i32]),
         "yeti_grad_lin_elast_work": (i32, [vp, ctypes.POINTER(U1Model), vp,
                                            vp, i64, i32, i32, i32, vp, vp,
                                            i32]),

@@ -277,6 +277,7 @@ struct SetupArgs {
     double *coef64;            // may be null
     float *coef32;             // may be null
     double *jw;                // |detJ|
+    double *sdiag;             // [block][9]: sums of S[(c,d),(c,d)]
     int *flags;                // bit0: detJ > 0 seen, bit1: < 0, bit2: bad
 };
 
@@ -312,6 +313,7 @@ __global__ void __launch_bounds__(kWQThreads) k_wq_setup(SetupArgs a) {
                        c, X, Y, Z, F);
     const int nqb = c.nqb;
     int flags = 0;
+    double sd[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
     for (int q = threadIdx.x; q < nqb; q += blockDim.x) {
         double f[4][4];   // [lambda][component]
         for (int l = 0; l < 4; l++)
@@ -351,6 +353,7 @@ __global__ void __launch_bounds__(kWQThreads) k_wq_setup(SetupArgs a) {
                     s += iJ[k][d] * t;
                 }
                 s *= scale;
+                if (Jn == I) sd[I] += s;
                 const int e = sym9(I, Jn);
                 if (a.coef64) a.coef64[base + (int64_t)e * nqb + q] = s;
                 if (a.coef32) a.coef32[base + (int64_t)e * nqb + q] = (float)s;
@@ -359,6 +362,22 @@ __global__ void __launch_bounds__(kWQThreads) k_wq_setup(SetupArgs a) {
         a.jw[c.qoff + q] = fabs(det);
     }
     if (flags) atomicOr(a.flags, flags);
+    // block sums of the coefficient diagonal (fixed order: warp tree, then
+    // warps in index order)
+    __syncthreads();
+    double *red = sm;   // the tiles are no longer needed
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    for (int I = 0; I < 9; I++) {
+        double v = sd[I];
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+        if (lane == 0) red[I * 8 + wid] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x < 9) {
+        double v = 0.0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); w++) v += red[threadIdx.x * 8 + w];
+        a.sdiag[(int64_t)blockIdx.x * 9 + threadIdx.x] = v;
+    }
 }
 
 // ------------------------------------------------------------------ apply
@@ -792,6 +811,8 @@ YETI_API int yeti_wq_setup(yeti_ctx *ctx, const int32_t p[3],
     sa.coef64 = op->coef64.ptr ? op->coef64.as<double>() : nullptr;
     sa.coef32 = op->coef32.ptr ? op->coef32.as<float>() : nullptr;
     sa.jw = op->jw.as<double>();
+    YETI_TRY(op->sdiag.alloc(ctx, (size_t)op->nblocks * 9 * sizeof(double)));
+    sa.sdiag = op->sdiag.as<double>();
     sa.flags = flags.as<int>();
     {
         const size_t smem = smem_bytes(op.get(), 4, 2, sizeof(double));

@@ -72,6 +72,41 @@ struct WQStreamPlan {
     DevBuf err;              // int: a kernel's bounded wait gave up
 };
 
+// Device-side scalars of one CG solve (wq_pcg.cu); the fast-diagonalisation
+// kernels finish the r.z reduction of an iteration into them.
+struct CGScal {
+    double rz, pAp, alpha, beta, rr, bb, tol2, scale;
+    double pause2;         // stop a chunk once rr <= pause2 (0: never)
+    int done, iter, breakdown, maxit;
+    int paused;            // done was set by pause2, not by the tolerance
+    unsigned int ticket;   // blocks of a fused reduction that have finished
+};
+
+// Fast-diagonalisation preconditioner (wq_fd.cu): per displacement component
+// c, the separable operator sum_d a[c][d] K_d (x) M (x) M on the component's
+// free box, inverted through the generalised eigenpairs K_d U = M_d U Lambda
+// of the 1-D WQ matrices; optionally scaled by sqrt(diag(P) / diag(K)).
+struct WQFdPlan {
+    int variant = -1;          // YETI_PCG_FD bits it was built for (-1: none)
+    int lo[3][3], m[3][3];     // free box per [component][direction]
+    int64_t goff[3][3];        // U (fwd) at goff, U^T (bwd) at goff + m*m
+    int64_t doff[3][3];        // a[c][d] * lambda_d
+    bool scaled = false;
+    DevBuf g64, g32, d64, d32, s64, s32;   // matrices, eigenvalues, scaling
+    DevBuf t64, t32;           // two intermediate vectors
+    DevBuf parts;              // partials of the r.z reduction
+    int max_grid = 0;
+};
+// FD reduction modes of the last (u, backward) pass.
+enum FdRed { FD_NONE = 0, FD_ITER = 1, FD_START = 2, FD_REPLACE = 3 };
+// Build the plan for the YETI_PCG_FD* bits of `variant` (no-op when built).
+int wq_fd_prepare(yeti_wq_op *op, int variant, bool f32);
+// out = P in.  red FD_ITER: beta = r.z / rz, rz = r.z into *cg; FD_START:
+// rz = r.z and p = z; FD_REPLACE: rz = r.z.  (in is r for those modes.)
+template <class T>
+int wq_fd_apply(yeti_wq_op *op, const T *in, T *out, const int *done, int red,
+                T *p, CGScal *cg, cudaStream_t s);
+
 bool wq_stream_supported(const yeti_wq_op *op);
 // Build the tile tables and work segments (after the 1-D rules).
 int wq_stream_setup(yeti_wq_op *op, const WQRule1D R[3]);
@@ -147,6 +182,8 @@ struct yeti_wq_op {
     yeti::DevBuf dinv64, dinv32;
     yeti::DevBuf ws64, ws32, scal, parts;   // PCG workspaces
     yeti::WQStreamPlan st;
+    yeti::DevBuf sdiag;     // per element block: sums of S[(c,d),(c,d)] (9)
+    yeti::WQFdPlan fd;
     double setup_ms = 0.0;
     int64_t bytes_data = 0;
 };

@@ -1,0 +1,710 @@
+// Fast-diagonalisation (FD) preconditioner of the WQ elasticity operator:
+// the reference's fast_diagonalization_3d (src/yeti_iga/iga_wq_mf/fsrc/
+// tensor_algebra.f90:1107-1161) with its eigen_decomposition (:992-1105),
+// find_parametric_diag_3d (:1452-1482) and scaling_FastDiag (:1598-1625), as
+// used by wq_mf_cg_3d (mf_wq_solver.f90:803-953), generalised from the
+// scalar problem to the three displacement components.
+//
+// For component c the preconditioner inverts the separable operator
+//     P_c = a[c][u] K_u (x) M_v (x) M_w + a[c][v] M_u (x) K_v (x) M_w
+//         + a[c][w] M_u (x) M_v (x) K_w
+// on the component's free box (the dofs off its clamped faces).  K_d / M_d
+// are the 1-D WQ stiffness and mass matrices W11 B1^T and W00 B0^T
+// (eigen_decomposition's KK and MM).  With K_d U_d = M_d U_d Lambda_d and
+// U_d^T M_d U_d = I,
+//     P_c^{-1} = (U_w (x) U_v (x) U_u) diag(1 / Lambda_c) (U_w (x) U_v (x) U_u)^T,
+//     Lambda_c(i,j,k) = a[c][u] lu_i + a[c][v] lv_j + a[c][w] lw_k.
+// a[c][d] is 1 (the reference's method 'C') or the mean over the WQ points
+// of the coefficient S[(c,d),(c,d)] (the elastic counterpart of the
+// Jacobian-mean lengths of jacobien_mean_3d, tensor_algebra.f90:1384-1448:
+// method 'JM').  The scaled form ('JMS') applies z = s (P^{-1} (s r)) with
+// s = sqrt(diag(P) / diag(K)).
+//
+// Device work per application: six passes of dense 1-D products along u, v,
+// w (forward with U^T, the eigenvalue division fused into the w pass, then
+// backward with U).  Each pass is a small-K GEMM over the lines of the box,
+// tiled in shared memory (16-deep K chunks, 4x4 register tiles); the
+// vectors (a few MB) stay in L2 between passes.
+#include <algorithm>
+#include <cmath>
+#include <map>
+#include <tuple>
+#include <vector>
+
+#include "reduce.cuh"
+#include "wq.cuh"
+
+namespace yeti {
+
+constexpr int kFdThreads = 256;
+constexpr int kFdTA = 128;     // max output rows per CTA
+constexpr int kFdTL = 128;     // max lines per CTA
+constexpr int kFdMaxM = 512;   // largest 1-D free size accepted
+constexpr size_t kFdSmem = 200 * 1024;   // staged G and line tiles per CTA
+
+// ------------------------------------------------------------------ host
+// Symmetric eigenpairs of A (n x n, row-major, destroyed) by cyclic Jacobi
+// rotations (Golub & Van Loan, Matrix Computations, sec. 8.5): A = V diag(w)
+// V^T, V's columns the eigenvectors.  Returns false if it did not converge.
+static bool sym_eig_jacobi(int n, std::vector<double> &A, std::vector<double> &w,
+                           std::vector<double> &V) {
+    V.assign((size_t)n * n, 0.0);
+    for (int i = 0; i < n; i++) V[(size_t)i * n + i] = 1.0;
+    auto at = [&](int i, int j) -> double & { return A[(size_t)i * n + j]; };
+    double fro = 0.0;
+    for (double v : A) fro += v * v;
+    fro = std::sqrt(fro);
+    bool ok = false;
+    for (int sweep = 0; sweep < 60; sweep++) {
+        double off = 0.0;
+        for (int i = 0; i < n; i++)
+            for (int j = i + 1; j < n; j++) off += at(i, j) * at(i, j);
+        if (std::sqrt(2.0 * off) <= 1e-15 * fro) {
+            ok = true;
+            break;
+        }
+        for (int p = 0; p < n - 1; p++)
+            for (int q = p + 1; q < n; q++) {
+                const double apq = at(p, q);
+                if (std::fabs(apq) <= 1e-300) continue;
+                const double theta = (at(q, q) - at(p, p)) / (2.0 * apq);
+                const double t = (theta >= 0 ? 1.0 : -1.0) /
+                                 (std::fabs(theta) + std::sqrt(1.0 + theta * theta));
+                const double cs = 1.0 / std::sqrt(1.0 + t * t), sn = t * cs;
+                // A <- J^T A J with J the rotation in the (p, q) plane
+                for (int k = 0; k < n; k++) {
+                    const double akp = at(k, p), akq = at(k, q);
+                    at(k, p) = cs * akp - sn * akq;
+                    at(k, q) = sn * akp + cs * akq;
+                }
+                for (int k = 0; k < n; k++) {
+                    const double apk = at(p, k), aqk = at(q, k);
+                    at(p, k) = cs * apk - sn * aqk;
+                    at(q, k) = sn * apk + cs * aqk;
+                }
+                at(p, q) = at(q, p) = 0.0;
+                for (int k = 0; k < n; k++) {
+                    double *vr = &V[(size_t)k * n];
+                    const double vkp = vr[p], vkq = vr[q];
+                    vr[p] = cs * vkp - sn * vkq;
+                    vr[q] = sn * vkp + cs * vkq;
+                }
+            }
+    }
+    w.resize(n);
+    for (int i = 0; i < n; i++) w[i] = at(i, i);
+    return ok;
+}
+
+// Generalised symmetric-definite pencil K U = M U diag(lam), U^T M U = I,
+// through M = L L^T and the standard form L^{-1} K L^{-T}.
+static bool gen_eig(int n, const std::vector<double> &K, const std::vector<double> &M,
+                    std::vector<double> &lam, std::vector<double> &U) {
+    std::vector<double> L((size_t)n * n, 0.0);
+    for (int j = 0; j < n; j++) {
+        double d = M[(size_t)j * n + j];
+        for (int k = 0; k < j; k++) d -= L[(size_t)j * n + k] * L[(size_t)j * n + k];
+        if (!(d > 0.0)) return false;
+        const double ljj = std::sqrt(d);
+        L[(size_t)j * n + j] = ljj;
+        for (int i = j + 1; i < n; i++) {
+            double v = M[(size_t)i * n + j];
+            for (int k = 0; k < j; k++) v -= L[(size_t)i * n + k] * L[(size_t)j * n + k];
+            L[(size_t)i * n + j] = v / ljj;
+        }
+    }
+    // Y = L^{-1} K (forward substitution per column), C = L^{-1} Y^T
+    std::vector<double> Y((size_t)n * n), C((size_t)n * n);
+    for (int col = 0; col < n; col++)
+        for (int i = 0; i < n; i++) {
+            double v = K[(size_t)i * n + col];
+            for (int k = 0; k < i; k++) v -= L[(size_t)i * n + k] * Y[(size_t)k * n + col];
+            Y[(size_t)i * n + col] = v / L[(size_t)i * n + i];
+        }
+    for (int col = 0; col < n; col++)
+        for (int i = 0; i < n; i++) {
+            double v = Y[(size_t)col * n + i];   // (Y^T)[i][col]
+            for (int k = 0; k < i; k++) v -= L[(size_t)i * n + k] * C[(size_t)k * n + col];
+            C[(size_t)i * n + col] = v / L[(size_t)i * n + i];
+        }
+    for (int i = 0; i < n; i++)
+        for (int j = i + 1; j < n; j++) {
+            const double s = 0.5 * (C[(size_t)i * n + j] + C[(size_t)j * n + i]);
+            C[(size_t)i * n + j] = C[(size_t)j * n + i] = s;
+        }
+    std::vector<double> Q;
+    if (!sym_eig_jacobi(n, C, lam, Q)) return false;
+    // U = L^{-T} Q (back substitution per column)
+    U.assign((size_t)n * n, 0.0);
+    for (int col = 0; col < n; col++)
+        for (int i = n - 1; i >= 0; i--) {
+            double v = Q[(size_t)i * n + col];
+            for (int k = i + 1; k < n; k++) v -= L[(size_t)k * n + i] * U[(size_t)k * n + col];
+            U[(size_t)i * n + col] = v / L[(size_t)i * n + i];
+        }
+    return true;
+}
+
+// 1-D WQ matrices of one direction restricted to functions [lo, hi),
+// symmetrised: M = W00 B0^T, K = W11 B1^T (eigen_decomposition's MM, KK).
+static void wq_1d_matrices(const WQRule1D &R, int lo, int hi, std::vector<double> &K,
+                           std::vector<double> &M) {
+    const int m = hi - lo, nq = R.nqp;
+    K.assign((size_t)m * m, 0.0);
+    M.assign((size_t)m * m, 0.0);
+    for (int i = 0; i < m; i++)
+        for (int j = 0; j < m; j++) {
+            const double *w0 = &R.W00[(size_t)(lo + i) * nq], *b0 = &R.B0[(size_t)(lo + j) * nq];
+            const double *w1 = &R.W11[(size_t)(lo + i) * nq], *b1 = &R.B1[(size_t)(lo + j) * nq];
+            double sm = 0.0, sk = 0.0;
+            for (int q = 0; q < nq; q++) {
+                sm += w0[q] * b0[q];
+                sk += w1[q] * b1[q];
+            }
+            M[(size_t)i * m + j] = sm;
+            K[(size_t)i * m + j] = sk;
+        }
+    for (int i = 0; i < m; i++)
+        for (int j = i + 1; j < m; j++) {
+            const double a = 0.5 * (M[(size_t)i * m + j] + M[(size_t)j * m + i]);
+            const double b = 0.5 * (K[(size_t)i * m + j] + K[(size_t)j * m + i]);
+            M[(size_t)i * m + j] = M[(size_t)j * m + i] = a;
+            K[(size_t)i * m + j] = K[(size_t)j * m + i] = b;
+        }
+}
+
+// ---------------------------------------------------------------- device
+template <class T>
+struct FdArgs {
+    const T *in;
+    T *out;
+    const T *g;        // G for this pass: out_row = sum_k G[k][row] in_k
+    const T *dsc;      // a[c][d] * lambda_d
+    const T *s;        // scaling (nullptr: none)
+    const T *r;        // residual (reduction modes)
+    T *p;              // FD_START: p = z
+    const int *done;
+    CGScal *cg;
+    double *parts;
+    int red;
+    int n[3];
+    int64_t ncp;
+    int lo[3][3], m[3][3];
+    int64_t goff[3];   // per component, for this pass
+    int64_t doff[3][3];
+    int nag[3], nlg[3], ntA[3], cta_end[3];
+};
+
+// Tiles of one pass for one component: ntA tiles of TA = 4 nag output rows
+// times tiles of TL = 4 nlg lines, the whole contraction (m rows of G and of
+// the lines) staged in shared memory: m (TA + TL) elements per CTA.
+struct FdTile {
+    int ntA, nag, nlg, ctas;
+};
+static FdTile fd_tile(int m, int64_t nlines, size_t esize) {
+    FdTile t;
+    t.ntA = (m + kFdTA - 1) / kFdTA;
+    for (;;) {
+        t.nag = ((m + t.ntA - 1) / t.ntA + 3) / 4;
+        t.nlg = std::min(kFdTL / 4, kFdThreads / t.nag);
+        while (t.nlg > 4 && (size_t)m * (4 * t.nag + 4 * t.nlg + 4) * esize > kFdSmem) t.nlg--;
+        if ((size_t)m * (4 * t.nag + 4 * t.nlg + 4) * esize <= kFdSmem) break;
+        t.ntA++;
+    }
+    t.ctas = t.ntA * (int)((nlines + 4 * t.nlg - 1) / (4 * t.nlg));
+    return t;
+}
+
+// Asynchronous global -> shared copy of one element (cp.async, sm_80+);
+// valid == false writes zero and reads nothing.
+template <class T>
+__device__ __forceinline__ void cp_elem(T *sdst, const T *gsrc, bool valid) {
+    const unsigned saddr = (unsigned)__cvta_generic_to_shared(sdst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], %2, %3;\n" ::"r"(saddr), "l"(gsrc),
+                 "n"((int)sizeof(T)), "r"(valid ? (int)sizeof(T) : 0)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
+template <class T> struct Vec4;
+template <> struct Vec4<float> {
+    static __device__ __forceinline__ void ld(const float *p, float v[4]) {
+        const float4 q = *reinterpret_cast<const float4 *>(p);
+        v[0] = q.x; v[1] = q.y; v[2] = q.z; v[3] = q.w;
+    }
+};
+template <> struct Vec4<double> {
+    static __device__ __forceinline__ void ld(const double *p, double v[4]) {
+        const double2 q0 = *reinterpret_cast<const double2 *>(p);
+        const double2 q1 = *reinterpret_cast<const double2 *>(p + 2);
+        v[0] = q0.x; v[1] = q0.y; v[2] = q1.x; v[3] = q1.y;
+    }
+};
+
+// One pass along axis AX: out_row(line) = sum_k G[k][row] in_k(line).
+// EPI 1: divide by Lambda; EPI 2: multiply by s, r.z partials and the
+// reduction mode.  The G columns and the lines are staged in shared memory
+// by cp.async (all copies in flight at once), then contracted from there.
+template <class T, int AX, int EPI>
+__global__ void __launch_bounds__(kFdThreads) k_fd_pass(FdArgs<T> a) {
+    extern __shared__ __align__(16) unsigned char fd_smem[];
+    __shared__ int64_t lb[kFdTL];
+    __shared__ int2 lc[kFdTL];   // (i1, i2) of a line
+    __shared__ double sh[32];
+    if (a.done && *a.done) return;
+    int b = blockIdx.x, c = 0;
+    while (c < 2 && b >= a.cta_end[c]) c++;
+    if (c > 0) b -= a.cta_end[c - 1];
+    constexpr int D1 = AX == 0 ? 1 : 0, D2 = AX == 2 ? 1 : 2;
+    const int nag = a.nag[c], nlg = a.nlg[c], ntA = a.ntA[c];
+    const int m = a.m[c][AX], m1 = a.m[c][D1], m2 = a.m[c][D2];
+    const int64_t nlines = (int64_t)m1 * m2;
+    const int TA = 4 * nag, TL = 4 * nlg, TLp = TL + 4;
+    T *Gs = reinterpret_cast<T *>(fd_smem);   // [m][TA]
+    T *Xs = Gs + (size_t)m * TA;              // [m][TLp]
+    const int a0 = (b % ntA) * TA;
+    const int64_t l0 = (int64_t)(b / ntA) * TL;
+    const int64_t st[3] = {1, (int64_t)a.n[0], (int64_t)a.n[0] * a.n[1]};
+    const int64_t sk = st[AX];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    for (int ll = tid; ll < TL; ll += kFdThreads) {
+        const int64_t l = l0 + ll;
+        int64_t base = -1;
+        int i1 = 0, i2 = 0;
+        if (l < nlines) {
+            i1 = (int)(l % m1);
+            i2 = (int)(l / m1);
+            base = c * a.ncp + (int64_t)a.lo[c][AX] * sk + (int64_t)(a.lo[c][D1] + i1) * st[D1] +
+                   (int64_t)(a.lo[c][D2] + i2) * st[D2];
+        }
+        lb[ll] = base;
+        lc[ll] = make_int2(i1, i2);
+    }
+    // G columns a0 .. a0 + TA of every row k (a warp per row)
+    const T *G = a.g + a.goff[c];
+    for (int k = warp; k < m; k += kFdThreads / 32) {
+        const T *src = G + (int64_t)k * m;
+        for (int aa = lane; aa < TA; aa += 32) {
+            const int col = a0 + aa;
+            cp_elem(Gs + k * TA + aa, col < m ? src + col : G, col < m);
+        }
+    }
+    __syncthreads();   // lb
+    if (AX == 0) {
+        // lines are contiguous: a warp per line, lanes along k
+        for (int ll = warp; ll < TL; ll += kFdThreads / 32) {
+            const int64_t base = lb[ll];
+            for (int k = lane; k < m; k += 32)
+                cp_elem(Xs + k * TLp + ll, base >= 0 ? a.in + base + k : a.in, base >= 0);
+        }
+    } else {
+        // row k of the tile is contiguous along the lines: a warp per row
+        for (int k = warp; k < m; k += kFdThreads / 32) {
+            for (int ll = lane; ll < TL; ll += 32) {
+                const int64_t base = lb[ll];
+                cp_elem(Xs + k * TLp + ll, base >= 0 ? a.in + base + (int64_t)k * sk : a.in,
+                        base >= 0);
+            }
+        }
+    }
+    cp_wait_all();
+    __syncthreads();
+    int ag, lg;
+    if (AX == 0) {
+        ag = tid % nag;
+        lg = tid / nag;
+    } else {
+        lg = tid % nlg;
+        ag = tid / nlg;
+    }
+    const bool act = tid < nag * nlg;
+    T acc[4][4];
+#pragma unroll
+    for (int i = 0; i < 4; i++)
+#pragma unroll
+        for (int j = 0; j < 4; j++) acc[i][j] = T(0);
+    if (act) {
+        const T *gp = Gs + 4 * ag, *xp = Xs + 4 * lg;
+#pragma unroll 4
+        for (int k = 0; k < m; k++) {
+            T gv[4], xv[4];
+            Vec4<T>::ld(gp + k * TA, gv);
+            Vec4<T>::ld(xp + k * TLp, xv);
+#pragma unroll
+            for (int i = 0; i < 4; i++)
+#pragma unroll
+                for (int j = 0; j < 4; j++) acc[i][j] += gv[i] * xv[j];
+        }
+    }
+    double rz = 0.0;
+    if (act) {
+#pragma unroll
+        for (int i = 0; i < 4; i++) {
+            const int row = a0 + 4 * ag + i;
+            if (row >= m) continue;
+#pragma unroll
+            for (int j = 0; j < 4; j++) {
+                const int ll = 4 * lg + j;
+                const int64_t base = lb[ll];
+                if (base < 0) continue;
+                const int64_t idx = base + (int64_t)row * sk;
+                T v = acc[i][j];
+                if (EPI == 1) {
+                    int e3[3];
+                    e3[AX] = row;
+                    e3[D1] = lc[ll].x;
+                    e3[D2] = lc[ll].y;
+                    const T lam = a.dsc[a.doff[c][0] + e3[0]] + a.dsc[a.doff[c][1] + e3[1]] +
+                                  a.dsc[a.doff[c][2] + e3[2]];
+                    v = v / lam;
+                }
+                if (EPI == 2) {
+                    if (a.s) v *= a.s[idx];
+                    if (a.red != FD_NONE) rz += (double)a.r[idx] * (double)v;
+                    if (a.red == FD_START) a.p[idx] = v;
+                }
+                a.out[idx] = v;
+            }
+        }
+    }
+    if (EPI != 2 || a.red == FD_NONE) return;
+    rz = block_sum(rz, sh);
+    if (threadIdx.x == 0) __stcg(&a.parts[blockIdx.x], rz);
+    if (!last_block(&a.cg->ticket)) return;
+    double srz = 0.0;
+    for (int i = threadIdx.x; i < (int)gridDim.x; i += blockDim.x) srz += __ldcg(&a.parts[i]);
+    srz = block_sum(srz, sh);
+    if (threadIdx.x == 0) {
+        CGScal *s = a.cg;
+        s->ticket = 0;
+        if (a.red == FD_ITER) {
+            const double old = s->rz;
+            s->beta = srz / old;
+            if (!isfinite(srz) || !(old != 0.0)) {
+                s->breakdown = 1;
+                s->done = 1;
+            }
+        }
+        s->rz = srz;
+    }
+}
+
+// out = s in (elementwise; s is zero off the free boxes)
+template <class T>
+__global__ void k_fd_scale_in(const T *in, const T *sv, T *out, int64_t n, const int *done) {
+    if (done && *done) return;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x)
+        out[i] = in[i] * sv[i];
+}
+
+// s = sqrt(diag(P) / diag(K)) on every component's free box, 0 elsewhere;
+// diag(P) from the 1-D diagonals (find_parametric_diag_3d).
+__global__ void k_fd_scaling(const double *diagK, const double *kdmd, double *s64, float *s32, int3 n, int64_t ncp, int lo0, int lo1,
+                             int lo2, int m0, int m1, int m2, int c, int64_t off_u,
+                             int64_t off_v, int64_t off_w, double au, double av, double aw) {
+    const int64_t tot = (int64_t)m0 * m1 * m2;
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < tot;
+         t += (int64_t)gridDim.x * blockDim.x) {
+        const int i = (int)(t % m0), j = (int)((t / m0) % m1), k = (int)(t / ((int64_t)m0 * m1));
+        const double ku = kdmd[off_u + i], mu = kdmd[off_u + m0 + i];
+        const double kv = kdmd[off_v + j], mv = kdmd[off_v + m1 + j];
+        const double kw = kdmd[off_w + k], mw = kdmd[off_w + m2 + k];
+        const double dp = au * ku * mv * mw + av * mu * kv * mw + aw * mu * mv * kw;
+        const int64_t idx = c * ncp + (int64_t)(lo0 + i) + (int64_t)n.x * ((lo1 + j) + (int64_t)n.y * (lo2 + k));
+        const double v = sqrt(dp / diagK[idx]);
+        if (s64) s64[idx] = v;
+        if (s32) s32[idx] = (float)v;
+    }
+}
+
+// ------------------------------------------------------------------ plan
+int wq_fd_prepare(yeti_wq_op *op, int variant, bool f32) {
+    WQFdPlan &F = op->fd;
+    variant &= (YETI_PCG_FD | YETI_PCG_FD_SCALED | YETI_PCG_FD_UNIT);
+    if (F.variant == variant && (!f32 || F.g32.ptr)) return YETI_OK;
+    yeti_ctx *ctx = op->ctx;
+    cudaStream_t s = ctx->stream;
+    const bool unit = (variant & YETI_PCG_FD_UNIT) != 0;
+    const bool scaled = (variant & YETI_PCG_FD_SCALED) != 0;
+    // free boxes
+    for (int c = 0; c < 3; c++) {
+        YETI_CHECK(op->cmask[c] != 0, YETI_EINVAL,
+                   "fast diagonalisation: component %d has no clamped face (singular)", c);
+        for (int d = 0; d < 3; d++) {
+            const int lo = (op->cmask[c] >> (2 * d)) & 1;
+            const int hi = op->n[d] - ((op->cmask[c] >> (2 * d + 1)) & 1);
+            F.lo[c][d] = lo;
+            F.m[c][d] = hi - lo;
+            YETI_CHECK(F.m[c][d] >= 1 && F.m[c][d] <= kFdMaxM, YETI_EINVAL,
+                       "fast diagonalisation: %d free functions along direction %d "
+                       "(1..%d supported)", F.m[c][d], d, kFdMaxM);
+        }
+    }
+    // coefficients a[c][d]
+    double acoef[3][3];
+    if (unit) {
+        for (int c = 0; c < 3; c++)
+            for (int d = 0; d < 3; d++) acoef[c][d] = 1.0;
+    } else {
+        std::vector<double> sd((size_t)op->nblocks * 9);
+        YETI_CUDA(cudaMemcpyAsync(sd.data(), op->sdiag.ptr, sd.size() * sizeof(double),
+                                  cudaMemcpyDeviceToHost, s));
+        YETI_CUDA(cudaStreamSynchronize(s));
+        double sum[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+        for (int64_t b = 0; b < op->nblocks; b++)
+            for (int k = 0; k < 9; k++) sum[k] += sd[(size_t)b * 9 + k];
+        for (int c = 0; c < 3; c++)
+            for (int d = 0; d < 3; d++) {
+                acoef[c][d] = sum[3 * c + d] / (double)op->nqp_total;
+                YETI_CHECK(acoef[c][d] > 0.0 && std::isfinite(acoef[c][d]), YETI_ENUMERIC,
+                           "fast diagonalisation: mean coefficient %g", acoef[c][d]);
+            }
+    }
+    // eigenpairs per distinct (p, nel, lo, hi)
+    WQRule1D R[3];
+    for (int d = 0; d < 3; d++)
+        YETI_CHECK(wq_rule_1d(op->p[d], op->nel[d], R[d]) == 0, YETI_EINVAL,
+                   "fast diagonalisation: WQ rule failed");
+    struct Eig {
+        std::vector<double> lam, U, kd, md;
+    };
+    std::map<std::tuple<int, int, int, int>, Eig> cache;
+    Eig *E[3][3];
+    for (int c = 0; c < 3; c++)
+        for (int d = 0; d < 3; d++) {
+            const int lo = F.lo[c][d], hi = lo + F.m[c][d];
+            auto key = std::make_tuple(op->p[d], op->nel[d], lo, hi);
+            auto it = cache.find(key);
+            if (it == cache.end()) {
+                Eig e;
+                std::vector<double> K, M;
+                wq_1d_matrices(R[d], lo, hi, K, M);
+                const int m = hi - lo;
+                e.kd.resize(m);
+                e.md.resize(m);
+                for (int i = 0; i < m; i++) {
+                    e.kd[i] = K[(size_t)i * m + i];
+                    e.md[i] = M[(size_t)i * m + i];
+                }
+                YETI_CHECK(gen_eig(m, K, M, e.lam, e.U), YETI_ENUMERIC,
+                           "fast diagonalisation: eigen decomposition failed (direction %d)", d);
+                it = cache.emplace(key, std::move(e)).first;
+            }
+            E[c][d] = &it->second;
+        }
+    // Lambda_c > 0 needs at least one direction without a zero eigenvalue
+    for (int c = 0; c < 3; c++) {
+        double lmin = 0.0;
+        for (int d = 0; d < 3; d++)
+            lmin += acoef[c][d] * *std::min_element(E[c][d]->lam.begin(), E[c][d]->lam.end());
+        YETI_CHECK(lmin > 0.0, YETI_ENUMERIC,
+                   "fast diagonalisation: separable operator of component %d is singular", c);
+    }
+    // device tables: G (U then U^T) per (c, d); a * lambda; 1-D diagonals
+    std::vector<double> g, dsc, kdmd;
+    for (int c = 0; c < 3; c++)
+        for (int d = 0; d < 3; d++) {
+            const int m = F.m[c][d];
+            const Eig &e = *E[c][d];
+            F.goff[c][d] = (int64_t)g.size();
+            g.insert(g.end(), e.U.begin(), e.U.end());
+            for (int i = 0; i < m; i++)
+                for (int j = 0; j < m; j++) g.push_back(e.U[(size_t)j * m + i]);
+            F.doff[c][d] = (int64_t)dsc.size();
+            for (int i = 0; i < m; i++) dsc.push_back(acoef[c][d] * e.lam[i]);
+            for (int i = 0; i < m; i++) kdmd.push_back(e.kd[i]);
+            for (int i = 0; i < m; i++) kdmd.push_back(e.md[i]);
+        }
+    YETI_TRY(upload(ctx, F.g64, g.data(), g.size()));
+    YETI_TRY(upload(ctx, F.d64, dsc.data(), dsc.size()));
+    F.g32.release();
+    F.d32.release();
+    if (f32) {
+        std::vector<float> gf(g.begin(), g.end()), df(dsc.begin(), dsc.end());
+        YETI_TRY(upload(ctx, F.g32, gf.data(), gf.size()));
+        YETI_TRY(upload(ctx, F.d32, df.data(), df.size()));
+    }
+    // scaling vector
+    F.scaled = scaled;
+    F.s64.release();
+    F.s32.release();
+    if (scaled) {
+        DevBuf dk;
+        YETI_TRY(upload(ctx, dk, kdmd.data(), kdmd.size()));
+        YETI_TRY(F.s64.alloc(ctx, op->ndof * sizeof(double)));
+        YETI_CUDA(cudaMemsetAsync(F.s64.ptr, 0, op->ndof * sizeof(double), s));
+        if (f32) {
+            YETI_TRY(F.s32.alloc(ctx, op->ndof * sizeof(float)));
+            YETI_CUDA(cudaMemsetAsync(F.s32.ptr, 0, op->ndof * sizeof(float), s));
+        }
+        for (int c = 0; c < 3; c++) {
+            // kdmd offsets: twice the dsc offsets (kd then md per block)
+            k_fd_scaling<<<592, 256, 0, s>>>(
+                op->diag.as<double>(), dk.as<double>(), F.s64.as<double>(),
+                f32 ? F.s32.as<float>() : nullptr, make_int3(op->n[0], op->n[1], op->n[2]),
+                op->ncp, F.lo[c][0], F.lo[c][1], F.lo[c][2], F.m[c][0], F.m[c][1], F.m[c][2], c,
+                2 * F.doff[c][0], 2 * F.doff[c][1], 2 * F.doff[c][2], acoef[c][0], acoef[c][1],
+                acoef[c][2]);
+            count_launches(1);
+        }
+        YETI_CUDA(cudaGetLastError());
+        YETI_CUDA(cudaStreamSynchronize(s));   // dk is freed on return
+    }
+    // intermediates and reduction partials
+    YETI_TRY(F.t64.alloc(ctx, 2 * op->ndof * sizeof(double)));
+    F.t32.release();
+    if (f32) YETI_TRY(F.t32.alloc(ctx, 2 * op->ndof * sizeof(float)));
+    int maxg = 0;
+    for (int ax = 0; ax < 3; ax++) {
+        int tot = 0;
+        for (int c = 0; c < 3; c++) {
+            const int64_t nl = (int64_t)F.m[c][(ax == 0) ? 1 : 0] * F.m[c][(ax == 2) ? 1 : 2];
+            tot += std::max(fd_tile(F.m[c][ax], nl, sizeof(double)).ctas,
+                            fd_tile(F.m[c][ax], nl, sizeof(float)).ctas);
+        }
+        maxg = std::max(maxg, tot);
+    }
+    F.max_grid = maxg;
+    YETI_TRY(F.parts.alloc(ctx, (size_t)maxg * sizeof(double)));
+    F.variant = variant;
+    return YETI_OK;
+}
+
+template <class T> struct FdBufs;
+template <> struct FdBufs<double> {
+    static const double *g(const WQFdPlan &F) { return F.g64.as<double>(); }
+    static const double *d(const WQFdPlan &F) { return F.d64.as<double>(); }
+    static const double *s(const WQFdPlan &F) { return F.s64.as<double>(); }
+    static double *t(const WQFdPlan &F) { return F.t64.as<double>(); }
+};
+template <> struct FdBufs<float> {
+    static const float *g(const WQFdPlan &F) { return F.g32.as<float>(); }
+    static const float *d(const WQFdPlan &F) { return F.d32.as<float>(); }
+    static const float *s(const WQFdPlan &F) { return F.s32.as<float>(); }
+    static float *t(const WQFdPlan &F) { return F.t32.as<float>(); }
+};
+
+template <class T, int AX, int EPI>
+static int fd_pass(yeti_wq_op *op, FdArgs<T> a, bool bwd, cudaStream_t s) {
+    const WQFdPlan &F = op->fd;
+    int tot = 0;
+    size_t smem = 0;
+    for (int c = 0; c < 3; c++) {
+        const int m = F.m[c][AX];
+        const int64_t nl = (int64_t)F.m[c][AX == 0 ? 1 : 0] * F.m[c][AX == 2 ? 1 : 2];
+        const FdTile t = fd_tile(m, nl, sizeof(T));
+        a.nag[c] = t.nag;
+        a.nlg[c] = t.nlg;
+        a.ntA[c] = t.ntA;
+        tot += t.ctas;
+        a.cta_end[c] = tot;
+        a.goff[c] = F.goff[c][AX] + (bwd ? (int64_t)m * m : 0);
+        smem = std::max(smem, (size_t)m * (4 * t.nag + 4 * t.nlg + 4) * sizeof(T));
+    }
+    // always the same maximum: concurrent callers cannot lower it under
+    // each other's launch
+    if (smem > 48 * 1024)
+        YETI_CUDA(cudaFuncSetAttribute(k_fd_pass<T, AX, EPI>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kFdSmem));
+    k_fd_pass<T, AX, EPI><<<tot, kFdThreads, smem, s>>>(a);
+    count_launches(1);
+    return YETI_OK;
+}
+
+template <class T>
+int wq_fd_apply(yeti_wq_op *op, const T *in, T *out, const int *done, int red, T *p,
+                CGScal *cg, cudaStream_t s) {
+    const WQFdPlan &F = op->fd;
+    FdArgs<T> a;
+    a.g = FdBufs<T>::g(F);
+    a.dsc = FdBufs<T>::d(F);
+    a.s = F.scaled ? FdBufs<T>::s(F) : nullptr;
+    a.r = in;
+    a.p = p;
+    a.done = done;
+    a.cg = cg;
+    a.parts = F.parts.as<double>();
+    a.red = red;
+    for (int d = 0; d < 3; d++) a.n[d] = op->n[d];
+    a.ncp = op->ncp;
+    for (int c = 0; c < 3; c++)
+        for (int d = 0; d < 3; d++) {
+            a.lo[c][d] = F.lo[c][d];
+            a.m[c][d] = F.m[c][d];
+            a.doff[c][d] = F.doff[c][d];
+        }
+    T *t0 = FdBufs<T>::t(F), *t1 = t0 + op->ndof;
+    a.in = in;
+    if (F.scaled) {
+        // t1 = s r on the free boxes (the first pass reads the boxes only)
+        k_fd_scale_in<T><<<592, 256, 0, s>>>(in, a.s, t1, op->ndof, done);
+        count_launches(1);
+        a.in = t1;
+    }
+    a.out = t0;
+    YETI_TRY((fd_pass<T, 0, 0>(op, a, false, s)));
+    a.in = t0;
+    a.out = t1;
+    YETI_TRY((fd_pass<T, 1, 0>(op, a, false, s)));
+    a.in = t1;
+    a.out = t0;
+    YETI_TRY((fd_pass<T, 2, 1>(op, a, false, s)));
+    a.in = t0;
+    a.out = t1;
+    YETI_TRY((fd_pass<T, 2, 0>(op, a, true, s)));
+    a.in = t1;
+    a.out = t0;
+    YETI_TRY((fd_pass<T, 1, 0>(op, a, true, s)));
+    a.in = t0;
+    a.out = out;
+    YETI_TRY((fd_pass<T, 0, 2>(op, a, true, s)));
+    YETI_CUDA(cudaGetLastError());
+    return YETI_OK;
+}
+
+template int wq_fd_apply<double>(yeti_wq_op *, const double *, double *, const int *, int,
+                                 double *, CGScal *, cudaStream_t);
+template int wq_fd_apply<float>(yeti_wq_op *, const float *, float *, const int *, int, float *,
+                                CGScal *, cudaStream_t);
+
+}  // namespace yeti
+
+using namespace yeti;
+
+YETI_API int yeti_wq_fd_apply(yeti_wq_op *op, const void *r, void *z, int prec, int variant,
+                              int mem) {
+    YETI_CHECK(op && r && z, YETI_EINVAL, "yeti_wq_fd_apply: NULL argument");
+    YETI_CHECK(prec == YETI_PREC_F64 || prec == YETI_PREC_F32, YETI_EINVAL,
+               "yeti_wq_fd_apply: prec %d", prec);
+    YETI_CHECK((variant & YETI_PCG_FD) && !(variant & ~(YETI_PCG_FD | YETI_PCG_FD_SCALED |
+                                                       YETI_PCG_FD_UNIT)),
+               YETI_EINVAL, "yeti_wq_fd_apply: variant %d", variant);
+    DeviceGuard guard(op->ctx->device);
+    const bool f32 = prec == YETI_PREC_F32;
+    YETI_TRY(wq_fd_prepare(op, variant, f32));
+    cudaStream_t s = op->ctx->stream;
+    const size_t es = f32 ? sizeof(float) : sizeof(double);
+    const size_t bytes = (size_t)op->ndof * es;
+    DevBuf dr, dz;
+    const void *rin = r;
+    void *zout = z;
+    if (mem == YETI_MEM_HOST) {
+        YETI_TRY(dr.alloc(op->ctx, bytes));
+        YETI_TRY(dz.alloc(op->ctx, bytes));
+        YETI_CUDA(cudaMemcpyAsync(dr.ptr, r, bytes, cudaMemcpyHostToDevice, s));
+        rin = dr.ptr;
+        zout = dz.ptr;
+    }
+    YETI_CUDA(cudaMemsetAsync(zout, 0, bytes, s));
+    if (f32)
+        YETI_TRY(wq_fd_apply<float>(op, (const float *)rin, (float *)zout, nullptr, FD_NONE,
+                                    nullptr, nullptr, s));
+    else
+        YETI_TRY(wq_fd_apply<double>(op, (const double *)rin, (double *)zout, nullptr, FD_NONE,
+                                     nullptr, nullptr, s));
+    if (mem == YETI_MEM_HOST)
+        YETI_CUDA(cudaMemcpyAsync(z, zout, bytes, cudaMemcpyDeviceToHost, s));
+    YETI_CUDA(cudaStreamSynchronize(s));
+    return YETI_OK;
+}

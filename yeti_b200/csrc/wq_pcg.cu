@@ -13,6 +13,7 @@
 #include <cmath>
 #include <cstring>
 
+#include "reduce.cuh"
 #include "wq.cuh"
 
 namespace yeti {
@@ -20,54 +21,6 @@ namespace yeti {
 constexpr int kRedBlocks = 592;     // 4 x 148 SMs
 constexpr int kRedThreads = 256;
 constexpr int kChunk = 16;          // iterations enqueued per host check
-
-struct CGScal {
-    double rz, pAp, alpha, beta, rr, bb, tol2, scale;
-    int done, iter, breakdown, maxit;
-    unsigned int ticket;   // blocks of a fused reduction that have finished
-};
-
-// Last-block-done: every block publishes its partials, then takes a ticket;
-// the block that takes the last one sees all partials (fixed summation
-// order, so the result does not depend on block timing) and resets the
-// ticket for the next reduction.
-__device__ __forceinline__ bool last_block(unsigned int *ticket) {
-    __shared__ bool last;
-    __threadfence();
-    __syncthreads();
-    if (threadIdx.x == 0) last = atomicAdd(ticket, 1u) == gridDim.x - 1;
-    __syncthreads();
-    if (last) __threadfence();
-    return last;
-}
-
-__device__ __forceinline__ double block_sum(double v, double *sh) {
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
-    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    if (lane == 0) sh[wid] = v;
-    __syncthreads();
-    v = 0.0;
-    if (wid == 0) {
-        v = lane < (int)(blockDim.x >> 5) ? sh[lane] : 0.0;
-        for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
-    }
-    __syncthreads();
-    return v;
-}
-
-__device__ __forceinline__ double block_max(double v, double *sh) {
-    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_down_sync(0xffffffffu, v, o));
-    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    if (lane == 0) sh[wid] = v;
-    __syncthreads();
-    v = 0.0;
-    if (wid == 0) {
-        v = lane < (int)(blockDim.x >> 5) ? sh[lane] : 0.0;
-        for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_down_sync(0xffffffffu, v, o));
-    }
-    __syncthreads();
-    return v;
-}
 
 // Sum of nparts partials (single block, fixed order).
 __device__ inline double sum_parts(const double *parts, int nparts, int stride,
@@ -100,6 +53,15 @@ k_absmax(const A *a, int64_t n, double *parts) {
         v = fmax(v, fabs((double)a[i]));
     v = block_max(v, sh);
     if (threadIdx.x == 0) parts[blockIdx.x] = v;
+}
+
+// End of an iteration: stop the chunk once the residual has dropped to
+// pause2 (a reliable update follows on the host, the direction is kept).
+__global__ void k_pause(CGScal *s) {
+    if (!s->done && s->rr <= s->pause2) {
+        s->done = 1;
+        s->paused = 1;
+    }
 }
 
 // p = z + beta p; Ap = 0
@@ -143,7 +105,8 @@ k_dot_alpha(const T *p, const T *Ap, int64_t n, double *parts, CGScal *s) {
     }
 }
 
-// x += a p; r -= a Ap; z = dinv r; then (last block) beta, rz, rr, stop test
+// x += a p; r -= a Ap; z = dinv r; then (last block) beta, rz, rr, stop test.
+// dinv == nullptr (another preconditioner): no z, r.z or beta here.
 template <class T>
 __global__ void __launch_bounds__(kRedThreads)
 k_update_beta(T *x, T *r, const T *p, const T *Ap, const T *dinv, T *z, int64_t n,
@@ -157,9 +120,11 @@ k_update_beta(T *x, T *r, const T *p, const T *Ap, const T *dinv, T *z, int64_t 
         x[i] += a * p[i];
         const T ri = r[i] - a * Ap[i];
         r[i] = ri;
-        const T zi = dinv[i] * ri;
-        z[i] = zi;
-        rz += (double)ri * (double)zi;
+        if (dinv) {
+            const T zi = dinv[i] * ri;
+            z[i] = zi;
+            rz += (double)ri * (double)zi;
+        }
         rr += (double)ri * (double)ri;
     }
     rz = block_sum(rz, sh);
@@ -180,8 +145,10 @@ k_update_beta(T *x, T *r, const T *p, const T *Ap, const T *dinv, T *z, int64_t 
         s->ticket = 0;
         s->iter += 1;
         s->rr = srr;
-        s->beta = srz / s->rz;
-        s->rz = srz;
+        if (dinv) {
+            s->beta = srz / s->rz;
+            s->rz = srz;
+        }
         if (!isfinite(srr)) {
             s->breakdown = 1;
             s->done = 1;
@@ -199,7 +166,8 @@ __global__ void k_residual(const double *b, const double *Ax,
         r[i] = dinv[i] != 0.0 ? b[i] - Ax[i] : 0.0;
 }
 
-// CG start: z = dinv r, p = z, Ap = 0, partials of r.z and r.r
+// CG start: z = dinv r, p = z, Ap = 0, partials of r.z and r.r (dinv ==
+// nullptr: Ap = 0 and r.r only; the preconditioner sets z, p and r.z)
 template <class T>
 __global__ void __launch_bounds__(kRedThreads)
 k_start(const T *r, const T *dinv, T *z, T *p, T *Ap, int64_t n,
@@ -208,11 +176,13 @@ k_start(const T *r, const T *dinv, T *z, T *p, T *Ap, int64_t n,
     double rz = 0.0, rr = 0.0;
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
          i += (int64_t)gridDim.x * blockDim.x) {
-        const T zi = dinv[i] * r[i];
-        z[i] = zi;
-        p[i] = zi;
+        if (dinv) {
+            const T zi = dinv[i] * r[i];
+            z[i] = zi;
+            p[i] = zi;
+            rz += (double)r[i] * (double)zi;
+        }
         Ap[i] = T(0);
-        rz += (double)r[i] * (double)zi;
         rr += (double)r[i] * (double)r[i];
     }
     rz = block_sum(rz, sh);
@@ -282,11 +252,15 @@ k_ru_replace(const double *r64, float *r32, float *z32, float *p32,
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
          i += (int64_t)gridDim.x * blockDim.x) {
         const float ri = (float)(r64[i] * inv_s);
-        const float zi = dinv[i] * ri;
         r32[i] = ri;
-        z32[i] = zi;
-        p32[i] = restart ? zi : p32[i] * factor;
-        rz += (double)ri * (double)zi;
+        if (dinv) {
+            const float zi = dinv[i] * ri;
+            z32[i] = zi;
+            p32[i] = restart ? zi : p32[i] * factor;
+            rz += (double)ri * (double)zi;
+        } else if (!restart) {
+            p32[i] *= factor;
+        }
         rr += (double)ri * (double)ri;
     }
     rz = block_sum(rz, sh);
@@ -308,6 +282,7 @@ __global__ void k_ru_scal(const double *parts, int nparts, CGScal *s,
         s->tol2 = tol2;
         s->maxit = maxit;
         s->done = 0;
+        s->paused = 0;
     }
 }
 
@@ -335,7 +310,7 @@ k_bi_alpha_s(const double *parts, int nparts, BiScal *s) {
     }
 }
 
-// s = r - alpha v; sh = dinv s; t = 0
+// s = r - alpha v; sh = dinv s (unless dinv == nullptr); t = 0
 template <class T>
 __global__ void __launch_bounds__(kRedThreads)
 k_bi_s(const T *r, const T *v, const T *dinv, T *sv, T *shat, T *t, int64_t n,
@@ -346,7 +321,7 @@ k_bi_s(const T *r, const T *v, const T *dinv, T *sv, T *shat, T *t, int64_t n,
          i += (int64_t)gridDim.x * blockDim.x) {
         const T si = r[i] - a * v[i];
         sv[i] = si;
-        shat[i] = dinv[i] * si;
+        if (dinv) shat[i] = dinv[i] * si;
         t[i] = T(0);
     }
 }
@@ -430,7 +405,7 @@ __global__ void k_bi_beta(const double *parts, int nparts, BiScal *s) {
     }
 }
 
-// p = r + beta (p - omega v); ph = dinv p; v = 0
+// p = r + beta (p - omega v); ph = dinv p (unless dinv == nullptr); v = 0
 template <class T>
 __global__ void __launch_bounds__(kRedThreads)
 k_bi_p(T *p, T *ph, const T *r, T *v, const T *dinv, int64_t n,
@@ -441,12 +416,13 @@ k_bi_p(T *p, T *ph, const T *r, T *v, const T *dinv, int64_t n,
          i += (int64_t)gridDim.x * blockDim.x) {
         const T pi = r[i] + b * (p[i] - w * v[i]);
         p[i] = pi;
-        ph[i] = dinv[i] * pi;
+        if (dinv) ph[i] = dinv[i] * pi;
         v[i] = T(0);
     }
 }
 
-// start: rhat = r, p = r, ph = dinv r, v = 0, partials of r.r
+// start: rhat = r, p = r, ph = dinv r (unless dinv == nullptr), v = 0,
+// partials of r.r
 template <class T>
 __global__ void __launch_bounds__(kRedThreads)
 k_bi_start(const T *r, T *rhat, T *p, T *ph, T *v, const T *dinv, int64_t n,
@@ -457,7 +433,7 @@ k_bi_start(const T *r, T *rhat, T *p, T *ph, T *v, const T *dinv, int64_t n,
          i += (int64_t)gridDim.x * blockDim.x) {
         rhat[i] = r[i];
         p[i] = r[i];
-        ph[i] = dinv[i] * r[i];
+        if (dinv) ph[i] = dinv[i] * r[i];
         v[i] = T(0);
         rr += (double)r[i] * (double)r[i];
     }
@@ -532,9 +508,11 @@ static int ensure_workspace(yeti_wq_op *op, bool f32) {
 
 // Enqueue up to kChunk CG iterations (every kernel exits at once when the
 // device flag is set).
+// dinv == nullptr: the fast-diagonalisation preconditioner gives z, r.z and
+// beta after the update.
 template <class T>
 static int cg_chunk(yeti_wq_op *op, int prec, T *x, T *r, T *z, T *p, T *Ap,
-                    const T *dinv, CGScal *ds) {
+                    const T *dinv, CGScal *ds, bool pause = false) {
     cudaStream_t s = op->ctx->stream;
     const int64_t n = op->ndof;
     double *parts = op->parts.as<double>();
@@ -542,8 +520,13 @@ static int cg_chunk(yeti_wq_op *op, int prec, T *x, T *r, T *z, T *p, T *Ap,
         YETI_TRY(wq_apply_dev(op, p, Ap, prec, &ds->done, s));
         k_dot_alpha<T><<<kRedBlocks, kRedThreads, 0, s>>>(p, Ap, n, parts, ds);
         k_update_beta<T><<<kRedBlocks, kRedThreads, 0, s>>>(x, r, p, Ap, dinv, z, n, parts, ds);
+        if (!dinv) YETI_TRY(wq_fd_apply<T>(op, r, z, &ds->done, FD_ITER, nullptr, ds, s));
         k_pupdate<T><<<kRedBlocks, kRedThreads, 0, s>>>(p, z, Ap, n, ds);
         count_launches(3);
+        if (pause) {
+            k_pause<<<1, 1, 0, s>>>(ds);
+            count_launches(1);
+        }
     }
     YETI_CUDA(cudaGetLastError());
     return YETI_OK;
@@ -575,12 +558,14 @@ static int bi_loop(yeti_wq_op *op, int prec, T *x, T *r, T *rhat, T *p, T *ph,
             k_dot<T, T><<<kRedBlocks, kRedThreads, 0, s>>>(rhat, v, n, parts, &ds->done);
             k_bi_alpha_s<T><<<1, kRedThreads, 0, s>>>(parts, kRedBlocks, ds);
             k_bi_s<T><<<kRedBlocks, kRedThreads, 0, s>>>(r, v, dinv, sv, shat, t, n, ds);
+            if (!dinv) YETI_TRY(wq_fd_apply<T>(op, sv, shat, &ds->done, FD_NONE, nullptr, nullptr, s));
             YETI_TRY(wq_apply_dev(op, shat, t, prec, &ds->done, s));
             k_bi_ts<T><<<kRedBlocks, kRedThreads, 0, s>>>(t, sv, n, parts, ds);
             k_bi_omega<<<1, kRedThreads, 0, s>>>(parts, kRedBlocks, ds);
             k_bi_update<T><<<kRedBlocks, kRedThreads, 0, s>>>(x, r, rhat, ph, shat, sv, t, n, parts, ds);
             k_bi_beta<<<1, kRedThreads, 0, s>>>(parts, kRedBlocks, ds);
             k_bi_p<T><<<kRedBlocks, kRedThreads, 0, s>>>(p, ph, r, v, dinv, n, ds);
+            if (!dinv) YETI_TRY(wq_fd_apply<T>(op, p, ph, &ds->done, FD_NONE, nullptr, nullptr, s));
             count_launches(8);
         }
         YETI_CUDA(cudaGetLastError());
@@ -760,15 +745,19 @@ YETI_API int yeti_wq_pcg(yeti_wq_op *op, const double *b, double *x,
                          double rtol, int maxit, int mode,
                          yeti_cg_stats *stats, int mem) {
     YETI_CHECK(op && b && x, YETI_EINVAL, "yeti_wq_pcg: NULL argument");
-    YETI_CHECK(mode >= 0 && mode <= 3, YETI_EINVAL, "yeti_wq_pcg: mode %d", mode);
+    YETI_CHECK(mode >= 0 && mode < 32 &&
+                   ((mode & (YETI_PCG_FD_SCALED | YETI_PCG_FD_UNIT)) == 0 || (mode & YETI_PCG_FD)),
+               YETI_EINVAL, "yeti_wq_pcg: mode %d", mode);
     YETI_CHECK(rtol > 0 && maxit > 0, YETI_EINVAL, "yeti_wq_pcg: rtol %g maxit %d", rtol, maxit);
     YETI_CHECK(op->coef64.ptr, YETI_EINVAL,
                "yeti_wq_pcg: the FP64 operator is required (true residual)");
-    const bool mixed = (mode & 1) != 0, bicg = (mode & 2) != 0;
+    const bool mixed = (mode & YETI_PCG_MIXED) != 0, bicg = (mode & YETI_PCG_BICGSTAB) != 0;
+    const bool fd = (mode & YETI_PCG_FD) != 0;
     YETI_CHECK(!mixed || op->coef32.ptr, YETI_EINVAL,
                "yeti_wq_pcg: mixed precision needs the FP32 operator (YETI_WQ_F32)");
     DeviceGuard guard(op->ctx->device);
     YETI_TRY(ensure_workspace(op, mixed));
+    if (fd) YETI_TRY(wq_fd_prepare(op, mode, mixed));
     cudaStream_t s = op->ctx->stream;
     const int64_t n = op->ndof;
     double *W = op->ws64.as<double>();
@@ -790,6 +779,14 @@ YETI_API int yeti_wq_pcg(yeti_wq_op *op, const double *b, double *x,
     YETI_CUDA(cudaMemcpyAsync(db, b, n * sizeof(double), h2d, s));
     YETI_CUDA(cudaMemcpyAsync(dx, x, n * sizeof(double), h2d, s));
     const double *dinv = op->dinv64.as<double>();
+    // Jacobi: the kernels apply dinv; FD: nullptr, the FD passes give z
+    const double *pre = fd ? nullptr : dinv;
+    if (fd) {
+        // the FD passes write the free boxes only: clamped entries stay 0
+        for (double *v : {dz, dp, dph, dsh}) YETI_CUDA(cudaMemsetAsync(v, 0, n * sizeof(double), s));
+        if (mixed)
+            YETI_CUDA(cudaMemsetAsync(op->ws32.ptr, 0, 10 * n * sizeof(float), s));
+    }
     k_mask<<<kRedBlocks, kRedThreads, 0, s>>>(db, dinv, n);
     k_mask<<<kRedBlocks, kRedThreads, 0, s>>>(dx, dinv, n);
     k_dot<double, double><<<kRedBlocks, kRedThreads, 0, s>>>(db, db, n, parts, nullptr);
@@ -809,21 +806,23 @@ YETI_API int yeti_wq_pcg(yeti_wq_op *op, const double *b, double *x,
         memset(&init, 0, sizeof(init));
         init.bb = bb;
         YETI_CUDA(cudaMemcpyAsync(ds, &init, sizeof(CGScal), cudaMemcpyHostToDevice, s));
-        k_start<double><<<kRedBlocks, kRedThreads, 0, s>>>(dr, dinv, dz, dp, dAp, n, parts);
+        k_start<double><<<kRedBlocks, kRedThreads, 0, s>>>(dr, pre, dz, dp, dAp, n, parts);
         k_start_scal<<<1, kRedThreads, 0, s>>>(parts, kRedBlocks, ds, rtol * rtol, maxit);
         count_launches(2);
+        if (fd) YETI_TRY(wq_fd_apply<double>(op, dr, dz, &ds->done, FD_START, dp, ds, s));
         YETI_CUDA(cudaGetLastError());
-        YETI_TRY(cg_loop<double>(op, YETI_PREC_F64, dx, dr, dz, dp, dAp, dinv, ds, &hs));
+        YETI_TRY(cg_loop<double>(op, YETI_PREC_F64, dx, dr, dz, dp, dAp, pre, ds, &hs));
         iters = hs.iter;
         f64 += hs.iter;
         if (hs.breakdown) status = YETI_EBREAKDOWN;
         outer = 1;
     } else if (!mixed && bicg) {
-        k_bi_start<double><<<kRedBlocks, kRedThreads, 0, s>>>(dr, drh, dp, dph, dAp, dinv, n, parts);
+        k_bi_start<double><<<kRedBlocks, kRedThreads, 0, s>>>(dr, drh, dp, dph, dAp, pre, n, parts);
         k_bi_start_scal<<<1, kRedThreads, 0, s>>>(parts, kRedBlocks, bs, tol2, maxit);
         count_launches(2);
+        if (fd) YETI_TRY(wq_fd_apply<double>(op, dr, dph, &bs->done, FD_NONE, nullptr, nullptr, s));
         YETI_CUDA(cudaGetLastError());
-        YETI_TRY(bi_loop<double>(op, YETI_PREC_F64, dx, dr, drh, dp, dph, dAp, dsv, dsh, dtt, dinv, bs, &hb));
+        YETI_TRY(bi_loop<double>(op, YETI_PREC_F64, dx, dr, drh, dp, dph, dAp, dsv, dsh, dtt, pre, bs, &hb));
         iters = hb.iter;
         f64 += 2 * hb.iter;
         if (hb.breakdown) status = YETI_EBREAKDOWN;
@@ -837,7 +836,7 @@ YETI_API int yeti_wq_pcg(yeti_wq_op *op, const double *b, double *x,
         // rescaled).
         float *V = op->ws32.as<float>();
         float *r32 = V, *z32 = V + n, *p32 = V + 2 * n, *Ap32 = V + 3 * n, *d32 = V + 4 * n;
-        const float *dinv32 = op->dinv32.as<float>();
+        const float *dinv32 = fd ? nullptr : op->dinv32.as<float>();
         const double delta2 = 1e-2;   // replace when ||r|| fell by 10x
         double rr64 = 0.0;
         k_dot<double, double><<<kRedBlocks, kRedThreads, 0, s>>>(dr, dr, n, parts, nullptr);
@@ -850,13 +849,17 @@ YETI_API int yeti_wq_pcg(yeti_wq_op *op, const double *b, double *x,
             CGScal init;
             memset(&init, 0, sizeof(init));
             init.bb = 1.0;
+            // FD converges by decades per chunk, past what the FP32
+            // recursion tracks: replace at every 10x drop, on the device
+            init.pause2 = fd ? delta2 : 0.0;
             YETI_CUDA(cudaMemcpyAsync(ds, &init, sizeof(CGScal), cudaMemcpyHostToDevice, s));
             k_start_scal<<<1, kRedThreads, 0, s>>>(parts, kRedBlocks, ds, tol2 / rr64, maxit);
             count_launches(3);
+            if (fd) YETI_TRY(wq_fd_apply<float>(op, r32, z32, &ds->done, FD_START, p32, ds, s));
             YETI_CUDA(cudaGetLastError());
             double rr_ref = 1.0;
             for (;;) {
-                YETI_TRY(cg_chunk<float>(op, YETI_PREC_F32, d32, r32, z32, p32, Ap32, dinv32, ds));
+                YETI_TRY(cg_chunk<float>(op, YETI_PREC_F32, d32, r32, z32, p32, Ap32, dinv32, ds, fd));
                 YETI_CUDA(cudaMemcpyAsync(&hs, ds, sizeof(CGScal), cudaMemcpyDeviceToHost, s));
                 YETI_CUDA(cudaStreamSynchronize(s));
                 const int it = hs.iter;
@@ -877,12 +880,17 @@ YETI_API int yeti_wq_pcg(yeti_wq_op *op, const double *b, double *x,
                 if (rr64 <= tol2 || it >= maxit) break;
                 const double sc_new = std::sqrt(rr64);
                 // a replacement after the FP32 recursion met the tolerance
-                // restarts the direction (its last update was skipped)
+                // restarts the direction (its last update was skipped); after
+                // a pause the iteration was complete and the direction stays
+                const int restart = (hs.done && !hs.paused) ? 1 : 0;
                 k_ru_replace<<<kRedBlocks, kRedThreads, 0, s>>>(dr, r32, z32, p32, dinv32, n,
                                                                 1.0 / sc_new, (float)(sc / sc_new),
-                                                                hs.done ? 1 : 0, parts);
+                                                                restart, parts);
                 k_ru_scal<<<1, kRedThreads, 0, s>>>(parts, kRedBlocks, ds, tol2 / rr64, maxit);
                 count_launches(2);
+                if (fd)
+                    YETI_TRY(wq_fd_apply<float>(op, r32, z32, &ds->done,
+                                                restart ? FD_START : FD_REPLACE, p32, ds, s));
                 YETI_CUDA(cudaGetLastError());
                 sc = sc_new;
                 rr_ref = 1.0;
@@ -894,7 +902,7 @@ YETI_API int yeti_wq_pcg(yeti_wq_op *op, const double *b, double *x,
         float *V = op->ws32.as<float>();
         float *r32 = V, *rh = V + n, *p32 = V + 2 * n, *ph = V + 3 * n, *v32 = V + 4 * n,
               *sv = V + 5 * n, *shh = V + 6 * n, *t32 = V + 7 * n, *d32 = V + 8 * n;
-        const float *dinv32 = op->dinv32.as<float>();
+        const float *dinv32 = fd ? nullptr : op->dinv32.as<float>();
         const double eta2 = 1e-8;   // inner relative tolerance 1e-4
         for (outer = 0; outer < 50; outer++) {
             double rr64 = 0.0;
@@ -908,6 +916,7 @@ YETI_API int yeti_wq_pcg(yeti_wq_op *op, const double *b, double *x,
             k_bi_start<float><<<kRedBlocks, kRedThreads, 0, s>>>(r32, rh, p32, ph, v32, dinv32, n, parts);
             k_bi_start_scal<<<1, kRedThreads, 0, s>>>(parts, kRedBlocks, bs, eta2, maxit - iters);
             count_launches(3);
+            if (fd) YETI_TRY(wq_fd_apply<float>(op, r32, ph, &bs->done, FD_NONE, nullptr, nullptr, s));
             YETI_TRY(bi_loop<float>(op, YETI_PREC_F32, d32, r32, rh, p32, ph, v32, sv, shh, t32, dinv32, bs, &hb));
             iters += hb.iter;
             f32 += 2 * hb.iter;

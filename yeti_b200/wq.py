@@ -19,6 +19,24 @@ from .patches import face_mask, free_mask
 
 WQ_F64, WQ_F32 = 1, 2
 
+# Preconditioners of yeti_wq_pcg (mode bits of include/yeti_b200.h).
+PCG_FD, PCG_FD_SCALED, PCG_FD_UNIT = 4, 8, 16
+FD_VARIANTS = {
+    "fd": PCG_FD,                        # a[c][d] = mean S[(c,d),(c,d)]
+    "fd_scaled": PCG_FD | PCG_FD_SCALED,  # ... and sqrt(diag P / diag K)
+    "fd_unit": PCG_FD | PCG_FD_UNIT,      # a[c][d] = 1
+}
+# The reference's Method strings of wq_mf_cg_3d (mf_wq_solver.f90:803-953).
+REFERENCE_METHODS = {"WP": "jacobi", "C": "fd_unit", "JM": "fd", "JMS": "fd_scaled"}
+
+
+def _precond_bits(precond):
+    if precond == "jacobi":
+        return 0
+    if precond not in FD_VARIANTS:
+        raise ValueError(f"precond {precond!r}: 'jacobi' or one of {sorted(FD_VARIANTS)}")
+    return FD_VARIANTS[precond]
+
 
 class WQElasticity:
     """WQ operator of a patch (see ``yeti_b200.patches.cube_patch``).
@@ -92,16 +110,18 @@ class WQElasticity:
 
     # --------------------------------------------------------------- solver
     def pcg(self, b, rtol=1e-8, maxit=20000, mixed=False, x0=None,
-            method="cg"):
-        """Jacobi-preconditioned Krylov solve of K x = b.
+            method="cg", precond="jacobi"):
+        """Preconditioned Krylov solve of K x = b.
 
         method 'cg' (mf_wq_solver.f90:764-802) or 'bicgstab'
         (mf_wq_solver.f90:958-1308).  mixed=True: FP32 operator and Krylov
         vectors with the FP64 true residual (CG: reliable updates; BiCGSTAB:
-        iterative refinement).  b, x0: numpy (host) or torch CUDA float64
-        tensors.  Returns (x, stats dict)."""
+        iterative refinement).  precond: 'jacobi' or a fast-diagonalisation
+        variant of FD_VARIANTS (mf_wq_solver.f90:803-953).  b, x0: numpy
+        (host) or torch CUDA float64 tensors.  Returns (x, stats dict)."""
         st = CGStats()
         mode = (1 if mixed else 0) | (2 if method == "bicgstab" else 0)
+        mode |= _precond_bits(precond)
         if isinstance(b, np.ndarray):
             bb = np.ascontiguousarray(b, dtype=np.float64)
             x = np.zeros_like(bb) if x0 is None else np.array(x0, dtype=np.float64)
@@ -116,15 +136,33 @@ class WQElasticity:
         check(rc, "yeti_wq_pcg")
         return x, st.as_dict()
 
+    def fd_apply(self, r, precond="fd_scaled", prec=PREC_F64):
+        """z = P^{-1} r for a fast-diagonalisation variant of FD_VARIANTS
+        (numpy host arrays: float64 for PREC_F64, float32 for PREC_F32)."""
+        if precond not in FD_VARIANTS:
+            raise ValueError(f"precond {precond!r}: one of {sorted(FD_VARIANTS)}")
+        dt = np.float64 if prec == PREC_F64 else np.float32
+        rr = np.ascontiguousarray(r, dtype=dt)
+        z = np.empty_like(rr)
+        check(lib().yeti_wq_fd_apply(self.handle, ptr(rr), ptr(z), prec,
+                                     FD_VARIANTS[precond], MEM_HOST),
+              "yeti_wq_fd_apply")
+        return z
+
     def mf_conj_grad(self, bi, nbIterations, epsilon, method="WP",
                      directsol=None, isCG=True, mixed=False):
         """Twin of fortran_mf_wq.mf_conj_grad (fortran_mf_wq.py:545-560):
         returns (sol, residue, error) with residue/error the reference's
-        inf-norm measures at the start and the end of the solve."""
-        if method != "WP":
-            raise NotImplementedError("Jacobi preconditioning only ('WP')")
+        inf-norm measures at the start and the end of the solve.  method:
+        'WP' (Jacobi) or the fast-diagonalisation forms 'C', 'JM', 'JMS'
+        (wq_mf_cg_3d, mf_wq_solver.f90:803-953, per displacement
+        component)."""
+        if method not in REFERENCE_METHODS:
+            raise NotImplementedError(
+                f"method {method!r}: supported {sorted(REFERENCE_METHODS)}")
         x, st = self.pcg(bi, rtol=epsilon, maxit=nbIterations, mixed=mixed,
-                         method="cg" if isCG else "bicgstab")
+                         method="cg" if isCG else "bicgstab",
+                         precond=REFERENCE_METHODS[method])
         residue = np.array([1.0, st["rel_residual_inf"]])
         error = np.array([1.0, 0.0])
         if directsol is not None:
