@@ -338,12 +338,21 @@ def extra_configs(args, device):
     sync()
     t_solve = time.perf_counter() - t0
     err = (torch.linalg.norm(x - xref) / torch.linalg.norm(xref)).item()
+    op.pcg(b, rtol=1e-8, mixed=True, precond="fd")   # builds the plan
+    sync()
+    t0 = time.perf_counter()
+    xf, stf = op.pcg(b, rtol=1e-8, mixed=True, precond="fd")
+    sync()
+    t_fd = time.perf_counter() - t0
+    err_fd = (torch.linalg.norm(xf - xref) / torch.linalg.norm(xref)).item()
     out["wq_p4_128x128x32"] = {
         "ndof": op.ndof, "nqp": op.nqp, "apply_f32_us": t_app * 1e6,
         "achieved_gbs": alg / t_app / 1e9, "peak_gbs": peak, "frac": alg / t_app / 1e9 / peak,
         "peak_kind": peak_kind_note(kind), "mixed_solve_s": t_solve,
         "iterations": st["iterations"], "rel_residual": st["rel_residual"],
-        "rel_error_vs_fp64": err, "fp64_ref_rel_residual": st_ref["rel_residual"]}
+        "rel_error_vs_fp64": err, "fp64_ref_rel_residual": st_ref["rel_residual"],
+        "fd_mixed_solve_s": t_fd, "fd_iterations": stf["iterations"],
+        "fd_rel_residual": stf["rel_residual"], "fd_rel_error_vs_fp64": err_fd}
     del op
     return out
 
@@ -455,6 +464,27 @@ def main():
     torch.cuda.synchronize()
     ms64 = e0.elapsed_time(e1) / max(1, args.steps)
 
+    # the same solves with the fast-diagonalisation preconditioner (the
+    # reference's FD branch of wq_mf_cg_3d, 'JM'), device-resident
+    fd = {}
+    for mixed in (False, True):
+        op.pcg(b, rtol=args.rtol, mixed=mixed, precond="fd")   # builds the plan
+        torch.cuda.synchronize()
+        e0.record()
+        for _ in range(max(1, args.steps)):
+            xf, stf = op.pcg(b, rtol=args.rtol, mixed=mixed, precond="fd")
+        e1.record()
+        torch.cuda.synchronize()
+        msf = e0.elapsed_time(e1) / max(1, args.steps)
+        fd["mixed" if mixed else "fp64"] = {
+            "value": ws * op.nfree / (msf / 1e3), "ms_per_step": msf,
+            "iterations": stf["iterations"], "outer_iterations": stf["outer_iterations"],
+            "rel_residual": stf["rel_residual"],
+            "rel_error_vs_fp64_ref": (torch.linalg.norm(xf - xref) / torch.linalg.norm(xref)).item()}
+    fd["mixed_over_jacobi_mixed"] = fd["mixed"]["value"] / value
+    fd["preconditioner"] = ("fast diagonalisation per displacement component, a[c][d] = mean "
+                            "coefficient diagonal ('JM'); FP32 in the mixed solve")
+
     # end to end through the public API with pinned host buffers
     bh = torch.empty(op.ndof, dtype=torch.float64, pin_memory=True)
     bh.copy_(torch.from_numpy(b_host))
@@ -503,6 +533,7 @@ def main():
             "fp64": {"value": ws * op.nfree / (ms64 / 1e3), "ms_per_step": ms64,
                      "iterations": st64["iterations"], "rel_error_vs_fp64_ref": err64},
             "mixed_over_fp64": (value / ws) / (op.nfree / (ms64 / 1e3)),
+            "fd_pcg": fd,
             "setup_s": setup_s,
             "e2e": {"value": ws * op.nfree * args.steps / (ms_e2e / 1e3), "unit": "DOF/s",
                     "h2d_bytes_per_step": 2 * op.ndof * 8,

@@ -191,40 +191,48 @@ struct FdArgs {
     int64_t ncp;
     int lo[3][3], m[3][3];
     int64_t goff[3];   // per component, for this pass
+    int64_t goff2[3];  // fused w pass: the backward matrix
     int64_t doff[3][3];
     int nag[3], nlg[3], ntA[3], cta_end[3];
 };
 
 // Tiles of one pass for one component: ntA tiles of TA = 4 nag output rows
 // times tiles of TL = 4 nlg lines, the whole contraction (m rows of G and of
-// the lines) staged in shared memory: m (TA + TL) elements per CTA.
+// the lines) staged in shared memory.  The fused w pass (two G matrices)
+// needs one row tile.  Lines per CTA are cut until the pass has at least two
+// CTAs per SM (148 SMs) so that no SM idles behind a neighbour with twice
+// its work.
 struct FdTile {
-    int ntA, nag, nlg, ctas;
+    int ntA, nag, nlg, ctas, threads;
+    size_t smem;
 };
-static FdTile fd_tile(int m, int64_t nlines, size_t esize) {
+static FdTile fd_tile(int m, int64_t nlines, size_t esize, bool fused) {
     FdTile t;
-    t.ntA = (m + kFdTA - 1) / kFdTA;
+    const int ng = fused ? 2 : 1;
+    t.ntA = fused ? 1 : (m + kFdTA - 1) / kFdTA;
+    auto bytes = [&](int nag, int nlg) {
+        return (size_t)m * (ng * 4 * nag + 4 * nlg + 4) * esize;
+    };
+    auto ctas = [&](int ntA, int nlg) {
+        return ntA * (int)((nlines + 4 * nlg - 1) / (4 * nlg));
+    };
     for (;;) {
         t.nag = ((m + t.ntA - 1) / t.ntA + 3) / 4;
-        t.nlg = std::min(kFdTL / 4, kFdThreads / t.nag);
-        while (t.nlg > 4 && (size_t)m * (4 * t.nag + 4 * t.nlg + 4) * esize > kFdSmem) t.nlg--;
-        if ((size_t)m * (4 * t.nag + 4 * t.nlg + 4) * esize <= kFdSmem) break;
+        // the most lines per CTA that still give the pass (three components)
+        // two CTAs per SM
+        int nlg = std::min(kFdTL / 4, kFdThreads / t.nag);
+        while (nlg > 4 && ctas(t.ntA, nlg) < (2 * 148 + 2) / 3) nlg--;
+        while (nlg > 4 && bytes(t.nag, nlg) > kFdSmem) nlg--;
+        t.nlg = nlg;
+        if (bytes(t.nag, nlg) <= kFdSmem || fused) break;
         t.ntA++;
     }
-    t.ctas = t.ntA * (int)((nlines + 4 * t.nlg - 1) / (4 * t.nlg));
+    t.smem = bytes(t.nag, t.nlg);
+    t.ctas = ctas(t.ntA, t.nlg);
+    t.threads = (t.nag * t.nlg + 31) / 32 * 32;
+    if (fused && t.smem > kFdSmem) t.ctas = -1;   // not possible: separate passes
     return t;
 }
-
-// Asynchronous global -> shared copy of one element (cp.async, sm_80+);
-// valid == false writes zero and reads nothing.
-template <class T>
-__device__ __forceinline__ void cp_elem(T *sdst, const T *gsrc, bool valid) {
-    const unsigned saddr = (unsigned)__cvta_generic_to_shared(sdst);
-    asm volatile("cp.async.ca.shared.global [%0], [%1], %2, %3;\n" ::"r"(saddr), "l"(gsrc),
-                 "n"((int)sizeof(T)), "r"(valid ? (int)sizeof(T) : 0)
-                 : "memory");
-}
-__device__ __forceinline__ void cp_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
 
 template <class T> struct Vec4;
 template <> struct Vec4<float> {
@@ -241,10 +249,57 @@ template <> struct Vec4<double> {
     }
 };
 
+template <class T>
+__device__ __forceinline__ void fma44(T acc[4][4], const T g[4], const T x[4]) {
+#pragma unroll
+    for (int i = 0; i < 4; i++)
+#pragma unroll
+        for (int j = 0; j < 4; j++) acc[i][j] += g[i] * x[j];
+}
+
+// acc[i][j] = sum_{k < m} gp[k ldg + i] xp[k ldx + j], the next row's
+// operands loaded while the current row's products issue.
+template <class T>
+__device__ __forceinline__ void fd_contract(const T *gp, int ldg, const T *xp, int ldx, int m,
+                                            T acc[4][4]) {
+#pragma unroll
+    for (int i = 0; i < 4; i++)
+#pragma unroll
+        for (int j = 0; j < 4; j++) acc[i][j] = T(0);
+    T g0[4], x0[4], g1[4], x1[4];
+    Vec4<T>::ld(gp, g0);
+    Vec4<T>::ld(xp, x0);
+    int k = 0;
+    for (; k + 1 < m; k += 2) {
+        Vec4<T>::ld(gp + (k + 1) * ldg, g1);
+        Vec4<T>::ld(xp + (k + 1) * ldx, x1);
+        fma44(acc, g0, x0);
+        if (k + 2 < m) {
+            Vec4<T>::ld(gp + (k + 2) * ldg, g0);
+            Vec4<T>::ld(xp + (k + 2) * ldx, x0);
+        }
+        fma44(acc, g1, x1);
+    }
+    if (k < m) fma44(acc, g0, x0);
+}
+
+// Asynchronous global -> shared copy of one element (cp.async, sm_80+);
+// valid == false writes zero and reads nothing.
+template <class T>
+__device__ __forceinline__ void cp_elem(T *sdst, const T *gsrc, bool valid) {
+    const unsigned saddr = (unsigned)__cvta_generic_to_shared(sdst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], %2, %3;\n" ::"r"(saddr), "l"(gsrc),
+                 "n"((int)sizeof(T)), "r"(valid ? (int)sizeof(T) : 0)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
 // One pass along axis AX: out_row(line) = sum_k G[k][row] in_k(line).
 // EPI 1: divide by Lambda; EPI 2: multiply by s, r.z partials and the
-// reduction mode.  The G columns and the lines are staged in shared memory
-// by cp.async (all copies in flight at once), then contracted from there.
+// reduction mode; EPI 3 (AX == 2, one row tile): forward product, division
+// by Lambda and backward product in one CTA, the intermediate kept in shared
+// memory.  The G columns and the lines are staged by cp.async (all copies in
+// flight at once), then contracted from shared memory.
 template <class T, int AX, int EPI>
 __global__ void __launch_bounds__(kFdThreads) k_fd_pass(FdArgs<T> a) {
     extern __shared__ __align__(16) unsigned char fd_smem[];
@@ -260,14 +315,16 @@ __global__ void __launch_bounds__(kFdThreads) k_fd_pass(FdArgs<T> a) {
     const int m = a.m[c][AX], m1 = a.m[c][D1], m2 = a.m[c][D2];
     const int64_t nlines = (int64_t)m1 * m2;
     const int TA = 4 * nag, TL = 4 * nlg, TLp = TL + 4;
-    T *Gs = reinterpret_cast<T *>(fd_smem);   // [m][TA]
-    T *Xs = Gs + (size_t)m * TA;              // [m][TLp]
+    T *Gs = reinterpret_cast<T *>(fd_smem);    // [m][TA]
+    T *G2 = Gs + (size_t)m * TA;               // EPI 3: [m][TA]
+    T *Xs = EPI == 3 ? G2 + (size_t)m * TA : G2;   // [m][TLp]
     const int a0 = (b % ntA) * TA;
     const int64_t l0 = (int64_t)(b / ntA) * TL;
     const int64_t st[3] = {1, (int64_t)a.n[0], (int64_t)a.n[0] * a.n[1]};
     const int64_t sk = st[AX];
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    for (int ll = tid; ll < TL; ll += kFdThreads) {
+    const int nthr = blockDim.x, nwarp = nthr >> 5;
+    for (int ll = tid; ll < TL; ll += nthr) {
         const int64_t l = l0 + ll;
         int64_t base = -1;
         int i1 = 0, i2 = 0;
@@ -282,24 +339,32 @@ __global__ void __launch_bounds__(kFdThreads) k_fd_pass(FdArgs<T> a) {
     }
     // G columns a0 .. a0 + TA of every row k (a warp per row)
     const T *G = a.g + a.goff[c];
-    for (int k = warp; k < m; k += kFdThreads / 32) {
+    for (int k = warp; k < m; k += nwarp) {
         const T *src = G + (int64_t)k * m;
         for (int aa = lane; aa < TA; aa += 32) {
             const int col = a0 + aa;
             cp_elem(Gs + k * TA + aa, col < m ? src + col : G, col < m);
         }
     }
+    if (EPI == 3) {
+        const T *Gb = a.g + a.goff2[c];
+        for (int k = warp; k < m; k += nwarp) {
+            const T *src = Gb + (int64_t)k * m;
+            for (int aa = lane; aa < TA; aa += 32)
+                cp_elem(G2 + k * TA + aa, aa < m ? src + aa : Gb, aa < m);
+        }
+    }
     __syncthreads();   // lb
     if (AX == 0) {
         // lines are contiguous: a warp per line, lanes along k
-        for (int ll = warp; ll < TL; ll += kFdThreads / 32) {
+        for (int ll = warp; ll < TL; ll += nwarp) {
             const int64_t base = lb[ll];
             for (int k = lane; k < m; k += 32)
                 cp_elem(Xs + k * TLp + ll, base >= 0 ? a.in + base + k : a.in, base >= 0);
         }
     } else {
         // row k of the tile is contiguous along the lines: a warp per row
-        for (int k = warp; k < m; k += kFdThreads / 32) {
+        for (int k = warp; k < m; k += nwarp) {
             for (int ll = lane; ll < TL; ll += 32) {
                 const int64_t base = lb[ll];
                 cp_elem(Xs + k * TLp + ll, base >= 0 ? a.in + base + (int64_t)k * sk : a.in,
@@ -319,22 +384,27 @@ __global__ void __launch_bounds__(kFdThreads) k_fd_pass(FdArgs<T> a) {
     }
     const bool act = tid < nag * nlg;
     T acc[4][4];
+    if (act) fd_contract(Gs + 4 * ag, TA, Xs + 4 * lg, TLp, m, acc);
+    if (EPI == 3) {
+        // divide by Lambda, park the eigen-space values in Xs, contract back
+        __syncthreads();
+        if (act) {
 #pragma unroll
-    for (int i = 0; i < 4; i++)
+            for (int i = 0; i < 4; i++) {
+                const int e = 4 * ag + i;
+                if (e >= m) continue;
 #pragma unroll
-        for (int j = 0; j < 4; j++) acc[i][j] = T(0);
-    if (act) {
-        const T *gp = Gs + 4 * ag, *xp = Xs + 4 * lg;
-#pragma unroll 4
-        for (int k = 0; k < m; k++) {
-            T gv[4], xv[4];
-            Vec4<T>::ld(gp + k * TA, gv);
-            Vec4<T>::ld(xp + k * TLp, xv);
-#pragma unroll
-            for (int i = 0; i < 4; i++)
-#pragma unroll
-                for (int j = 0; j < 4; j++) acc[i][j] += gv[i] * xv[j];
+                for (int j = 0; j < 4; j++) {
+                    const int ll = 4 * lg + j;
+                    const int2 q = lc[ll];
+                    const T lam = a.dsc[a.doff[c][0] + q.x] + a.dsc[a.doff[c][1] + q.y] +
+                                  a.dsc[a.doff[c][2] + e];
+                    Xs[e * TLp + ll] = lb[ll] >= 0 ? acc[i][j] / lam : T(0);
+                }
+            }
         }
+        __syncthreads();
+        if (act) fd_contract(G2 + 4 * ag, TA, Xs + 4 * lg, TLp, m, acc);
     }
     double rz = 0.0;
     if (act) {
@@ -556,15 +626,16 @@ int wq_fd_prepare(yeti_wq_op *op, int variant, bool f32) {
     F.t32.release();
     if (f32) YETI_TRY(F.t32.alloc(ctx, 2 * op->ndof * sizeof(float)));
     int maxg = 0;
-    for (int ax = 0; ax < 3; ax++) {
-        int tot = 0;
-        for (int c = 0; c < 3; c++) {
-            const int64_t nl = (int64_t)F.m[c][(ax == 0) ? 1 : 0] * F.m[c][(ax == 2) ? 1 : 2];
-            tot += std::max(fd_tile(F.m[c][ax], nl, sizeof(double)).ctas,
-                            fd_tile(F.m[c][ax], nl, sizeof(float)).ctas);
+    for (int ax = 0; ax < 3; ax++)
+        for (int fused = 0; fused < 2; fused++) {
+            int tot = 0;
+            for (int c = 0; c < 3; c++) {
+                const int64_t nl = (int64_t)F.m[c][(ax == 0) ? 1 : 0] * F.m[c][(ax == 2) ? 1 : 2];
+                for (size_t es : {sizeof(double), sizeof(float)})
+                    tot += std::max(0, fd_tile(F.m[c][ax], nl, es, fused).ctas);
+            }
+            maxg = std::max(maxg, tot);
         }
-        maxg = std::max(maxg, tot);
-    }
     F.max_grid = maxg;
     YETI_TRY(F.parts.alloc(ctx, (size_t)maxg * sizeof(double)));
     F.variant = variant;
@@ -588,28 +659,42 @@ template <> struct FdBufs<float> {
 template <class T, int AX, int EPI>
 static int fd_pass(yeti_wq_op *op, FdArgs<T> a, bool bwd, cudaStream_t s) {
     const WQFdPlan &F = op->fd;
-    int tot = 0;
+    int tot = 0, threads = 32;
     size_t smem = 0;
     for (int c = 0; c < 3; c++) {
         const int m = F.m[c][AX];
         const int64_t nl = (int64_t)F.m[c][AX == 0 ? 1 : 0] * F.m[c][AX == 2 ? 1 : 2];
-        const FdTile t = fd_tile(m, nl, sizeof(T));
+        const FdTile t = fd_tile(m, nl, sizeof(T), EPI == 3);
+        YETI_CHECK(t.ctas > 0, YETI_EINVAL, "fast diagonalisation: no tiling for m=%d", m);
         a.nag[c] = t.nag;
         a.nlg[c] = t.nlg;
         a.ntA[c] = t.ntA;
         tot += t.ctas;
         a.cta_end[c] = tot;
         a.goff[c] = F.goff[c][AX] + (bwd ? (int64_t)m * m : 0);
-        smem = std::max(smem, (size_t)m * (4 * t.nag + 4 * t.nlg + 4) * sizeof(T));
+        a.goff2[c] = F.goff[c][AX] + (int64_t)m * m;
+        smem = std::max(smem, t.smem);
+        threads = std::max(threads, t.threads);
     }
-    // always the same maximum: concurrent callers cannot lower it under
-    // each other's launch
-    if (smem > 48 * 1024)
-        YETI_CUDA(cudaFuncSetAttribute(k_fd_pass<T, AX, EPI>,
-                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kFdSmem));
-    k_fd_pass<T, AX, EPI><<<tot, kFdThreads, smem, s>>>(a);
+    // every component's tile fits `threads` (nag nlg <= threads).  The
+    // 48 KB default covers static plus dynamic shared memory, so opt in on
+    // every launch; the attribute is always the same maximum, so concurrent
+    // callers cannot lower it under each other's launch
+    YETI_CUDA(cudaFuncSetAttribute(k_fd_pass<T, AX, EPI>,
+                                   cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kFdSmem));
+    k_fd_pass<T, AX, EPI><<<tot, threads, smem, s>>>(a);
     count_launches(1);
     return YETI_OK;
+}
+
+// The w pass can run fused (forward, division, backward in one CTA) when
+// every component's w tile is a single row tile that fits.
+static bool fd_w_fused(const WQFdPlan &F, size_t esize) {
+    for (int c = 0; c < 3; c++) {
+        if (F.m[c][2] > kFdTA) return false;
+        if (fd_tile(F.m[c][2], (int64_t)F.m[c][0] * F.m[c][1], esize, true).ctas <= 0) return false;
+    }
+    return true;
 }
 
 template <class T>
@@ -649,14 +734,19 @@ int wq_fd_apply(yeti_wq_op *op, const T *in, T *out, const int *done, int red, T
     YETI_TRY((fd_pass<T, 1, 0>(op, a, false, s)));
     a.in = t1;
     a.out = t0;
-    YETI_TRY((fd_pass<T, 2, 1>(op, a, false, s)));
+    if (fd_w_fused(F, sizeof(T))) {
+        YETI_TRY((fd_pass<T, 2, 3>(op, a, false, s)));
+    } else {
+        YETI_TRY((fd_pass<T, 2, 1>(op, a, false, s)));
+        a.in = t0;
+        a.out = t1;
+        YETI_TRY((fd_pass<T, 2, 0>(op, a, true, s)));
+        std::swap(t0, t1);
+    }
     a.in = t0;
     a.out = t1;
-    YETI_TRY((fd_pass<T, 2, 0>(op, a, true, s)));
-    a.in = t1;
-    a.out = t0;
     YETI_TRY((fd_pass<T, 1, 0>(op, a, true, s)));
-    a.in = t0;
+    a.in = t1;
     a.out = out;
     YETI_TRY((fd_pass<T, 0, 2>(op, a, true, s)));
     YETI_CUDA(cudaGetLastError());
