@@ -54,6 +54,10 @@ def parse():
                     help="Poisson arrival rate of the serving stream (requests/s)")
     ap.add_argument("--serve-budget-gb", type=float, default=32.0)
     ap.add_argument("--no-serve", action="store_true")
+    ap.add_argument("--serve-precond", default="fd", choices=["jacobi", "fd"],
+                    help="preconditioner of the served solves")
+    ap.add_argument("--serve-method", default="bicgstab", choices=["cg", "bicgstab"],
+                    help="Krylov method of the served solves")
     ap.add_argument("--no-extra", action="store_true",
                     help="skip the assembly, gradient and p=4 block measurements")
     return ap.parse_args()
@@ -230,13 +234,15 @@ def run_reference(args):
 def serve_stream(args, device):
     """The serving workload: a seeded stream of requests (cube-like NURBS
     patches, p in {2,3}, 4..32 elements per direction, 1..8 Gaussian
-    right-hand sides, FP64 Jacobi-PCG to 1e-8) with Poisson arrivals at
-    --serve-rate, through the persistent loop (yeti_b200.serve.Server)."""
+    right-hand sides, FP64 preconditioned Krylov solves to 1e-8:
+    --serve-method, --serve-precond) with Poisson arrivals at --serve-rate,
+    through the persistent loop (yeti_b200.serve.Server)."""
     from yeti_b200.serve import Server, run_stream, synthetic_requests
     reqs = synthetic_requests(args.serve_requests, seed=WORKLOAD["seed"] + 7)
     budget = int(args.serve_budget_gb * (1 << 30))
     with Server(device=device, hbm_budget_bytes=budget, max_active=128) as srv:
-        out = run_stream(srv, reqs, args.serve_rate, seed=WORKLOAD["seed"] + 8, rtol=1e-8)
+        out = run_stream(srv, reqs, args.serve_rate, seed=WORKLOAD["seed"] + 8, rtol=1e-8,
+                         precond=args.serve_precond, method=args.serve_method)
         st = srv.stats()
     lat = out["latency_ms"]
     its = [sum(r["iterations"]) for r in out["results"] if r is not None]
@@ -250,7 +256,8 @@ def serve_stream(args, device):
             "thread_ms": {"setup": st["setup_ms"], "retire": st["retire_ms"],
                           "poll": st["poll_ms"]},
             "max_active": 128, "hbm_budget_bytes": budget, "rtol": 1e-8,
-            "precision": "FP64 operator and Krylov vectors"}
+            "precision": "FP64 operator and Krylov vectors",
+            "preconditioner": args.serve_precond, "method": args.serve_method}
 
 
 def _median_ms(fn, reps, sync):

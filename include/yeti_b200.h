@@ -238,7 +238,9 @@ int yeti_grad_lin_elast_work(yeti_ctx *ctx, const yeti_u1_model *model,
  * Submitted requests wait in arrival order and are admitted while fewer than
  * max_active are active and their estimated device bytes fit in
  * hbm_budget_bytes (0: no bound) beside the active ones.  An admitted request
- * gets its WQ operator (FP64 data) and one Jacobi-PCG per right-hand side;
+ * gets its WQ operator (FP64 data) and one FP64 preconditioned Krylov solve
+ * per right-hand side (the request's mode: CG or BiCGSTAB, Jacobi or fast
+ * diagonalisation);
  * the solves of all active requests run concurrently on the device (CUDA
  * graphs of 16 iterations on a pool of streams) with operators and Krylov
  * state resident in HBM.  Submit, poll and wait may be called from any host
@@ -256,6 +258,9 @@ typedef struct {
     const double *rhs;            /* nrhs x 3*ncp host, component-major    */
     double rtol;                  /* ||r||_2 <= rtol ||b||_2               */
     int32_t maxit;
+    int32_t mode;                 /* FP64 Krylov method and preconditioner:
+                                     0 Jacobi CG; YETI_PCG_BICGSTAB and the
+                                     YETI_PCG_FD* bits as yeti_wq_pcg      */
 } yeti_serve_request;
 
 typedef struct {

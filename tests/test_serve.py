@@ -34,8 +34,15 @@ def test_synthetic_requests_are_seeded():
     assert all(1 <= r["nrhs"] <= 8 for r in a)
 
 
+KINDS = [("jacobi", "cg"), ("fd", "cg"), ("fd", "bicgstab"), ("jacobi", "bicgstab")]
+
+
 @pytest.mark.gpu
-def test_result_alone_equals_result_in_the_mix(cuda_ok):
+@pytest.mark.parametrize("precond,method", KINDS[:3])
+def test_result_alone_equals_result_in_the_mix(cuda_ok, precond, method):
+    """The target request alone, then among CG / BiCGSTAB, Jacobi / fast-
+    diagonalisation requests running concurrently (several right-hand sides
+    share one operator): the same solution."""
     from yeti_b200.serve import Server
     clamp = {"w0": (0, 1, 2)}
     target = _request((7, 6, 9), 3, 11, 3)
@@ -43,11 +50,17 @@ def test_result_alone_equals_result_in_the_mix(cuda_ok):
               _request((4, 4, 4), 2, 41, 1), _request((9, 8, 7), 2, 51, 2),
               _request((6, 11, 5), 3, 61, 3)]
     with Server(max_active=1) as srv:
-        x_alone, info_alone = srv.wait(srv.submit(target[0], 1.0, 0.3, clamp, target[1], rtol=1e-10))
+        x_alone, info_alone = srv.wait(srv.submit(target[0], 1.0, 0.3, clamp, target[1],
+                                                  rtol=1e-10, precond=precond, method=method))
     with Server(max_active=16) as srv:
-        t_before = [srv.submit(o[0], 1.0, 0.25, clamp, o[1], rtol=1e-10) for o in others[:3]]
-        t = srv.submit(target[0], 1.0, 0.3, clamp, target[1], rtol=1e-10)
-        t_after = [srv.submit(o[0], 1.0, 0.35, clamp, o[1], rtol=1e-10) for o in others[3:]]
+        t_before = [srv.submit(o[0], 1.0, 0.25, clamp, o[1], rtol=1e-10,
+                               precond=KINDS[i][0], method=KINDS[i][1])
+                    for i, o in enumerate(others[:3])]
+        t = srv.submit(target[0], 1.0, 0.3, clamp, target[1], rtol=1e-10, precond=precond,
+                       method=method)
+        t_after = [srv.submit(o[0], 1.0, 0.35, clamp, o[1], rtol=1e-10,
+                              precond=KINDS[(i + 1) % 4][0], method=KINDS[(i + 1) % 4][1])
+                   for i, o in enumerate(others[3:])]
         x_mix, info_mix = srv.wait(t)
         for tt in t_before + t_after:
             _, inf = srv.wait(tt)
@@ -60,16 +73,18 @@ def test_result_alone_equals_result_in_the_mix(cuda_ok):
 
 
 @pytest.mark.gpu
-def test_served_solution_matches_one_shot_solver(cuda_ok):
+@pytest.mark.parametrize("precond,method", KINDS)
+def test_served_solution_matches_one_shot_solver(cuda_ok, precond, method):
     from yeti_b200.serve import Server
     from yeti_b200.wq import WQElasticity
     clamp = {"w0": (0, 1, 2)}
     patch, rhs = _request((8, 7, 6), 3, 5, 2)
     with Server() as srv:
-        x, info = srv.wait(srv.submit(patch, 1.0, 0.3, clamp, rhs, rtol=1e-10))
+        x, info = srv.wait(srv.submit(patch, 1.0, 0.3, clamp, rhs, rtol=1e-10, precond=precond,
+                                      method=method))
     op = WQElasticity(patch, 1.0, 0.3, clamp, precisions="f64")
     for k in range(2):
-        xr, st = op.pcg(rhs[k], rtol=1e-10)
+        xr, st = op.pcg(rhs[k], rtol=1e-10, precond=precond, method=method)
         assert _rel(x[k], xr) < 1e-8
         assert info["iterations"][k] > 0
 
@@ -100,3 +115,21 @@ def test_oversized_request_is_refused(cuda_ok):
     with Server(hbm_budget_bytes=8 << 20) as srv:
         with pytest.raises(YetiError):
             srv.submit(patch, 1.0, 0.3, {"w0": (0, 1, 2)}, rhs)
+
+
+@pytest.mark.gpu
+def test_fd_bicgstab_converges_where_fd_cg_stalls(cuda_ok):
+    """A request of the serving stream (p=2, 4x24x28 elements, Gaussian
+    right-hand sides) on which FD-preconditioned CG stalls near 1e-7 (the
+    operator is not symmetric; the oracle stalls the same way): the served
+    FD-BiCGSTAB solve reaches 1e-8."""
+    from yeti_b200.serve import Server, synthetic_requests
+    r = synthetic_requests(267, seed=20261203 + 7)[266]
+    assert tuple(r["patch"]["nel"]) == (4, 24, 28)
+    rhs = np.random.default_rng(r["rhs_seed"]).standard_normal((r["nrhs"], r["ndof"]))
+    with Server() as srv:
+        x, info = srv.wait(srv.submit(r["patch"], r["E"], r["nu"], r["clamp"], rhs, rtol=1e-8,
+                                      maxit=2000, precond="fd", method="bicgstab"))
+    assert info["status"] == 0
+    assert max(info["rel_residual"][:r["nrhs"]]) <= 1e-8
+    assert max(info["iterations"][:r["nrhs"]]) < 200

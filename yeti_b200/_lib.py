@@ -63,7 +63,7 @@ class ServeRequest(ctypes.Structure):
         ("cps", c_p), ("weights", c_p), ("E", ctypes.c_double),
         ("nu", ctypes.c_double), ("dirichlet", ctypes.c_uint8 * 18),
         ("nrhs", ctypes.c_int32), ("rhs", c_p), ("rtol", ctypes.c_double),
-        ("maxit", ctypes.c_int32),
+        ("maxit", ctypes.c_int32), ("mode", ctypes.c_int32),
     ]
 
 

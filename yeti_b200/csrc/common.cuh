@@ -127,6 +127,12 @@ struct DeviceGuard {
 // Is `p` device-accessible memory (device or managed)?
 bool is_device_pointer(const void *p);
 
+// Let `func` (a kernel) use the device's whole opt-in shared memory: the
+// same value on every call, so host threads that launch the kernel
+// concurrently cannot lower the limit under each other's launch.  Fails with
+// YETI_EUNSUPPORTED when `need` dynamic bytes exceed it.
+int set_smem_optin(const void *func, int device, size_t need, const char *what);
+
 // Process-wide count of kernel launches issued by the library (reported by
 // yeti_kernel_launches(); lets callers verify the device path ran).
 void count_launches(uint64_t n);

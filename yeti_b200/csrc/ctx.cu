@@ -1,4 +1,5 @@
 // Context management, error reporting and device-memory accounting.
+#include <algorithm>
 #include <atomic>
 #include <cstdarg>
 #include <cstring>
@@ -53,6 +54,18 @@ void dev_free(yeti_ctx *ctx, void *ptr, size_t bytes) {
 static std::atomic<uint64_t> g_launches{0};
 
 void count_launches(uint64_t n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+
+int set_smem_optin(const void *func, int device, size_t need, const char *what) {
+    int optin = 0;
+    YETI_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device));
+    cudaFuncAttributes fa;
+    YETI_CUDA(cudaFuncGetAttributes(&fa, func));
+    const int dyn = optin - (int)fa.sharedSizeBytes;
+    YETI_CHECK(need <= (size_t)std::max(dyn, 0), YETI_EUNSUPPORTED,
+               "%s needs %zu bytes of dynamic shared memory (limit %d)", what, need, dyn);
+    YETI_CUDA(cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn));
+    return YETI_OK;
+}
 
 bool is_device_pointer(const void *p) {
     cudaPointerAttributes a;

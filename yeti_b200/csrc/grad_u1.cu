@@ -672,7 +672,7 @@ YETI_API int yeti_grad_lin_elast_work(yeti_ctx *ctx, const yeti_u1_model *m,
         const size_t smem = sizeof(double) * ((size_t)(6 + 3 * nadj) * P.nn + P.nn + std::max(vol, face));
         YETI_CHECK(smem <= (size_t)smem_optin, YETI_EUNSUPPORTED,
                    "shape gradient: element needs %zu bytes of shared memory", smem);
-        YETI_CUDA(cudaFuncSetAttribute(k_u1_grad, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        YETI_TRY(set_smem_optin((const void *)k_u1_grad, ctx->device, smem, "shape gradient element"));
         k_u1_grad<<<(unsigned)elems.size(), 256, smem, s>>>(g);
         count_launches(1);
         YETI_CUDA(cudaGetLastError());

@@ -54,7 +54,7 @@ struct Request {
     int p[3] = {0, 0, 0}, nel[3] = {0, 0, 0};
     std::vector<double> cps, weights, rhs;
     double E = 0, nu = 0, rtol = 0;
-    int maxit = 0, nrhs = 0;
+    int maxit = 0, nrhs = 0, mode = 0;
     uint8_t dir[18] = {};
     int64_t ndof = 0;
     size_t est = 0;
@@ -72,16 +72,22 @@ struct Request {
 
 // Device bytes a request may hold at its peak: the FP64 coefficients twice
 // (element-block and streaming layouts during the re-layout), |det J|, the
-// diagonal and its inverse, six vectors per right-hand side, and tables.
+// diagonal and its inverse, six vectors per right-hand side (CG; BiCGSTAB
+// eleven), and tables; with fast diagonalisation two more vectors per
+// right-hand side and the plan's two intermediate vectors and 1-D matrices.
 size_t estimate_bytes(const Request &r) {
-    int64_t nqp = 1, ncp = 1;
+    int64_t nqp = 1, ncp = 1, mat = 0;
     for (int d = 0; d < 3; d++) {
         nqp *= 2 * (r.p[d] + r.nel[d]) - 1;
         ncp *= r.p[d] + r.nel[d];
+        mat += 2 * (int64_t)(r.p[d] + r.nel[d]) * (r.p[d] + r.nel[d]);
     }
     const int64_t ndof = 3 * ncp;
+    const int64_t fd = (r.mode & YETI_PCG_FD) ? 1 : 0;
+    const int64_t vec = (r.mode & YETI_PCG_BICGSTAB) ? 11 : 6;
     return (size_t)(nqp * 45 * 8 * 2 + nqp * 8 + ndof * 8 * 2 +
-                    (int64_t)r.nrhs * (6 * ndof * 8 + 65536)) + ((size_t)4 << 20);
+                    (int64_t)r.nrhs * ((vec + 2 * fd) * ndof * 8 + 65536) +
+                    fd * (2 * ndof * 8 + 3 * mat * 8)) + ((size_t)4 << 20);
 }
 
 }  // namespace
@@ -173,7 +179,7 @@ struct yeti_server {
                 st = streams[rr++ % (int)streams.size()];
             }
             rc = cgsolve_begin(*cs, op, st, slot, r->rhs.data() + (size_t)k * r->ndof, r->rtol,
-                               r->maxit, cap);
+                               r->maxit, cap, r->mode);
             cs->host_scal = slot;   // returned by finish whatever happened
             if (rc == YETI_OK) rc = cgsolve_launch(*cs);
             r->solves.push_back(std::move(cs));
@@ -373,6 +379,13 @@ YETI_API int yeti_serve_submit(yeti_server *srv, const yeti_serve_request *q, in
                "yeti_serve_submit: nrhs %d not in 1..%d", q->nrhs, kMaxRhs);
     YETI_CHECK(q->rtol > 0 && q->maxit > 0, YETI_EINVAL, "yeti_serve_submit: rtol %g maxit %d",
                q->rtol, q->maxit);
+    {
+        const int fd_bits = YETI_PCG_FD | YETI_PCG_FD_SCALED | YETI_PCG_FD_UNIT;
+        YETI_CHECK((q->mode & ~(fd_bits | YETI_PCG_BICGSTAB)) == 0 &&
+                       ((q->mode & fd_bits) == 0 || (q->mode & YETI_PCG_FD)),
+                   YETI_EINVAL, "yeti_serve_submit: mode %d (FP64 CG/BiCGSTAB, Jacobi/FD)",
+                   q->mode);
+    }
     std::unique_ptr<Request> r(new Request());
     int64_t ncp = 1;
     for (int d = 0; d < 3; d++) {
@@ -391,6 +404,7 @@ YETI_API int yeti_serve_submit(yeti_server *srv, const yeti_serve_request *q, in
     r->nu = q->nu;
     r->rtol = q->rtol;
     r->maxit = q->maxit;
+    r->mode = q->mode;
     r->nrhs = q->nrhs;
     std::memcpy(r->dir, q->dirichlet, 18);
     r->est = estimate_bytes(*r);

@@ -659,8 +659,7 @@ static int launch_apply(yeti_wq_op *op, const T *u, T *Ku, const int *done,
     a.Ku = Ku;
     a.done = done;
     const size_t smem = smem_bytes(op, 3, 6, sizeof(T));
-    YETI_TRY(wq_smem_limit(op->ctx, smem));
-    YETI_CUDA(cudaFuncSetAttribute(k_wq_apply<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    YETI_TRY(set_smem_optin((const void *)k_wq_apply<T>, op->ctx->device, smem, "WQ apply block"));
     k_wq_apply<T><<<(unsigned)op->nblocks, kWQThreads, smem, s>>>(a);
     count_launches(1);
     YETI_CUDA(cudaGetLastError());
@@ -817,7 +816,7 @@ YETI_API int yeti_wq_setup(yeti_ctx *ctx, const int32_t p[3],
     {
         const size_t smem = smem_bytes(op.get(), 4, 2, sizeof(double));
         YETI_TRY(wq_smem_limit(ctx, smem));
-        YETI_CUDA(cudaFuncSetAttribute(k_wq_setup, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        YETI_TRY(set_smem_optin((const void *)k_wq_setup, ctx->device, smem, "WQ setup block"));
         k_wq_setup<<<(unsigned)op->nblocks, kWQThreads, smem, ctx->stream>>>(sa);
         count_launches(1);
         YETI_CUDA(cudaGetLastError());
@@ -839,7 +838,7 @@ YETI_API int yeti_wq_setup(yeti_ctx *ctx, const int32_t p[3],
             da.v = make_view<double>(op.get(), op->tiles64, op->coef64);
             for (int d = 0; d < 3; d++) da.dtiles[d] = op->dtiles[d].as<double>();
             da.diag = op->diag.as<double>();
-            YETI_CUDA(cudaFuncSetAttribute(k_wq_diag<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+            YETI_TRY(set_smem_optin((const void *)k_wq_diag<double>, ctx->device, smem, "WQ diagonal block"));
             k_wq_diag<double><<<(unsigned)op->nblocks, kWQThreads, smem, ctx->stream>>>(da);
             count_launches(1);
         } else {
@@ -856,7 +855,7 @@ YETI_API int yeti_wq_setup(yeti_ctx *ctx, const int32_t p[3],
             da.v = make_view<float>(op.get(), op->tiles32, op->coef32);
             for (int d = 0; d < 3; d++) da.dtiles[d] = dt[d].as<float>();
             da.diag = op->diag.as<double>();
-            YETI_CUDA(cudaFuncSetAttribute(k_wq_diag<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+            YETI_TRY(set_smem_optin((const void *)k_wq_diag<float>, ctx->device, smem, "WQ diagonal block"));
             k_wq_diag<float><<<(unsigned)op->nblocks, kWQThreads, smem, ctx->stream>>>(da);
             count_launches(1);
             YETI_CUDA(cudaStreamSynchronize(ctx->stream));
@@ -973,7 +972,7 @@ YETI_API int yeti_wq_body_force(yeti_wq_op *op, const double f[3], double *F,
     a.F = FF;
     const size_t smem = smem_bytes(op, 3, 6, sizeof(double));
     YETI_TRY(wq_smem_limit(op->ctx, smem));
-    YETI_CUDA(cudaFuncSetAttribute(k_wq_force, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    YETI_TRY(set_smem_optin((const void *)k_wq_force, op->ctx->device, smem, "WQ force block"));
     k_wq_force<<<(unsigned)op->nblocks, kWQThreads, smem, s>>>(a);
     count_launches(1);
     YETI_CUDA(cudaGetLastError());

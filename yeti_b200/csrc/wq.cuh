@@ -103,9 +103,14 @@ enum FdRed { FD_NONE = 0, FD_ITER = 1, FD_START = 2, FD_REPLACE = 3 };
 int wq_fd_prepare(yeti_wq_op *op, int variant, bool f32);
 // out = P in.  red FD_ITER: beta = r.z / rz, rz = r.z into *cg; FD_START:
 // rz = r.z and p = z; FD_REPLACE: rz = r.z.  (in is r for those modes.)
+// tmp (2 ndof) and parts (wq_fd_parts(op) doubles): the caller's
+// workspace, for solves that share the operator concurrently; nullptr:
+// the plan's own.  Launch-only (graph-capturable) once the plan exists.
 template <class T>
 int wq_fd_apply(yeti_wq_op *op, const T *in, T *out, const int *done, int red,
-                T *p, CGScal *cg, cudaStream_t s);
+                T *p, CGScal *cg, cudaStream_t s, T *tmp = nullptr, double *parts = nullptr);
+// Doubles of reduction partials one FD application needs.
+int wq_fd_parts(const yeti_wq_op *op);
 
 bool wq_stream_supported(const yeti_wq_op *op);
 // Build the tile tables and work segments (after the 1-D rules).
@@ -115,13 +120,16 @@ int wq_stream_setup(yeti_wq_op *op, const WQRule1D R[3]);
 int wq_stream_permute(yeti_wq_op *op);
 template <class T>
 int wq_stream_apply(yeti_wq_op *op, const T *u, T *Ku, const int *done, cudaStream_t s);
-// One FP64 Jacobi-PCG solve of a WQ operator (x0 = 0) that advances in
+// One FP64 preconditioned Krylov solve (CG or BiCGSTAB; Jacobi or fast
+// diagonalisation) of a WQ operator (x0 = 0) that advances in
 // chunks of iterations captured once in a CUDA graph, on its own stream and
 // without host synchronisation: the serving loop launches a chunk, polls its
 // event, and launches the next until the device-side scalars say done.  The
 // workspace is allocated stream-ordered on that stream.
 struct CgSolve {
     yeti_wq_op *op = nullptr;
+    bool fd = false;             // fast-diagonalisation preconditioner
+    bool bicg = false;           // BiCGSTAB instead of CG
     cudaStream_t stream = nullptr;
     void *dmem = nullptr;        // b x r z p Ap (6n doubles), partials, scalars
     void *host_scal = nullptr;   // pinned copy of the scalars (owned by the caller)
@@ -138,9 +146,10 @@ struct CgSolve {
 size_t cgsolve_scal_bytes();
 // The chunk graph is captured on `capture` when given (a stream no other
 // thread enqueues into while it is captured), else on s.
+// mode: YETI_PCG_BICGSTAB and the YETI_PCG_FD* bits (clear: Jacobi CG).
 int cgsolve_begin(CgSolve &cs, yeti_wq_op *op, cudaStream_t s, void *host_scal,
                   const double *b_host, double rtol, int maxit,
-                  cudaStream_t capture = nullptr);
+                  cudaStream_t capture = nullptr, int mode = 0);
 // Enqueue the next chunk (graph launch + event).
 int cgsolve_launch(CgSolve &cs);
 // *state: 0 a chunk is in flight, 1 chunk done and more iterations needed,

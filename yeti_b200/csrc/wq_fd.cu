@@ -489,10 +489,27 @@ __global__ void k_fd_scaling(const double *diagK, const double *kdmd, double *s6
 }
 
 // ------------------------------------------------------------------ plan
+template <class T>
+static int fd_set_attrs() {
+    const int b = (int)kFdSmem;
+    const cudaFuncAttribute a = cudaFuncAttributeMaxDynamicSharedMemorySize;
+    YETI_CUDA(cudaFuncSetAttribute(k_fd_pass<T, 0, 0>, a, b));
+    YETI_CUDA(cudaFuncSetAttribute(k_fd_pass<T, 1, 0>, a, b));
+    YETI_CUDA(cudaFuncSetAttribute(k_fd_pass<T, 2, 0>, a, b));
+    YETI_CUDA(cudaFuncSetAttribute(k_fd_pass<T, 2, 1>, a, b));
+    YETI_CUDA(cudaFuncSetAttribute(k_fd_pass<T, 2, 3>, a, b));
+    YETI_CUDA(cudaFuncSetAttribute(k_fd_pass<T, 0, 2>, a, b));
+    return YETI_OK;
+}
+
 int wq_fd_prepare(yeti_wq_op *op, int variant, bool f32) {
     WQFdPlan &F = op->fd;
     variant &= (YETI_PCG_FD | YETI_PCG_FD_SCALED | YETI_PCG_FD_UNIT);
     if (F.variant == variant && (!f32 || F.g32.ptr)) return YETI_OK;
+    // the passes stage up to kFdSmem bytes: opt in once per device (the
+    // attribute is always this maximum, so concurrent callers agree)
+    YETI_TRY(fd_set_attrs<double>());
+    YETI_TRY(fd_set_attrs<float>());
     yeti_ctx *ctx = op->ctx;
     cudaStream_t s = ctx->stream;
     const bool unit = (variant & YETI_PCG_FD_UNIT) != 0;
@@ -638,6 +655,9 @@ int wq_fd_prepare(yeti_wq_op *op, int variant, bool f32) {
         }
     F.max_grid = maxg;
     YETI_TRY(F.parts.alloc(ctx, (size_t)maxg * sizeof(double)));
+    // the tables were uploaded (and, on a stream-ordered context,
+    // allocated) on the context's stream; solves may run on other streams
+    YETI_CUDA(cudaStreamSynchronize(s));
     F.variant = variant;
     return YETI_OK;
 }
@@ -677,11 +697,8 @@ static int fd_pass(yeti_wq_op *op, FdArgs<T> a, bool bwd, cudaStream_t s) {
         threads = std::max(threads, t.threads);
     }
     // every component's tile fits `threads` (nag nlg <= threads).  The
-    // 48 KB default covers static plus dynamic shared memory, so opt in on
-    // every launch; the attribute is always the same maximum, so concurrent
-    // callers cannot lower it under each other's launch
-    YETI_CUDA(cudaFuncSetAttribute(k_fd_pass<T, AX, EPI>,
-                                   cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kFdSmem));
+    // shared-memory opt-in (the 48 KB default covers static plus dynamic
+    // memory) is set by wq_fd_prepare on this device, outside any capture
     k_fd_pass<T, AX, EPI><<<tot, threads, smem, s>>>(a);
     count_launches(1);
     return YETI_OK;
@@ -699,7 +716,7 @@ static bool fd_w_fused(const WQFdPlan &F, size_t esize) {
 
 template <class T>
 int wq_fd_apply(yeti_wq_op *op, const T *in, T *out, const int *done, int red, T *p,
-                CGScal *cg, cudaStream_t s) {
+                CGScal *cg, cudaStream_t s, T *tmp, double *parts) {
     const WQFdPlan &F = op->fd;
     FdArgs<T> a;
     a.g = FdBufs<T>::g(F);
@@ -709,7 +726,7 @@ int wq_fd_apply(yeti_wq_op *op, const T *in, T *out, const int *done, int red, T
     a.p = p;
     a.done = done;
     a.cg = cg;
-    a.parts = F.parts.as<double>();
+    a.parts = parts ? parts : F.parts.as<double>();
     a.red = red;
     for (int d = 0; d < 3; d++) a.n[d] = op->n[d];
     a.ncp = op->ncp;
@@ -719,7 +736,7 @@ int wq_fd_apply(yeti_wq_op *op, const T *in, T *out, const int *done, int red, T
             a.m[c][d] = F.m[c][d];
             a.doff[c][d] = F.doff[c][d];
         }
-    T *t0 = FdBufs<T>::t(F), *t1 = t0 + op->ndof;
+    T *t0 = tmp ? tmp : FdBufs<T>::t(F), *t1 = t0 + op->ndof;
     a.in = in;
     if (F.scaled) {
         // t1 = s r on the free boxes (the first pass reads the boxes only)
@@ -754,9 +771,11 @@ int wq_fd_apply(yeti_wq_op *op, const T *in, T *out, const int *done, int red, T
 }
 
 template int wq_fd_apply<double>(yeti_wq_op *, const double *, double *, const int *, int,
-                                 double *, CGScal *, cudaStream_t);
+                                 double *, CGScal *, cudaStream_t, double *, double *);
 template int wq_fd_apply<float>(yeti_wq_op *, const float *, float *, const int *, int, float *,
-                                CGScal *, cudaStream_t);
+                                CGScal *, cudaStream_t, float *, double *);
+
+int wq_fd_parts(const yeti_wq_op *op) { return op->fd.max_grid; }
 
 }  // namespace yeti
 

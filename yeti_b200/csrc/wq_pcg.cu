@@ -456,6 +456,23 @@ __global__ void k_bi_start_scal(const double *parts, int nparts, BiScal *s,
     }
 }
 
+// as k_bi_start_scal with the tolerance relative to the start residual
+// (x0 = 0: r = b)
+__global__ void k_bi_start_scal_rel(const double *parts, int nparts, BiScal *s,
+                                    double rel2, int maxit) {
+    __shared__ double sh[32];
+    const double rr = sum_parts(parts, nparts, 1, 0, sh);
+    if (threadIdx.x == 0) {
+        s->rho = rr;
+        s->rr = rr;
+        s->iter = 0;
+        s->breakdown = 0;
+        s->maxit = maxit;
+        s->tol2 = rel2 * rr;
+        s->done = (rr <= s->tol2) || maxit <= 0 || !(rr == rr);
+    }
+}
+
 // dinv = 1/diag on free dofs, 0 on clamped ones; b masked likewise
 template <class T>
 __global__ void k_dinv(const double *diag, T *dinv, int64_t ncp, int3 n,
@@ -589,7 +606,7 @@ static int ensure_dinv64(yeti_wq_op *op) {
     return YETI_OK;
 }
 
-size_t cgsolve_scal_bytes() { return sizeof(CGScal); }
+size_t cgsolve_scal_bytes() { return std::max(sizeof(CGScal), sizeof(BiScal)); }
 
 void CgSolve::release() {
     if (chunk) cudaGraphExecDestroy(chunk);
@@ -601,14 +618,23 @@ void CgSolve::release() {
     in_flight = false;
 }
 
+// Workspace of a resumable solve: vectors, partials, the scalars (CGScal or
+// BiScal), the FD workspace.  CG: b x r z p Ap; BiCGSTAB: b x r (z unused)
+// p v (in Ap) and rhat ph s shat t.
 struct SolveView {
     double *b, *x, *r, *z, *p, *Ap, *parts;
+    double *rhat, *ph, *sv, *shat, *t;   // BiCGSTAB
     CGScal *s;
+    BiScal *bs;
+    double *fdt, *fdparts;   // FD: two intermediate vectors, partials
 };
+
+static int solve_vectors(bool bicg) { return bicg ? 11 : 6; }
 
 static SolveView solve_view(const CgSolve &cs) {
     const int64_t n = cs.op->ndof;
     double *W = static_cast<double *>(cs.dmem);
+    const int nv = solve_vectors(cs.bicg);
     SolveView v;
     v.b = W;
     v.x = W + n;
@@ -616,37 +642,77 @@ static SolveView solve_view(const CgSolve &cs) {
     v.z = W + 3 * n;
     v.p = W + 4 * n;
     v.Ap = W + 5 * n;
-    v.parts = W + 6 * n;
-    v.s = reinterpret_cast<CGScal *>(W + 6 * n + 2 * cs.nblk);
+    v.rhat = cs.bicg ? W + 6 * n : nullptr;
+    v.ph = cs.bicg ? W + 7 * n : nullptr;
+    v.sv = cs.bicg ? W + 8 * n : nullptr;
+    v.shat = cs.bicg ? W + 9 * n : nullptr;
+    v.t = cs.bicg ? W + 10 * n : nullptr;
+    v.parts = W + nv * n;
+    v.s = reinterpret_cast<CGScal *>(W + nv * n + 2 * cs.nblk);
+    v.bs = reinterpret_cast<BiScal *>(v.s);
+    // the scalar slots are multiples of 8 bytes: the FD workspace stays aligned
+    v.fdt = reinterpret_cast<double *>(reinterpret_cast<char *>(v.s) + 2 * cgsolve_scal_bytes());
+    v.fdparts = v.fdt + 2 * n;
     return v;
 }
 
 int cgsolve_begin(CgSolve &cs, yeti_wq_op *op, cudaStream_t st, void *host_scal,
-                  const double *b_host, double rtol, int maxit, cudaStream_t capture) {
+                  const double *b_host, double rtol, int maxit, cudaStream_t capture,
+                  int mode) {
     YETI_CHECK(op && host_scal && b_host && op->coef64.ptr, YETI_EINVAL,
                "cgsolve_begin: missing operator data");
+    const int fd_bits = YETI_PCG_FD | YETI_PCG_FD_SCALED | YETI_PCG_FD_UNIT;
+    YETI_CHECK((mode & ~(fd_bits | YETI_PCG_BICGSTAB)) == 0 &&
+                   ((mode & fd_bits) == 0 || (mode & YETI_PCG_FD)),
+               YETI_EINVAL, "cgsolve_begin: mode %d", mode);
     YETI_TRY(ensure_dinv64(op));
+    const bool fd = (mode & YETI_PCG_FD) != 0, bicg = (mode & YETI_PCG_BICGSTAB) != 0;
+    if (fd) YETI_TRY(wq_fd_prepare(op, mode, false));
     cs.release();
     cs.op = op;
+    cs.fd = fd;
+    cs.bicg = bicg;
     cs.stream = st;
     cs.host_scal = host_scal;
     const int64_t n = op->ndof;
     cs.nblk = (int)std::max<int64_t>(1, std::min<int64_t>(kRedBlocks, (n + kRedThreads - 1) / kRedThreads));
-    const size_t bytes = (6 * n + 2 * (size_t)cs.nblk) * sizeof(double) + 2 * sizeof(CGScal);
+    const size_t fd_doubles = fd ? 2 * (size_t)n + (size_t)wq_fd_parts(op) : 0;
+    const size_t bytes = ((size_t)solve_vectors(bicg) * n + 2 * (size_t)cs.nblk + fd_doubles) *
+                             sizeof(double) + 2 * cgsolve_scal_bytes();
     YETI_CUDA(cudaMallocAsync(&cs.dmem, bytes, st));
     const SolveView v = solve_view(cs);
     const double *dinv = op->dinv64.as<double>();
+    const double *pre = fd ? nullptr : dinv;
     const int nb = cs.nblk;
     YETI_CUDA(cudaMemcpyAsync(v.b, b_host, n * sizeof(double), cudaMemcpyHostToDevice, st));
     YETI_CUDA(cudaMemsetAsync(v.x, 0, n * sizeof(double), st));
-    YETI_CUDA(cudaMemsetAsync(v.s, 0, sizeof(CGScal), st));
+    YETI_CUDA(cudaMemsetAsync(v.s, 0, cgsolve_scal_bytes(), st));
+    if (fd) {
+        // the FD passes write the free boxes only: clamped entries stay 0
+        for (double *w : {v.z, v.p, v.ph, v.shat})
+            if (w) YETI_CUDA(cudaMemsetAsync(w, 0, n * sizeof(double), st));
+    }
     k_mask<<<nb, kRedThreads, 0, st>>>(v.b, dinv, n);
     YETI_CUDA(cudaMemcpyAsync(v.r, v.b, n * sizeof(double), cudaMemcpyDeviceToDevice, st));
-    k_dot<double, double><<<nb, kRedThreads, 0, st>>>(v.b, v.b, n, v.parts, nullptr);
-    k_set_bb<<<1, kRedThreads, 0, st>>>(v.parts, nb, v.s);
-    k_start<double><<<nb, kRedThreads, 0, st>>>(v.r, dinv, v.z, v.p, v.Ap, n, v.parts);
-    k_start_scal<<<1, kRedThreads, 0, st>>>(v.parts, nb, v.s, rtol * rtol, maxit);
-    count_launches(5);
+    if (!bicg) {
+        k_dot<double, double><<<nb, kRedThreads, 0, st>>>(v.b, v.b, n, v.parts, nullptr);
+        k_set_bb<<<1, kRedThreads, 0, st>>>(v.parts, nb, v.s);
+        k_start<double><<<nb, kRedThreads, 0, st>>>(v.r, pre, v.z, v.p, v.Ap, n, v.parts);
+        k_start_scal<<<1, kRedThreads, 0, st>>>(v.parts, nb, v.s, rtol * rtol, maxit);
+        count_launches(5);
+        if (fd)
+            YETI_TRY(wq_fd_apply<double>(op, v.r, v.z, &v.s->done, FD_START, v.p, v.s, st, v.fdt,
+                                         v.fdparts));
+    } else {
+        // rhat = r, p = r, ph = P r, v = 0 (v lives in Ap)
+        k_bi_start<double><<<nb, kRedThreads, 0, st>>>(v.r, v.rhat, v.p, v.ph, v.Ap, pre, n,
+                                                       v.parts);
+        k_bi_start_scal_rel<<<1, kRedThreads, 0, st>>>(v.parts, nb, v.bs, rtol * rtol, maxit);
+        count_launches(3);
+        if (fd)
+            YETI_TRY(wq_fd_apply<double>(op, v.r, v.ph, &v.bs->done, FD_NONE, nullptr, nullptr, st,
+                                         v.fdt, v.fdparts));
+    }
     YETI_CUDA(cudaGetLastError());
     // one chunk of iterations, captured once
     cudaGraph_t g = nullptr;
@@ -654,13 +720,38 @@ int cgsolve_begin(CgSolve &cs, yeti_wq_op *op, cudaStream_t st, void *host_scal,
     YETI_CUDA(cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal));
     int rc = YETI_OK;
     for (int k = 0; k < kChunk && rc == YETI_OK; k++) {
-        rc = wq_apply_dev(op, v.p, v.Ap, YETI_PREC_F64, &v.s->done, cap);
-        k_dot_alpha<double><<<nb, kRedThreads, 0, cap>>>(v.p, v.Ap, n, v.parts, v.s);
-        k_update_beta<double><<<nb, kRedThreads, 0, cap>>>(v.x, v.r, v.p, v.Ap, dinv, v.z, n,
-                                                          v.parts, v.s);
-        k_pupdate<double><<<nb, kRedThreads, 0, cap>>>(v.p, v.z, v.Ap, n, v.s);
+        if (!bicg) {
+            rc = wq_apply_dev(op, v.p, v.Ap, YETI_PREC_F64, &v.s->done, cap);
+            k_dot_alpha<double><<<nb, kRedThreads, 0, cap>>>(v.p, v.Ap, n, v.parts, v.s);
+            k_update_beta<double><<<nb, kRedThreads, 0, cap>>>(v.x, v.r, v.p, v.Ap, pre, v.z, n,
+                                                              v.parts, v.s);
+            if (fd && rc == YETI_OK)
+                rc = wq_fd_apply<double>(op, v.r, v.z, &v.s->done, FD_ITER, nullptr, v.s, cap,
+                                         v.fdt, v.fdparts);
+            k_pupdate<double><<<nb, kRedThreads, 0, cap>>>(v.p, v.z, v.Ap, n, v.s);
+        } else {
+            // the BiCGSTAB iteration of bi_loop (v in Ap)
+            BiScal *bs = v.bs;
+            rc = wq_apply_dev(op, v.ph, v.Ap, YETI_PREC_F64, &bs->done, cap);
+            k_dot<double, double><<<nb, kRedThreads, 0, cap>>>(v.rhat, v.Ap, n, v.parts, &bs->done);
+            k_bi_alpha_s<double><<<1, kRedThreads, 0, cap>>>(v.parts, nb, bs);
+            k_bi_s<double><<<nb, kRedThreads, 0, cap>>>(v.r, v.Ap, pre, v.sv, v.shat, v.t, n, bs);
+            if (fd && rc == YETI_OK)
+                rc = wq_fd_apply<double>(op, v.sv, v.shat, &bs->done, FD_NONE, nullptr, nullptr,
+                                         cap, v.fdt, v.fdparts);
+            if (rc == YETI_OK) rc = wq_apply_dev(op, v.shat, v.t, YETI_PREC_F64, &bs->done, cap);
+            k_bi_ts<double><<<nb, kRedThreads, 0, cap>>>(v.t, v.sv, n, v.parts, bs);
+            k_bi_omega<<<1, kRedThreads, 0, cap>>>(v.parts, nb, bs);
+            k_bi_update<double><<<nb, kRedThreads, 0, cap>>>(v.x, v.r, v.rhat, v.ph, v.shat, v.sv,
+                                                            v.t, n, v.parts, bs);
+            k_bi_beta<<<1, kRedThreads, 0, cap>>>(v.parts, nb, bs);
+            k_bi_p<double><<<nb, kRedThreads, 0, cap>>>(v.p, v.ph, v.r, v.Ap, pre, n, bs);
+            if (fd && rc == YETI_OK)
+                rc = wq_fd_apply<double>(op, v.p, v.ph, &bs->done, FD_NONE, nullptr, nullptr, cap,
+                                         v.fdt, v.fdparts);
+        }
     }
-    cudaMemcpyAsync(cs.host_scal, v.s, sizeof(CGScal), cudaMemcpyDeviceToHost, cap);
+    cudaMemcpyAsync(cs.host_scal, v.s, cgsolve_scal_bytes(), cudaMemcpyDeviceToHost, cap);
     const cudaError_t ce = cudaStreamEndCapture(cap, &g);
     YETI_TRY(rc);
     YETI_CUDA(ce);
@@ -674,7 +765,7 @@ int cgsolve_begin(CgSolve &cs, yeti_wq_op *op, cudaStream_t st, void *host_scal,
 int cgsolve_launch(CgSolve &cs) {
     YETI_CUDA(cudaGraphLaunch(cs.chunk, cs.stream));
     YETI_CUDA(cudaEventRecord(cs.ev, cs.stream));
-    count_launches(4 * kChunk);
+    count_launches((cs.bicg ? (cs.fd ? 20 : 10) : (cs.fd ? 9 : 4)) * kChunk);
     cs.in_flight = true;
     return YETI_OK;
 }
@@ -689,9 +780,20 @@ int cgsolve_poll(CgSolve &cs, int *state) {
         YETI_CUDA(q);
         cs.in_flight = false;
     }
-    const CGScal *h = static_cast<const CGScal *>(cs.host_scal);
-    cs.iterations = h->iter;
-    *state = h->breakdown ? 3 : (h->done ? 2 : 1);
+    int iter, done, breakdown;
+    if (cs.bicg) {
+        const BiScal *h = static_cast<const BiScal *>(cs.host_scal);
+        iter = h->iter;
+        done = h->done;
+        breakdown = h->breakdown;
+    } else {
+        const CGScal *h = static_cast<const CGScal *>(cs.host_scal);
+        iter = h->iter;
+        done = h->done;
+        breakdown = h->breakdown;
+    }
+    cs.iterations = iter;
+    *state = breakdown ? 3 : (done ? 2 : 1);
     return YETI_OK;
 }
 

@@ -20,6 +20,7 @@ import numpy as np
 
 from ._lib import (ServeRequest, ServeResult, YetiError, check, lib, ptr)
 from .patches import cube_patch, face_mask
+from .wq import _precond_bits
 
 
 class Server:
@@ -32,9 +33,11 @@ class Server:
         self._sizes = {}
         self._keep = {}
 
-    def submit(self, patch, E, nu, clamp_faces, rhs, rtol=1e-8, maxit=20000):
+    def submit(self, patch, E, nu, clamp_faces, rhs, rtol=1e-8, maxit=20000,
+               precond="jacobi", method="cg"):
         """Queue a solve of `patch` for each row of rhs ((nrhs, 3*ncp)).
-        Returns a ticket at once."""
+        precond: 'jacobi' or a fast-diagonalisation variant ('fd', ...);
+        method: 'cg' or 'bicgstab'.  Returns a ticket at once."""
         p = [int(v) for v in patch["p"]]
         nel = [int(v) for v in patch["nel"]]
         cps = np.ascontiguousarray(np.asarray(patch["cps"], dtype=np.float64).T)
@@ -51,6 +54,9 @@ class Server:
         q.dirichlet[:] = face_mask(clamp_faces).tolist()
         q.nrhs = rhs.shape[0]
         q.rtol, q.maxit = float(rtol), int(maxit)
+        if method not in ("cg", "bicgstab"):
+            raise ValueError(f"method {method!r}")
+        q.mode = _precond_bits(precond) | (2 if method == "bicgstab" else 0)
         t = ctypes.c_int64()
         check(lib().yeti_serve_submit(self.handle, ctypes.byref(q), ctypes.byref(t)),
               "yeti_serve_submit")
@@ -140,7 +146,8 @@ def synthetic_requests(n, seed, p_choices=(2, 3), nel_range=(4, 32),
     return out
 
 
-def run_stream(server, requests, rate_per_s, seed, rtol=1e-8):
+def run_stream(server, requests, rate_per_s, seed, rtol=1e-8, precond="jacobi",
+               method="cg"):
     """Submit `requests` with Poisson arrivals at rate_per_s (seeded) and
     collect every result.  Returns per-request latencies (ms), the wall time
     from the first submission to the last result (s), and the solved DOF
@@ -169,7 +176,8 @@ def run_stream(server, requests, rate_per_s, seed, rtol=1e-8):
         if delay > 0:
             time.sleep(delay)
         rhs = np.random.default_rng(r["rhs_seed"]).standard_normal((r["nrhs"], r["ndof"]))
-        tickets[i] = server.submit(r["patch"], r["E"], r["nu"], r["clamp"], rhs, rtol=rtol)
+        tickets[i] = server.submit(r["patch"], r["E"], r["nu"], r["clamp"], rhs, rtol=rtol,
+                                   precond=precond, method=method)
     th.join()
     wall = time.perf_counter() - t0
     lat = np.array([res["total_ms"] for res in results if res is not None])
