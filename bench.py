@@ -486,7 +486,7 @@ def main():
         fd["mixed" if mixed else "fp64"] = {
             "value": ws * op.nfree / (msf / 1e3), "ms_per_step": msf,
             "iterations": stf["iterations"], "outer_iterations": stf["outer_iterations"],
-            "rel_residual": stf["rel_residual"],
+            "solve_ms_device": stf["solve_ms"], "rel_residual": stf["rel_residual"],
             "rel_error_vs_fp64_ref": (torch.linalg.norm(xf - xref) / torch.linalg.norm(xref)).item()}
     fd["mixed_over_jacobi_mixed"] = fd["mixed"]["value"] / value
     fd["preconditioner"] = ("fast diagonalisation per displacement component, a[c][d] = mean "
