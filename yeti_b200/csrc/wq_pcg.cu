@@ -940,6 +940,8 @@ YETI_API int yeti_wq_pcg(yeti_wq_op *op, const double *b, double *x,
         float *r32 = V, *z32 = V + n, *p32 = V + 2 * n, *Ap32 = V + 3 * n, *d32 = V + 4 * n;
         const float *dinv32 = fd ? nullptr : op->dinv32.as<float>();
         const double delta2 = 1e-2;   // replace when ||r|| fell by 10x
+        // with FD: on the device, when ||r|| fell by 100x (FP32 tracks that)
+        const double kFdPause2 = 1e-4;
         double rr64 = 0.0;
         k_dot<double, double><<<kRedBlocks, kRedThreads, 0, s>>>(dr, dr, n, parts, nullptr);
         count_launches(1);
@@ -952,8 +954,9 @@ YETI_API int yeti_wq_pcg(yeti_wq_op *op, const double *b, double *x,
             memset(&init, 0, sizeof(init));
             init.bb = 1.0;
             // FD converges by decades per chunk, past what the FP32
-            // recursion tracks: replace at every 10x drop, on the device
-            init.pause2 = fd ? delta2 : 0.0;
+            // recursion tracks: stop the chunk on the device for a
+            // replacement at every 100x drop
+            init.pause2 = fd ? kFdPause2 : 0.0;
             YETI_CUDA(cudaMemcpyAsync(ds, &init, sizeof(CGScal), cudaMemcpyHostToDevice, s));
             k_start_scal<<<1, kRedThreads, 0, s>>>(parts, kRedBlocks, ds, tol2 / rr64, maxit);
             count_launches(3);
