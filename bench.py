@@ -319,6 +319,24 @@ def extra_configs(args, device):
     out["gradient_p2_32x32x2"] = {
         "nb_cp": int(sol.shape[1]), "gpu_ms_host_buffers": t_g, "cpu_oracle_ms": t_go,
         "cpu_cores": 1, "max_rel_diff_vs_oracle": float(np.abs(got - ref).max() / np.abs(ref).max())}
+    # volume and its shape gradient on the C3 geometry (the constraint of the
+    # shape optimisation beside the compliance)
+    from yeti_b200.stiffmtrx_elemstorage import SYSTEM_ARG_NAMES
+    from yeti_b200.volume import volume_and_gradient
+    d3 = dict(zip(SYSTEM_ARG_NAMES, a3))
+    A3 = [np.ones(np.atleast_1d(d3["nb_elem_patch"]).size, dtype=np.int64),
+          np.asarray(d3["COORDS3D"], dtype=np.float64), d3["IEN"], d3["nb_elem_patch"],
+          d3["Nkv"], d3["Ukv"], d3["Nijk"], d3["weight"], d3["Jpqr"], d3["ELT_TYPE"],
+          d3["PROPS"], d3["JPROPS"], d3["TENSOR"], d3["MCRD"], d3["NBINT"], d3["NNODE"]]
+    volume_and_gradient(A3)
+    t_v = _median_ms(lambda: volume_and_gradient(A3), 5, sync)
+    v_gpu, g_gpu = volume_and_gradient(A3)
+    t0 = time.perf_counter()
+    v_cpu, g_cpu = oracle.volume(A3)
+    t_vo = (time.perf_counter() - t0) * 1e3
+    out["volume_gradient_p2_32x32x2"] = {
+        "volume": v_gpu, "gpu_ms_host_buffers": t_v, "cpu_oracle_ms": t_vo, "cpu_cores": 1,
+        "bit_identical": bool(v_gpu == v_cpu and np.array_equal(g_gpu, g_cpu))}
     # C5: p=4 128x128x32 WQ block
     P = cube_patch((128, 128, 32), 4, size=(4.0, 4.0, 1.0), perturb=0.1, wrange=(0.8, 1.2),
                    seed=WORKLOAD["seed"] + 5)

@@ -231,6 +231,17 @@ int yeti_grad_lin_elast_work(yeti_ctx *ctx, const yeti_u1_model *model,
                              int include_surface_loads, double *gwint,
                              double *gwext, int mem);
 
+/* Volume of the model's active U1 elements and, when grad != NULL, its
+ * gradient with respect to the control-point coordinates (3, nb_cp), Fortran
+ * order, `mem`).  Replaces optim.volume.computevolume / computegradvolume
+ * (computeVolume, src/yeti_iga/optim/volume.f90:20-210; computeGradVolume,
+ * optim/gradvolume.f90:16-355; called at
+ * preprocessing/igaparametrization/OPT_modelling.py:508-531), whose
+ * listpatch selects whole patches: set `active` to 1 on their elements.
+ * The determinant is signed, as the reference's.  vol is host memory. */
+int yeti_volume_u1(yeti_ctx *ctx, const yeti_u1_model *model, double *vol,
+                   double *grad, int mem);
+
 /* ------------------------------------------------------------------------
  * Serving: persistent request loop (no counterpart in the reference)
  * ------------------------------------------------------------------------

@@ -159,3 +159,27 @@ def grad_lin_elast_work(args, sol, adj, compute_int=True, compute_ext=True,
     if rc != 0:
         raise RuntimeError(f"oracle gradient failed with code {rc}")
     return gi, ge
+
+
+def volume(area_inputs, gradient=True):
+    """Oracle twin of volume.computevolume / computegradvolume
+    (src/yeti_iga/optim/volume.f90:20-210, gradvolume.f90:16-355) for U1
+    patches.  area_inputs: the list of IGAparametrization.get_inputs4area.
+    Returns (V, dV/dP of shape (3, nb_cp) or None)."""
+    (listpatch, COORDS3D, IEN, nb_elem_patch, Nkv, Ukv, Nijk, weight, Jpqr,
+     ELT_TYPE, PROPS, JPROPS, TENSOR, MCRD, NBINT, nnode) = area_inputs[:16]
+    coords = np.asarray(COORDS3D, dtype=np.float64)
+    nb_cp = coords.shape[1]
+    nep = _i64(nb_elem_patch)
+    _check_u1(ELT_TYPE, TENSOR, nep.size)
+    keep = [_f64(coords), _i64(IEN), nep, _i64(Nkv), _f64(Ukv), _i64(Nijk),
+            _f64(weight), _i64(Jpqr), _i64(nnode), _i64(NBINT), _i64(listpatch)]
+    vol = ctypes.c_double()
+    grad = np.zeros((3, nb_cp), order="F") if gradient else None
+    f = lib().oracle_volume
+    f.restype = ctypes.c_int
+    rc = f(ctypes.c_int64(nep.size), ctypes.c_int64(nb_cp), *[_p(k) for k in keep],
+           ctypes.byref(vol), _p(grad) if gradient else None)
+    if rc != 0:
+        raise RuntimeError(f"oracle_volume failed ({rc})")
+    return vol.value, grad

@@ -522,3 +522,94 @@ int oracle_grad_lin_elast_work(
     }
     return 0;
 }
+
+/* computeVolume (src/yeti_iga/optim/volume.f90:20-210) and computeGradVolume
+ * (optim/gradvolume.f90:16-355), 3-D classical patches, restated loop for
+ * loop: every element of a patch with listpatch = 1, every Gauss point,
+ * VOL += det(AI) detJ and gradV(:, k) += (AIxAJ(:,3) dR(i,3) + AIxAJ(:,1)
+ * dR(i,1) + AIxAJ(:,2) dR(i,2)) detJ as running sums.  grad may be NULL. */
+int oracle_volume(int64_t nb_patch, int64_t nb_cp, const double *coords,
+                  const int64_t *ien, const int64_t *nb_elem_patch, const int64_t *nkv,
+                  const double *ukv, const int64_t *nijk, const double *weight,
+                  const int64_t *jpqr, const int64_t *nnode, const int64_t *nbint,
+                  const int64_t *listpatch, double *vol, double *grad)
+{
+    double V = 0.0;
+    if (grad) memset(grad, 0, sizeof(double) * 3 * nb_cp);
+    int64_t jelem = 0, ukv_off = 0, ien_off = 0;
+    for (int64_t ip = 0; ip < nb_patch; ip++) {
+        int p[3];
+        const double *U[3];
+        for (int d = 0; d < 3; d++) p[d] = (int)jpqr[3 * ip + d];
+        U[0] = ukv + ukv_off;
+        U[1] = U[0] + nkv[3 * ip];
+        U[2] = U[1] + nkv[3 * ip + 1];
+        int nn = (int)nnode[ip];
+        if (nn > GMAXNN) return -3;
+        if (listpatch[ip] == 1) {
+            int nq = (int)nbint[ip];
+            int ng = (int)pow((double)nq, 1.0 / 3.0);
+            if (ng < 1) ng = 1;
+            while (ng * ng * ng < nq) ng++;
+            double gx[32], gw[32];
+            g_gauss_legendre(ng, gx, gw);
+            double *R = (double *)malloc(sizeof(double) * nn);
+            double *dR = (double *)malloc(sizeof(double) * 3 * nn);
+            double *ce = (double *)malloc(sizeof(double) * 3 * nn);
+            for (int64_t ie = 0; ie < nb_elem_patch[ip]; ie++) {
+                const int64_t *ien_e = ien + ien_off + ie * nn;
+                const int64_t je = jelem + ie;
+                int ni[3];
+                double u1[3], u2[3];
+                for (int d = 0; d < 3; d++) {
+                    ni[d] = (int)nijk[3 * je + d];
+                    u1[d] = U[d][ni[d] - 1];
+                    u2[d] = U[d][ni[d]];
+                }
+                for (int a = 0; a < nn; a++)
+                    for (int c = 0; c < 3; c++) ce[3 * a + c] = coords[3 * (ien_e[a] - 1) + c];
+                int q = 0;
+                for (int i0 = 0; i0 < ng; i0++)
+                    for (int j0 = 0; j0 < ng; j0++)
+                        for (int k0 = 0; k0 < ng; k0++, q++) {
+                            if (q >= nq) break;
+                            double t[3] = {gx[i0], gx[j0], gx[k0]};
+                            double detJ = gw[i0] * gw[j0] * gw[k0], xi[3];
+                            for (int i = 0; i < 3; i++) {
+                                xi[i] = ((u2[i] - u1[i]) * t[i] + (u2[i] + u1[i])) * 0.5;
+                                detJ = detJ * 0.5 * (u2[i] - u1[i]);
+                            }
+                            g_evalnurbs(p, U, ni, weight + ien_off + ie * nn, xi, R, dR);
+                            double AI[3][3] = {{0}};   /* AI[k] = column k */
+                            for (int k = 0; k < 3; k++)
+                                for (int a = 0; a < nn; a++)
+                                    for (int c = 0; c < 3; c++)
+                                        AI[k][c] = AI[k][c] + dR[3 * a + k] * ce[3 * a + c];
+                            /* MatrixDet with AA(i, j) = AI[j-1][i-1] */
+                            double det = AI[1][0] * AI[2][1] * AI[0][2] - AI[2][0] * AI[1][1] * AI[0][2] +
+                                         AI[2][0] * AI[0][1] * AI[1][2] - AI[0][0] * AI[2][1] * AI[1][2] +
+                                         AI[0][0] * AI[1][1] * AI[2][2] - AI[1][0] * AI[0][1] * AI[2][2];
+                            V = V + det * detJ;
+                            if (!grad) continue;
+                            double AxA[3][3];
+                            g_cross(AI[0], AI[1], AxA[2]);
+                            g_cross(AI[1], AI[2], AxA[0]);
+                            g_cross(AI[2], AI[0], AxA[1]);
+                            for (int a = 0; a < nn; a++) {
+                                int64_t k = ien_e[a] - 1;
+                                for (int c = 0; c < 3; c++)
+                                    grad[c + 3 * k] = grad[c + 3 * k] +
+                                        (AxA[2][c] * dR[3 * a + 2] + AxA[0][c] * dR[3 * a] +
+                                         AxA[1][c] * dR[3 * a + 1]) * detJ;
+                            }
+                        }
+            }
+            free(R); free(dR); free(ce);
+        }
+        jelem += nb_elem_patch[ip];
+        for (int d = 0; d < 3; d++) ukv_off += nkv[3 * ip + d];
+        ien_off += nb_elem_patch[ip] * nn;
+    }
+    *vol = V;
+    return 0;
+}

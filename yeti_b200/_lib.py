@@ -118,6 +118,7 @@ def _declare(lib):
         "yeti_grad_lin_elast_work": (i32, [vp, ctypes.POINTER(U1Model), vp,
                                            vp, i64, i32, i32, i32, vp, vp,
                                            i32]),
+        "yeti_volume_u1": (i32, [vp, ctypes.POINTER(U1Model), vp, vp, i32]),
     }
     for name, (res, args) in sig.items():
         if hasattr(lib, name):

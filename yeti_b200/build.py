@@ -26,7 +26,8 @@ NVCC_FLAGS = ["-O3", "-lineinfo", "-std=c++17", "--expt-relaxed-constexpr",
 # Per-file extra flags.  The Gauss-quadrature assembly and shape gradient
 # mirror the reference's operation order exactly, which requires no FMA
 # contraction.
-EXTRA_FLAGS = {"assemble_u1.cu": ["-fmad=false"], "grad_u1.cu": ["-fmad=false"]}
+EXTRA_FLAGS = {"assemble_u1.cu": ["-fmad=false"], "grad_u1.cu": ["-fmad=false"],
+               "volume_u1.cu": ["-fmad=false"]}
 
 
 def nvcc():

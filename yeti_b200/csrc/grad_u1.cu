@@ -60,31 +60,7 @@ struct GradArgs {
 // evalnurbs at parametric xi: R[nn], dR[3*a+i]
 __device__ void eval_nurbs(const GradArgs &a, const int *ni, const double *xi,
                            const double *we, double *R, double *dR) {
-    double FN[kMaxDeg1], dFN[kMaxDeg1], FM[kMaxDeg1], dFM[kMaxDeg1],
-        FL[kMaxDeg1], dFL[kMaxDeg1];
-    bspline_ders(ni[0], a.p0, xi[0], a.U0, FN, dFN);
-    bspline_ders(ni[1], a.p1, xi[1], a.U1, FM, dFM);
-    bspline_ders(ni[2], a.p2, xi[2], a.U2, FL, dFL);
-    int n = 0;
-    double S = 0.0, sx0 = 0.0, sx1 = 0.0, sx2 = 0.0;
-    for (int k = 0; k <= a.p2; k++)
-        for (int j = 0; j <= a.p1; j++)
-            for (int i = 0; i <= a.p0; i++, n++) {
-                R[n] = FN[a.p0 - i] * FM[a.p1 - j] * FL[a.p2 - k] * we[n];
-                S = S + R[n];
-                dR[3 * n] = dFN[a.p0 - i] * FM[a.p1 - j] * FL[a.p2 - k] * we[n];
-                sx0 = sx0 + dR[3 * n];
-                dR[3 * n + 1] = FN[a.p0 - i] * dFM[a.p1 - j] * FL[a.p2 - k] * we[n];
-                sx1 = sx1 + dR[3 * n + 1];
-                dR[3 * n + 2] = FN[a.p0 - i] * FM[a.p1 - j] * dFL[a.p2 - k] * we[n];
-                sx2 = sx2 + dR[3 * n + 2];
-            }
-    const double inv = 1.0 / S;
-    const double sx[3] = {sx0, sx1, sx2};
-    for (int q = 0; q < a.nn; q++) {
-        R[q] = R[q] * inv;
-        for (int i = 0; i < 3; i++) dR[3 * q + i] = (dR[3 * q + i] - R[q] * sx[i]) * inv;
-    }
+    nurbs_eval_elem(a.p0, a.p1, a.p2, a.U0, a.U1, a.U2, a.nn, ni, xi, we, R, dR);
 }
 
 __device__ __forceinline__ void gcross(const double *u, const double *v, double *w) {

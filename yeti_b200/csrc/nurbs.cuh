@@ -50,6 +50,42 @@ __host__ __device__ inline void bspline_ders(int ni, int p, double u,
     }
 }
 
+// Rational basis R[nn] and its parametric derivatives dR[3 a + i] of one
+// element at xi: the tensor product with reversed 1-D indices (the
+// descending local node order of the reference's IEN), times the element's
+// weights, then divided by their sum (evalnurbs,
+// src/yeti_iga/main/evaluatenurbsfcts.f:94-209, in its operation order).
+__device__ inline void nurbs_eval_elem(int p0, int p1, int p2, const double *U0,
+                                       const double *U1, const double *U2, int nn,
+                                       const int *ni, const double *xi, const double *we,
+                                       double *R, double *dR) {
+    double FN[kMaxDeg1], dFN[kMaxDeg1], FM[kMaxDeg1], dFM[kMaxDeg1], FL[kMaxDeg1],
+        dFL[kMaxDeg1];
+    bspline_ders(ni[0], p0, xi[0], U0, FN, dFN);
+    bspline_ders(ni[1], p1, xi[1], U1, FM, dFM);
+    bspline_ders(ni[2], p2, xi[2], U2, FL, dFL);
+    int n = 0;
+    double S = 0.0, sx0 = 0.0, sx1 = 0.0, sx2 = 0.0;
+    for (int k = 0; k <= p2; k++)
+        for (int j = 0; j <= p1; j++)
+            for (int i = 0; i <= p0; i++, n++) {
+                R[n] = FN[p0 - i] * FM[p1 - j] * FL[p2 - k] * we[n];
+                S = S + R[n];
+                dR[3 * n] = dFN[p0 - i] * FM[p1 - j] * FL[p2 - k] * we[n];
+                sx0 = sx0 + dR[3 * n];
+                dR[3 * n + 1] = FN[p0 - i] * dFM[p1 - j] * FL[p2 - k] * we[n];
+                sx1 = sx1 + dR[3 * n + 1];
+                dR[3 * n + 2] = FN[p0 - i] * FM[p1 - j] * dFL[p2 - k] * we[n];
+                sx2 = sx2 + dR[3 * n + 2];
+            }
+    const double inv = 1.0 / S;
+    const double sx[3] = {sx0, sx1, sx2};
+    for (int q = 0; q < nn; q++) {
+        R[q] = R[q] * inv;
+        for (int i = 0; i < 3; i++) dR[3 * q + i] = (dR[3 * q + i] - R[q] * sx[i]) * inv;
+    }
+}
+
 // Gauss-Legendre nodes/weights of order n on [-1, 1] (ascending): roots of
 // the Legendre polynomial P_n by Newton iteration on its recurrence.
 void gauss_legendre_host(int n, double *x, double *w);
