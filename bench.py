@@ -303,6 +303,23 @@ def extra_configs(args, device):
         "nb_data": int(kd.size), "gpu_ms_device_out": t_gpu, "gpu_ms_host_buffers": t_gpu_host,
         "cpu_oracle_ms": t_cpu, "cpu_cores": 1,
         "bit_identical": bool(np.array_equal(kd, ko) and np.array_equal(F, Fo))}
+    # consistent mass matrix of the same model (parity: bit-identical COO)
+    from yeti_b200.massmtrx import build_cmassmatrix
+    from yeti_b200.stiffmtrx_elemstorage import SYSTEM_ARG_NAMES as _SAN
+    d1 = dict(zip(_SAN, a1))
+    m_in = [d1["activeElement"], d1["nb_data"], np.asarray(d1["COORDS3D"], dtype=np.float64),
+            d1["IEN"], d1["nb_elem_patch"], d1["Nkv"], d1["Ukv"], d1["Nijk"], d1["weight"],
+            d1["Jpqr"], d1["ELT_TYPE"], d1["PROPS"], d1["JPROPS"], np.full(1, 7.85),
+            d1["TENSOR"], d1["ind_dof_free"], d1["nb_dof_free"], d1["MCRD"], d1["NBINT"],
+            d1["NNODE"]]
+    build_cmassmatrix(*m_in, device_out=True)
+    t_m = _median_ms(lambda: build_cmassmatrix(*m_in, device_out=True), 20, sync)
+    md = build_cmassmatrix(*m_in)[0]
+    t0 = time.perf_counter()
+    mo = oracle.build_cmassmatrix(m_in)[0]
+    t_mo = (time.perf_counter() - t0) * 1e3
+    out["mass_matrix_p2_16x4x4"] = {"gpu_ms_device_out": t_m, "cpu_oracle_ms": t_mo,
+                                    "cpu_cores": 1, "bit_identical": bool(np.array_equal(md, mo))}
     # C3: shape gradient (adjoint kernel; parity vs the CPU oracle)
     a3 = _system_args("quarter_annulus_p2_32x32x2")
     U, _ = _solve(a3, np.asarray(a3[2], dtype=np.float64))

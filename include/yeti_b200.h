@@ -117,6 +117,16 @@ typedef struct {
 int yeti_assemble_u1_coo(yeti_ctx *ctx, const yeti_u1_model *model,
                          int64_t nb_data, double *kdata, int32_t *krow,
                          int32_t *kcol, double *F, int mem);
+/* Consistent mass matrix of the active U1 elements in the same COO slot
+ * order (replaces massmtrx.build_cmassmatrix: build_CMASSMatrix,
+ * src/yeti_iga/main/compute_CMASSMatrix.f:30-199, with UMASSMAT_byCP's U1
+ * branch, main/UMASSMAT.f; called at
+ * preprocessing/igaparametrization/OPT_modelling.py:369-371).  Density:
+ * model->rho per patch; loads and material moduli are ignored.  The caller
+ * adds the transpose as for the stiffness (M = Mside + Mside^T). */
+int yeti_assemble_u1_mass_coo(yeti_ctx *ctx, const yeti_u1_model *model,
+                              int64_t nb_data, double *mdata, int32_t *mrow,
+                              int32_t *mcol, int mem);
 
 /* ------------------------------------------------------------------------
  * Weighted-quadrature (WQ) matrix-free elasticity on one NURBS patch

@@ -183,3 +183,28 @@ def volume(area_inputs, gradient=True):
     if rc != 0:
         raise RuntimeError(f"oracle_volume failed ({rc})")
     return vol.value, grad
+
+
+def build_cmassmatrix(inputs):
+    """Oracle twin of massmtrx.build_cmassmatrix (compute_CMASSMatrix.f:30-199,
+    UMASSMAT.f U1 branch).  inputs: the list of
+    IGAparametrization.get_inputs4massmat.  Returns (Mdata, Mrow, Mcol)."""
+    (activeElement, nb_data, COORDS3D, IEN, nb_elem_patch, Nkv, Ukv, Nijk, weight,
+     Jpqr, ELT_TYPE, PROPS, JPROPS, RHO, TENSOR, ind_dof_free, nb_dof_free, MCRD,
+     NBINT, nnode) = inputs[:20]
+    coords = np.asarray(COORDS3D, dtype=np.float64)
+    nep = _i64(nb_elem_patch)
+    _check_u1(ELT_TYPE, TENSOR, nep.size)
+    act = _i64(activeElement)
+    keep = [_f64(coords), _i64(IEN), nep, _i64(Nkv), _f64(Ukv), _i64(Nijk), _f64(weight),
+            _i64(Jpqr), _i64(nnode), _i64(NBINT), _f64(np.atleast_1d(RHO)), act]
+    n = int(nb_data)
+    md, mr, mc = np.empty(n), np.empty(n, dtype=np.int32), np.empty(n, dtype=np.int32)
+    f = lib().oracle_build_cmassmatrix
+    f.restype = ctypes.c_int
+    i64 = ctypes.c_int64
+    rc = f(i64(nep.size), i64(act.size), i64(coords.shape[1]), *[_p(k) for k in keep],
+           i64(n), _p(md), _p(mr), _p(mc))
+    if rc != 0:
+        raise RuntimeError(f"oracle_build_cmassmatrix failed ({rc})")
+    return md, mr, mc

@@ -575,3 +575,98 @@ int oracle_sys_linmat_lindef_static(
     if (count > nb_data) return -5;
     return err;
 }
+
+/* build_CMASSMatrix (src/yeti_iga/main/compute_CMASSMatrix.f:30-199) with
+ * UMASSMAT_byCP's U1 branch (main/UMASSMAT.f): per Gauss point
+ * dvol = rho (w_q DetJac) (DetJac signed, as shap returns it), and for every
+ * node pair i <= j the diagonal of the 3x3 block gets (dvol R_j) R_i.  The
+ * blocks are scattered in the stiffness assembly's COO slot order, the
+ * diagonal of the diagonal blocks halved. */
+int oracle_build_cmassmatrix(
+    int64_t nb_patch, int64_t nb_elem, int64_t nb_cp,
+    const double *coords, const int64_t *ien, const int64_t *nb_elem_patch,
+    const int64_t *nkv, const double *ukv, const int64_t *nijk,
+    const double *weight, const int64_t *jpqr, const int64_t *nnode,
+    const int64_t *nbint, const double *rho, const int64_t *active,
+    int64_t nb_data, double *mdata, int32_t *mrow, int32_t *mcol)
+{
+    (void)nb_cp;
+    (void)nb_elem;
+    memset(mdata, 0, sizeof(double) * nb_data);
+    memset(mrow, 0, sizeof(int32_t) * nb_data);
+    memset(mcol, 0, sizeof(int32_t) * nb_data);
+    int64_t count = 0, jelem = 0, ukv_off = 0, ien_off = 0, w_off = 0;
+    for (int64_t ip = 0; ip < nb_patch; ip++) {
+        patch_t pt;
+        for (int d = 0; d < 3; d++) {
+            pt.p[d] = (int)jpqr[3 * ip + d];
+            pt.nkv[d] = (int)nkv[3 * ip + d];
+        }
+        if (pt.nkv[2] <= 0 || pt.nkv[1] <= 0) return -2;
+        pt.U[0] = ukv + ukv_off;
+        pt.U[1] = pt.U[0] + pt.nkv[0];
+        pt.U[2] = pt.U[1] + pt.nkv[1];
+        pt.nnode = (pt.p[0] + 1) * (pt.p[1] + 1) * (pt.p[2] + 1);
+        if (pt.nnode != nnode[ip] || pt.nnode > MAXNN) return -3;
+        const int nn = pt.nnode, nbi = (int)nbint[ip];
+        int ng = (int)pow((double)nbi, 1.0 / 3.0);
+        if (ng < 1) ng = 1;
+        while (ng * ng * ng < nbi) ng++;
+        double *gp = (double *)malloc(sizeof(double) * 4 * ng * ng * ng);
+        gauss_volume(ng, gp);
+        double *cm = (double *)malloc(sizeof(double) * (size_t)nn * (nn + 1) / 2);
+        double *R = (double *)malloc(sizeof(double) * nn);
+        double *dRdx = (double *)malloc(sizeof(double) * 3 * nn);
+        elem_t el;
+        for (int64_t ie = 0; ie < nb_elem_patch[ip]; ie++, jelem++) {
+            const int64_t *ien_e = ien + ien_off + ie * nn;
+            if (active[jelem] != 1) continue;
+            for (int a = 0; a < nn; a++)
+                for (int d = 0; d < 3; d++)
+                    el.coords[3 * a + d] = coords[3 * (ien_e[a] - 1) + d];
+            el.w = weight + w_off + ie * nn;
+            for (int d = 0; d < 3; d++) {
+                el.ni[d] = (int)nijk[3 * jelem + d];
+                el.u1[d] = pt.U[d][el.ni[d] - 1];
+                el.u2[d] = pt.U[d][el.ni[d]];
+            }
+            memset(cm, 0, sizeof(double) * (size_t)nn * (nn + 1) / 2);
+            for (int q = 0; q < nbi; q++) {
+                double detj = shap(&pt, &el, gp + 4 * q + 1, R, dRdx);
+                double dvol = gp[4 * q] * detj;
+                dvol = rho[ip] * dvol;
+                int c = 0;
+                for (int j = 0; j < nn; j++) {
+                    double t1 = dvol * R[j];
+                    for (int i = 0; i <= j; i++, c++) cm[c] = cm[c] + t1 * R[i];
+                }
+            }
+            int i = 0;
+            for (int cpj = 0; cpj < nn; cpj++) {
+                int64_t dofj = (ien_e[cpj] - 1) * 3;
+                for (int cpi = 0; cpi < cpj; cpi++, i++) {
+                    int64_t dofi = (ien_e[cpi] - 1) * 3;
+                    for (int ll = 0; ll < 3; ll++)
+                        for (int k2 = 0; k2 < 3; k2++, count++) {
+                            mdata[count] = k2 == ll ? cm[i] : 0.0;
+                            mrow[count] = (int32_t)(dofi + k2);
+                            mcol[count] = (int32_t)(dofj + ll);
+                        }
+                }
+                for (int ll = 0; ll < 3; ll++)
+                    for (int k2 = 0; k2 <= ll; k2++, count++) {
+                        mdata[count] = k2 == ll ? cm[i] * 0.5 : 0.0;
+                        mrow[count] = (int32_t)(dofj + k2);
+                        mcol[count] = (int32_t)(dofj + ll);
+                    }
+                i++;
+            }
+        }
+        free(gp); free(cm); free(R); free(dRdx);
+        for (int d = 0; d < 3; d++) ukv_off += pt.nkv[d];
+        ien_off += nb_elem_patch[ip] * nn;
+        w_off += nb_elem_patch[ip] * nn;
+    }
+    if (count > nb_data) return -5;
+    return 0;
+}

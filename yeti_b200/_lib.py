@@ -119,6 +119,8 @@ def _declare(lib):
                                            vp, i64, i32, i32, i32, vp, vp,
                                            i32]),
         "yeti_volume_u1": (i32, [vp, ctypes.POINTER(U1Model), vp, vp, i32]),
+        "yeti_assemble_u1_mass_coo": (i32, [vp, ctypes.POINTER(U1Model), i64, vp, vp,
+                                            vp, i32]),
     }
     for name, (res, args) in sig.items():
         if hasattr(lib, name):

@@ -403,6 +403,120 @@ k_u1_stiffness(StiffArgs a) {
     }
 }
 
+// Consistent mass matrix (build_CMASSMatrix, compute_CMASSMatrix.f:30-199,
+// with UMASSMAT_byCP's U1 branch, UMASSMAT.f): the stiffness kernel's layout
+// with, per Gauss point, R and dvol = rho (w_q DetJac) (DetJac signed, as
+// shap returns it) in shared memory; one thread per node pair (i <= j)
+// accumulates (dvol R_j) R_i over the points in order onto the diagonal of
+// the 3x3 block and writes the block into the pair's COO slots (diagonal of
+// the diagonal blocks halved, off-diagonal entries 0).
+struct MassArgs {
+    int p0, p1, p2, nn, nq, qchunk;
+    const double *U0, *U1, *U2;
+    const double *gauss;
+    const double *coords;
+    const int32_t *ien;
+    const double *w;
+    const int32_t *span;
+    const int64_t *slot;
+    double rho;
+    double *mdata;
+    int32_t *mrow, *mcol;
+};
+
+__global__ void __launch_bounds__(256) k_u1_mass(MassArgs a) {
+    extern __shared__ double smem[];
+    const int nn = a.nn;
+    double *xe = smem;                          // 3*nn element CP coordinates
+    double *we = xe + 3 * nn;                   // nn element weights
+    double *Rq = we + nn;                       // qchunk * nn basis values
+    double *dv = Rq + (size_t)a.qchunk * nn;    // qchunk
+    __shared__ double su1[3], su2[3];
+    __shared__ int sni[3];
+    const int e = blockIdx.x;
+    const int tid = threadIdx.x;
+    const int32_t *ien = a.ien + (size_t)e * nn;
+    for (int i = tid; i < nn; i += blockDim.x) {
+        int cp = ien[i];
+        xe[3 * i] = a.coords[3 * cp];
+        xe[3 * i + 1] = a.coords[3 * cp + 1];
+        xe[3 * i + 2] = a.coords[3 * cp + 2];
+        we[i] = a.w[(size_t)e * nn + i];
+    }
+    if (tid < 3) {
+        const double *U = tid == 0 ? a.U0 : (tid == 1 ? a.U1 : a.U2);
+        int ni = a.span[3 * e + tid];
+        sni[tid] = ni;
+        su1[tid] = U[ni - 1];
+        su2[tid] = U[ni];
+    }
+    const int npairs = nn * (nn + 1) / 2;
+    const int64_t base = a.slot[e];
+    for (int q0 = 0; q0 < a.nq; q0 += a.qchunk) {
+        const int nqc = min(a.qchunk, a.nq - q0);
+        __syncthreads();
+        // ---- stage A: basis values and dvol at the chunk's Gauss points
+        for (int ql = tid; ql < nqc; ql += blockDim.x) {
+            const double *g = a.gauss + 4 * (q0 + ql);
+            double Fv[6 * kMaxDeg1];
+            double J[3][3], inv;
+            rational_derivs(a.p0, a.p1, a.p2, nn, a.U0, a.U1, a.U2, sni, su1, su2, g + 1,
+                            we, xe, nullptr, J, &inv, Fv);
+            const double *FN = Fv, *FM = Fv + 2 * kMaxDeg1, *FL = Fv + 4 * kMaxDeg1;
+            double *R = Rq + (size_t)ql * nn;
+            int n = 0;
+            for (int k = 0; k <= a.p2; k++)
+                for (int j = 0; j <= a.p1; j++)
+                    for (int i = 0; i <= a.p0; i++, n++)
+                        R[n] = FN[a.p0 - i] * FM[a.p1 - j] * FL[a.p2 - k] * we[n] * inv;
+            const double dvol = g[0] * parent_det(J, su1, su2);
+            dv[ql] = a.rho * dvol;
+        }
+        __syncthreads();
+        // ---- stage B: one thread per control-point pair (i <= j)
+        for (int t = tid; t < npairs; t += blockDim.x) {
+            int j = (int)((sqrt(8.0 * t + 1.0) - 1.0) * 0.5);
+            while (j * (j + 1) / 2 > t) j--;
+            while ((j + 1) * (j + 2) / 2 <= t) j++;
+            const int i = t - j * (j + 1) / 2;
+            double m = 0.0;
+            for (int q = 0; q < nqc; q++) {
+                const double t1 = dv[q] * Rq[(size_t)q * nn + j];
+                m += t1 * Rq[(size_t)q * nn + i];
+            }
+            const int64_t jb = base + 9LL * j * (j - 1) / 2 + 6LL * j;
+            const int dofi = 3 * ien[i], dofj = 3 * ien[j];
+            if (i < j) {
+                const int64_t s = jb + 9LL * i;
+                for (int ll = 0; ll < 3; ll++)
+                    for (int kk = 0; kk < 3; kk++) {
+                        const int64_t o = s + 3 * ll + kk;
+                        double v = kk == ll ? m : 0.0;
+                        if (q0 > 0) v += a.mdata[o];
+                        a.mdata[o] = v;
+                        if (q0 == 0) {
+                            a.mrow[o] = dofi + kk;
+                            a.mcol[o] = dofj + ll;
+                        }
+                    }
+            } else {
+                const int64_t s = jb + 9LL * j;
+                for (int ll = 0; ll < 3; ll++)
+                    for (int kk = 0; kk <= ll; kk++) {
+                        const int64_t o = s + ll * (ll + 1) / 2 + kk;
+                        double v = kk == ll ? m * 0.5 : 0.0;
+                        if (q0 > 0) v += a.mdata[o];
+                        a.mdata[o] = v;
+                        if (q0 == 0) {
+                            a.mrow[o] = dofj + kk;
+                            a.mcol[o] = dofj + ll;
+                        }
+                    }
+            }
+        }
+    }
+}
+
 // Distributed loads (UELMAT.f90:121-223), deterministic and in the reference's
 // operation order.  Phase 1 (k_u1_elem_rhs) evaluates the RHS of each loaded
 // element into a buffer: per-point data first (one thread per quadrature
@@ -872,6 +986,84 @@ YETI_API int yeti_assemble_u1_coo(yeti_ctx *ctx, const yeti_u1_model *m,
         YETI_CUDA(cudaMemcpyAsync(krow, r_, nb_data * sizeof(int32_t), cudaMemcpyDeviceToHost, ctx->stream));
         YETI_CUDA(cudaMemcpyAsync(kcol, c_, nb_data * sizeof(int32_t), cudaMemcpyDeviceToHost, ctx->stream));
         YETI_CUDA(cudaMemcpyAsync(F, f_, ndof * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    }
+    // the model's device arrays are released on return: wait for the work
+    YETI_CUDA(cudaStreamSynchronize(ctx->stream));
+    return YETI_OK;
+}
+
+YETI_API int yeti_assemble_u1_mass_coo(yeti_ctx *ctx, const yeti_u1_model *m,
+                                       int64_t nb_data, double *mdata, int32_t *mrow,
+                                       int32_t *mcol, int mem) {
+    YETI_CHECK(ctx && m && mdata && mrow && mcol, YETI_EINVAL,
+               "yeti_assemble_u1_mass_coo: NULL argument");
+    YETI_CHECK(mem == YETI_MEM_HOST || mem == YETI_MEM_DEVICE, YETI_EINVAL,
+               "yeti_assemble_u1_mass_coo: bad mem flag %d", mem);
+    DeviceGuard guard(ctx->device);
+    U1Model M;
+    YETI_TRY(u1_prepare(ctx, m, M));
+    YETI_CHECK(M.nb_data <= nb_data, YETI_EINVAL,
+               "nb_data %lld smaller than the %lld slots of the active elements",
+               (long long)nb_data, (long long)M.nb_data);
+    YETI_CHECK(m->rho, YETI_EINVAL, "yeti_assemble_u1_mass_coo: no densities");
+    DevBuf dM, dR, dC;
+    double *m_ = mdata;
+    int32_t *r_ = mrow, *c_ = mcol;
+    if (mem == YETI_MEM_HOST) {
+        YETI_TRY(dM.alloc(ctx, nb_data * sizeof(double)));
+        YETI_TRY(dR.alloc(ctx, nb_data * sizeof(int32_t)));
+        YETI_TRY(dC.alloc(ctx, nb_data * sizeof(int32_t)));
+        m_ = dM.as<double>();
+        r_ = dR.as<int32_t>();
+        c_ = dC.as<int32_t>();
+    }
+    if (M.nb_data < nb_data) {   // slots beyond the active elements stay 0
+        YETI_CUDA(cudaMemsetAsync(m_ + M.nb_data, 0, (nb_data - M.nb_data) * sizeof(double), ctx->stream));
+        YETI_CUDA(cudaMemsetAsync(r_ + M.nb_data, 0, (nb_data - M.nb_data) * sizeof(int32_t), ctx->stream));
+        YETI_CUDA(cudaMemsetAsync(c_ + M.nb_data, 0, (nb_data - M.nb_data) * sizeof(int32_t), ctx->stream));
+    }
+    int smem_optin = 0;
+    YETI_CUDA(cudaDeviceGetAttribute(&smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, ctx->device));
+    const size_t smem_cap = std::min<size_t>(smem_optin, 200 * 1024);
+    YETI_CUDA(cudaFuncSetAttribute(k_u1_mass, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_cap));
+    for (size_t ip = 0; ip < M.patches.size(); ip++) {
+        U1Patch &P = M.patches[ip];
+        if (!P.nactive) continue;
+        const size_t fixed = sizeof(double) * 4 * P.nn;
+        const size_t perq = sizeof(double) * (P.nn + 1);
+        YETI_CHECK(fixed + perq <= smem_cap, YETI_EUNSUPPORTED,
+                   "element with %d nodes does not fit shared memory", P.nn);
+        const int qchunk = (int)std::min<size_t>(P.nq, (smem_cap - fixed) / perq);
+        MassArgs a;
+        a.p0 = P.p[0]; a.p1 = P.p[1]; a.p2 = P.p[2];
+        a.nn = P.nn; a.nq = P.nq; a.qchunk = qchunk;
+        a.U0 = P.knots.as<double>();
+        a.U1 = a.U0 + P.nkv[0];
+        a.U2 = a.U1 + P.nkv[1];
+        a.gauss = P.gauss.as<double>();
+        a.coords = M.coords.as<double>();
+        a.ien = P.ien.as<int32_t>();
+        a.w = P.w.as<double>();
+        a.span = P.span.as<int32_t>();
+        a.slot = P.slotd.as<int64_t>();
+        a.rho = P.rho;
+        a.mdata = m_; a.mrow = r_; a.mcol = c_;
+        const size_t smem = fixed + perq * qchunk;
+        int64_t left = P.nactive, off = 0;
+        while (left > 0) {   // grid.x limit
+            const int64_t n = std::min<int64_t>(left, 1 << 30);
+            MassArgs b = a;
+            b.ien += off * P.nn; b.w += off * P.nn; b.span += off * 3; b.slot += off;
+            k_u1_mass<<<(unsigned)n, 256, smem, ctx->stream>>>(b);
+            count_launches(1);
+            YETI_CUDA(cudaGetLastError());
+            left -= n; off += n;
+        }
+    }
+    if (mem == YETI_MEM_HOST) {
+        YETI_CUDA(cudaMemcpyAsync(mdata, m_, nb_data * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+        YETI_CUDA(cudaMemcpyAsync(mrow, r_, nb_data * sizeof(int32_t), cudaMemcpyDeviceToHost, ctx->stream));
+        YETI_CUDA(cudaMemcpyAsync(mcol, c_, nb_data * sizeof(int32_t), cudaMemcpyDeviceToHost, ctx->stream));
     }
     // the model's device arrays are released on return: wait for the work
     YETI_CUDA(cudaStreamSynchronize(ctx->stream));
