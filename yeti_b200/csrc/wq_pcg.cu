@@ -13,6 +13,8 @@
 #include <cmath>
 #include <cstring>
 
+#include <cooperative_groups.h>
+
 #include "reduce.cuh"
 #include "wq.cuh"
 
@@ -53,6 +55,104 @@ k_absmax(const A *a, int64_t n, double *parts) {
         v = fmax(v, fabs((double)a[i]));
     v = block_max(v, sh);
     if (threadIdx.x == 0) parts[blockIdx.x] = v;
+}
+
+// a * b rounded to T (never contracted into a following add)
+__device__ __forceinline__ float mul_rn(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ double mul_rn(double a, double b) { return __dmul_rn(a, b); }
+
+// block_sum's total (which only thread 0 holds) given to every thread
+__device__ __forceinline__ double block_sum_all(double v, double *sh) {
+    __shared__ double total;
+    v = block_sum(v, sh);
+    if (threadIdx.x == 0) total = v;
+    __syncthreads();
+    v = total;
+    __syncthreads();   // before a later call overwrites total
+    return v;
+}
+
+// One Jacobi-PCG iteration after the apply, in one cooperative launch: the
+// work of k_dot_alpha, k_update_beta and k_pupdate with two grid-wide
+// barriers instead of three launches and their last-block reductions.  No
+// vector is kept across a barrier (p, r and the inverse diagonal are read
+// again from L2; z = dinv r is recomputed from the stored r, the same value);
+// every block sums the partials in the same fixed order, so all blocks take
+// the same alpha, beta and stop decision and the results equal the
+// three-kernel path's.  parts: 3 * gridDim.x doubles.
+template <class T>
+__global__ void __launch_bounds__(kRedThreads, 4)   // 4 x 148 = kRedBlocks co-resident
+k_cg_fused(T *x, T *r, T *p, T *Ap, const T *dinv, int64_t n, double *parts, CGScal *s) {
+    __shared__ double sh[32];
+    if (s->done) return;   // read by every block before anyone can set it
+    cooperative_groups::grid_group grid = cooperative_groups::this_grid();
+    const int64_t gt = (int64_t)gridDim.x * blockDim.x;
+    const int64_t i0 = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    const int nb = (int)gridDim.x;
+    const double rz_old = s->rz, tol2 = s->tol2;
+    const int iter = s->iter, maxit = s->maxit;
+    double v = 0.0;
+    for (int64_t i = i0; i < n; i += gt) v += (double)p[i] * (double)Ap[i];
+    v = block_sum(v, sh);
+    if (threadIdx.x == 0) __stcg(&parts[blockIdx.x], v);
+    grid.sync();
+    double pAp = 0.0;
+    for (int i = threadIdx.x; i < nb; i += blockDim.x) pAp += __ldcg(&parts[i]);
+    pAp = block_sum_all(pAp, sh);
+    if (!(pAp > 0.0) || !isfinite(pAp)) {   // the same decision in every block
+        if (blockIdx.x == 0 && threadIdx.x == 0) {
+            s->pAp = pAp;
+            s->breakdown = 1;
+            s->done = 1;
+        }
+        return;
+    }
+    const double alpha = rz_old / pAp;
+    const T a = (T)alpha;
+    double rz = 0.0, rr = 0.0;
+    for (int64_t i = i0; i < n; i += gt) {
+        x[i] += a * p[i];
+        const T ri = r[i] - a * Ap[i];
+        r[i] = ri;
+        const T zi = dinv[i] * ri;
+        rz += (double)ri * (double)zi;
+        rr += (double)ri * (double)ri;
+    }
+    rz = block_sum(rz, sh);
+    rr = block_sum(rr, sh);
+    if (threadIdx.x == 0) {
+        __stcg(&parts[nb + 2 * blockIdx.x], rz);
+        __stcg(&parts[nb + 2 * blockIdx.x + 1], rr);
+    }
+    grid.sync();
+    double srz = 0.0, srr = 0.0;
+    for (int i = threadIdx.x; i < nb; i += blockDim.x) {
+        srz += __ldcg(&parts[nb + 2 * i]);
+        srr += __ldcg(&parts[nb + 2 * i + 1]);
+    }
+    srz = block_sum_all(srz, sh);
+    srr = block_sum_all(srr, sh);
+    const int it = iter + 1;
+    const double beta = srz / rz_old;
+    const bool bad = !isfinite(srr);
+    const bool stop = bad || srr <= tol2 || it >= maxit;
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        s->pAp = pAp;
+        s->alpha = alpha;
+        s->iter = it;
+        s->rr = srr;
+        s->beta = beta;
+        s->rz = srz;
+        if (bad) s->breakdown = 1;
+        if (stop) s->done = 1;
+    }
+    if (stop) return;
+    const T bt = (T)beta;
+    for (int64_t i = i0; i < n; i += gt) {
+        const T zi = mul_rn(dinv[i], r[i]);   // z as the three-kernel path stores it
+        p[i] = zi + bt * p[i];
+        Ap[i] = T(0);
+    }
 }
 
 // End of an iteration: stop the chunk once the residual has dropped to
@@ -502,7 +602,7 @@ static int ensure_workspace(yeti_wq_op *op, bool f32) {
     if (!op->ws64.ptr) YETI_TRY(op->ws64.alloc(op->ctx, 12 * n * sizeof(double)));
     if (f32 && !op->ws32.ptr) YETI_TRY(op->ws32.alloc(op->ctx, 10 * n * sizeof(float)));
     if (!op->scal.ptr) YETI_TRY(op->scal.alloc(op->ctx, 4 * sizeof(CGScal)));
-    if (!op->parts.ptr) YETI_TRY(op->parts.alloc(op->ctx, 2 * kRedBlocks * sizeof(double)));
+    if (!op->parts.ptr) YETI_TRY(op->parts.alloc(op->ctx, 4 * kRedBlocks * sizeof(double)));
     cudaStream_t s = op->ctx->stream;
     if (!op->dinv64.ptr) {
         YETI_TRY(op->dinv64.alloc(op->ctx, n * sizeof(double)));
@@ -527,12 +627,39 @@ static int ensure_workspace(yeti_wq_op *op, bool f32) {
 // device flag is set).
 // dinv == nullptr: the fast-diagonalisation preconditioner gives z, r.z and
 // beta after the update.
+// Can the iteration's vector work run as one cooperative k_cg_fused launch
+// (all kRedBlocks blocks co-resident)?
+template <class T>
+static bool cg_fused_ok(const yeti_wq_op *op) {
+    int dev = op->ctx->device, coop = 0, sms = 0, per_sm = 0;
+    if (cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_cg_fused<T>, kRedThreads, 0) !=
+            cudaSuccess) {
+        (void)cudaGetLastError();
+        return false;
+    }
+    return coop && (int64_t)per_sm * sms >= kRedBlocks;
+}
+
 template <class T>
 static int cg_chunk(yeti_wq_op *op, int prec, T *x, T *r, T *z, T *p, T *Ap,
                     const T *dinv, CGScal *ds, bool pause = false) {
     cudaStream_t s = op->ctx->stream;
     const int64_t n = op->ndof;
     double *parts = op->parts.as<double>();
+    if (dinv && !pause && cg_fused_ok<T>(op)) {
+        for (int k = 0; k < kChunk; k++) {
+            YETI_TRY(wq_apply_dev(op, p, Ap, prec, &ds->done, s));
+            int64_t nn = n;
+            void *args[] = {&x, &r, &p, &Ap, (void *)&dinv, &nn, &parts, &ds};
+            YETI_CUDA(cudaLaunchCooperativeKernel((const void *)k_cg_fused<T>, dim3(kRedBlocks),
+                                                  dim3(kRedThreads), args, 0, s));
+            count_launches(1);
+        }
+        YETI_CUDA(cudaGetLastError());
+        return YETI_OK;
+    }
     for (int k = 0; k < kChunk; k++) {
         YETI_TRY(wq_apply_dev(op, p, Ap, prec, &ds->done, s));
         k_dot_alpha<T><<<kRedBlocks, kRedThreads, 0, s>>>(p, Ap, n, parts, ds);
