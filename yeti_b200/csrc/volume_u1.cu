@@ -147,12 +147,23 @@ __global__ void k_volume_sum(const double *vterm, int64_t n, double *vol) {
 }
 
 // grad[j] = sum over the terms idx[ptr[j] .. ptr[j+1]) in order
-__global__ void k_volume_gather(int64_t n, const int64_t *ptr, const int64_t *idx,
-                                const double *gterm, double *grad) {
+// grad[c + 3 cp] = sum, over the active elements holding cp (in element
+// order) and their points q (in order), of the point term of (q, a, c), a the
+// control point's local index: ent[k] is the term of (q = 0, a, c = 0) of the
+// k-th element of cp, qs[k] = (points, term stride between points).
+__global__ void k_volume_gather(int64_t n, const int64_t *ptr, const int64_t *ent,
+                                const int2 *qs, const double *gterm, double *grad) {
     const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (t >= n) return;
+    const int64_t cp = t / 3;
+    const int c = (int)(t - 3 * cp);
     double acc = 0.0;
-    for (int64_t k = ptr[t]; k < ptr[t + 1]; k++) acc = acc + gterm[idx[k]];
+    for (int64_t k = ptr[cp]; k < ptr[cp + 1]; k++) {
+        const double *g = gterm + ent[k] + c;
+        const int nq = qs[k].x;
+        const int64_t st = qs[k].y;
+        for (int q = 0; q < nq; q++) acc = acc + g[q * st];
+    }
     grad[t] = acc;
 }
 
@@ -183,7 +194,7 @@ YETI_API int yeti_volume_u1(yeti_ctx *ctx, const yeti_u1_model *m, double *vol,
         nterm += P.nactive * P.nq;
         ngterm += P.nactive * P.nq * P.nn * 3;
     }
-    DevBuf dv, dvt, dgt, dgrad, dptr, didx;
+    DevBuf dv, dvt, dgt, dgrad, dptr, didx, dqs;
     YETI_TRY(dv.alloc(ctx, sizeof(double)));
     if (nterm == 0) {
         *vol = 0.0;
@@ -226,11 +237,12 @@ YETI_API int yeti_volume_u1(yeti_ctx *ctx, const yeti_u1_model *m, double *vol,
     count_launches(1);
     YETI_CUDA(cudaGetLastError());
     if (want_grad) {
-        // per (component, control point): its terms in element, point order
+        // per control point: the active elements holding it, in element
+        // order (the three components and the points of each element are
+        // walked by the gather kernel in the same order)
         const int64_t nout = 3 * ncp;
-        std::vector<int64_t> cnt(nout + 1, 0);
-        int64_t ien_off = 0;
         std::vector<int64_t> patch_ien(M.patches.size(), 0);
+        int64_t ien_off = 0;
         for (size_t ip = 0; ip < M.patches.size(); ip++) {
             patch_ien[ip] = ien_off;
             ien_off += M.patches[ip].nelem * M.patches[ip].nn;
@@ -239,37 +251,37 @@ YETI_API int yeti_volume_u1(yeti_ctx *ctx, const yeti_u1_model *m, double *vol,
             const int64_t jel = P.act[le];
             return m->ien[patch_ien[ip] + (jel - P.elem_begin) * P.nn + a] - 1;
         };
+        std::vector<int64_t> cnt(ncp + 1, 0);
         for (const Seg &sg : segs) {
             const U1Patch &P = M.patches[sg.patch];
             for (int64_t le = 0; le < P.nactive; le++)
-                for (int a = 0; a < P.nn; a++) {
-                    const int64_t cp = cp_of(P, sg.patch, le, a);
-                    for (int c = 0; c < 3; c++) cnt[c + 3 * cp + 1] += P.nq;
-                }
+                for (int a = 0; a < P.nn; a++) cnt[cp_of(P, sg.patch, le, a) + 1]++;
         }
-        for (int64_t i = 0; i < nout; i++) cnt[i + 1] += cnt[i];
-        std::vector<int64_t> idx(std::max<int64_t>(cnt[nout], 1)), fill(cnt.begin(), cnt.end() - 1);
+        for (int64_t i = 0; i < ncp; i++) cnt[i + 1] += cnt[i];
+        const size_t nent = (size_t)std::max<int64_t>(cnt[ncp], 1);
+        std::vector<int64_t> ent(nent, 0), fill(cnt.begin(), cnt.end() - 1);
+        std::vector<int2> qs(nent, make_int2(0, 0));
         int64_t base = 0;
         for (const Seg &sg : segs) {
             const U1Patch &P = M.patches[sg.patch];
             for (int64_t le = 0; le < P.nactive; le++)
-                for (int q = 0; q < P.nq; q++)
-                    for (int a = 0; a < P.nn; a++) {
-                        const int64_t cp = cp_of(P, sg.patch, le, a);
-                        const int64_t tq = base + ((le * P.nq + q) * (int64_t)P.nn + a) * 3;
-                        for (int c = 0; c < 3; c++) idx[fill[c + 3 * cp]++] = tq + c;
-                    }
+                for (int a = 0; a < P.nn; a++) {
+                    const int64_t k = fill[cp_of(P, sg.patch, le, a)]++;
+                    ent[k] = base + (le * P.nq * (int64_t)P.nn + a) * 3;
+                    qs[k] = make_int2(P.nq, P.nn * 3);
+                }
             base += P.nactive * P.nq * P.nn * 3;
         }
         YETI_TRY(upload(ctx, dptr, cnt.data(), cnt.size()));
-        YETI_TRY(upload(ctx, didx, idx.data(), idx.size()));
+        YETI_TRY(upload(ctx, didx, ent.data(), ent.size()));
+        YETI_TRY(upload(ctx, dqs, qs.data(), qs.size()));
         double *g_d = grad;
         if (mem == YETI_MEM_HOST) {
             YETI_TRY(dgrad.alloc(ctx, nout * sizeof(double)));
             g_d = dgrad.as<double>();
         }
         k_volume_gather<<<(unsigned)((nout + 255) / 256), 256, 0, s>>>(
-            nout, dptr.as<int64_t>(), didx.as<int64_t>(), dgt.as<double>(), g_d);
+            nout, dptr.as<int64_t>(), didx.as<int64_t>(), dqs.as<int2>(), dgt.as<double>(), g_d);
         count_launches(1);
         YETI_CUDA(cudaGetLastError());
         if (mem == YETI_MEM_HOST)
