@@ -17,6 +17,10 @@ class ReferenceWQ:
         from yeti_b200.patches import free_mask
         L = lib()
         L.oracle_wq_create.restype = ctypes.c_void_p
+        # every pointer declared, or ctypes passes the addresses as C ints
+        vp = ctypes.c_void_p
+        L.oracle_wq_create.argtypes = [vp, vp, vp, vp, vp, ctypes.c_double,
+                                       ctypes.c_double, vp]
         L.oracle_wq_apply.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
         L.oracle_wq_free.argtypes = [ctypes.c_void_p]
         L.oracle_cg_vector_seconds.restype = ctypes.c_double
