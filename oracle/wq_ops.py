@@ -27,8 +27,8 @@ This oracle composes them into the elastic operator
 with the reference's B-spline test and trial functions, on the exact NURBS
 geometry: the Jacobian J = dx/dxi of x = sum w_a N_a P_a / sum w_a N_a.
 
-Two deliberate differences from the reference's code, both documented in
-DESIGN.md: the coefficient uses the geometric orientation
+Two deliberate differences from the reference's code: the coefficient uses
+the geometric orientation
 S = ext(invJ) MDM ext(invJ)^T |detJ| with invJ = (dx/dxi)^{-1} (the
 reference's product is transposed, which only agrees for symmetric
 Jacobians), and the Jacobian includes the NURBS weights.  Rational

@@ -3,7 +3,7 @@ GPU kernel vs oracle (bit-identical) and vs finite differences.
 
 The reference's own pin (benchs/grad_solid/test_grad_solid_unit_cube_centrif.py)
 asserts AN == FD within rtol 1e-5 on the p=1 unit cube under a centrifugal
-load; the north-star bar is 1e-6 relative to central FD (h = 1e-6).
+load; the bar here is 1e-6 relative to central FD (h = 1e-6).
 """
 import numpy as np
 import pytest
