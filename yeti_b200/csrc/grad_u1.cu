@@ -666,24 +666,26 @@ YETI_API int yeti_grad_lin_elast_work(yeti_ctx *ctx, const yeti_u1_model *m,
             off += (int64_t)(ebufs_i[i]->bytes / sizeof(double));
         }
     }
-    std::vector<std::vector<int64_t>> lists(nout);
-    for (auto &D : done) {
-        const U1Patch &P = M.patches[D.patch];
-        const int64_t jel = P.act[D.local];
-        const int64_t base = ien_offset[D.patch] + (jel - P.elem_begin) * P.nn;
-        for (int a = 0; a < P.nn; a++) {
-            const int64_t cp = m->ien[base + a] - 1;
-            for (int c = 0; c < 3; c++)
-                for (int k = 0; k < nadj; k++)
-                    lists[k + nadj * (c + 3 * cp)].push_back(D.off + k + nadj * (c + 3 * a));
+    // CSR of the element entries of each output, elements in order: count,
+    // then fill in the same loop order
+    std::vector<int64_t> ptr(nout + 1, 0);
+    auto walk = [&](auto &&visit) {
+        for (auto &D : done) {
+            const U1Patch &P = M.patches[D.patch];
+            const int64_t jel = P.act[D.local];
+            const int64_t base = ien_offset[D.patch] + (jel - P.elem_begin) * P.nn;
+            for (int a = 0; a < P.nn; a++) {
+                const int64_t cp = m->ien[base + a] - 1;
+                for (int c = 0; c < 3; c++)
+                    for (int k = 0; k < nadj; k++)
+                        visit(k + nadj * (c + 3 * cp), D.off + k + nadj * (c + 3 * a));
+            }
         }
-    }
-    std::vector<int64_t> ptr(nout + 1, 0), idx;
-    for (int64_t i = 0; i < nout; i++) {
-        ptr[i + 1] = ptr[i] + (int64_t)lists[i].size();
-        idx.insert(idx.end(), lists[i].begin(), lists[i].end());
-    }
-    if (idx.empty()) idx.push_back(0);
+    };
+    walk([&](int64_t o, int64_t) { ptr[o + 1]++; });
+    for (int64_t i = 0; i < nout; i++) ptr[i + 1] += ptr[i];
+    std::vector<int64_t> idx(std::max<int64_t>(ptr[nout], 1), 0), fill(ptr.begin(), ptr.end() - 1);
+    walk([&](int64_t o, int64_t e) { idx[fill[o]++] = e; });
     DevBuf &dptr = newbuf();
     DevBuf &didx = newbuf();
     YETI_TRY(upload(ctx, dptr, ptr.data(), ptr.size()));

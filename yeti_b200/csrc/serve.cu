@@ -178,8 +178,11 @@ struct yeti_server {
                 free_slots.pop_back();
                 st = streams[rr++ % (int)streams.size()];
             }
+            // FD-preconditioned solves take tens of iterations: short chunks
+            // (cheaper graphs, fewer iterations launched past convergence)
+            const int chunk = (r->mode & YETI_PCG_FD) ? 8 : 0;
             rc = cgsolve_begin(*cs, op, st, slot, r->rhs.data() + (size_t)k * r->ndof, r->rtol,
-                               r->maxit, cap, r->mode);
+                               r->maxit, cap, r->mode, chunk);
             cs->host_scal = slot;   // returned by finish whatever happened
             if (rc == YETI_OK) rc = cgsolve_launch(*cs);
             r->solves.push_back(std::move(cs));

@@ -136,6 +136,7 @@ struct CgSolve {
     cudaGraphExec_t chunk = nullptr;
     cudaEvent_t ev = nullptr;
     int nblk = 0;
+    int chunk_iters = 0;         // iterations per chunk graph
     bool in_flight = false;
     int iterations = 0;
     double rel_residual = 0.0;   // true FP64 residual of the returned x
@@ -147,9 +148,12 @@ size_t cgsolve_scal_bytes();
 // The chunk graph is captured on `capture` when given (a stream no other
 // thread enqueues into while it is captured), else on s.
 // mode: YETI_PCG_BICGSTAB and the YETI_PCG_FD* bits (clear: Jacobi CG).
+// chunk: iterations per chunk graph (0: the default, 16); the capture and
+// instantiation cost and the iterations launched past convergence both grow
+// with it, the host round trips shrink.
 int cgsolve_begin(CgSolve &cs, yeti_wq_op *op, cudaStream_t s, void *host_scal,
                   const double *b_host, double rtol, int maxit,
-                  cudaStream_t capture = nullptr, int mode = 0);
+                  cudaStream_t capture = nullptr, int mode = 0, int chunk = 0);
 // Enqueue the next chunk (graph launch + event).
 int cgsolve_launch(CgSolve &cs);
 // *state: 0 a chunk is in flight, 1 chunk done and more iterations needed,

@@ -785,9 +785,10 @@ static SolveView solve_view(const CgSolve &cs) {
 
 int cgsolve_begin(CgSolve &cs, yeti_wq_op *op, cudaStream_t st, void *host_scal,
                   const double *b_host, double rtol, int maxit, cudaStream_t capture,
-                  int mode) {
+                  int mode, int chunk) {
     YETI_CHECK(op && host_scal && b_host && op->coef64.ptr, YETI_EINVAL,
                "cgsolve_begin: missing operator data");
+    YETI_CHECK(chunk >= 0 && chunk <= 256, YETI_EINVAL, "cgsolve_begin: chunk %d", chunk);
     const int fd_bits = YETI_PCG_FD | YETI_PCG_FD_SCALED | YETI_PCG_FD_UNIT;
     YETI_CHECK((mode & ~(fd_bits | YETI_PCG_BICGSTAB)) == 0 &&
                    ((mode & fd_bits) == 0 || (mode & YETI_PCG_FD)),
@@ -801,6 +802,7 @@ int cgsolve_begin(CgSolve &cs, yeti_wq_op *op, cudaStream_t st, void *host_scal,
     cs.bicg = bicg;
     cs.stream = st;
     cs.host_scal = host_scal;
+    cs.chunk_iters = chunk ? chunk : kChunk;
     const int64_t n = op->ndof;
     cs.nblk = (int)std::max<int64_t>(1, std::min<int64_t>(kRedBlocks, (n + kRedThreads - 1) / kRedThreads));
     const size_t fd_doubles = fd ? 2 * (size_t)n + (size_t)wq_fd_parts(op) : 0;
@@ -846,7 +848,7 @@ int cgsolve_begin(CgSolve &cs, yeti_wq_op *op, cudaStream_t st, void *host_scal,
     cudaStream_t cap = capture ? capture : st;
     YETI_CUDA(cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal));
     int rc = YETI_OK;
-    for (int k = 0; k < kChunk && rc == YETI_OK; k++) {
+    for (int k = 0; k < cs.chunk_iters && rc == YETI_OK; k++) {
         if (!bicg) {
             rc = wq_apply_dev(op, v.p, v.Ap, YETI_PREC_F64, &v.s->done, cap);
             k_dot_alpha<double><<<nb, kRedThreads, 0, cap>>>(v.p, v.Ap, n, v.parts, v.s);
@@ -892,7 +894,7 @@ int cgsolve_begin(CgSolve &cs, yeti_wq_op *op, cudaStream_t st, void *host_scal,
 int cgsolve_launch(CgSolve &cs) {
     YETI_CUDA(cudaGraphLaunch(cs.chunk, cs.stream));
     YETI_CUDA(cudaEventRecord(cs.ev, cs.stream));
-    count_launches((cs.bicg ? (cs.fd ? 20 : 10) : (cs.fd ? 9 : 4)) * kChunk);
+    count_launches((cs.bicg ? (cs.fd ? 20 : 10) : (cs.fd ? 9 : 4)) * cs.chunk_iters);
     cs.in_flight = true;
     return YETI_OK;
 }
