@@ -180,7 +180,7 @@ struct yeti_server {
             }
             // FD-preconditioned solves take tens of iterations: short chunks
             // (cheaper graphs, fewer iterations launched past convergence)
-            const int chunk = (r->mode & YETI_PCG_FD) ? 8 : 0;
+            const int chunk = (r->mode & YETI_PCG_FD) ? 4 : 0;
             rc = cgsolve_begin(*cs, op, st, slot, r->rhs.data() + (size_t)k * r->ndof, r->rtol,
                                r->maxit, cap, r->mode, chunk);
             cs->host_scal = slot;   // returned by finish whatever happened
