@@ -91,8 +91,22 @@ k_cg_fused(T *x, T *r, T *p, T *Ap, const T *dinv, int64_t n, double *parts, CGS
     const int nb = (int)gridDim.x;
     const double rz_old = s->rz, tol2 = s->tol2;
     const int iter = s->iter, maxit = s->maxit;
+    // each thread's elements i0, i0 + gt, ... in order, U at a time with
+    // their loads issued together (the sums keep the one-by-one order)
+    constexpr int U = sizeof(T) == 4 ? 4 : 2;
     double v = 0.0;
-    for (int64_t i = i0; i < n; i += gt) v += (double)p[i] * (double)Ap[i];
+    for (int64_t i = i0; i < n; i += U * gt) {
+        T pv[U], av[U];
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+            const int64_t j = i + u * gt;
+            pv[u] = j < n ? p[j] : T(0);
+            av[u] = j < n ? Ap[j] : T(0);
+        }
+#pragma unroll
+        for (int u = 0; u < U; u++)
+            if (i + u * gt < n) v += (double)pv[u] * (double)av[u];
+    }
     v = block_sum(v, sh);
     if (threadIdx.x == 0) __stcg(&parts[blockIdx.x], v);
     grid.sync();
@@ -110,13 +124,29 @@ k_cg_fused(T *x, T *r, T *p, T *Ap, const T *dinv, int64_t n, double *parts, CGS
     const double alpha = rz_old / pAp;
     const T a = (T)alpha;
     double rz = 0.0, rr = 0.0;
-    for (int64_t i = i0; i < n; i += gt) {
-        x[i] += a * p[i];
-        const T ri = r[i] - a * Ap[i];
-        r[i] = ri;
-        const T zi = dinv[i] * ri;
-        rz += (double)ri * (double)zi;
-        rr += (double)ri * (double)ri;
+    for (int64_t i = i0; i < n; i += U * gt) {
+        T xv[U], pv[U], rv[U], av[U], dv[U];
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+            const int64_t j = i + u * gt;
+            const bool in = j < n;
+            xv[u] = in ? x[j] : T(0);
+            pv[u] = in ? p[j] : T(0);
+            rv[u] = in ? r[j] : T(0);
+            av[u] = in ? Ap[j] : T(0);
+            dv[u] = in ? dinv[j] : T(0);
+        }
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+            const int64_t j = i + u * gt;
+            if (j >= n) continue;
+            x[j] = xv[u] + a * pv[u];
+            const T ri = rv[u] - a * av[u];
+            r[j] = ri;
+            const T zi = dv[u] * ri;
+            rz += (double)ri * (double)zi;
+            rr += (double)ri * (double)ri;
+        }
     }
     rz = block_sum(rz, sh);
     rr = block_sum(rr, sh);
@@ -148,10 +178,24 @@ k_cg_fused(T *x, T *r, T *p, T *Ap, const T *dinv, int64_t n, double *parts, CGS
     }
     if (stop) return;
     const T bt = (T)beta;
-    for (int64_t i = i0; i < n; i += gt) {
-        const T zi = mul_rn(dinv[i], r[i]);   // z as the three-kernel path stores it
-        p[i] = zi + bt * p[i];
-        Ap[i] = T(0);
+    for (int64_t i = i0; i < n; i += U * gt) {
+        T dv[U], rv[U], pv[U];
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+            const int64_t j = i + u * gt;
+            const bool in = j < n;
+            dv[u] = in ? dinv[j] : T(0);
+            rv[u] = in ? r[j] : T(0);
+            pv[u] = in ? p[j] : T(0);
+        }
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+            const int64_t j = i + u * gt;
+            if (j >= n) continue;
+            const T zi = mul_rn(dv[u], rv[u]);   // z as the three-kernel path stores it
+            p[j] = zi + bt * pv[u];
+            Ap[j] = T(0);
+        }
     }
 }
 
