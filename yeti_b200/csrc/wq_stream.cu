@@ -158,15 +158,20 @@ __device__ __forceinline__ void mbar_init(uint64_t *bar) {
 }
 // One bulk copy global -> shared that completes the barrier's current phase.
 // dst and src 16-byte aligned, bytes a multiple of 16.
+// The coefficient stream is read once per apply and is several times the L2:
+// its lines are marked evict-first, so that the solver's vectors (u, Ku and
+// the Krylov vectors, a few MB each) stay in L2 across the apply.
 __device__ __forceinline__ void bulk_load(void *dst, const void *src, uint32_t bytes, uint64_t *bar) {
+    uint64_t policy;
+    asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(policy));
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)),
                  "r"(bytes)
                  : "memory");
     asm volatile(
-        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-            smem_addr(dst)),
-        "l"(src), "r"(bytes), "r"(smem_addr(bar))
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes.L2::cache_hint [%0], [%1], "
+        "%2, [%3], %4;" ::"r"(smem_addr(dst)),
+        "l"(src), "r"(bytes), "r"(smem_addr(bar)), "l"(policy)
         : "memory");
 }
 // Wait for the phase with the given parity, at most kWaitTries polls.
