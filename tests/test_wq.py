@@ -154,3 +154,20 @@ def test_reference_algorithm_cpu_matches_oracle(case):
     b = ReferenceWQ(P, 1.0, 0.3, clamp)
     u = np.random.default_rng(1).standard_normal(a.ndof)
     assert _rel(b.apply(u), a.apply(u)) < 1e-13
+
+
+def test_reference_algorithm_cpu_declares_pointers():
+    """Large arrays can live at addresses beyond 32 bits (the bench's CPU
+    baseline runs the C port on the 64^3 workload): every pointer argument of
+    the port is declared, so ctypes passes full addresses; a patch with
+    arrays of a few hundred KB still matches the numpy oracle."""
+    import ctypes
+    from oracle.wq_cpu import ReferenceWQ
+    P = cube_patch((22, 20, 16), 2, perturb=0.1, wrange=(0.9, 1.1), seed=6)
+    a = WQOracle(P, 1.0, 0.3, {"w0": (0, 1, 2)})
+    b = ReferenceWQ(P, 1.0, 0.3, {"w0": (0, 1, 2)})
+    for f in (b.L.oracle_wq_create, b.L.oracle_wq_apply, b.L.oracle_wq_free):
+        assert f.argtypes is not None
+        assert all(t in (ctypes.c_void_p, ctypes.c_double) for t in f.argtypes)
+    u = np.random.default_rng(2).standard_normal(a.ndof)
+    assert _rel(b.apply(u), a.apply(u)) < 1e-13
