@@ -187,7 +187,12 @@ struct yeti_server {
             if (rc == YETI_OK) rc = cgsolve_launch(*cs);
             r->solves.push_back(std::move(cs));
             if (rc != YETI_OK) {
-                finish(r, rc, yeti_last_error());
+                // the failed solve may have start work queued on st that reads
+                // the operator: let it end before finish frees the operator
+                const std::string err = yeti_last_error();
+                cudaStreamSynchronize(st);
+                (void)cudaGetLastError();
+                finish(r, rc, err);
                 return;
             }
         }
