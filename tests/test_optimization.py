@@ -6,11 +6,13 @@ Bars: the responses at x equal the GPU compliance and volume of the moved
 model exactly; the analytic gradients (adjoint kernel, volume gradient,
 propagated through the design map) match central finite differences of the
 same responses within 1e-6 relative (volume) and 1e-5 relative (compliance,
-whose differences carry the direct solve's rounding); an SLSQP loop
+whose differences carry the direct solve's rounding); the displacement at a
+parametric point and its three-adjoint gradient match differences within
+1e-6 (step 1e-4); an SLSQP loop
 (scipy) over four thickness variables of the cantilever lowers its
 compliance at fixed volume.  The host logic (listpatch validation, the
-propagation through a coarse-to-fine map, the finite-difference helper)
-runs on the CPU.
+propagation through a coarse-to-fine map, the finite-difference helper, the
+rational basis at a parametric point) runs on the CPU.
 """
 import numpy as np
 import pytest
@@ -100,6 +102,45 @@ def test_finite_difference_helper():
     np.testing.assert_allclose(opt._sensitivity_fd(f, x, 1e-7, False), exact, rtol=1e-5)
 
 
+def test_point_basis_geometry():
+    """The rational basis at a parametric point: it sums to 1, interpolates
+    the corner control point, reproduces the cantilever's affine map
+    x = (10 xi, eta, zeta) (linear precision of B-splines) and keeps the
+    quarter annulus's exact arcs (in-plane radius constant along eta)."""
+    opt, args = cantilever_problem()
+    X = np.asarray(dict(zip(SYSTEM_ARG_NAMES, args))["COORDS3D"], dtype=np.float64)
+    rng = np.random.default_rng(7)
+    for xi in list(rng.random((20, 3))) + [np.array([0.0, 0.0, 0.0]), np.array([1.0, 1.0, 1.0]),
+                                          np.array([0.5, 0.25, 0.75])]:
+        cps, R = opt.point_basis(xi)
+        assert abs(R.sum() - 1.0) < 1e-14
+        x = R @ X[:, cps].T
+        np.testing.assert_allclose(x, [10 * xi[0], xi[1], xi[2]], atol=1e-13)
+    cps, R = opt.point_basis([0.0, 0.0, 0.0])
+    corner = np.argmin(np.abs(X - X.min(axis=1, keepdims=True)).sum(axis=0))
+    assert R.max() == pytest.approx(1.0, abs=1e-15) and cps[np.argmax(R)] == corner
+    with pytest.raises(ValueError, match="outside"):
+        opt.point_basis([1.2, 0.5, 0.5])
+    _, a2 = load_fixture("quarter_annulus_p2_4x4x2")
+    Xa = np.asarray(dict(zip(SYSTEM_ARG_NAMES, a2))["COORDS3D"], dtype=np.float64)
+    ann = ShapeOptimization(a2, 1, lambda c0, x: c0)
+    for u in (0.0, 0.3, 0.77, 1.0):
+        radii = []
+        for v in np.linspace(0.0, 1.0, 9):
+            cps, R = ann.point_basis([u, v, 0.4])
+            x = R @ Xa[:, cps].T
+            radii.append(np.hypot(x[0], x[1]))
+        assert np.ptp(radii) < 1e-12 * max(radii)
+
+
+def test_displacement_fd_shape():
+    """Vector responses give (nb_var, m) differences."""
+    opt, _ = cantilever_problem()
+    g = opt._sensitivity_fd(lambda y: np.array([y[0] ** 2, y[1] * y[2], y[3]]),
+                            np.array([1.0, 2.0, 3.0, 4.0]), 1e-6, True)
+    np.testing.assert_allclose(g, [[2, 0, 0], [0, 3, 0], [0, 2, 0], [0, 0, 1]], atol=1e-8)
+
+
 # ---------------------------------------------------------------------- GPU
 @pytest.mark.gpu
 def test_responses_equal_moved_model(cuda_ok):
@@ -134,6 +175,31 @@ def test_analytic_gradients_vs_finite_differences(cuda_ok):
     assert np.linalg.norm(gc - fc) <= 1e-5 * np.linalg.norm(fc)
     # thicker near the clamp lowers the compliance most
     assert gc[0] < gc[1] < gc[2] < gc[3] < 0
+
+
+@pytest.mark.gpu
+def test_displacement_and_its_analytic_gradient(cuda_ok):
+    """u(xi) = sum R_a(xi) U_a of the GPU solution, and du/dx from three
+    adjoint solves and the GPU adjoint kernel (three adjoints in one call)
+    against central differences.  The step is 1e-4: the differences of this
+    slender, stiff model carry the direct solve's rounding divided by the
+    step (2e-6 relative at 1e-6, 3e-8 at 1e-4 with the CPU oracle)."""
+    from yeti_b200.gradient import _solve
+    opt, args = cantilever_problem()
+    x = np.array([0.05, -0.02, 0.03, 0.01])
+    for xi in ([1.0, 0.5, 1.0], [0.6, 0.3, 0.8]):
+        U = _solve(args, opt.analysis_coords(x))[0]
+        cps, R = opt.point_basis(xi)
+        u = opt.displacement(x, xi)
+        np.testing.assert_array_equal(u, R @ U.reshape(-1, 3)[cps])
+        ga = opt.grad_displacement_analytic(x, xi)
+        gf = opt.grad_displacement_finite_differences(x, xi, eps=1e-4, centered=True)
+        assert ga.shape == gf.shape == (4, 3)
+        assert np.linalg.norm(ga - gf) <= 1e-6 * np.linalg.norm(gf)
+    # the tip deflects downwards under the -z traction; lifting the top face
+    # near the clamp stiffens the beam: d u_z / d x_0 > 0
+    assert opt.displacement(x, [1.0, 0.5, 0.5])[2] < 0
+    assert opt.grad_displacement_analytic(x, [1.0, 0.5, 0.5])[0, 2] > 0
 
 
 @pytest.mark.gpu

@@ -11,7 +11,13 @@ the ``OPTmodelling`` functions behind it
 * ``compliance`` / ``grad_compliance_analytic`` /
   ``grad_compliance_finite_differences`` (``iga_optimization.py:162-221``,
   ``OPT_modelling.py:534-565``): C = 1/2 U.F, adjoint U_A = U/2,
-  dC/dP = dW_int + 2 dW_ext.
+  dC/dP = dW_int + 2 dW_ext;
+* ``displacement`` / ``grad_displacement_analytic`` /
+  ``grad_displacement_finite_differences`` (``iga_optimization.py:223-298``,
+  ``OPT_modelling.py:568-608``): u(xi) = sum_a R_a(xi) U_a, one adjoint per
+  component with the right-hand side R_a(xi) on that component's dofs
+  (``adjointRHSdisp``, ``optim/adjointRHS_disp.f:19-100``),
+  du_c/dP = dW_int + dW_ext of adjoint c.
 
 The design variables x move the design model's control points through
 ``update_function(coords_0, x) -> coords`` (3, nb_cp_design); the analysis
@@ -30,14 +36,17 @@ Every response runs the GPU kernels of libyeti_b200.so: the COO assembly
 the free-dof system is solved directly on the host, as the reference does.
 The reference's ``update_function`` edits an ``IgaModel`` in place; here it
 returns the new coordinates, and the refinement is given as the matrix the
-reference builds from its ``Refinement``.  The displacement response
-(``compute_displacement``) and VTU output are not part of this module.
+reference builds from its ``Refinement``.  The rational basis at the point
+of a displacement response is evaluated on the host (one element's
+(p+1)^3 values, as the reference does); VTU output stays with YETI's
+writers.
 """
 import numpy as np
 import scipy.sparse as sp
+import scipy.sparse.linalg as spla
 
 from .gradient import _solve, grad_from_system_args
-from .stiffmtrx_elemstorage import SYSTEM_ARG_NAMES
+from .stiffmtrx_elemstorage import SYSTEM_ARG_NAMES, sys_linmat_lindef_static
 from .volume import volume_and_gradient
 
 __all__ = ["ShapeOptimization"]
@@ -101,6 +110,7 @@ class ShapeOptimization:
         self.nb_patch = int(np.atleast_1d(self._d["nb_elem_patch"]).size)
         self._cache_x = None
         self._cache_sol = None
+        self._tables = None
 
     # ------------------------------------------------------------ geometry
     def _check_x(self, x):
@@ -209,17 +219,127 @@ class ShapeOptimization:
 
     def _sensitivity_fd(self, fun, x, eps, centered):
         """Forward or central differences per design variable
-        (_sensitivityFD, OPT_modelling.py:411-437)."""
+        (_sensitivityFD, OPT_modelling.py:411-437): shape (nb_var,) for a
+        scalar response, (nb_var, m) for a response of m values."""
         x = self._check_x(x)
-        f0 = None if centered else fun(x)
-        g = np.zeros(self.nb_var)
+        f = lambda y: np.asarray(fun(y), dtype=np.float64)
+        f0 = None if centered else f(x)
+        rows = []
         for i in range(self.nb_var):
             xp = x.copy()
             xp[i] += eps
             if centered:
                 xm = x.copy()
                 xm[i] -= eps
-                g[i] = (fun(xp) - fun(xm)) / (2.0 * eps)
+                rows.append((f(xp) - f(xm)) / (2.0 * eps))
             else:
-                g[i] = (fun(xp) - f0) / eps
-        return g
+                rows.append((f(xp) - f0) / eps)
+        return np.array(rows)
+
+    # ------------------------------------------------------------ displacement
+    def _patch_tables(self):
+        """Per patch: element count, knot counts, degrees, nodes per
+        element, and the offsets of its first element, of its nodes in the
+        flat IEN / weight arrays and of its knots in Ukv."""
+        if self._tables is None:
+            d = self._d
+            nep = np.atleast_1d(np.asarray(d["nb_elem_patch"], dtype=np.int64))
+            nkv = np.asarray(d["Nkv"], dtype=np.int64).reshape(3, -1, order="F")
+            jpqr = np.asarray(d["Jpqr"], dtype=np.int64).reshape(3, -1, order="F")
+            nnode = np.atleast_1d(np.asarray(d["NNODE"], dtype=np.int64))
+            e0 = np.concatenate([[0], np.cumsum(nep)[:-1]])
+            n0 = np.concatenate([[0], np.cumsum(nep * nnode)[:-1]])
+            k0 = np.concatenate([[0], np.cumsum(nkv.sum(axis=0))[:-1]])
+            nijk = np.asarray(d["Nijk"], dtype=np.int64).reshape(3, -1, order="F")
+            self._tables = (nep, nkv, jpqr, nnode, e0, n0, k0, nijk)
+        return self._tables
+
+    def point_basis(self, xi, ipatch=0):
+        """Control points (0-based) and rational basis values R of the
+        element of patch ipatch holding the parametric point xi
+        (updateElementNumber + evalnurbs, evaluatenurbsfcts.f:94-209): the
+        knot span of each coordinate (the last non-empty one at the end of
+        the knot vector), the element with those spans (Nijk), the reversed
+        tensor product of the B-spline values times the element's weights,
+        divided by their sum."""
+        nep, nkv, jpqr, nnode, e0, n0, k0, nijk = self._patch_tables()
+        if not 0 <= ipatch < nep.size:
+            raise ValueError(f"ipatch {ipatch} outside 0..{nep.size - 1}")
+        xi = np.asarray(xi, dtype=np.float64).ravel()
+        if xi.size != 3:
+            raise ValueError("xi must hold 3 parametric coordinates")
+        U = np.asarray(self._d["Ukv"], dtype=np.float64).ravel()
+        off = int(k0[ipatch])
+        spans, vals = [], []
+        for dd in range(3):
+            kv = U[off:off + nkv[dd, ipatch]]
+            off += int(nkv[dd, ipatch])
+            p = int(jpqr[dd, ipatch])
+            u = float(xi[dd])
+            if not kv[0] <= u <= kv[-1]:
+                raise ValueError(f"xi[{dd}] = {u} outside [{kv[0]}, {kv[-1]}]")
+            ni = min(int(np.searchsorted(kv, u, side="right")), kv.size - p - 1)
+            # Cox-de Boor on span [kv[ni-1], kv[ni]] (The NURBS Book A2.2)
+            N = np.zeros(p + 1)
+            N[0] = 1.0
+            left, right = np.zeros(p + 1), np.zeros(p + 1)
+            for j in range(1, p + 1):
+                left[j] = u - kv[ni - j]
+                right[j] = kv[ni + j - 1] - u
+                saved = 0.0
+                for r in range(j):
+                    temp = N[r] / (right[r + 1] + left[j - r])
+                    N[r] = saved + right[r + 1] * temp
+                    saved = left[j - r] * temp
+                N[j] = saved
+            spans.append(ni)
+            vals.append(N[::-1])   # local node i <-> function p - i
+        first, count = int(e0[ipatch]), int(nep[ipatch])
+        hit = np.nonzero(np.all(nijk[:, first:first + count] == np.array(spans)[:, None],
+                                axis=0))[0]
+        if hit.size == 0:
+            raise ValueError(f"no element of patch {ipatch} holds xi = {xi}")
+        le = int(hit[0])
+        nn = int(nnode[ipatch])
+        base = int(n0[ipatch]) + le * nn
+        w = np.asarray(self._d["weight"], dtype=np.float64).ravel()[base:base + nn]
+        cps = np.asarray(self._d["IEN"], dtype=np.int64).ravel()[base:base + nn] - 1
+        R = (vals[2][:, None, None] * vals[1][None, :, None] * vals[0][None, None, :]).ravel() * w
+        return cps, R / R.sum()
+
+    def displacement(self, x, xi, ipatch=0):
+        """Displacement (3,) at the parametric point xi of patch ipatch
+        (compute_displacement, OPT_modelling.py:568-576)."""
+        _, U, _ = self._state(x)
+        cps, R = self.point_basis(xi, ipatch)
+        return R @ U.reshape(-1, 3)[cps]
+
+    def grad_displacement_analytic(self, x, xi, ipatch=0):
+        """du/dx, shape (nb_var, 3): three adjoint solves with the point's
+        basis on each component, the GPU adjoint kernel with three adjoints,
+        dW_int + dW_ext per component, propagated
+        (compute_gradDisplacement_AN, OPT_modelling.py:595-608)."""
+        X, U, _ = self._state(x)
+        cps, R = self.point_basis(xi, ipatch)
+        n = U.size
+        FA = np.zeros((n, 3))
+        for c in range(3):
+            FA[3 * cps + c, c] = R
+        a = list(self.args)
+        a[2] = X
+        kdata, krow, kcol, _ = sys_linmat_lindef_static(*a)
+        K = sp.coo_matrix((kdata, (krow, kcol)), shape=(n, n)).tocsc()
+        K = K + K.T
+        idof = np.asarray(self.args[26])[:int(self.args[27])] - 1
+        UA = np.zeros((n, 3))
+        UA[idof] = np.asarray(spla.spsolve(K[idof, :][:, idof], FA[idof])).reshape(-1, 3)
+        sol = U.reshape(-1, 3).T
+        adj = np.stack([UA[:, c].reshape(-1, 3).T for c in range(3)])
+        gi, ge = grad_from_system_args(a, sol, adj, True, True, self.include_surface_loads)
+        return np.stack([self.propagate(x, gi[c] + ge[c]) for c in range(3)], axis=1)
+
+    def grad_displacement_finite_differences(self, x, xi, ipatch=0, eps=1.e-6,
+                                             centered=False):
+        """du/dx by differences, shape (nb_var, 3)."""
+        return self._sensitivity_fd(lambda y: self.displacement(y, xi, ipatch), x, eps,
+                                    centered)
