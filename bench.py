@@ -299,10 +299,30 @@ def extra_configs(args, device):
     t0 = time.perf_counter()
     ko, _, _, Fo = oracle.sys_linmat_lindef_static(*a1)
     t_cpu = (time.perf_counter() - t0) * 1e3
+    # the whole C1 path: assembly, K = Kside + Kside^T, sparse direct solve of
+    # the free dofs (scipy, on the host, as the reference does); displacement
+    # against the same path on the oracle's COO
+    import scipy.sparse as sp
+    import scipy.sparse.linalg as spla
+    X1 = np.asarray(a1[2], dtype=np.float64)
+    t_solve = _median_ms(lambda: _solve(a1, X1), 5, sync)
+    U1, _ = _solve(a1, X1)
+    n1 = Fo.size
+    t0 = time.perf_counter()
+    ko2, ro2, co2, Fo2 = oracle.sys_linmat_lindef_static(*a1)
+    K1 = sp.coo_matrix((ko2, (ro2, co2)), shape=(n1, n1)).tocsc()
+    K1 = K1 + K1.T
+    idof1 = np.asarray(a1[26])[:int(a1[27])] - 1
+    Uo = np.zeros(n1)
+    Uo[idof1] = spla.spsolve(K1[idof1, :][:, idof1], Fo2[idof1])
+    t_cpu_solve = (time.perf_counter() - t0) * 1e3
     out["assembly_p2_16x4x4"] = {
         "nb_data": int(kd.size), "gpu_ms_device_out": t_gpu, "gpu_ms_host_buffers": t_gpu_host,
         "cpu_oracle_ms": t_cpu, "cpu_cores": 1,
-        "bit_identical": bool(np.array_equal(kd, ko) and np.array_equal(F, Fo))}
+        "bit_identical": bool(np.array_equal(kd, ko) and np.array_equal(F, Fo)),
+        "assemble_and_solve_ms": t_solve, "cpu_oracle_assemble_and_solve_ms": t_cpu_solve,
+        "displacement_max_rel_diff_vs_oracle": float(np.abs(U1 - Uo).max() / np.abs(Uo).max()),
+        "tip_min_uz": float(U1[2::3].min())}
     # consistent mass matrix of the same model (parity: bit-identical COO)
     from yeti_b200.massmtrx import build_cmassmatrix
     from yeti_b200.stiffmtrx_elemstorage import SYSTEM_ARG_NAMES as _SAN
