@@ -396,19 +396,21 @@ def extra_configs(args, device):
     xref, st_ref = op.pcg(b, rtol=1e-12, maxit=50000)
     sync()
     t0 = time.perf_counter()
-    x, st = op.pcg(b, rtol=1e-8, mixed=True, maxit=50000)
+    # rtol 1e-9, as on the 64^3 block: a 1e-8 residual leaves the error just
+    # above the 1e-8 bar (1.04e-8 measured)
+    x, st = op.pcg(b, rtol=1e-9, mixed=True, maxit=50000)
     sync()
     t_solve = time.perf_counter() - t0
     err = (torch.linalg.norm(x - xref) / torch.linalg.norm(xref)).item()
-    op.pcg(b, rtol=1e-8, mixed=True, precond="fd")   # builds the plan
+    op.pcg(b, rtol=1e-9, mixed=True, precond="fd")   # builds the plan
     sync()
     t0 = time.perf_counter()
-    xf, stf = op.pcg(b, rtol=1e-8, mixed=True, precond="fd")
+    xf, stf = op.pcg(b, rtol=1e-9, mixed=True, precond="fd")
     sync()
     t_fd = time.perf_counter() - t0
     err_fd = (torch.linalg.norm(xf - xref) / torch.linalg.norm(xref)).item()
     out["wq_p4_128x128x32"] = {
-        "ndof": op.ndof, "nqp": op.nqp, "apply_f32_us": t_app * 1e6,
+        "ndof": op.ndof, "nqp": op.nqp, "rtol": 1e-9, "apply_f32_us": t_app * 1e6,
         "achieved_gbs": alg / t_app / 1e9, "peak_gbs": peak, "frac": alg / t_app / 1e9 / peak,
         "peak_kind": peak_kind_note(kind), "mixed_solve_s": t_solve,
         "iterations": st["iterations"], "rel_residual": st["rel_residual"],

@@ -186,12 +186,22 @@ int yeti_wq_apply(yeti_wq_op *op, const void *u, void *Ku, int prec, int mem);
  * memory is all reserved by another allocator, or a latency-critical loop that
  * must not pay cudaMalloc/cudaFree's implicit synchronisation -- the two
  * vectors are staged in one file-scope device array of at most 2,097,152 dofs
- * per vector (32 MiB, held by every GPU that loads the library until exit);
- * larger operators return YETI_EINVAL.  The first call on a device looks the
- * array's device address up (cudaGetSymbolAddress); make that first call
- * before any stream capture.  All calls share the array: calls that overlap on
- * the GPU race. */
+ * per vector (32 MiB, held until the process exits); larger operators return
+ * YETI_EINVAL.  The first call on a device looks the array's device address
+ * up (cudaGetSymbolAddress); under CUDA's default lazy module loading that
+ * lookup is also when the 32 MiB are committed on the device.  Make that
+ * first call before device memory is all reserved and before any stream
+ * capture.  All calls share the array: calls that overlap on the GPU race.
+ * Returns YETI_ETIMEDOUT, as yeti_wq_apply does, when a bounded device wait
+ * gave up. */
 int yeti_wq_apply_static(yeti_wq_op *op, const void *u, void *Ku, int prec);
+/* Polls of each bounded wait for a coefficient copy in the streaming apply
+ * (default 65536; tries < 0 restores it).  A wait that runs out makes the
+ * apply (and the solvers) return YETI_ETIMEDOUT with invalid results and the
+ * device context intact.  Applies to launches issued after the call
+ * (graphs captured before keep the old bound).  Diagnostic knob; no
+ * counterpart in the reference. */
+int yeti_wq_set_wait_limit(yeti_wq_op *op, int tries);
 /* Diagonal of K (3*ncp doubles; clamped dofs hold 1). */
 int yeti_wq_diag(yeti_wq_op *op, double *d, int mem);
 /* Body-force load vector for a constant force density f[3]

@@ -21,38 +21,10 @@
 #define GMAXP 10
 #define GMAXNN 1331
 
-static void g_gauss_legendre(int n, double *x, double *w)
-{
-    for (int i = 0; i < n; i++) {
-        double z = -cos(M_PI * (i + 0.75) / (n + 0.5)), pp = 0.0;
-        for (int it = 0; it < 100; it++) {
-            double p1 = 1.0, p2 = 0.0;
-            for (int k = 1; k <= n; k++) {
-                double p3 = p2;
-                p2 = p1;
-                p1 = ((2.0 * k - 1.0) * z * p2 - (k - 1.0) * p3) / k;
-            }
-            pp = n * (z * p1 - p2) / (z * z - 1.0);
-            double dz = p1 / pp;
-            z -= dz;
-            if (fabs(dz) < 1e-17) break;
-        }
-        double p1 = 1.0, p2 = 0.0;
-        for (int k = 1; k <= n; k++) {
-            double p3 = p2;
-            p2 = p1;
-            p1 = ((2.0 * k - 1.0) * z * p2 - (k - 1.0) * p3) / k;
-        }
-        pp = n * (z * p1 - p2) / (z * z - 1.0);
-        x[i] = z;
-        w[i] = 2.0 / ((1.0 - z * z) * pp * pp);
-    }
-    for (int i = 0; i < n / 2; i++) {
-        double a = 0.5 * (x[n - 1 - i] - x[i]), b = 0.5 * (w[n - 1 - i] + w[i]);
-        x[i] = -a; x[n - 1 - i] = a; w[i] = b; w[n - 1 - i] = b;
-    }
-    if (n % 2) x[n / 2] = 0.0;
-}
+/* Gauss-Legendre rule of order n (GaussLegendre.f90:27-153), shared with
+ * the assembly oracle (yeti_oracle.c). */
+void oracle_gauss_legendre(int n, double *x, double *w);
+#define g_gauss_legendre oracle_gauss_legendre
 
 static void g_ders(int ni, int p, double u, const double *U, double *N, double *dN)
 {

@@ -3,11 +3,17 @@ single NURBS patch.
 
 TEST INFRASTRUCTURE ONLY (see oracle/__init__.py).
 
-Parity unpinned: the reference has no elastic WQ operator to compare with;
-the 1-D rules used here are pinned to the reference's Python twin
-(tests/golden/wq_rules.npz), and the operator is checked for exactness on
-affine patches, against a dense direct solve and against the reference's
-rank-one algorithm (oracle/oracle_wq.c) in tests/test_wq.py.
+Pinned to the reference's own Python WQ assembly (methods_wq.WQ,
+iga_wq_mf/ThermoMechaIGA/pysrc/lib/methods_wq.py:76-108, with its
+eval_jacobien_pps / eval_K_C_coefficient, create_model.py:531-601) by
+tests/golden/wq_operator.npz (generator: tests/golden/make_wq_operator_golden.py):
+the elastic operator, assembled there block by block from the Fortran's
+coefficient formula, on geometries with symmetric Jacobians (where the
+Fortran's orientation and the geometric one agree); the Jacobian, the
+conductivity coefficient and the scalar operator on perturbed patches.  The
+1-D rules are pinned to the reference's Python twin (tests/golden/
+wq_rules.npz); tests/test_wq.py adds exactness on affine patches, a dense
+direct solve and the reference's rank-one algorithm (oracle/oracle_wq.c).
 
 The reference ships the WQ matrix-free operator for the scalar (thermal)
 problem only, with B-spline geometry:
@@ -64,17 +70,21 @@ def mdm_matrix(E, nu):
 
 
 def _fwd(f, Bu, Bv, Bw):
-    """(nw, nv, nu) field on functions -> (qw, qv, qu) values at points."""
-    t = np.einsum("wvu,uq->wvq", f, Bu)
-    t = np.einsum("wvq,vr->wrq", t, Bv)
-    return np.einsum("wrq,ws->srq", t, Bw)
+    """(nw, nv, nu) field on functions -> (qw, qv, qu) values at points:
+    t[w,v,q] = sum_u f[w,v,u] Bu[u,q], then along v, then along w (matrix
+    products, so that the full-size operators run through BLAS)."""
+    t = f @ Bu                                   # (w, v, q)
+    t = np.matmul(Bv.T, t)                       # (w, r, q)
+    nw, nr, nq = t.shape
+    return (Bw.T @ t.reshape(nw, nr * nq)).reshape(-1, nr, nq)
 
 
 def _bwd(h, Wu, Wv, Ww):
     """(qw, qv, qu) point values -> (nw, nv, nu) with the 1-D weights."""
-    t = np.einsum("srq,uq->sru", h, Wu)
-    t = np.einsum("sru,vr->svu", t, Wv)
-    return np.einsum("svu,ws->wvu", t, Ww)
+    t = h @ Wu.T                                 # (s, r, u)
+    t = np.matmul(Wv, t)                         # (s, v, u)
+    ns, nv, nu = t.shape
+    return (Ww @ t.reshape(ns, nv * nu)).reshape(-1, nv, nu)
 
 
 class WQOracle:
@@ -122,6 +132,7 @@ class WQOracle:
             for l in range(3):
                 J[c, l] = (D[c][l] - x[c] * gW[l]) / W
         Jq = np.moveaxis(J, (0, 1), (-2, -1))     # (..., 3, 3)
+        self.J = J                                # J[c, l] = dx_c / dxi_l
         self.detJ = np.linalg.det(Jq)
         invJ = np.linalg.inv(Jq)                  # invJ[..., k, d] = dxi_k/dx_d
         MDM = mdm_matrix(E, nu)
@@ -147,6 +158,30 @@ class WQOracle:
                     acc = acc + self.bwd(h, k, l)
             out[i] = acc
         return (out * self.mask).ravel()
+
+    def conductivity_coef(self):
+        """Scalar conductivity coefficient inv(J) inv(J)^T |det J| per point,
+        (3, 3, nqp) with the points u fastest (eval_K_C_coefficient,
+        create_model.py:570-601, with an identity conductivity)."""
+        Jq = np.moveaxis(self.J, (0, 1), (-2, -1))
+        invJ = np.linalg.inv(Jq)
+        C = invJ @ np.swapaxes(invJ, -1, -2) * np.abs(self.detJ)[..., None, None]
+        return np.moveaxis(C, (-2, -1), (0, 1)).reshape(3, 3, -1)
+
+    def apply_scalar(self, u, coef):
+        """Scalar WQ operator sum_{k,l} W^{(k,l)} (coef_kl * (B^{(l)})^T u)
+        on one field of control-point values (mf_wq_get_ku_3d,
+        mf_wq_solver.f90:284-544; no clamps).  coef: (3, 3, nqp), points u
+        fastest."""
+        shp = self.mask.shape[1:]
+        u = np.asarray(u, dtype=np.float64).reshape(shp)
+        C = np.asarray(coef).reshape((3, 3) + self.detJ.shape)
+        G = [self.fwd(u, l) for l in (1, 2, 3)]
+        out = np.zeros(shp)
+        for k in (1, 2, 3):
+            for l in (1, 2, 3):
+                out += self.bwd(C[k - 1, l - 1] * G[l - 1], k, l)
+        return out.ravel()
 
     def diag(self):
         S = self.S

@@ -21,14 +21,74 @@
 #define MAXP 10            /* maximum degree per direction */
 #define MAXNN 1331         /* maximum nodes per element (p=10 cubed) */
 
-/* ------------------------------------------------------------------ */
-/* Gauss-Legendre rule of order n on [-1,1]                             */
-/* (GaussLegendre.f90:27-153 tabulates orders 1..9; the nodes are the  */
-/* roots of P_n, computed here by Newton iteration on the three-term   */
-/* recurrence, and the weights are 2/((1-x^2) P_n'(x)^2).)             */
-/* ------------------------------------------------------------------ */
-static void gauss_legendre(int n, double *x, double *w)
+/* Gauss-Legendre rules of orders 1..9 on [-1, 1]: the nodes of the upper
+ * half (ascending, x >= 0) and their weights, as tabulated by the reference
+ * (GaussLegendre.f90:41-153, 30 significant digits; these are the standard
+ * published values of the rules, rounded to double by the compiler).  The
+ * lower half mirrors them exactly; the order-3 weights are the divisions
+ * 5/9 and 8/9, as the reference writes them. */
+static const double kGLX[10][5] = {
+    {0, 0, 0, 0, 0},
+    {0.0},
+    {0.577350269189625764509148780502},
+    {0.0, 0.774596669241483377035853079956},
+    {0.339981043584856264802665759103, 0.861136311594052575223946488893},
+    {0.0, 0.538469310105683091036314420700, 0.906179845938663992797626878299},
+    {0.238619186083196908630501721681, 0.661209386466264513661399595020,
+     0.932469514203152027812301554494},
+    {0.0, 0.405845151377397166906606412077, 0.741531185599394439863864773281,
+     0.949107912342758524526189684048},
+    {0.183434642495649804939476142360, 0.525532409916328985817739049189,
+     0.796666477413626739591553936476, 0.960289856497536231683560868569},
+    {0.0, 0.324253423403808929038538014643, 0.613371432700590397308702039341,
+     0.836031107326635794299429788070, 0.968160239507626089835576202904},
+};
+static const double kGLW[10][5] = {
+    {0, 0, 0, 0, 0},
+    {2.0},
+    {1.0},
+    {0.0, 0.0},   /* 8/9, 5/9: computed */
+    {0.652145154862546142626936050778, 0.347854845137453857373063949222},
+    {0.568888888888888888888888888889, 0.478628670499366468041291514836,
+     0.236926885056189087514264040720},
+    {0.467913934572691047389870343990, 0.360761573048138607569833513838,
+     0.171324492379170345040296142173},
+    {0.417959183673469387755102040816, 0.381830050505118944950369775489,
+     0.279705391489276667901467771424, 0.129484966168869693270611432679},
+    {0.362683783378361982965150449277, 0.313706645877887287337962201987,
+     0.222381034453374470544355994426, 0.101228536290376259152531354310},
+    {0.330239355001259763164525069287, 0.312347077040002840068630406584,
+     0.260610696402935462318742869419, 0.180648160694857404058472031243,
+     0.812743883615744119718921581105e-01},
+};
+
+/* Rule of order n from the table (1 <= n <= 9): ascending nodes x[0..n-1]. */
+static void gauss_table(int n, double *x, double *w)
 {
+    for (int j = 0; j < (n + 1) / 2; j++) {
+        const double xv = kGLX[n][j];
+        const double wv = n == 3 ? (j == 0 ? 8.0 / 9.0 : 5.0 / 9.0) : kGLW[n][j];
+        const int hi = n / 2 + j;                              /* x >= 0 */
+        const int lo = n % 2 ? n / 2 - j : n / 2 - 1 - j;      /* mirror */
+        x[lo] = -xv;
+        w[lo] = wv;
+        x[hi] = xv;   /* odd n, j = 0: the centre, +0.0 as tabulated */
+        w[hi] = wv;
+    }
+}
+
+/* ------------------------------------------------------------------ */
+/* Gauss-Legendre rule of order n on [-1,1] (Gauss, GaussLegendre.f90: */
+/* 27-153): the table for orders 1..9; beyond, where the reference has */
+/* no rule, the roots of P_n by Newton iteration on the three-term     */
+/* recurrence with the weights 2/((1-x^2) P_n'(x)^2).                  */
+/* ------------------------------------------------------------------ */
+void oracle_gauss_legendre(int n, double *x, double *w)
+{
+    if (n >= 1 && n <= 9) {
+        gauss_table(n, x, w);
+        return;
+    }
     for (int i = 0; i < n; i++) {
         /* initial guess: Chebyshev-like approximation of the i-th root,
          * ascending order */
@@ -74,7 +134,7 @@ static void gauss_legendre(int n, double *x, double *w)
 static void gauss_volume(int n, double *out)
 {
     double x[16], w[16];
-    gauss_legendre(n, x, w);
+    oracle_gauss_legendre(n, x, w);
     int q = 0;
     for (int i = 0; i < n; i++)
         for (int j = 0; j < n; j++)
@@ -90,7 +150,7 @@ static void gauss_volume(int n, double *out)
 static void gauss_face(int n, int face, double *out)
 {
     double x[16], w[16];
-    gauss_legendre(n, x, w);
+    oracle_gauss_legendre(n, x, w);
     for (int j = 0; j < n; j++)
         for (int i = 0; i < n; i++) {
             double *g = out + 4 * (i + n * j);

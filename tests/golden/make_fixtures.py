@@ -28,7 +28,7 @@ import types
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-REF = os.environ.get("YETI_REFERENCE", "/root/reference")
+REF = os.environ.get("YETI_REFERENCE", "")
 MODELS = os.path.join(HERE, "models")
 
 
@@ -79,8 +79,8 @@ def _getinddof(mcrd, bc_target, bc_target_nbelem, bc_values, nb_dof_tot,
 
 def _install_stubs():
     pkg_dir = os.path.join(REF, "src", "yeti_iga")
-    if not os.path.isdir(pkg_dir):
-        raise SystemExit(f"reference source not found under {REF}")
+    if not REF or not os.path.isdir(pkg_dir):
+        raise SystemExit("set YETI_REFERENCE to the root of the reference source tree")
 
     def mod(name, **attrs):
         m = types.ModuleType(name)

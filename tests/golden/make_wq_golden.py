@@ -26,9 +26,15 @@ import types
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-REF = os.environ.get("YETI_REFERENCE", "/root/reference")
-BASE = os.path.join(REF, "src/yeti_iga/iga_wq_mf/ThermoMechaIGA/pysrc/lib/"
-                    "base_functions.py")
+LIB = "src/yeti_iga/iga_wq_mf/ThermoMechaIGA/pysrc/lib"
+
+
+def reference_root():
+    """Root of the reference source tree, from $YETI_REFERENCE."""
+    ref = os.environ.get("YETI_REFERENCE")
+    if not ref or not os.path.isdir(os.path.join(ref, LIB)):
+        raise SystemExit("set YETI_REFERENCE to the root of the reference source tree")
+    return ref
 CASES = [(2, 2), (2, 3), (2, 5), (2, 8), (3, 2), (3, 4), (3, 6), (3, 9),
          (4, 3), (4, 7), (4, 10)]
 
@@ -101,7 +107,8 @@ def load_base_functions():
     wq.basis_weights = types.ModuleType("iga_wq_mf.basis_weights")
     sys.modules["iga_wq_mf"] = wq
     sys.modules["iga_wq_mf.basis_weights"] = wq.basis_weights
-    spec = importlib.util.spec_from_file_location("ref_base_functions", BASE)
+    base = os.path.join(reference_root(), LIB, "base_functions.py")
+    spec = importlib.util.spec_from_file_location("ref_base_functions", base)
     mod = importlib.util.module_from_spec(spec)
     spec.loader.exec_module(mod)
     return mod

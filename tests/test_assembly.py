@@ -85,6 +85,64 @@ def test_oracle_stiffness_is_symmetric_psd_with_rigid_modes():
 
 
 # ------------------------------------------------------------------ GPU parity
+# Gauss-Legendre rules of GaussLegendre.f90:41-153 (orders 1..9, the
+# standard published nodes and weights to 30 significant digits): upper-half
+# nodes (ascending, x >= 0) and weights; order 3's weights are the divisions
+# 8/9 and 5/9.
+GL_TABLE = {
+    1: (["0.0"], ["2.0"]),
+    2: (["0.577350269189625764509148780502"], ["1.0"]),
+    3: (["0.0", "0.774596669241483377035853079956"], [8.0 / 9.0, 5.0 / 9.0]),
+    4: (["0.339981043584856264802665759103", "0.861136311594052575223946488893"],
+        ["0.652145154862546142626936050778", "0.347854845137453857373063949222"]),
+    5: (["0.0", "0.538469310105683091036314420700", "0.906179845938663992797626878299"],
+        ["0.568888888888888888888888888889", "0.478628670499366468041291514836",
+         "0.236926885056189087514264040720"]),
+    6: (["0.238619186083196908630501721681", "0.661209386466264513661399595020",
+         "0.932469514203152027812301554494"],
+        ["0.467913934572691047389870343990", "0.360761573048138607569833513838",
+         "0.171324492379170345040296142173"]),
+    7: (["0.0", "0.405845151377397166906606412077", "0.741531185599394439863864773281",
+         "0.949107912342758524526189684048"],
+        ["0.417959183673469387755102040816", "0.381830050505118944950369775489",
+         "0.279705391489276667901467771424", "0.129484966168869693270611432679"]),
+    8: (["0.183434642495649804939476142360", "0.525532409916328985817739049189",
+         "0.796666477413626739591553936476", "0.960289856497536231683560868569"],
+        ["0.362683783378361982965150449277", "0.313706645877887287337962201987",
+         "0.222381034453374470544355994426", "0.101228536290376259152531354310"]),
+    9: (["0.0", "0.324253423403808929038538014643", "0.613371432700590397308702039341",
+         "0.836031107326635794299429788070", "0.968160239507626089835576202904"],
+        ["0.330239355001259763164525069287", "0.312347077040002840068630406584",
+         "0.260610696402935462318742869419", "0.180648160694857404058472031243",
+         "0.812743883615744119718921581105E-01"]),
+}
+
+
+@pytest.mark.parametrize("n", range(1, 10))
+def test_oracle_gauss_rule_is_the_reference_table_bit_for_bit(n):
+    """The oracle's rule (the one the GPU assembly's parity tests compare
+    with bit for bit) equals the reference's table, each literal rounded to
+    double as a Fortran compiler rounds it (Python's float is correctly
+    rounded)."""
+    import ctypes
+    xs, ws = GL_TABLE[n]
+    up_x = [float(v) for v in xs]
+    up_w = [float(v) for v in ws]
+    if n % 2:
+        ref_x = [-v for v in up_x[:0:-1]] + up_x
+        ref_w = up_w[:0:-1] + up_w
+    else:
+        ref_x = [-v for v in up_x[::-1]] + up_x
+        ref_w = up_w[::-1] + up_w
+    x = np.zeros(n)
+    w = np.zeros(n)
+    f = oracle.lib().oracle_gauss_legendre
+    f.argtypes = [ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p]
+    f(n, x.ctypes.data, w.ctypes.data)
+    assert x.tobytes() == np.array(ref_x).tobytes()
+    assert w.tobytes() == np.array(ref_w).tobytes()
+
+
 def _gpu_vs_oracle(name):
     from yeti_b200.stiffmtrx_elemstorage import sys_linmat_lindef_static
     d, args = load_fixture(name)

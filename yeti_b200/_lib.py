@@ -110,6 +110,7 @@ def _declare(lib):
         "yeti_wq_info": (i32, [vp, vp, vp, vp, vp, vp]),
         "yeti_wq_apply": (i32, [vp, vp, vp, i32, i32]),
         "yeti_wq_apply_static": (i32, [vp, vp, vp, i32]),
+        "yeti_wq_set_wait_limit": (i32, [vp, i32]),
         "yeti_wq_diag": (i32, [vp, vp, i32]),
         "yeti_wq_body_force": (i32, [vp, vp, vp, i32]),
         "yeti_wq_pcg": (i32, [vp, vp, vp, dbl, i32, i32,

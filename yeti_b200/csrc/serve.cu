@@ -9,8 +9,10 @@
 //              bytes of the request fit in the HBM budget next to the active
 //              ones;
 //   setup      (worker) the WQ operator on the device (yeti_wq_setup, FP64
-//              data) and the start of one resumable FP64 Jacobi-PCG per
-//              right-hand side (CgSolve) on a stream of the pool;
+//              data) and the start of one resumable FP64 Krylov solve per
+//              right-hand side (CgSolve) in the request's mode: CG or
+//              BiCGSTAB, Jacobi or fast-diagonalisation preconditioned (the
+//              bench serves with fast-diagonalisation BiCGSTAB);
 //   solve      (engine) the solves advance in chunks of iterations captured
 //              in a CUDA graph, so that the solves of all active requests
 //              overlap on the device; the engine polls chunk events and

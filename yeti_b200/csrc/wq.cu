@@ -924,6 +924,12 @@ YETI_API int yeti_wq_apply(yeti_wq_op *op, const void *u, void *Ku, int prec,
     return YETI_OK;
 }
 
+YETI_API int yeti_wq_set_wait_limit(yeti_wq_op *op, int tries) {
+    YETI_CHECK(op, YETI_EINVAL, "yeti_wq_set_wait_limit: NULL op");
+    op->st.wait_tries = tries < 0 ? (1 << 16) : tries;
+    return YETI_OK;
+}
+
 YETI_API int yeti_wq_diag(yeti_wq_op *op, double *d, int mem) {
     YETI_CHECK(op && d, YETI_EINVAL, "yeti_wq_diag: NULL argument");
     DeviceGuard guard(op->ctx->device);

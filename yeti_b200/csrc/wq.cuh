@@ -70,6 +70,7 @@ struct WQStreamPlan {
     DevBuf elem[3], band64[3], band32[3], wq0, tq0[2], tnq[2], treg[2];
     DevBuf tile_off, tile_pstride, seg[2], cta_seg[2];
     DevBuf err;              // int: a kernel's bounded wait gave up
+    int wait_tries = 1 << 16;   // polls of a wait for a coefficient copy
 };
 
 // Device-side scalars of one CG solve (wq_pcg.cu); the fast-diagonalisation

@@ -8,8 +8,12 @@
 // entry point stages the vectors in one file-scope device array instead.
 //
 // Limits and sharing: the array holds two vectors of at most
-// kStaticMaxDof doubles (2 x 16 MiB = 32 MiB); every GPU that loads the
-// library keeps it until the process exits.  All calls on a device share the
+// kStaticMaxDof doubles (2 x 16 MiB = 32 MiB).  The library's device code is
+// loaded lazily by default (CUDA_MODULE_LOADING=LAZY): the array is then
+// committed on a device by the first call there (its address lookup loads
+// this file's module), and held until the process exits.  Make that first
+// call before another allocator reserves all of the device's memory, and
+// before any stream capture.  All calls on a device share the
 // same array and it keeps the last call's contents (the output half is
 // cleared on every call); calls that overlap on the GPU -- from several
 // threads, or on several streams -- race on it.
@@ -75,5 +79,8 @@ YETI_API int yeti_wq_apply_static(yeti_wq_op *op, const void *u, void *Ku,
     YETI_TRY(wq_apply_dev(op, du, dk, prec, nullptr, s));
     YETI_CUDA(cudaMemcpyAsync(Ku, dk, nb, cudaMemcpyDeviceToHost, s));
     YETI_CUDA(cudaStreamSynchronize(s));
+    // a bounded wait of the streaming apply that gave up: report it (and
+    // clear the operator's flag, which belongs to this call)
+    YETI_TRY(wq_stream_check(op));
     return YETI_OK;
 }

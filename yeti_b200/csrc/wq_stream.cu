@@ -174,9 +174,9 @@ __device__ __forceinline__ void bulk_load(void *dst, const void *src, uint32_t b
         "l"(src), "r"(bytes), "r"(smem_addr(bar)), "l"(policy)
         : "memory");
 }
-// Wait for the phase with the given parity, at most kWaitTries polls.
-__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity) {
-    for (int i = 0; i < kWaitTries; i++) {
+// Wait for the phase with the given parity, at most `tries` polls.
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, int tries) {
+    for (int i = 0; i < tries; i++) {
         uint32_t ok;
         asm volatile(
             "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
@@ -367,6 +367,7 @@ struct StreamArgs {
     int64_t ncp;
     int cmask[3];
     int *err;                  // set to 1 when a bounded wait gave up
+    int wait_tries;            // polls of a wait for a coefficient copy
 };
 
 template <class T, int P>
@@ -518,10 +519,11 @@ __global__ void __launch_bounds__(kThreads, 2) k_wq_apply_stream(StreamArgs<T> a
                 }
                 if constexpr (kStaged) {
                     // this plane's coefficient block has landed in shared memory
-                    const bool ok = mbar_wait(bar, phase);
+                    const bool ok = mbar_wait(bar, phase, a.wait_tries);
                     if (__syncthreads_or(!ok)) {
                         if (tid == 0) atomicOr(a.err, 1);
-                        mbar_wait(bar, phase);   // let a copy still in flight land
+                        // let the copy still in flight land (default bound)
+                        mbar_wait(bar, phase, kWaitTries);
                         return;
                     }
                     phase ^= 1;
@@ -1026,6 +1028,7 @@ static int launch_stream(yeti_wq_op *op, const T *u, T *Ku, const int *done, cud
     }
     a.wq0 = st.wq0.as<int>();
     a.err = st.err.as<int>();
+    a.wait_tries = st.wait_tries;
     a.nqw = op->nqp[2];
     a.seg = st.seg[which].as<int4>();
     a.cta_seg = st.cta_seg[which].as<int>();

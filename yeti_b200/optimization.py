@@ -261,7 +261,8 @@ class ShapeOptimization:
         knot span of each coordinate (the last non-empty one at the end of
         the knot vector), the element with those spans (Nijk), the reversed
         tensor product of the B-spline values times the element's weights,
-        divided by their sum."""
+        divided by their sum.  ipatch is 0-based: the reference's 1-based
+        numpatch minus one."""
         nep, nkv, jpqr, nnode, e0, n0, k0, nijk = self._patch_tables()
         if not 0 <= ipatch < nep.size:
             raise ValueError(f"ipatch {ipatch} outside 0..{nep.size - 1}")
@@ -309,7 +310,8 @@ class ShapeOptimization:
 
     def displacement(self, x, xi, ipatch=0):
         """Displacement (3,) at the parametric point xi of patch ipatch
-        (compute_displacement, OPT_modelling.py:568-576)."""
+        (compute_displacement, OPT_modelling.py:568-576).  ipatch is 0-based:
+        the reference's numpatch (1-based, default 1) minus one."""
         _, U, _ = self._state(x)
         cps, R = self.point_basis(xi, ipatch)
         return R @ U.reshape(-1, 3)[cps]
@@ -318,7 +320,8 @@ class ShapeOptimization:
         """du/dx, shape (nb_var, 3): three adjoint solves with the point's
         basis on each component, the GPU adjoint kernel with three adjoints,
         dW_int + dW_ext per component, propagated
-        (compute_gradDisplacement_AN, OPT_modelling.py:595-608)."""
+        (compute_gradDisplacement_AN, OPT_modelling.py:595-608).  ipatch is
+        0-based (the reference's numpatch - 1)."""
         X, U, _ = self._state(x)
         cps, R = self.point_basis(xi, ipatch)
         n = U.size
@@ -340,6 +343,6 @@ class ShapeOptimization:
 
     def grad_displacement_finite_differences(self, x, xi, ipatch=0, eps=1.e-6,
                                              centered=False):
-        """du/dx by differences, shape (nb_var, 3)."""
+        """du/dx by differences, shape (nb_var, 3); ipatch 0-based."""
         return self._sensitivity_fd(lambda y: self.displacement(y, xi, ipatch), x, eps,
                                     centered)
