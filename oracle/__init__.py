@@ -34,6 +34,13 @@ def lib():
     return _lib
 
 
+def threads():
+    """OpenMP threads the oracle's element loops and WQ port use."""
+    L = lib()
+    L.oracle_wq_threads.restype = ctypes.c_int
+    return int(L.oracle_wq_threads())
+
+
 def _i64(a):
     return np.ascontiguousarray(np.asarray(a).ravel(order="F"), dtype=np.int64)
 

@@ -447,35 +447,51 @@ int oracle_grad_lin_elast_work(
         U[2] = U[1] + nkv[3 * ip + 1];
         int nn = (int)nnode[ip];
         if (nn > GMAXNN) return -3;
-        double *ce = (double *)malloc(sizeof(double) * 3 * nn);
-        double *ue = (double *)malloc(sizeof(double) * 3 * nn);
-        double *uae = (double *)malloc(sizeof(double) * 3 * nn * nadj);
-        double *gi = (double *)malloc(sizeof(double) * nadj * 3 * nn);
-        double *ge = (double *)malloc(sizeof(double) * nadj * 3 * nn);
-        for (int64_t ie = 0; ie < nb_elem_patch[ip]; ie++, jelem++) {
-            const int64_t *ien_e = ien + ien_off + ie * nn;
-            if (active[jelem] != 1) continue;
-            int ni[3];
-            double u1[3], u2[3];
-            for (int d = 0; d < 3; d++) {
-                ni[d] = (int)nijk[3 * jelem + d];
-                u1[d] = U[d][ni[d] - 1];
-                u2[d] = U[d][ni[d]];
-            }
-            for (int a = 0; a < nn; a++) {
-                int64_t cp = ien_e[a] - 1;
-                for (int c = 0; c < 3; c++) {
-                    ce[3 * a + c] = coords[3 * cp + c];
-                    ue[3 * a + c] = sol[3 * cp + c];
-                    for (int k = 0; k < nadj; k++)
-                        uae[3 * a + c + 3 * nn * k] = adj[k + nadj * (c + 3 * cp)];
+        /* elements in parallel (OpenMP), each into its own slot of gi_all /
+         * ge_all; the scatter into gwint / gwext follows in element order,
+         * so the sums have the bits of the sequential loop */
+        const int64_t nep = nb_elem_patch[ip], j0 = jelem;
+        const size_t ne = (size_t)nadj * 3 * nn;
+        double *gi_all = (double *)calloc((size_t)nep * ne, sizeof(double));
+        double *ge_all = (double *)calloc((size_t)nep * ne, sizeof(double));
+#pragma omp parallel
+        {
+            double *ce = (double *)malloc(sizeof(double) * 3 * nn);
+            double *ue = (double *)malloc(sizeof(double) * 3 * nn);
+            double *uae = (double *)malloc(sizeof(double) * 3 * nn * nadj);
+#pragma omp for schedule(dynamic, 4)
+            for (int64_t ie = 0; ie < nep; ie++) {
+                const int64_t je = j0 + ie;
+                const int64_t *ien_e = ien + ien_off + ie * nn;
+                if (active[je] != 1) continue;
+                int ni[3];
+                double u1[3], u2[3];
+                for (int d = 0; d < 3; d++) {
+                    ni[d] = (int)nijk[3 * je + d];
+                    u1[d] = U[d][ni[d] - 1];
+                    u2[d] = U[d][ni[d]];
                 }
+                for (int a = 0; a < nn; a++) {
+                    int64_t cp = ien_e[a] - 1;
+                    for (int c = 0; c < 3; c++) {
+                        ce[3 * a + c] = coords[3 * cp + c];
+                        ue[3 * a + c] = sol[3 * cp + c];
+                        for (int k = 0; k < nadj; k++)
+                            uae[3 * a + c + 3 * nn * k] = adj[k + nadj * (c + 3 * cp)];
+                    }
+                }
+                g_element((int)nadj, nn, (int)nbint[ip], ce, ue, uae, p, U, ni, u1, u2,
+                          weight + w_off + ie * nn, matprops[2 * ip], matprops[2 * ip + 1], rho[ip],
+                          je + 1, (int)nb_load, inddload, load_target_nbelem, jdltype, adlmag,
+                          addinfos, compute_int, compute_ext, include_surface, nodal_dist,
+                          (int)nb_n_dist, ien_e, gi_all + ie * ne, ge_all + ie * ne);
             }
-            g_element((int)nadj, nn, (int)nbint[ip], ce, ue, uae, p, U, ni, u1, u2,
-                      weight + w_off + ie * nn, matprops[2 * ip], matprops[2 * ip + 1], rho[ip],
-                      jelem + 1, (int)nb_load, inddload, load_target_nbelem, jdltype, adlmag,
-                      addinfos, compute_int, compute_ext, include_surface, nodal_dist,
-                      (int)nb_n_dist, ien_e, gi, ge);
+            free(ce); free(ue); free(uae);
+        }
+        for (int64_t ie = 0; ie < nep; ie++) {
+            if (active[j0 + ie] != 1) continue;
+            const int64_t *ien_e = ien + ien_off + ie * nn;
+            const double *gi = gi_all + ie * ne, *ge = ge_all + ie * ne;
             for (int a = 0; a < nn; a++) {
                 int64_t cp = ien_e[a] - 1;
                 for (int c = 0; c < 3; c++)
@@ -487,7 +503,8 @@ int oracle_grad_lin_elast_work(
                     }
             }
         }
-        free(ce); free(ue); free(uae); free(gi); free(ge);
+        jelem += nep;
+        free(gi_all); free(ge_all);
         for (int d = 0; d < 3; d++) ukv_off += nkv[3 * ip + d];
         ien_off += nb_elem_patch[ip] * nn;
         w_off += nb_elem_patch[ip] * nn;
@@ -525,58 +542,85 @@ int oracle_volume(int64_t nb_patch, int64_t nb_cp, const double *coords,
             while (ng * ng * ng < nq) ng++;
             double gx[32], gw[32];
             g_gauss_legendre(ng, gx, gw);
-            double *R = (double *)malloc(sizeof(double) * nn);
-            double *dR = (double *)malloc(sizeof(double) * 3 * nn);
-            double *ce = (double *)malloc(sizeof(double) * 3 * nn);
-            for (int64_t ie = 0; ie < nb_elem_patch[ip]; ie++) {
-                const int64_t *ien_e = ien + ien_off + ie * nn;
-                const int64_t je = jelem + ie;
-                int ni[3];
-                double u1[3], u2[3];
-                for (int d = 0; d < 3; d++) {
-                    ni[d] = (int)nijk[3 * je + d];
-                    u1[d] = U[d][ni[d] - 1];
-                    u2[d] = U[d][ni[d]];
-                }
-                for (int a = 0; a < nn; a++)
-                    for (int c = 0; c < 3; c++) ce[3 * a + c] = coords[3 * (ien_e[a] - 1) + c];
-                int q = 0;
-                for (int i0 = 0; i0 < ng; i0++)
-                    for (int j0 = 0; j0 < ng; j0++)
-                        for (int k0 = 0; k0 < ng; k0++, q++) {
-                            if (q >= nq) break;
-                            double t[3] = {gx[i0], gx[j0], gx[k0]};
-                            double detJ = gw[i0] * gw[j0] * gw[k0], xi[3];
-                            for (int i = 0; i < 3; i++) {
-                                xi[i] = ((u2[i] - u1[i]) * t[i] + (u2[i] + u1[i])) * 0.5;
-                                detJ = detJ * 0.5 * (u2[i] - u1[i]);
-                            }
-                            g_evalnurbs(p, U, ni, weight + ien_off + ie * nn, xi, R, dR);
-                            double AI[3][3] = {{0}};   /* AI[k] = column k */
-                            for (int k = 0; k < 3; k++)
+            /* the terms of every Gauss point are evaluated in parallel
+             * (OpenMP over elements) into term buffers; the running sums
+             * are then replayed in the loop order above, so V and grad have
+             * the bits of the sequential loop */
+            const int64_t nep = nb_elem_patch[ip];
+            const int nqe = ng * ng * ng < nq ? ng * ng * ng : nq;
+            const size_t per_q = 1 + (grad ? 3 * (size_t)nn : 0);
+            double *terms = (double *)malloc(sizeof(double) * (size_t)nep * nqe * per_q);
+#pragma omp parallel
+            {
+                double *R = (double *)malloc(sizeof(double) * nn);
+                double *dR = (double *)malloc(sizeof(double) * 3 * nn);
+                double *ce = (double *)malloc(sizeof(double) * 3 * nn);
+#pragma omp for schedule(dynamic, 4)
+                for (int64_t ie = 0; ie < nep; ie++) {
+                    const int64_t *ien_e = ien + ien_off + ie * nn;
+                    const int64_t je = jelem + ie;
+                    double *tq = terms + (size_t)ie * nqe * per_q;
+                    int ni[3];
+                    double u1[3], u2[3];
+                    for (int d = 0; d < 3; d++) {
+                        ni[d] = (int)nijk[3 * je + d];
+                        u1[d] = U[d][ni[d] - 1];
+                        u2[d] = U[d][ni[d]];
+                    }
+                    for (int a = 0; a < nn; a++)
+                        for (int c = 0; c < 3; c++) ce[3 * a + c] = coords[3 * (ien_e[a] - 1) + c];
+                    int q = 0;
+                    for (int i0 = 0; i0 < ng; i0++)
+                        for (int j0 = 0; j0 < ng; j0++)
+                            for (int k0 = 0; k0 < ng; k0++, q++) {
+                                if (q >= nq) break;
+                                double t[3] = {gx[i0], gx[j0], gx[k0]};
+                                double detJ = gw[i0] * gw[j0] * gw[k0], xi[3];
+                                for (int i = 0; i < 3; i++) {
+                                    xi[i] = ((u2[i] - u1[i]) * t[i] + (u2[i] + u1[i])) * 0.5;
+                                    detJ = detJ * 0.5 * (u2[i] - u1[i]);
+                                }
+                                g_evalnurbs(p, U, ni, weight + ien_off + ie * nn, xi, R, dR);
+                                double AI[3][3] = {{0}};   /* AI[k] = column k */
+                                for (int k = 0; k < 3; k++)
+                                    for (int a = 0; a < nn; a++)
+                                        for (int c = 0; c < 3; c++)
+                                            AI[k][c] = AI[k][c] + dR[3 * a + k] * ce[3 * a + c];
+                                /* MatrixDet with AA(i, j) = AI[j-1][i-1] */
+                                double det = AI[1][0] * AI[2][1] * AI[0][2] - AI[2][0] * AI[1][1] * AI[0][2] +
+                                             AI[2][0] * AI[0][1] * AI[1][2] - AI[0][0] * AI[2][1] * AI[1][2] +
+                                             AI[0][0] * AI[1][1] * AI[2][2] - AI[1][0] * AI[0][1] * AI[2][2];
+                                double *tp = tq + (size_t)q * per_q;
+                                tp[0] = det * detJ;
+                                if (!grad) continue;
+                                double AxA[3][3];
+                                g_cross(AI[0], AI[1], AxA[2]);
+                                g_cross(AI[1], AI[2], AxA[0]);
+                                g_cross(AI[2], AI[0], AxA[1]);
                                 for (int a = 0; a < nn; a++)
                                     for (int c = 0; c < 3; c++)
-                                        AI[k][c] = AI[k][c] + dR[3 * a + k] * ce[3 * a + c];
-                            /* MatrixDet with AA(i, j) = AI[j-1][i-1] */
-                            double det = AI[1][0] * AI[2][1] * AI[0][2] - AI[2][0] * AI[1][1] * AI[0][2] +
-                                         AI[2][0] * AI[0][1] * AI[1][2] - AI[0][0] * AI[2][1] * AI[1][2] +
-                                         AI[0][0] * AI[1][1] * AI[2][2] - AI[1][0] * AI[0][1] * AI[2][2];
-                            V = V + det * detJ;
-                            if (!grad) continue;
-                            double AxA[3][3];
-                            g_cross(AI[0], AI[1], AxA[2]);
-                            g_cross(AI[1], AI[2], AxA[0]);
-                            g_cross(AI[2], AI[0], AxA[1]);
-                            for (int a = 0; a < nn; a++) {
-                                int64_t k = ien_e[a] - 1;
-                                for (int c = 0; c < 3; c++)
-                                    grad[c + 3 * k] = grad[c + 3 * k] +
-                                        (AxA[2][c] * dR[3 * a + 2] + AxA[0][c] * dR[3 * a] +
-                                         AxA[1][c] * dR[3 * a + 1]) * detJ;
+                                        tp[1 + 3 * a + c] =
+                                            (AxA[2][c] * dR[3 * a + 2] + AxA[0][c] * dR[3 * a] +
+                                             AxA[1][c] * dR[3 * a + 1]) * detJ;
                             }
-                        }
+                }
+                free(R); free(dR); free(ce);
             }
-            free(R); free(dR); free(ce);
+            for (int64_t ie = 0; ie < nep; ie++) {
+                const int64_t *ien_e = ien + ien_off + ie * nn;
+                const double *tq = terms + (size_t)ie * nqe * per_q;
+                for (int q = 0; q < nqe; q++) {
+                    const double *tp = tq + (size_t)q * per_q;
+                    V = V + tp[0];
+                    if (!grad) continue;
+                    for (int a = 0; a < nn; a++) {
+                        int64_t k = ien_e[a] - 1;
+                        for (int c = 0; c < 3; c++)
+                            grad[c + 3 * k] = grad[c + 3 * k] + tp[1 + 3 * a + c];
+                    }
+                }
+            }
+            free(terms);
         }
         jelem += nb_elem_patch[ip];
         for (int d = 0; d < 3; d++) ukv_off += nkv[3 * ip + d];

@@ -34,6 +34,7 @@ typedef struct {
     int64_t ncp, nqp;
     csr_t BT[3][2];   /* B0^T, B1^T: (nqp_d x nfun_d) */
     csr_t W[3][4];    /* W00 W01 W10 W11: (nfun_d x nqp_d) */
+    csr_t WB[3][4];   /* W_t (.) B_(t & 1), elementwise (nfun_d x nqp_d): diagonal */
     double *coef;     /* nqp * 45: upper triangle of S */
     unsigned char *mask;   /* 3*ncp: 1 free, 0 clamped */
 } wq_t;
@@ -123,6 +124,15 @@ void *oracle_wq_create(const int *n, const int *q, const double *const *rules,
         csr_from_dense(&op->BT[d][0], R[0], n[d], q[d], 1);
         csr_from_dense(&op->BT[d][1], R[1], n[d], q[d], 1);
         for (int t = 0; t < 4; t++) csr_from_dense(&op->W[d][t], R[2 + t], n[d], q[d], 0);
+        /* find_physical_diag_3d (tensor_algebra.f90:1484-1596) contracts the
+         * coefficient with the products (W (.) B) of each direction */
+        double *wb = (double *)malloc(sizeof(double) * (size_t)n[d] * q[d]);
+        for (int t = 0; t < 4; t++) {
+            const double *B = R[t & 1];
+            for (size_t k = 0; k < (size_t)n[d] * q[d]; k++) wb[k] = R[2 + t][k] * B[k];
+            csr_from_dense(&op->WB[d][t], wb, n[d], q[d], 0);
+        }
+        free(wb);
     }
     op->ncp = (int64_t)n[0] * n[1] * n[2];
     op->nqp = (int64_t)q[0] * q[1] * q[2];
@@ -203,7 +213,10 @@ void oracle_wq_free(void *h)
     for (int d = 0; d < 3; d++) {
         csr_free(&op->BT[d][0]);
         csr_free(&op->BT[d][1]);
-        for (int t = 0; t < 4; t++) csr_free(&op->W[d][t]);
+        for (int t = 0; t < 4; t++) {
+            csr_free(&op->W[d][t]);
+            csr_free(&op->WB[d][t]);
+        }
     }
     free(op->coef);
     free(op->mask);
@@ -285,4 +298,84 @@ double oracle_cg_vector_seconds(int64_t n, int reps)
     double t = (omp_get_wtime() - t0) / reps;
     free(x); free(r); free(p); free(Ap); free(z); free(di);
     return acc > -1.0 ? t : -t;
+}
+
+/* Diagonal of K (3*ncp; clamped dofs 1): for component c, the sum over the
+ * 9 (test, trial) derivative pairs (k, l) of the rank-one products of
+ * W_(k,l) (.) B_l in the three directions with the coefficient
+ * S[(c,k),(c,l)] -- find_physical_diag_3d (tensor_algebra.f90:1484-1596)
+ * per diagonal block, as wq_find_conductivity_diagonal_3d
+ * (mf_wq_solver.f90:6-164) calls it. */
+int oracle_wq_diag(void *h, double *d)
+{
+    wq_t *op = (wq_t *)h;
+    const int64_t NC = op->ncp, NQ = op->nqp;
+    double *cf = (double *)malloc(sizeof(double) * NQ);
+    double *out = (double *)malloc(sizeof(double) * NC);
+    for (int c = 0; c < 3; c++) {
+        memset(out, 0, sizeof(double) * NC);
+        for (int k = 0; k < 3; k++)
+            for (int l = 0; l < 3; l++) {
+                const int e = sym9(3 * c + k, 3 * c + l);
+                #pragma omp parallel for schedule(static)
+                for (int64_t qq = 0; qq < NQ; qq++) cf[qq] = op->coef[45 * qq + e];
+                sparsedot3(&op->WB[0][2 * (k == 0) + (l == 0)], &op->WB[1][2 * (k == 1) + (l == 1)],
+                           &op->WB[2][2 * (k == 2) + (l == 2)], cf, out);
+            }
+        for (int64_t a = 0; a < NC; a++) d[c * NC + a] = op->mask[c * NC + a] ? out[a] : 1.0;
+    }
+    free(cf);
+    free(out);
+    return 0;
+}
+
+/* `iters` consecutive iterations of the Jacobi-preconditioned CG of
+ * wq_mf_cg_3d (mf_wq_solver.f90:764-802: apply, alpha = r.z / p.Ap, x and r
+ * updates, z = r / diag, beta, p update) from x = 0, on the host cores, the
+ * whole loop timed as one.  Returns seconds per iteration; x (3*ncp) holds
+ * the iterate and *relres ||r||_2 / ||b||_2 on return. */
+double oracle_wq_pcg_seconds(void *h, const double *b, const double *diag, int iters, double *x,
+                             double *relres)
+{
+    wq_t *op = (wq_t *)h;
+    const int64_t n = 3 * op->ncp;
+    double *r = (double *)malloc(sizeof(double) * n), *z = (double *)malloc(sizeof(double) * n),
+           *p = (double *)malloc(sizeof(double) * n), *Ap = (double *)malloc(sizeof(double) * n);
+    double rz = 0.0, bb = 0.0;
+    #pragma omp parallel for reduction(+ : rz, bb)
+    for (int64_t i = 0; i < n; i++) {
+        x[i] = 0.0;
+        r[i] = op->mask[i] ? b[i] : 0.0;
+        z[i] = r[i] / diag[i];
+        p[i] = z[i];
+        rz += r[i] * z[i];
+        bb += r[i] * r[i];
+    }
+    double rr = bb;
+    const double t0 = omp_get_wtime();
+    for (int k = 0; k < iters; k++) {
+        oracle_wq_apply(h, p, Ap);
+        double pAp = 0.0;
+        #pragma omp parallel for reduction(+ : pAp)
+        for (int64_t i = 0; i < n; i++) pAp += p[i] * Ap[i];
+        const double alpha = rz / pAp;
+        double rzn = 0.0;
+        rr = 0.0;
+        #pragma omp parallel for reduction(+ : rzn, rr)
+        for (int64_t i = 0; i < n; i++) {
+            x[i] += alpha * p[i];
+            r[i] -= alpha * Ap[i];
+            z[i] = r[i] / diag[i];
+            rzn += r[i] * z[i];
+            rr += r[i] * r[i];
+        }
+        const double beta = rzn / rz;
+        rz = rzn;
+        #pragma omp parallel for
+        for (int64_t i = 0; i < n; i++) p[i] = z[i] + beta * p[i];
+    }
+    const double t = (omp_get_wtime() - t0) / (iters > 0 ? iters : 1);
+    *relres = sqrt(rr / bb);
+    free(r); free(z); free(p); free(Ap);
+    return t;
 }

@@ -23,6 +23,9 @@ class ReferenceWQ:
                                        ctypes.c_double, vp]
         L.oracle_wq_apply.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
         L.oracle_wq_free.argtypes = [ctypes.c_void_p]
+        L.oracle_wq_diag.argtypes = [vp, vp]
+        L.oracle_wq_pcg_seconds.restype = ctypes.c_double
+        L.oracle_wq_pcg_seconds.argtypes = [vp, vp, vp, ctypes.c_int, vp, vp]
         L.oracle_cg_vector_seconds.restype = ctypes.c_double
         L.oracle_cg_vector_seconds.argtypes = [ctypes.c_int64, ctypes.c_int]
         p, nel = patch["p"], patch["nel"]
@@ -55,6 +58,25 @@ class ReferenceWQ:
         self.L.oracle_wq_apply(self.h, u.ctypes.data, out.ctypes.data)
         return out
 
+    def diag(self):
+        """Diagonal of K (find_physical_diag_3d per diagonal block); clamped
+        dofs hold 1."""
+        d = np.empty(self.ndof)
+        self.L.oracle_wq_diag(self.h, d.ctypes.data)
+        return d
+
+    def pcg_seconds(self, b, diag, iters):
+        """`iters` consecutive Jacobi-PCG iterations from x = 0 (the loop of
+        wq_mf_cg_3d, mf_wq_solver.f90:764-802, with z = r / diag), timed as
+        one loop: (seconds per iteration, x, ||r|| / ||b||)."""
+        bb = np.ascontiguousarray(b, dtype=np.float64)
+        dd = np.ascontiguousarray(diag, dtype=np.float64)
+        x = np.empty_like(bb)
+        rel = ctypes.c_double(0.0)
+        t = self.L.oracle_wq_pcg_seconds(self.h, bb.ctypes.data, dd.ctypes.data, int(iters),
+                                         x.ctypes.data, ctypes.byref(rel))
+        return t, x, rel.value
+
     def close(self):
         if self.h:
             self.L.oracle_wq_free(self.h)
@@ -83,5 +105,26 @@ def time_reference_apply(patch, E, nu, clamp_faces, n_applies=1):
     res = {"seconds_per_apply": t_apply, "seconds_per_vector_ops": t_vec,
            "setup_s": setup, "nfree": op.nfree, "ndof": op.ndof,
            "threads": int(L.oracle_wq_threads())}
+    op.close()
+    return res
+
+
+def time_reference_cg(patch, E, nu, clamp_faces, iters=10, seed=0):
+    """Seconds per Jacobi-PCG iteration of the reference's algorithm on the
+    host cores: `iters` consecutive iterations (apply + vector work) timed as
+    one loop, on a seeded right-hand side."""
+    L = lib()
+    L.oracle_wq_threads.restype = ctypes.c_int
+    t0 = time.perf_counter()
+    op = ReferenceWQ(patch, E, nu, clamp_faces)
+    setup = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    d = op.diag()
+    t_diag = time.perf_counter() - t0
+    b = np.random.default_rng(seed).standard_normal(op.ndof) * op.mask
+    t_it, _, rel = op.pcg_seconds(b, d, iters)
+    res = {"seconds_per_iteration": t_it, "iterations_timed": int(iters),
+           "rel_residual_after": rel, "setup_s": setup, "diag_s": t_diag,
+           "nfree": op.nfree, "ndof": op.ndof, "threads": int(L.oracle_wq_threads())}
     op.close()
     return res

@@ -579,55 +579,83 @@ int oracle_sys_linmat_lindef_static(
         pt.nnode = (pt.p[0] + 1) * (pt.p[1] + 1) * (pt.p[2] + 1);
         if (pt.nnode != nnode[ip] || pt.nnode > MAXNN) return -3;
         const int nn = pt.nnode;
-        double *amatrx = (double *)malloc(sizeof(double) * 9 * (size_t)nn * (nn + 1) / 2);
-        double *rhs = (double *)malloc(sizeof(double) * 3 * nn);
-        elem_t el;
-        for (int64_t ie = 0; ie < nb_elem_patch[ip]; ie++, jelem++) {
-            const int64_t *ien_e = ien + ien_off + ie * nn;
-            if (active[jelem] != 1) continue;
-            for (int a = 0; a < nn; a++)
-                for (int d = 0; d < 3; d++)
-                    el.coords[3 * a + d] = coords[3 * (ien_e[a] - 1) + d];
-            el.w = weight + w_off + ie * nn;
-            for (int d = 0; d < 3; d++) {
-                el.ni[d] = (int)nijk[3 * jelem + d];
-                el.u1[d] = pt.U[d][el.ni[d] - 1];
-                el.u2[d] = pt.U[d][el.ni[d]];
-            }
-            if (uelmat_u1(&pt, &el, (int)nbint[ip], matprops[2 * ip],
-                          matprops[2 * ip + 1], rho[ip], jelem + 1, &ld, ien_e,
-                          rhs, amatrx)) {
-                err = -4;
-                break;
-            }
-            int i = 0;
-            for (int cpj = 0; cpj < nn; cpj++) {
-                int64_t dofj = (ien_e[cpj] - 1) * 3;
-                for (int cpi = 0; cpi < cpj; cpi++, i++) {
-                    int64_t dofi = (ien_e[cpi] - 1) * 3;
-                    for (int ll = 0; ll < 3; ll++)
-                        for (int k2 = 0; k2 < 3; k2++, count++) {
-                            kdata[count] = amatrx[9 * i + k2 + 3 * ll];
-                            krow[count] = (int32_t)(dofi + k2);
-                            kcol[count] = (int32_t)(dofj + ll);
-                        }
+        /* OpenMP over the elements, as sys_linmat_lindef_static_omp
+         * (build_system_elemStorage_OMP.f90:190-278): every active element
+         * owns a fixed run of COO slots; its load vector is kept and added
+         * to F after the loop, in element order, so that F has the same bits
+         * as the sequential sum */
+        const int64_t nep = nb_elem_patch[ip], j0 = jelem;
+        const int64_t ndat = 9 * (int64_t)nn * (nn - 1) / 2 + 6 * (int64_t)nn;
+        int64_t *slot = (int64_t *)malloc(sizeof(int64_t) * (nep + 1));
+        double *rhs_all = (double *)calloc((size_t)nep * 3 * nn, sizeof(double));
+        for (int64_t ie = 0; ie < nep; ie++) {
+            slot[ie] = count;
+            if (active[j0 + ie] == 1) count += ndat;
+        }
+        if (count > nb_data) { free(slot); free(rhs_all); return -5; }
+#pragma omp parallel
+        {
+            double *amatrx = (double *)malloc(sizeof(double) * 9 * (size_t)nn * (nn + 1) / 2);
+            elem_t el;
+#pragma omp for schedule(dynamic, 4)
+            for (int64_t ie = 0; ie < nep; ie++) {
+                const int64_t je = j0 + ie;
+                const int64_t *ien_e = ien + ien_off + ie * nn;
+                if (active[je] != 1) continue;
+                double *rhs = rhs_all + (size_t)ie * 3 * nn;
+                for (int a = 0; a < nn; a++)
+                    for (int d = 0; d < 3; d++)
+                        el.coords[3 * a + d] = coords[3 * (ien_e[a] - 1) + d];
+                el.w = weight + w_off + ie * nn;
+                for (int d = 0; d < 3; d++) {
+                    el.ni[d] = (int)nijk[3 * je + d];
+                    el.u1[d] = pt.U[d][el.ni[d] - 1];
+                    el.u2[d] = pt.U[d][el.ni[d]];
                 }
-                for (int ll = 0; ll < 3; ll++) {
-                    amatrx[9 * i + ll + 3 * ll] = amatrx[9 * i + ll + 3 * ll] * 0.5;
-                    for (int k2 = 0; k2 <= ll; k2++, count++) {
-                        kdata[count] = amatrx[9 * i + k2 + 3 * ll];
-                        krow[count] = (int32_t)(dofj + k2);
-                        kcol[count] = (int32_t)(dofj + ll);
+                if (uelmat_u1(&pt, &el, (int)nbint[ip], matprops[2 * ip],
+                              matprops[2 * ip + 1], rho[ip], je + 1, &ld, ien_e,
+                              rhs, amatrx)) {
+#pragma omp atomic write
+                    err = -4;
+                    continue;
+                }
+                int64_t at = slot[ie];
+                int i = 0;
+                for (int cpj = 0; cpj < nn; cpj++) {
+                    int64_t dofj = (ien_e[cpj] - 1) * 3;
+                    for (int cpi = 0; cpi < cpj; cpi++, i++) {
+                        int64_t dofi = (ien_e[cpi] - 1) * 3;
+                        for (int ll = 0; ll < 3; ll++)
+                            for (int k2 = 0; k2 < 3; k2++, at++) {
+                                kdata[at] = amatrx[9 * i + k2 + 3 * ll];
+                                krow[at] = (int32_t)(dofi + k2);
+                                kcol[at] = (int32_t)(dofj + ll);
+                            }
                     }
+                    for (int ll = 0; ll < 3; ll++) {
+                        amatrx[9 * i + ll + 3 * ll] = amatrx[9 * i + ll + 3 * ll] * 0.5;
+                        for (int k2 = 0; k2 <= ll; k2++, at++) {
+                            kdata[at] = amatrx[9 * i + k2 + 3 * ll];
+                            krow[at] = (int32_t)(dofj + k2);
+                            kcol[at] = (int32_t)(dofj + ll);
+                        }
+                    }
+                    i++;
                 }
-                i++;
             }
+            free(amatrx);
+        }
+        for (int64_t ie = 0; ie < nep; ie++) {
+            if (active[j0 + ie] != 1) continue;
+            const int64_t *ien_e = ien + ien_off + ie * nn;
+            const double *rhs = rhs_all + (size_t)ie * 3 * nn;
             for (int a = 0; a < nn; a++)
                 for (int d = 0; d < 3; d++)
                     F[(ien_e[a] - 1) * 3 + d] = F[(ien_e[a] - 1) * 3 + d] + rhs[3 * a + d];
         }
-        free(amatrx);
-        free(rhs);
+        jelem += nep;
+        free(slot);
+        free(rhs_all);
         for (int d = 0; d < 3; d++) ukv_off += pt.nkv[d];
         ien_off += nb_elem_patch[ip] * nn;
         w_off += nb_elem_patch[ip] * nn;
@@ -674,55 +702,76 @@ int oracle_build_cmassmatrix(
         while (ng * ng * ng < nbi) ng++;
         double *gp = (double *)malloc(sizeof(double) * 4 * ng * ng * ng);
         gauss_volume(ng, gp);
-        double *cm = (double *)malloc(sizeof(double) * (size_t)nn * (nn + 1) / 2);
-        double *R = (double *)malloc(sizeof(double) * nn);
-        double *dRdx = (double *)malloc(sizeof(double) * 3 * nn);
-        elem_t el;
-        for (int64_t ie = 0; ie < nb_elem_patch[ip]; ie++, jelem++) {
-            const int64_t *ien_e = ien + ien_off + ie * nn;
-            if (active[jelem] != 1) continue;
-            for (int a = 0; a < nn; a++)
-                for (int d = 0; d < 3; d++)
-                    el.coords[3 * a + d] = coords[3 * (ien_e[a] - 1) + d];
-            el.w = weight + w_off + ie * nn;
-            for (int d = 0; d < 3; d++) {
-                el.ni[d] = (int)nijk[3 * jelem + d];
-                el.u1[d] = pt.U[d][el.ni[d] - 1];
-                el.u2[d] = pt.U[d][el.ni[d]];
-            }
-            memset(cm, 0, sizeof(double) * (size_t)nn * (nn + 1) / 2);
-            for (int q = 0; q < nbi; q++) {
-                double detj = shap(&pt, &el, gp + 4 * q + 1, R, dRdx);
-                double dvol = gp[4 * q] * detj;
-                dvol = rho[ip] * dvol;
-                int c = 0;
-                for (int j = 0; j < nn; j++) {
-                    double t1 = dvol * R[j];
-                    for (int i = 0; i <= j; i++, c++) cm[c] = cm[c] + t1 * R[i];
-                }
-            }
-            int i = 0;
-            for (int cpj = 0; cpj < nn; cpj++) {
-                int64_t dofj = (ien_e[cpj] - 1) * 3;
-                for (int cpi = 0; cpi < cpj; cpi++, i++) {
-                    int64_t dofi = (ien_e[cpi] - 1) * 3;
-                    for (int ll = 0; ll < 3; ll++)
-                        for (int k2 = 0; k2 < 3; k2++, count++) {
-                            mdata[count] = k2 == ll ? cm[i] : 0.0;
-                            mrow[count] = (int32_t)(dofi + k2);
-                            mcol[count] = (int32_t)(dofj + ll);
-                        }
-                }
-                for (int ll = 0; ll < 3; ll++)
-                    for (int k2 = 0; k2 <= ll; k2++, count++) {
-                        mdata[count] = k2 == ll ? cm[i] * 0.5 : 0.0;
-                        mrow[count] = (int32_t)(dofj + k2);
-                        mcol[count] = (int32_t)(dofj + ll);
-                    }
-                i++;
-            }
+        /* OpenMP over the elements (the element loop of
+         * build_system_elemStorage_OMP.f90:190-278); each active element
+         * owns a fixed run of COO slots, so the result does not depend on
+         * the thread count */
+        const int64_t nep = nb_elem_patch[ip], j0 = jelem;
+        const int64_t ndat = 9 * (int64_t)nn * (nn - 1) / 2 + 6 * (int64_t)nn;
+        int64_t *slot = (int64_t *)malloc(sizeof(int64_t) * (nep + 1));
+        for (int64_t ie = 0; ie < nep; ie++) {
+            slot[ie] = count;
+            if (active[j0 + ie] == 1) count += ndat;
         }
-        free(gp); free(cm); free(R); free(dRdx);
+        if (count > nb_data) { free(slot); free(gp); return -5; }
+#pragma omp parallel
+        {
+            double *cm = (double *)malloc(sizeof(double) * (size_t)nn * (nn + 1) / 2);
+            double *R = (double *)malloc(sizeof(double) * nn);
+            double *dRdx = (double *)malloc(sizeof(double) * 3 * nn);
+            elem_t el;
+#pragma omp for schedule(dynamic, 4)
+            for (int64_t ie = 0; ie < nep; ie++) {
+                const int64_t je = j0 + ie;
+                const int64_t *ien_e = ien + ien_off + ie * nn;
+                if (active[je] != 1) continue;
+                for (int a = 0; a < nn; a++)
+                    for (int d = 0; d < 3; d++)
+                        el.coords[3 * a + d] = coords[3 * (ien_e[a] - 1) + d];
+                el.w = weight + w_off + ie * nn;
+                for (int d = 0; d < 3; d++) {
+                    el.ni[d] = (int)nijk[3 * je + d];
+                    el.u1[d] = pt.U[d][el.ni[d] - 1];
+                    el.u2[d] = pt.U[d][el.ni[d]];
+                }
+                memset(cm, 0, sizeof(double) * (size_t)nn * (nn + 1) / 2);
+                for (int q = 0; q < nbi; q++) {
+                    double detj = shap(&pt, &el, gp + 4 * q + 1, R, dRdx);
+                    double dvol = gp[4 * q] * detj;
+                    dvol = rho[ip] * dvol;
+                    int c = 0;
+                    for (int j = 0; j < nn; j++) {
+                        double t1 = dvol * R[j];
+                        for (int i = 0; i <= j; i++, c++) cm[c] = cm[c] + t1 * R[i];
+                    }
+                }
+                int64_t at = slot[ie];
+                int i = 0;
+                for (int cpj = 0; cpj < nn; cpj++) {
+                    int64_t dofj = (ien_e[cpj] - 1) * 3;
+                    for (int cpi = 0; cpi < cpj; cpi++, i++) {
+                        int64_t dofi = (ien_e[cpi] - 1) * 3;
+                        for (int ll = 0; ll < 3; ll++)
+                            for (int k2 = 0; k2 < 3; k2++, at++) {
+                                mdata[at] = k2 == ll ? cm[i] : 0.0;
+                                mrow[at] = (int32_t)(dofi + k2);
+                                mcol[at] = (int32_t)(dofj + ll);
+                            }
+                    }
+                    for (int ll = 0; ll < 3; ll++)
+                        for (int k2 = 0; k2 <= ll; k2++, at++) {
+                            mdata[at] = k2 == ll ? cm[i] * 0.5 : 0.0;
+                            mrow[at] = (int32_t)(dofj + k2);
+                            mcol[at] = (int32_t)(dofj + ll);
+                        }
+                    i++;
+                }
+            }
+            free(cm); free(R); free(dRdx);
+        }
+        jelem += nep;
+        free(slot);
+        free(gp);
         for (int d = 0; d < 3; d++) ukv_off += pt.nkv[d];
         ien_off += nb_elem_patch[ip] * nn;
         w_off += nb_elem_patch[ip] * nn;

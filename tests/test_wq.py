@@ -156,6 +156,27 @@ def test_reference_algorithm_cpu_matches_oracle(case):
     assert _rel(b.apply(u), a.apply(u)) < 1e-13
 
 
+@pytest.mark.parametrize("case", CASES[1:4])
+def test_reference_algorithm_cpu_diagonal_and_cg_loop(case):
+    """The timed CPU baseline's diagonal (find_physical_diag_3d per diagonal
+    block) and its Jacobi-PCG loop (wq_mf_cg_3d's iteration with z = r/diag)
+    reproduce the numpy oracle's diagonal and its PCG iterate after the same
+    number of iterations."""
+    from oracle.wq_cpu import ReferenceWQ
+    nel, p, pert, wr, clamp = case
+    P = cube_patch(nel, p, perturb=pert, wrange=wr, seed=5)
+    a = WQOracle(P, 1.0, 0.3, clamp)
+    b = ReferenceWQ(P, 1.0, 0.3, clamp)
+    d = b.diag()
+    assert _rel(d, a.diag()) < 1e-13
+    rhs = a.body_force([0.0, 0.0, -1.0])
+    t, x, rel = b.pcg_seconds(rhs, d, 7)
+    x0, it, _ = a.pcg(rhs, rtol=1e-300, maxit=7)
+    assert it == 7 and t > 0
+    assert _rel(x, x0) < 1e-10
+    assert np.isfinite(rel) and rel > 0
+
+
 def test_reference_algorithm_cpu_declares_pointers():
     """Large arrays can live at addresses beyond 32 bits (the bench's CPU
     baseline runs the C port on the 64^3 workload): every pointer argument of
@@ -166,8 +187,9 @@ def test_reference_algorithm_cpu_declares_pointers():
     P = cube_patch((22, 20, 16), 2, perturb=0.1, wrange=(0.9, 1.1), seed=6)
     a = WQOracle(P, 1.0, 0.3, {"w0": (0, 1, 2)})
     b = ReferenceWQ(P, 1.0, 0.3, {"w0": (0, 1, 2)})
-    for f in (b.L.oracle_wq_create, b.L.oracle_wq_apply, b.L.oracle_wq_free):
+    for f in (b.L.oracle_wq_create, b.L.oracle_wq_apply, b.L.oracle_wq_free,
+              b.L.oracle_wq_diag, b.L.oracle_wq_pcg_seconds):
         assert f.argtypes is not None
-        assert all(t in (ctypes.c_void_p, ctypes.c_double) for t in f.argtypes)
+        assert all(t in (ctypes.c_void_p, ctypes.c_double, ctypes.c_int) for t in f.argtypes)
     u = np.random.default_rng(2).standard_normal(a.ndof)
     assert _rel(b.apply(u), a.apply(u)) < 1e-13
