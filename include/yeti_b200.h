@@ -227,6 +227,17 @@ int yeti_wq_body_force(yeti_wq_op *op, const double f[3], double *F, int mem);
  * true residual satisfies ||r||_2 <= rtol ||b||_2. */
 int yeti_wq_pcg(yeti_wq_op *op, const double *b, double *x, double rtol,
                 int maxit, int mode, yeti_cg_stats *stats, int mem);
+/* As yeti_wq_pcg, FP64 modes only, with the reference's iteration history
+ * (the RelRes / RelError outputs of wq_mf_cg_3d and wq_mf_bicgstab_3d,
+ * mf_wq_solver.f90:656,697,785-792): relres[k] = max|r_k| / max|b| and, when
+ * directsol is given, relerr[k] = max|directsol - x_k| / max|directsol|, for
+ * k = 0..iterations (host arrays of maxit + 1 doubles; relerr may be NULL).
+ * Stops on the reference's test relres[k] <= rtol (mf_wq_solver.f90:931-936)
+ * instead of the 2-norm one. */
+int yeti_wq_pcg_history(yeti_wq_op *op, const double *b, double *x, double rtol,
+                        int maxit, int mode, const double *directsol,
+                        double *relres, double *relerr, yeti_cg_stats *stats,
+                        int mem);
 /* z = P^{-1} r for the fast-diagonalisation preconditioner selected by the
  * YETI_PCG_FD* bits of `variant` (fast_diagonalization_3d,
  * tensor_algebra.f90:1107-1161, per displacement component, with

@@ -115,6 +115,8 @@ def _declare(lib):
         "yeti_wq_body_force": (i32, [vp, vp, vp, i32]),
         "yeti_wq_pcg": (i32, [vp, vp, vp, dbl, i32, i32,
                               ctypes.POINTER(CGStats), i32]),
+        "yeti_wq_pcg_history": (i32, [vp, vp, vp, dbl, i32, i32, vp, vp, vp,
+                                      ctypes.POINTER(CGStats), i32]),
         "yeti_wq_fd_apply": (i32, [vp, vp, vp, i32, i32, i32]),
         "yeti_grad_lin_elast_work": (i32, [vp, ctypes.POINTER(U1Model), vp,
                                            vp, i64, i32, i32, i32, vp, vp,

@@ -208,6 +208,45 @@ __global__ void k_pause(CGScal *s) {
     }
 }
 
+// The reference's per-iteration measures (wq_mf_cg_3d, mf_wq_solver.f90:
+// 785-792): after iteration g, max|r| and (ds given) max|ds - x| into
+// hist[2g], hist[2g+1]; recorded only if iteration g ran (s->iter == g).  The
+// last block also applies the reference's stop test max|r| <= stop_abs
+// (mf_wq_solver.f90:931-936), stop_abs = eps max|b|.
+template <class S>
+__global__ void __launch_bounds__(kRedThreads)
+k_hist(const double *r, const double *x, const double *ds, int64_t n, double *parts,
+       unsigned int *ticket, double *hist, int g, double stop_abs, S *s) {
+    __shared__ double sh[32];
+    if (s->iter != g) return;
+    double mr = 0.0, me = 0.0;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        mr = fmax(mr, fabs(r[i]));
+        if (ds) me = fmax(me, fabs(ds[i] - x[i]));
+    }
+    mr = block_max(mr, sh);
+    me = block_max(me, sh);
+    if (threadIdx.x == 0) {
+        __stcg(&parts[2 * blockIdx.x], mr);
+        __stcg(&parts[2 * blockIdx.x + 1], me);
+    }
+    if (!last_block(ticket)) return;
+    double tr = 0.0, te = 0.0;
+    for (int i = threadIdx.x; i < (int)gridDim.x; i += blockDim.x) {
+        tr = fmax(tr, __ldcg(&parts[2 * i]));
+        te = fmax(te, __ldcg(&parts[2 * i + 1]));
+    }
+    tr = block_max(tr, sh);
+    te = block_max(te, sh);
+    if (threadIdx.x == 0) {
+        *ticket = 0;
+        hist[2 * g] = tr;
+        hist[2 * g + 1] = te;
+        if (tr <= stop_abs) s->done = 1;
+    }
+}
+
 // p = z + beta p; Ap = 0
 template <class T>
 __global__ void __launch_bounds__(kRedThreads)
@@ -1016,9 +1055,12 @@ static int host_sum(yeti_wq_op *op, const double *parts, int n, int stride,
 
 using namespace yeti;
 
-YETI_API int yeti_wq_pcg(yeti_wq_op *op, const double *b, double *x,
-                         double rtol, int maxit, int mode,
-                         yeti_cg_stats *stats, int mem) {
+// History mode (relres != nullptr): FP64 only; every iteration records the
+// reference's RelRes / RelError measures and the solve stops on its
+// inf-norm test max|r| <= rtol max|b| instead of the 2-norm one.
+static int pcg_run(yeti_wq_op *op, const double *b, double *x, double rtol, int maxit,
+                   int mode, yeti_cg_stats *stats, int mem, const double *dsol,
+                   double *relres, double *relerr) {
     YETI_CHECK(op && b && x, YETI_EINVAL, "yeti_wq_pcg: NULL argument");
     YETI_CHECK(mode >= 0 && mode < 32 &&
                    ((mode & (YETI_PCG_FD_SCALED | YETI_PCG_FD_UNIT)) == 0 || (mode & YETI_PCG_FD)),
@@ -1030,11 +1072,32 @@ YETI_API int yeti_wq_pcg(yeti_wq_op *op, const double *b, double *x,
     const bool fd = (mode & YETI_PCG_FD) != 0;
     YETI_CHECK(!mixed || op->coef32.ptr, YETI_EINVAL,
                "yeti_wq_pcg: mixed precision needs the FP32 operator (YETI_WQ_F32)");
+    const bool hist = relres != nullptr;
+    YETI_CHECK(!hist || !mixed, YETI_EINVAL,
+               "yeti_wq_pcg_history: the iteration history is recorded in FP64 only");
     DeviceGuard guard(op->ctx->device);
     YETI_TRY(ensure_workspace(op, mixed));
     if (fd) YETI_TRY(wq_fd_prepare(op, mode, mixed));
     cudaStream_t s = op->ctx->stream;
     const int64_t n = op->ndof;
+    // history: 2 (maxit + 1) maxima, the reduction ticket, the direct solution
+    DevBuf hbuf, dsbuf;
+    double *dhist = nullptr, *dds = nullptr;
+    unsigned int *hticket = nullptr;
+    if (hist) {
+        const size_t hbytes = (size_t)2 * (maxit + 1) * sizeof(double);
+        YETI_TRY(hbuf.alloc(op->ctx, hbytes + 256));
+        YETI_CUDA(cudaMemsetAsync(hbuf.ptr, 0, hbytes + 256, s));
+        dhist = hbuf.as<double>();
+        hticket = reinterpret_cast<unsigned int *>(hbuf.as<char>() + hbytes);
+        if (dsol) {
+            YETI_TRY(dsbuf.alloc(op->ctx, n * sizeof(double)));
+            YETI_CUDA(cudaMemcpyAsync(dsbuf.ptr, dsol, n * sizeof(double),
+                                      mem == YETI_MEM_HOST ? cudaMemcpyHostToDevice
+                                                           : cudaMemcpyDeviceToDevice, s));
+            dds = dsbuf.as<double>();
+        }
+    }
     double *W = op->ws64.as<double>();
     double *dx = W, *dr = W + n, *dz = W + 2 * n, *dp = W + 3 * n, *dAp = W + 4 * n,
            *db = W + 5 * n, *dt = W + 6 * n, *drh = W + 7 * n, *dph = W + 8 * n,
@@ -1076,7 +1139,91 @@ YETI_API int yeti_wq_pcg(yeti_wq_op *op, const double *b, double *x,
     YETI_CUDA(cudaGetLastError());
     int iters = 0, outer = 0, f64 = 1, f32 = 0, status = YETI_OK;
     const double tol2 = rtol * rtol * bb;
-    if (!mixed && !bicg) {
+    double bmax_h = 0.0, dsmax_h = 0.0, stop_abs = 0.0;
+    if (hist) {
+        k_absmax<double><<<kRedBlocks, kRedThreads, 0, s>>>(db, n, parts);
+        count_launches(1);
+        YETI_TRY(host_sum(op, parts, kRedBlocks, 1, 0, &bmax_h, true));
+        if (dds) {
+            k_absmax<double><<<kRedBlocks, kRedThreads, 0, s>>>(dds, n, parts);
+            count_launches(1);
+            YETI_TRY(host_sum(op, parts, kRedBlocks, 1, 0, &dsmax_h, true));
+        }
+        stop_abs = rtol * bmax_h;
+    }
+    if (!mixed && !bicg && hist) {
+        // the reference's CG loop with its per-iteration measures: one
+        // launch sequence per iteration (apply, alpha, updates, history with
+        // the inf-norm stop test, preconditioner, direction)
+        CGScal init;
+        memset(&init, 0, sizeof(init));
+        init.bb = bb;
+        YETI_CUDA(cudaMemcpyAsync(ds, &init, sizeof(CGScal), cudaMemcpyHostToDevice, s));
+        k_start<double><<<kRedBlocks, kRedThreads, 0, s>>>(dr, pre, dz, dp, dAp, n, parts);
+        k_start_scal<<<1, kRedThreads, 0, s>>>(parts, kRedBlocks, ds, 0.0, maxit);
+        k_hist<CGScal><<<kRedBlocks, kRedThreads, 0, s>>>(dr, dx, dds, n, parts, hticket, dhist, 0,
+                                                         stop_abs, ds);
+        count_launches(3);
+        if (fd) YETI_TRY(wq_fd_apply<double>(op, dr, dz, &ds->done, FD_START, dp, ds, s));
+        YETI_CUDA(cudaGetLastError());
+        for (int g0 = 0;; g0 += kChunk) {
+            for (int k = 0; k < kChunk; k++) {
+                YETI_TRY(wq_apply_dev(op, dp, dAp, YETI_PREC_F64, &ds->done, s));
+                k_dot_alpha<double><<<kRedBlocks, kRedThreads, 0, s>>>(dp, dAp, n, parts, ds);
+                k_update_beta<double><<<kRedBlocks, kRedThreads, 0, s>>>(dx, dr, dp, dAp, pre, dz, n,
+                                                                         parts, ds);
+                k_hist<CGScal><<<kRedBlocks, kRedThreads, 0, s>>>(dr, dx, dds, n, parts, hticket,
+                                                                 dhist, g0 + k + 1, stop_abs, ds);
+                if (fd) YETI_TRY(wq_fd_apply<double>(op, dr, dz, &ds->done, FD_ITER, nullptr, ds, s));
+                k_pupdate<double><<<kRedBlocks, kRedThreads, 0, s>>>(dp, dz, dAp, n, ds);
+                count_launches(4);
+            }
+            YETI_CUDA(cudaGetLastError());
+            YETI_CUDA(cudaMemcpyAsync(&hs, ds, sizeof(CGScal), cudaMemcpyDeviceToHost, s));
+            YETI_CUDA(cudaStreamSynchronize(s));
+            if (hs.done) break;
+        }
+        iters = hs.iter;
+        f64 += hs.iter;
+        if (hs.breakdown) status = YETI_EBREAKDOWN;
+        outer = 1;
+    } else if (!mixed && bicg && hist) {
+        k_bi_start<double><<<kRedBlocks, kRedThreads, 0, s>>>(dr, drh, dp, dph, dAp, pre, n, parts);
+        k_bi_start_scal<<<1, kRedThreads, 0, s>>>(parts, kRedBlocks, bs, 0.0, maxit);
+        k_hist<BiScal><<<kRedBlocks, kRedThreads, 0, s>>>(dr, dx, dds, n, parts, hticket, dhist, 0,
+                                                         stop_abs, bs);
+        count_launches(3);
+        if (fd) YETI_TRY(wq_fd_apply<double>(op, dr, dph, &bs->done, FD_NONE, nullptr, nullptr, s));
+        YETI_CUDA(cudaGetLastError());
+        for (int g0 = 0;; g0 += kChunk) {
+            for (int k = 0; k < kChunk; k++) {
+                YETI_TRY(wq_apply_dev(op, dph, dAp, YETI_PREC_F64, &bs->done, s));
+                k_dot<double, double><<<kRedBlocks, kRedThreads, 0, s>>>(drh, dAp, n, parts, &bs->done);
+                k_bi_alpha_s<double><<<1, kRedThreads, 0, s>>>(parts, kRedBlocks, bs);
+                k_bi_s<double><<<kRedBlocks, kRedThreads, 0, s>>>(dr, dAp, pre, dsv, dsh, dtt, n, bs);
+                if (fd) YETI_TRY(wq_fd_apply<double>(op, dsv, dsh, &bs->done, FD_NONE, nullptr, nullptr, s));
+                YETI_TRY(wq_apply_dev(op, dsh, dtt, YETI_PREC_F64, &bs->done, s));
+                k_bi_ts<double><<<kRedBlocks, kRedThreads, 0, s>>>(dtt, dsv, n, parts, bs);
+                k_bi_omega<<<1, kRedThreads, 0, s>>>(parts, kRedBlocks, bs);
+                k_bi_update<double><<<kRedBlocks, kRedThreads, 0, s>>>(dx, dr, drh, dph, dsh, dsv, dtt, n,
+                                                                       parts, bs);
+                k_bi_beta<<<1, kRedThreads, 0, s>>>(parts, kRedBlocks, bs);
+                k_hist<BiScal><<<kRedBlocks, kRedThreads, 0, s>>>(dr, dx, dds, n, parts, hticket,
+                                                                 dhist, g0 + k + 1, stop_abs, bs);
+                k_bi_p<double><<<kRedBlocks, kRedThreads, 0, s>>>(dp, dph, dr, dAp, pre, n, bs);
+                if (fd) YETI_TRY(wq_fd_apply<double>(op, dp, dph, &bs->done, FD_NONE, nullptr, nullptr, s));
+                count_launches(9);
+            }
+            YETI_CUDA(cudaGetLastError());
+            YETI_CUDA(cudaMemcpyAsync(&hb, bs, sizeof(BiScal), cudaMemcpyDeviceToHost, s));
+            YETI_CUDA(cudaStreamSynchronize(s));
+            if (hb.done) break;
+        }
+        iters = hb.iter;
+        f64 += 2 * hb.iter;
+        if (hb.breakdown) status = YETI_EBREAKDOWN;
+        outer = 1;
+    } else if (!mixed && !bicg) {
         CGScal init;
         memset(&init, 0, sizeof(init));
         init.bb = bb;
@@ -1232,7 +1379,18 @@ YETI_API int yeti_wq_pcg(yeti_wq_op *op, const double *b, double *x,
     YETI_CUDA(cudaStreamSynchronize(s));
     YETI_TRY(wq_stream_check(op));
     const double rel = bb > 0 ? std::sqrt(rr / bb) : 0.0;
-    if (status == YETI_OK && !(rel <= rtol)) status = YETI_ENOTCONV;
+    if (hist) {
+        std::vector<double> h((size_t)2 * (iters + 1));
+        YETI_CUDA(cudaMemcpy(h.data(), dhist, h.size() * sizeof(double), cudaMemcpyDeviceToHost));
+        for (int k = 0; k <= iters; k++) {
+            relres[k] = bmax_h > 0 ? h[2 * k] / bmax_h : 0.0;
+            if (relerr) relerr[k] = dsmax_h > 0 ? h[2 * k + 1] / dsmax_h : 0.0;
+        }
+        const double rinf = bmax > 0 ? rmax / bmax : 0.0;
+        if (status == YETI_OK && !(rinf <= rtol)) status = YETI_ENOTCONV;
+    } else if (status == YETI_OK && !(rel <= rtol)) {
+        status = YETI_ENOTCONV;
+    }
     if (stats) {
         stats->iterations = iters;
         stats->outer_iterations = outer;
@@ -1248,4 +1406,16 @@ YETI_API int yeti_wq_pcg(yeti_wq_op *op, const double *b, double *x,
         return status;
     }
     return YETI_OK;
+}
+
+YETI_API int yeti_wq_pcg(yeti_wq_op *op, const double *b, double *x, double rtol, int maxit,
+                         int mode, yeti_cg_stats *stats, int mem) {
+    return pcg_run(op, b, x, rtol, maxit, mode, stats, mem, nullptr, nullptr, nullptr);
+}
+
+YETI_API int yeti_wq_pcg_history(yeti_wq_op *op, const double *b, double *x, double rtol,
+                                 int maxit, int mode, const double *directsol, double *relres,
+                                 double *relerr, yeti_cg_stats *stats, int mem) {
+    YETI_CHECK(relres, YETI_EINVAL, "yeti_wq_pcg_history: NULL relres");
+    return pcg_run(op, b, x, rtol, maxit, mode, stats, mem, directsol, relres, relerr);
 }

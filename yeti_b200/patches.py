@@ -74,3 +74,71 @@ def free_mask(patch, clamp_faces):
             if dm[6 * c + f]:
                 out[c][on[f]] = 0.0
     return out.ravel()
+
+
+def patch_from_iga_model(model, ipatch=0):
+    """The WQ description of patch ipatch (0-based: the reference's numpatch
+    minus one) of a YETI ``IGAparametrization``, as ``fortran_mf_wq``
+    builds it from ``modelIGA`` (``thermoMechaModel.__set_bspline_properties``,
+    ``create_model.py:287-354``): degrees from ``_Jpqr``, element counts
+    ``_Nkv - (2p + 1)``, knot vectors ``_Ukv`` (uniform and open, the WQ
+    rule's hypothesis), control points ``_COORDS`` and weights
+    (``_weight``, per element).
+
+    The tensor position (iu, iv, iw) of every control point is read from the
+    connectivity, not assumed: YETI's element e with knot spans ``_Nijk[:, e]``
+    (1-based) lists its nodes with the u index fastest and every 1-D index
+    descending (``shap.f90:91-119``), so node a = i + (p+1)(j + (q+1)k)
+    has tensor index (Nijk[0,e]-1-i, Nijk[1,e]-1-j, Nijk[2,e]-1-k).
+
+    Returns (patch, cp_index): the patch dict of ``cube_patch``'s form and,
+    per tensor position (u fastest), the 0-based model control point."""
+    Jpqr = np.asarray(model._Jpqr).reshape(3, -1)
+    Nkv = np.asarray(model._Nkv).reshape(3, -1)
+    p = [int(Jpqr[d, ipatch]) for d in range(3)]
+    nel = [int(Nkv[d, ipatch]) - (2 * p[d] + 1) for d in range(3)]
+    for d in range(3):
+        kv = np.asarray(model._Ukv[ipatch][d], dtype=np.float64)
+        ref = np.concatenate([np.zeros(p[d] + 1), np.arange(1, nel[d]) / nel[d],
+                              np.ones(p[d] + 1)])
+        if kv.shape != ref.shape or np.abs(kv - ref).max() > 1e-12:
+            raise ValueError(f"patch {ipatch}: knot vector {d} is not uniform and open "
+                             "(the weighted-quadrature rules assume it)")
+    n = [p[d] + nel[d] for d in range(3)]
+    ncp = n[0] * n[1] * n[2]
+    nbp = np.asarray(model._elementsByPatch).ravel()
+    e0 = int(nbp[:ipatch].sum())
+    ien = np.asarray(model._IEN[ipatch]).reshape(int(nbp[ipatch]), -1)
+    nijk = np.asarray(model._Nijk).reshape(3, -1)
+    cp_index = np.full(ncp, -1, dtype=np.int64)
+    weights = np.zeros(ncp)
+    a = np.arange(ien.shape[1])
+    li = a % (p[0] + 1)
+    lj = (a // (p[0] + 1)) % (p[1] + 1)
+    lk = a // ((p[0] + 1) * (p[1] + 1))
+    for e in range(ien.shape[0]):
+        s = nijk[:, e0 + e]
+        t = (s[0] - 1 - li) + n[0] * ((s[1] - 1 - lj) + n[1] * (s[2] - 1 - lk))
+        cp_index[t] = ien[e] - 1
+        weights[t] = np.asarray(model._weight[e0 + e], dtype=np.float64)
+    if (cp_index < 0).any() or np.unique(cp_index).size != ncp:
+        raise ValueError(f"patch {ipatch}: the connectivity does not cover a tensor grid")
+    X = np.asarray(model._COORDS, dtype=np.float64)[:3]
+    patch = {"p": tuple(p), "nel": tuple(nel),
+             "cps": np.ascontiguousarray(X[:, cp_index]),
+             "weights": np.ascontiguousarray(weights)}
+    return patch, cp_index
+
+
+def clamp_faces_from_blocked(blocked):
+    """The reference's ``mechablockedboundaries`` ([[u0, u1], [v0, v1],
+    [w0, w1]] flags, all three components blocked on a flagged face:
+    ``block_boundaries(typeEl='D')``, create_model.py:434-529) as
+    clamp_faces."""
+    names = (("u0", "u1"), ("v0", "v1"), ("w0", "w1"))
+    out = {}
+    for d in range(3):
+        for s in range(2):
+            if blocked[d][s]:
+                out[names[d][s]] = (0, 1, 2)
+    return out

@@ -70,6 +70,45 @@ class WQElasticity:
         self.ncp, self.ndof, self.nfree, self.nqp, self.bytes = (v.value for v in vals)
         self.free_mask = free_mask(patch, self.clamp_faces)
 
+    @classmethod
+    def from_iga_model(cls, modelIGA, mechablockedboundaries=None, E=None, nu=None,
+                       ipatch=0, precisions="both", ctx=None):
+        """The operator of patch ipatch (0-based) of a YETI IGAparametrization,
+        as ``fortran_mf_wq(modelIGA, isThermal=False, isMechanical=True,
+        mechablockedboundaries=...)`` builds it (fortran_mf_wq.py:31-71):
+        mechablockedboundaries = [[u0, u1], [v0, v1], [w0, w1]] face flags
+        (default all blocked, as the reference), E and nu from the patch's
+        ``_MATERIAL_PROPERTIES`` unless given.  ``cp_index`` keeps the model
+        control point of every tensor position (``to_model_layout``)."""
+        from .patches import clamp_faces_from_blocked, patch_from_iga_model
+        patch, cp_index = patch_from_iga_model(modelIGA, ipatch)
+        mat = np.asarray(modelIGA._MATERIAL_PROPERTIES, dtype=np.float64).reshape(2, -1)
+        E = float(mat[0, ipatch]) if E is None else float(E)
+        nu = float(mat[1, ipatch]) if nu is None else float(nu)
+        if mechablockedboundaries is None:
+            mechablockedboundaries = [[1, 1], [1, 1], [1, 1]]
+        op = cls(patch, E, nu, clamp_faces_from_blocked(mechablockedboundaries),
+                 precisions=precisions, ctx=ctx)
+        op.cp_index = cp_index
+        op.nb_cp_model = int(modelIGA._nb_cp)
+        return op
+
+    def to_model_layout(self, x):
+        """A component-major WQ vector as the model's (3, nb_cp) array (the
+        layout of YETI's solution writers); model control points outside
+        the patch are 0."""
+        out = np.zeros((3, self.nb_cp_model))
+        out[:, self.cp_index] = np.asarray(x, dtype=np.float64).reshape(3, -1)
+        return out
+
+    def from_model_layout(self, U):
+        """The model's (3, nb_cp) (or interleaved nb_dof) array as a
+        component-major WQ vector of this patch."""
+        U = np.asarray(U, dtype=np.float64)
+        if U.ndim == 1:
+            U = U.reshape(-1, 3).T
+        return np.ascontiguousarray(U[:, self.cp_index]).ravel()
+
     # ------------------------------------------------------------- operator
     def eval_Ku(self, u, precision="f64"):
         """K u.  u: numpy array (host) or torch CUDA tensor (device, result
@@ -150,26 +189,34 @@ class WQElasticity:
         return z
 
     def mf_conj_grad(self, bi, nbIterations, epsilon, method="WP",
-                     directsol=None, isCG=True, mixed=False):
+                     directsol=None, isCG=True):
         """Twin of fortran_mf_wq.mf_conj_grad (fortran_mf_wq.py:545-560):
-        returns (sol, residue, error) with residue/error the reference's
-        inf-norm measures at the start and the end of the solve.  method:
-        'WP' (Jacobi) or the fast-diagonalisation forms 'C', 'JM', 'JMS'
-        (wq_mf_cg_3d, mf_wq_solver.f90:803-953, per displacement
-        component)."""
+        returns (sol, residue, error) with the reference's per-iteration
+        histories RelRes(k) = max|r_k| / max|b| and RelError(k) =
+        max|directsol - x_k| / max|directsol| (zeros without directsol),
+        k = 0..iterations, stopping when RelRes <= epsilon
+        (wq_mf_cg_3d / wq_mf_bicgstab_3d, mf_wq_solver.f90:642-1308).
+        method: 'WP' (Jacobi) or the fast-diagonalisation forms 'C', 'JM',
+        'JMS' (mf_wq_solver.f90:803-953, per displacement component).  FP64
+        throughout, as the reference."""
         if method not in REFERENCE_METHODS:
             raise NotImplementedError(
                 f"method {method!r}: supported {sorted(REFERENCE_METHODS)}")
-        x, st = self.pcg(bi, rtol=epsilon, maxit=nbIterations, mixed=mixed,
-                         method="cg" if isCG else "bicgstab",
-                         precond=REFERENCE_METHODS[method])
-        residue = np.array([1.0, st["rel_residual_inf"]])
-        error = np.array([1.0, 0.0])
-        if directsol is not None:
-            ds = np.asarray(directsol)
-            error[1] = np.abs(ds - x).max() / np.abs(ds).max()
-        self.last_stats = st
-        return x, residue, error
+        mode = (0 if isCG else 2) | _precond_bits(REFERENCE_METHODS[method])
+        bb = np.ascontiguousarray(bi, dtype=np.float64)
+        x = np.zeros_like(bb)
+        maxit = int(nbIterations)
+        relres = np.zeros(maxit + 1)
+        relerr = np.zeros(maxit + 1)
+        ds = None if directsol is None else np.ascontiguousarray(directsol, dtype=np.float64)
+        st = CGStats()
+        rc = lib().yeti_wq_pcg_history(self.handle, ptr(bb), ptr(x), float(epsilon), maxit,
+                                       mode, ptr(ds) if ds is not None else None,
+                                       ptr(relres), ptr(relerr), ctypes.byref(st), MEM_HOST)
+        check(rc, "yeti_wq_pcg_history")
+        k = int(st.iterations)
+        self.last_stats = st.as_dict()
+        return x, relres[:k + 1], relerr[:k + 1]
 
     def close(self):
         if getattr(self, "handle", None):
