@@ -217,6 +217,12 @@ int yeti_wq_body_force(yeti_wq_op *op, const double f[3], double *F, int mem);
 #define YETI_PCG_FD_SCALED 8   /* with YETI_PCG_FD: diagonal scaling
                                   sqrt(diag(P)/diag(K)) ('JMS', 'TDS')      */
 #define YETI_PCG_FD_UNIT 16    /* with YETI_PCG_FD: a[c][d] = 1 ('C')       */
+#define YETI_PCG_FD_TD 32      /* with YETI_PCG_FD: 1-D matrices weighted by
+                                  the tensor decomposition of the diagonal
+                                  coefficients ('TD', 'TDS' with
+                                  YETI_PCG_FD_SCALED;
+                                  tensor_decomposition_3d,
+                                  tensor_algebra.f90:1256-1382)            */
 
 /* Preconditioned Krylov solve of K x = b (x holds the initial guess;
  * replaces wq_mf_cg_3d / wq_mf_bicgstab_3d, mf_wq_solver.f90:642,958).

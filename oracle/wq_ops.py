@@ -235,7 +235,49 @@ class WQOracle:
         K = (R["W11"] @ R["B1"].T)[lo:hi, lo:hi]
         return 0.5 * (K + K.T), 0.5 * (M + M.T)
 
-    def fd_setup(self, scaled=False, unit=False):
+    def td_weights(self, c, sweeps=2):
+        """Per-point 1-D weights (M, K) of component c from `sweeps` sweeps
+        of tensor_decomposition_3d (tensor_algebra.f90:1256-1382) over its
+        diagonal coefficients S[(c,k),(c,k)]; the direction-3 slices run
+        over the w points (the reference bounds that loop by the v count,
+        the same whenever the two agree)."""
+        CC = [self.S[..., 3 * c + k, 3 * c + k] for k in range(3)]   # (qw, qv, qu)
+        nq = [CC[0].shape[2], CC[0].shape[1], CC[0].shape[0]]
+        M = [np.ones(nq[d]) for d in range(3)]
+        K = [np.ones(nq[d]) for d in range(3)]
+        axis = {0: 2, 1: 1, 2: 0}                 # grid axis of direction d
+        others = {d: tuple(a for a in range(3) if a != axis[d]) for d in range(3)}
+
+        def grid(v, d):
+            shape = [1, 1, 1]
+            shape[axis[d]] = v.size
+            return v.reshape(shape)
+        for _ in range(sweeps):
+            for k in range(3):
+                uu = [grid(M[d], d) for d in range(3)]
+                V = CC[k] * uu[k] / (uu[0] * uu[1] * uu[2])
+                K[k] = np.sqrt(V.min(axis=others[k]) * V.max(axis=others[k]))
+            for k in range(3):
+                uu = [grid(M[d], d) for d in range(3)]
+                ww = grid(K[k], k)
+                W = [CC[k] * uu[k] * uu[l] / (uu[0] * uu[1] * uu[2] * ww)
+                     for l in range(3) if l != k]
+                N = np.minimum(W[0], W[1])
+                X = np.maximum(W[0], W[1])
+                M[k] = np.sqrt(N.min(axis=others[k]) * X.max(axis=others[k]))
+        return M, K
+
+    def fd_1d_weighted(self, d, lo, hi, mw, kw):
+        """1-D matrices of the 'TD' branch of eigen_decomposition
+        (tensor_algebra.f90:1045-1071): W00 (B0 diag(mw))^T and W11 (B1
+        diag(kw))^T restricted, symmetric from the upper triangle."""
+        R = self.rules[d]
+        M = (R["W00"] @ (R["B0"] * mw[None, :]).T)[lo:hi, lo:hi]
+        K = (R["W11"] @ (R["B1"] * kw[None, :]).T)[lo:hi, lo:hi]
+        up = lambda A: np.triu(A) + np.triu(A, 1).T   # noqa: E731
+        return up(K), up(M)
+
+    def fd_setup(self, scaled=False, unit=False, td=False):
         """Per component: box, eigenpairs of K_d U = M_d U lam (scipy's
         generalised symmetric solver, U^T M U = I), coefficients a[c][d]
         (1, or the mean over the points of S[(c,d),(c,d)]) and, when scaled,
@@ -246,11 +288,16 @@ class WQOracle:
         plan = []
         for c in range(3):
             box = self.fd_box(c)
-            a = [1.0 if unit else float(self.S[..., 3 * c + d, 3 * c + d].mean())
+            a = [1.0 if (unit or td) else float(self.S[..., 3 * c + d, 3 * c + d].mean())
                  for d in range(3)]
             eig, dg = [], []
+            if td:
+                tM, tK = self.td_weights(c)
             for d, (lo, hi) in enumerate(box):
-                K, M = self.fd_1d(d, lo, hi)
+                if td:
+                    K, M = self.fd_1d_weighted(d, lo, hi, tM[d], tK[d])
+                else:
+                    K, M = self.fd_1d(d, lo, hi)
                 lam, U = eigh(K, M)
                 eig.append((lam, U))
                 dg.append((np.diag(K).copy(), np.diag(M).copy()))

@@ -21,7 +21,9 @@ CASES = [
     ((12, 11, 5), (4, 4, 4), 0.15, (0.8, 1.2), {"w0": (0, 1, 2), "w1": (2,)}),
     ((17, 12, 6), (3, 3, 3), 0.2, (0.8, 1.2), {"w0": (0, 1, 2)}),
 ]
-VARIANTS = [("fd", False, False), ("fd_scaled", True, False), ("fd_unit", False, True)]
+VARIANTS = [("fd", False, False, False), ("fd_scaled", True, False, False),
+            ("fd_unit", False, True, False), ("fd_td", False, False, True),
+            ("fd_td_scaled", True, False, True)]
 
 
 def _rel(a, b):
@@ -55,6 +57,24 @@ def test_oracle_fd_inverts_its_separable_operator(unit):
         assert all(np.abs(z[k]).max() == 0.0 for k in others)
 
 
+def test_oracle_td_weights_of_a_constant_coefficient():
+    """On an affine box with unit weights the diagonal coefficients are
+    constant; the tensor decomposition then returns constant weights whose
+    products reproduce them: K_k M_l M_m = S[(c,k),(c,k)] for {k, l, m} the
+    three directions."""
+    P = cube_patch((4, 3, 5), (2, 2, 2), size=(2.0, 1.0, 1.5))
+    op = WQOracle(P, 1.0, 0.3, {"w0": (0, 1, 2)})
+    for c in range(3):
+        M, K = op.td_weights(c)
+        for k in range(3):
+            cc = op.S[..., 3 * c + k, 3 * c + k]
+            assert np.ptp(cc) < 1e-12 * np.abs(cc).max()
+            others = [d for d in range(3) if d != k]
+            prod = K[k] * M[others[0]].mean() * M[others[1]].mean()
+            assert np.abs(prod - cc.mean()).max() < 1e-10 * cc.mean()
+            assert np.ptp(K[k]) < 1e-10 * K[k].mean()
+
+
 def test_oracle_fd_pcg_matches_direct_solve_in_fewer_iterations():
     P, clamp = _patch(CASES[0])
     op = WQOracle(P, 1.0, 0.3, clamp)
@@ -64,8 +84,8 @@ def test_oracle_fd_pcg_matches_direct_solve_in_fewer_iterations():
     xd = np.zeros_like(b)
     xd[m] = np.linalg.solve(K[np.ix_(m, m)], b[m])
     _, it_j, _ = op.pcg(b, rtol=1e-11)
-    for name, scaled, unit in VARIANTS:
-        plan = op.fd_setup(scaled, unit)
+    for name, scaled, unit, td in VARIANTS:
+        plan = op.fd_setup(scaled, unit, td)
         x, it, res = op.pcg(b, rtol=1e-11, precond=lambda v: op.fd_apply(v, plan))
         assert res < 1e-11 and _rel(x, xd) < 1e-9, name
         assert it < it_j, (name, it, it_j)
@@ -83,9 +103,9 @@ def _pair(case, E=1.0, nu=0.3, seed=7):
 @pytest.mark.parametrize("variant", VARIANTS, ids=[v[0] for v in VARIANTS])
 def test_fd_apply_matches_oracle(cuda_ok, case, variant):
     from yeti_b200._lib import PREC_F32, PREC_F64
-    name, scaled, unit = variant
+    name, scaled, unit, td = variant
     gpu, ora = _pair(case)
-    plan = ora.fd_setup(scaled, unit)
+    plan = ora.fd_setup(scaled, unit, td)
     r = np.random.default_rng(3).standard_normal(ora.ndof) * ora.mask.ravel()
     z_ref = ora.fd_apply(r, plan)
     z64 = gpu.fd_apply(r, name, PREC_F64)

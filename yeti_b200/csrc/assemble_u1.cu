@@ -360,20 +360,105 @@ __device__ inline double parent_det(const double J[3][3], const double *u1,
            A[0][1] * A[1][0] * A[2][2] - A[1][2] * A[2][1] * A[0][0];
 }
 
+// Shared-memory layout of one Gauss-point chunk of the stiffness kernel:
+// per point the six 1-D rows (FN dFN FM dFM FL dFL, kMaxDeg1 each), the
+// nn rational numerators, 3 nn derivative values and 16 scalars.
+constexpr int kStiffQS = 16;   // sx[3], 1/S, J (then J^-1) [9], dv
+__host__ __device__ inline size_t stiff_perq(int nn) {
+    return (size_t)6 * kMaxDeg1 + 4 * (size_t)nn + kStiffQS;
+}
+
+// Stage A of the Gauss kernels for a chunk of points q0..q0+nqc-1
+// (shap.f90:75-178): the 1-D B-spline rows, the rational numerators R0 and
+// dR/dxi of every (point, node), the per-point 1/S (qs[3]) and dx/dxi
+// (qs[4 + 3 r + c]).  The products of every (point, node) are formed in
+// parallel; each sum over the nodes stays one thread's loop in node order,
+// so the values are those of the point-serial evaluation bit for bit.
+__device__ void basis_chunk(const int pd[3], const double *const Ud[3], const int *sni,
+                            const double *su1, const double *su2, const double *gauss,
+                            int q0, int nqc, int nn, const double *xe, const double *we,
+                            double *B1, double *R0, double *dR, double *qs) {
+    const int tid = threadIdx.x, nth = blockDim.x;
+    const int p0 = pd[0], p1 = pd[1], p2 = pd[2];
+    // A1: 1-D B-spline values and derivatives, one thread per (point, dir)
+    for (int t = tid; t < 3 * nqc; t += nth) {
+        const int ql = t / 3, d = t - 3 * ql;
+        const double tq = gauss[4 * (q0 + ql) + 1 + d];
+        const double xi = ((su2[d] - su1[d]) * tq + (su2[d] + su1[d])) * 0.5;
+        double *f = B1 + ((size_t)ql * 6 + 2 * d) * kMaxDeg1;
+        bspline_ders(sni[d], pd[d], xi, Ud[d], f, f + kMaxDeg1);
+    }
+    __syncthreads();
+    // A2: the four numerator products of every (point, node)
+    for (int t = tid; t < nqc * nn; t += nth) {
+        const int ql = t / nn, n = t - ql * nn;
+        const int i = n % (p0 + 1), j = (n / (p0 + 1)) % (p1 + 1), k = n / ((p0 + 1) * (p1 + 1));
+        const double *f = B1 + (size_t)ql * 6 * kMaxDeg1;
+        const double FN = f[p0 - i], dFN = f[kMaxDeg1 + p0 - i];
+        const double FM = f[2 * kMaxDeg1 + p1 - j], dFM = f[3 * kMaxDeg1 + p1 - j];
+        const double FL = f[4 * kMaxDeg1 + p2 - k], dFL = f[5 * kMaxDeg1 + p2 - k];
+        const double wa = we[n];
+        R0[(size_t)ql * nn + n] = FN * FM * FL * wa;
+        double *d = dR + ((size_t)ql * nn + n) * 3;
+        d[0] = dFN * FM * FL * wa;
+        d[1] = FN * dFM * FL * wa;
+        d[2] = FN * FM * dFL * wa;
+    }
+    __syncthreads();
+    // A3: the sums over the nodes (one thread per (point, sum), node order)
+    for (int t = tid; t < 4 * nqc; t += nth) {
+        const int ql = t >> 2, c = t & 3;
+        double acc = 0.0;
+        if (c == 0) {
+            const double *r = R0 + (size_t)ql * nn;
+            for (int n = 0; n < nn; n++) acc += r[n];
+            qs[(size_t)ql * kStiffQS + 3] = 1.0 / acc;
+        } else {
+            const double *d = dR + (size_t)ql * nn * 3 + (c - 1);
+            for (int n = 0; n < nn; n++) acc += d[3 * n];
+            qs[(size_t)ql * kStiffQS + c - 1] = acc;
+        }
+    }
+    __syncthreads();
+    // A4: rational derivatives dR/dxi, one thread per (point, node)
+    for (int t = tid; t < nqc * nn; t += nth) {
+        const int ql = t / nn, n = t - ql * nn;
+        const double *sq = qs + (size_t)ql * kStiffQS;
+        const double inv = sq[3];
+        const double R = R0[(size_t)ql * nn + n] * inv;
+        double *d = dR + ((size_t)ql * nn + n) * 3;
+        d[0] = (d[0] - R * sq[0]) * inv;
+        d[1] = (d[1] - R * sq[1]) * inv;
+        d[2] = (d[2] - R * sq[2]) * inv;
+    }
+    __syncthreads();
+    // A5: dx/dxi, one thread per (point, entry), node order
+    for (int t = tid; t < 9 * nqc; t += nth) {
+        const int ql = t / 9, rc = t - 9 * ql, r = rc / 3, c = rc - 3 * r;
+        const double *d = dR + (size_t)ql * nn * 3 + c;
+        double acc = 0.0;
+        for (int n = 0; n < nn; n++) acc += xe[3 * n + r] * d[3 * n];
+        qs[(size_t)ql * kStiffQS + 4 + rc] = acc;
+    }
+    __syncthreads();
+}
+
 __global__ void __launch_bounds__(256)
 k_u1_stiffness(StiffArgs a) {
     extern __shared__ double smem[];
     const int nn = a.nn;
     double *xe = smem;                      // 3*nn element CP coordinates
     double *we = xe + 3 * nn;               // nn element weights
-    double *dR = we + nn;                   // qchunk * nn * 3
-    double *dv = dR + (size_t)a.qchunk * nn * 3;  // qchunk
+    double *B1 = we + nn;                   // qchunk * 6 * kMaxDeg1
+    double *R0 = B1 + (size_t)a.qchunk * 6 * kMaxDeg1;   // qchunk * nn
+    double *dR = R0 + (size_t)a.qchunk * nn;             // qchunk * nn * 3
+    double *qs = dR + (size_t)a.qchunk * nn * 3;         // qchunk * kStiffQS
     __shared__ double su1[3], su2[3];
     __shared__ int sni[3];
     const int e = blockIdx.x;
-    const int tid = threadIdx.x;
+    const int tid = threadIdx.x, nth = blockDim.x;
     const int32_t *ien = a.ien + (size_t)e * nn;
-    for (int i = tid; i < nn; i += blockDim.x) {
+    for (int i = tid; i < nn; i += nth) {
         int cp = ien[i];
         xe[3 * i] = a.coords[3 * cp];
         xe[3 * i + 1] = a.coords[3 * cp + 1];
@@ -390,24 +475,32 @@ k_u1_stiffness(StiffArgs a) {
     const int npairs = nn * (nn + 1) / 2;
     const int64_t base = a.slot[e];
     const double lam = a.lam, mu = a.mu, l2m = lam + 2.0 * mu;
+    const int pd[3] = {a.p0, a.p1, a.p2};
+    const double *Ud[3] = {a.U0, a.U1, a.U2};
     for (int q0 = 0; q0 < a.nq; q0 += a.qchunk) {
         const int nqc = min(a.qchunk, a.nq - q0);
         __syncthreads();
         // ---- stage A: basis derivatives at the chunk's Gauss points
-        for (int ql = tid; ql < nqc; ql += blockDim.x) {
-            const double *g = a.gauss + 4 * (q0 + ql);
-            double Fv[6 * kMaxDeg1];
-            double J[3][3], Ji[3][3], inv;
-            double *dRq = dR + (size_t)ql * nn * 3;
-            rational_derivs(a.p0, a.p1, a.p2, nn, a.U0, a.U1, a.U2, sni, su1,
-                            su2, g + 1, we, xe, dRq, J, &inv, Fv);
+        basis_chunk(pd, Ud, sni, su1, su2, a.gauss, q0, nqc, nn, xe, we, B1, R0, dR, qs);
+        // A6: inverse Jacobian and the point's weight
+        for (int ql = tid; ql < nqc; ql += nth) {
+            double *sq = qs + (size_t)ql * kStiffQS;
+            double J[3][3], Ji[3][3];
+            for (int r = 0; r < 3; r++)
+                for (int c = 0; c < 3; c++) J[r][c] = sq[4 + 3 * r + c];
             inv3(J, Ji);
-            dv[ql] = g[0] * fabs(parent_det(J, su1, su2));
-            for (int n = 0; n < nn; n++) {
-                double d0 = dRq[3 * n], d1 = dRq[3 * n + 1], d2 = dRq[3 * n + 2];
-                for (int c = 0; c < 3; c++)
-                    dRq[3 * n + c] = d0 * Ji[0][c] + d1 * Ji[1][c] + d2 * Ji[2][c];
-            }
+            sq[13] = a.gauss[4 * (q0 + ql)] * fabs(parent_det(J, su1, su2));
+            for (int r = 0; r < 3; r++)
+                for (int c = 0; c < 3; c++) sq[4 + 3 * r + c] = Ji[r][c];
+        }
+        __syncthreads();
+        // A7: physical gradients dR/dx, one thread per (point, node)
+        for (int t = tid; t < nqc * nn; t += nth) {
+            const int ql = t / nn, n = t - ql * nn;
+            const double *Ji = qs + (size_t)ql * kStiffQS + 4;
+            double *d = dR + ((size_t)ql * nn + n) * 3;
+            const double d0 = d[0], d1 = d[1], d2 = d[2];
+            for (int c = 0; c < 3; c++) d[c] = d0 * Ji[c] + d1 * Ji[3 + c] + d2 * Ji[6 + c];
         }
         __syncthreads();
         // ---- stage B: one thread per control-point pair (i <= j)
@@ -422,7 +515,7 @@ k_u1_stiffness(StiffArgs a) {
                 const double *B = dR + ((size_t)q * nn + j) * 3;
                 const double a0 = A[0], a1 = A[1], a2 = A[2];
                 const double b0 = B[0], b1 = B[1], b2 = B[2];
-                const double d = dv[q];
+                const double d = qs[(size_t)q * kStiffQS + 13];
                 // B_i^T D B_j for isotropic D (stiffmatrix.F90:167-216)
                 K[0][0] += (a0 * (l2m * b0) + a1 * (mu * b1) + a2 * (mu * b2)) * d;
                 K[1][1] += (a1 * (l2m * b1) + a0 * (mu * b0) + a2 * (mu * b2)) * d;
@@ -493,8 +586,10 @@ __global__ void __launch_bounds__(256) k_u1_mass(MassArgs a) {
     const int nn = a.nn;
     double *xe = smem;                          // 3*nn element CP coordinates
     double *we = xe + 3 * nn;                   // nn element weights
-    double *Rq = we + nn;                       // qchunk * nn basis values
-    double *dv = Rq + (size_t)a.qchunk * nn;    // qchunk
+    double *B1 = we + nn;                       // qchunk * 6 * kMaxDeg1
+    double *Rq = B1 + (size_t)a.qchunk * 6 * kMaxDeg1;   // qchunk * nn basis values
+    double *dR = Rq + (size_t)a.qchunk * nn;             // qchunk * nn * 3 (dR/dxi)
+    double *qs = dR + (size_t)a.qchunk * nn * 3;         // qchunk * kStiffQS
     __shared__ double su1[3], su2[3];
     __shared__ int sni[3];
     const int e = blockIdx.x;
@@ -516,25 +611,24 @@ __global__ void __launch_bounds__(256) k_u1_mass(MassArgs a) {
     }
     const int npairs = nn * (nn + 1) / 2;
     const int64_t base = a.slot[e];
+    const int pd[3] = {a.p0, a.p1, a.p2};
+    const double *Ud[3] = {a.U0, a.U1, a.U2};
     for (int q0 = 0; q0 < a.nq; q0 += a.qchunk) {
         const int nqc = min(a.qchunk, a.nq - q0);
         __syncthreads();
         // ---- stage A: basis values and dvol at the chunk's Gauss points
+        basis_chunk(pd, Ud, sni, su1, su2, a.gauss, q0, nqc, nn, xe, we, B1, Rq, dR, qs);
+        for (int t = tid; t < nqc * nn; t += blockDim.x) {
+            const int ql = t / nn;
+            Rq[t] = Rq[t] * qs[(size_t)ql * kStiffQS + 3];
+        }
         for (int ql = tid; ql < nqc; ql += blockDim.x) {
-            const double *g = a.gauss + 4 * (q0 + ql);
-            double Fv[6 * kMaxDeg1];
-            double J[3][3], inv;
-            rational_derivs(a.p0, a.p1, a.p2, nn, a.U0, a.U1, a.U2, sni, su1, su2, g + 1,
-                            we, xe, nullptr, J, &inv, Fv);
-            const double *FN = Fv, *FM = Fv + 2 * kMaxDeg1, *FL = Fv + 4 * kMaxDeg1;
-            double *R = Rq + (size_t)ql * nn;
-            int n = 0;
-            for (int k = 0; k <= a.p2; k++)
-                for (int j = 0; j <= a.p1; j++)
-                    for (int i = 0; i <= a.p0; i++, n++)
-                        R[n] = FN[a.p0 - i] * FM[a.p1 - j] * FL[a.p2 - k] * we[n] * inv;
-            const double dvol = g[0] * parent_det(J, su1, su2);
-            dv[ql] = a.rho * dvol;
+            double *sq = qs + (size_t)ql * kStiffQS;
+            double J[3][3];
+            for (int r = 0; r < 3; r++)
+                for (int c = 0; c < 3; c++) J[r][c] = sq[4 + 3 * r + c];
+            const double dvol = a.gauss[4 * (q0 + ql)] * parent_det(J, su1, su2);
+            sq[13] = a.rho * dvol;
         }
         __syncthreads();
         // ---- stage B: one thread per control-point pair (i <= j)
@@ -545,7 +639,7 @@ __global__ void __launch_bounds__(256) k_u1_mass(MassArgs a) {
             const int i = t - j * (j + 1) / 2;
             double m = 0.0;
             for (int q = 0; q < nqc; q++) {
-                const double t1 = dv[q] * Rq[(size_t)q * nn + j];
+                const double t1 = qs[(size_t)q * kStiffQS + 13] * Rq[(size_t)q * nn + j];
                 m += t1 * Rq[(size_t)q * nn + i];
             }
             const int64_t jb = base + 9LL * j * (j - 1) / 2 + 6LL * j;
@@ -878,7 +972,7 @@ YETI_API int yeti_assemble_u1_coo(yeti_ctx *ctx, const yeti_u1_model *m,
         U1Patch &P = M.patches[ip];
         if (!P.nactive) continue;
         const size_t fixed = sizeof(double) * 4 * P.nn;
-        const size_t perq = sizeof(double) * (3 * P.nn + 1);
+        const size_t perq = sizeof(double) * stiff_perq(P.nn);
         YETI_CHECK(fixed + perq <= smem_cap, YETI_EUNSUPPORTED,
                    "element with %d nodes does not fit shared memory", P.nn);
         int qchunk = (int)std::min<size_t>(P.nq, (smem_cap - fixed) / perq);
@@ -1094,7 +1188,7 @@ YETI_API int yeti_assemble_u1_mass_coo(yeti_ctx *ctx, const yeti_u1_model *m,
         U1Patch &P = M.patches[ip];
         if (!P.nactive) continue;
         const size_t fixed = sizeof(double) * 4 * P.nn;
-        const size_t perq = sizeof(double) * (P.nn + 1);
+        const size_t perq = sizeof(double) * stiff_perq(P.nn);
         YETI_CHECK(fixed + perq <= smem_cap, YETI_EUNSUPPORTED,
                    "element with %d nodes does not fit shared memory", P.nn);
         const int qchunk = (int)std::min<size_t>(P.nq, (smem_cap - fixed) / perq);

@@ -390,7 +390,7 @@ YETI_API int yeti_serve_submit(yeti_server *srv, const yeti_serve_request *q, in
     YETI_CHECK(q->rtol > 0 && q->maxit > 0, YETI_EINVAL, "yeti_serve_submit: rtol %g maxit %d",
                q->rtol, q->maxit);
     {
-        const int fd_bits = YETI_PCG_FD | YETI_PCG_FD_SCALED | YETI_PCG_FD_UNIT;
+        const int fd_bits = YETI_PCG_FD | YETI_PCG_FD_SCALED | YETI_PCG_FD_UNIT | YETI_PCG_FD_TD;
         YETI_CHECK((q->mode & ~(fd_bits | YETI_PCG_BICGSTAB)) == 0 &&
                        ((q->mode & fd_bits) == 0 || (q->mode & YETI_PCG_FD)),
                    YETI_EINVAL, "yeti_serve_submit: mode %d (FP64 CG/BiCGSTAB, Jacobi/FD)",

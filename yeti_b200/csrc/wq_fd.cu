@@ -628,10 +628,111 @@ static int fd_set_attrs() {
     return YETI_OK;
 }
 
+// 1-D matrices with per-point weights (eigen_decomposition's 'TD' branch,
+// tensor_algebra.f90:1045-1071): M = W00 (B0 diag(mw))^T and K = W11 (B1
+// diag(kw))^T on the rows lo..hi-1, symmetric from their upper triangle (the
+// triangle dsygvd reads, UPLO = 'U').
+static void wq_1d_matrices_weighted(const WQRule1D &R, int lo, int hi, const double *mw,
+                                    const double *kw, std::vector<double> &K,
+                                    std::vector<double> &M) {
+    const int m = hi - lo, nq = R.nqp;
+    K.assign((size_t)m * m, 0.0);
+    M.assign((size_t)m * m, 0.0);
+    for (int i = 0; i < m; i++)
+        for (int j = i; j < m; j++) {
+            const double *w0 = &R.W00[(size_t)(lo + i) * nq], *b0 = &R.B0[(size_t)(lo + j) * nq];
+            const double *w1 = &R.W11[(size_t)(lo + i) * nq], *b1 = &R.B1[(size_t)(lo + j) * nq];
+            double sm = 0.0, sk = 0.0;
+            for (int q = 0; q < nq; q++) {
+                sm += w0[q] * (b0[q] * mw[q]);
+                sk += w1[q] * (b1[q] * kw[q]);
+            }
+            M[(size_t)i * m + j] = M[(size_t)j * m + i] = sm;
+            K[(size_t)i * m + j] = K[(size_t)j * m + i] = sk;
+        }
+}
+
+// One sweep of tensor_decomposition_3d (tensor_algebra.f90:1256-1382) for
+// one displacement component: cc[k] the diagonal coefficient S[(c,k),(c,k)]
+// at every WQ point (u fastest), M[d] / K[d] the per-point 1-D weights of
+// direction d, updated in place.  Stiffness weights first: K_k(i) =
+// sqrt(min V max V) over the slice i of direction k, V = cc_k M_k /
+// (M_u M_v M_w); then mass weights: M_k(i) = sqrt(min N max W) over the
+// slice, from cc_k M_k M_l / (M_u M_v M_w K_k), l != k.  (The reference
+// bounds its direction-3 slice loops by the v count; the w count is used
+// here, which agrees whenever the two are equal.)
+static void td_sweep(const int nq[3], const double *const cc[3], std::vector<double> M[3],
+                     std::vector<double> K[3]) {
+    const int64_t n = (int64_t)nq[0] * nq[1] * nq[2];
+    for (int k = 0; k < 3; k++) {
+        std::vector<double> vmin(nq[k], INFINITY), vmax(nq[k], -INFINITY);
+        int64_t g = 0;
+        for (int i2 = 0; i2 < nq[2]; i2++)
+            for (int i1 = 0; i1 < nq[1]; i1++)
+                for (int i0 = 0; i0 < nq[0]; i0++, g++) {
+                    const int i[3] = {i0, i1, i2};
+                    const double uu[3] = {M[0][i0], M[1][i1], M[2][i2]};
+                    const double v = cc[k][g] * uu[k] / (uu[0] * uu[1] * uu[2]);
+                    vmin[i[k]] = std::min(vmin[i[k]], v);
+                    vmax[i[k]] = std::max(vmax[i[k]], v);
+                }
+        for (int a = 0; a < nq[k]; a++) K[k][a] = std::sqrt(vmin[a] * vmax[a]);
+    }
+    for (int k = 0; k < 3; k++) {
+        std::vector<double> nmin(nq[k], INFINITY), mmax(nq[k], -INFINITY);
+        int64_t g = 0;
+        for (int i2 = 0; i2 < nq[2]; i2++)
+            for (int i1 = 0; i1 < nq[1]; i1++)
+                for (int i0 = 0; i0 < nq[0]; i0++, g++) {
+                    const int i[3] = {i0, i1, i2};
+                    const double uu[3] = {M[0][i0], M[1][i1], M[2][i2]};
+                    const double ww[3] = {K[0][i0], K[1][i1], K[2][i2]};
+                    double lo = INFINITY, hi = -INFINITY;
+                    for (int l = 0; l < 3; l++) {
+                        if (l == k) continue;
+                        const double w = cc[k][g] * uu[k] * uu[l] / (uu[0] * uu[1] * uu[2] * ww[k]);
+                        lo = std::min(lo, w);
+                        hi = std::max(hi, w);
+                    }
+                    nmin[i[k]] = std::min(nmin[i[k]], lo);
+                    mmax[i[k]] = std::max(mmax[i[k]], hi);
+                }
+        for (int a = 0; a < nq[k]; a++) M[k][a] = std::sqrt(nmin[a] * mmax[a]);
+    }
+    (void)n;
+}
+
+// The diagonal coefficients S[(c,k),(c,k)] of every WQ point, in point
+// order (u fastest), gathered from the streaming FP64 layout: out[(3c+k) n + g].
+__global__ void k_fd_diag_coef(const double *coef, const int64_t *tile_off, const int *pstride,
+                               const int *tq0u, const int *tnqu, const int *tq0v,
+                               const int *tnqv, int ntu, int nqu, int nqv, int nqw,
+                               double *out) {
+    const int64_t n = (int64_t)nqu * nqv * nqw;
+    for (int64_t g = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; g < n;
+         g += (int64_t)gridDim.x * blockDim.x) {
+        const int qu = (int)(g % nqu), qv = (int)((g / nqu) % nqv);
+        const int qw = (int)(g / ((int64_t)nqu * nqv));
+        int tu = 0, tv = 0;
+        while (tq0u[tu] + tnqu[tu] <= qu) tu++;
+        while (tq0v[tv] + tnqv[tv] <= qv) tv++;
+        const int t = tu + ntu * tv;
+        const int npts = tnqu[tu] * tnqv[tv];
+        const int pt = (qv - tq0v[tv]) * tnqu[tu] + (qu - tq0u[tu]);
+        const double *blk = coef + tile_off[t] + (int64_t)qw * pstride[t] + pt;
+        for (int c = 0; c < 3; c++)
+            for (int k = 0; k < 3; k++)
+                out[(int64_t)(3 * c + k) * n + g] = blk[(int64_t)sym9(3 * c + k, 3 * c + k) * npts];
+    }
+}
+
 int wq_fd_prepare(yeti_wq_op *op, int variant, bool f32) {
     WQFdPlan &F = op->fd;
-    variant &= (YETI_PCG_FD | YETI_PCG_FD_SCALED | YETI_PCG_FD_UNIT);
+    variant &= (YETI_PCG_FD | YETI_PCG_FD_SCALED | YETI_PCG_FD_UNIT | YETI_PCG_FD_TD);
     if (F.variant == variant && (!f32 || F.g32.ptr)) return YETI_OK;
+    const bool td = (variant & YETI_PCG_FD_TD) != 0;
+    YETI_CHECK(!td || (op->st.active && op->coef64.ptr), YETI_EUNSUPPORTED,
+               "fast diagonalisation 'TD': needs an operator of one degree 2..5 with FP64 data");
     // the passes stage up to kFdSmem bytes: opt in once per device (the
     // attribute is always this maximum, so concurrent callers agree)
     YETI_TRY(fd_set_attrs<double>());
@@ -654,9 +755,9 @@ int wq_fd_prepare(yeti_wq_op *op, int variant, bool f32) {
                        "(1..%d supported)", F.m[c][d], d, kFdMaxM);
         }
     }
-    // coefficients a[c][d]
+    // coefficients a[c][d] ('TD': 1, the weights carry the coefficients)
     double acoef[3][3];
-    if (unit) {
+    if (unit || td) {
         for (int c = 0; c < 3; c++)
             for (int d = 0; d < 3; d++) acoef[c][d] = 1.0;
     } else {
@@ -679,20 +780,65 @@ int wq_fd_prepare(yeti_wq_op *op, int variant, bool f32) {
     for (int d = 0; d < 3; d++)
         YETI_CHECK(wq_rule_1d(op->p[d], op->nel[d], R[d]) == 0, YETI_EINVAL,
                    "fast diagonalisation: WQ rule failed");
+    // 'TD': per component, two sweeps of the tensor decomposition of the
+    // diagonal coefficients give per-point 1-D weights (wq_mf_cg_3d,
+    // mf_wq_solver.f90:809-826, per displacement component)
+    std::vector<double> tdM[3][3], tdK[3][3];
+    if (td) {
+        const int nq[3] = {op->nqp[0], op->nqp[1], op->nqp[2]};
+        const int64_t n = (int64_t)nq[0] * nq[1] * nq[2];
+        DevBuf dcc;
+        YETI_TRY(dcc.alloc(ctx, (size_t)9 * n * sizeof(double)));
+        WQStreamPlan &st = op->st;
+        k_fd_diag_coef<<<592, 256, 0, s>>>(op->coef64.as<double>(), st.tile_off.as<int64_t>(),
+                                           st.tile_pstride.as<int>(), st.tq0[0].as<int>(),
+                                           st.tnq[0].as<int>(), st.tq0[1].as<int>(),
+                                           st.tnq[1].as<int>(), st.ntile[0], nq[0], nq[1], nq[2],
+                                           dcc.as<double>());
+        count_launches(1);
+        YETI_CUDA(cudaGetLastError());
+        std::vector<double> cc((size_t)9 * n);
+        YETI_CUDA(cudaMemcpyAsync(cc.data(), dcc.ptr, cc.size() * sizeof(double),
+                                  cudaMemcpyDeviceToHost, s));
+        YETI_CUDA(cudaStreamSynchronize(s));
+        for (int c = 0; c < 3; c++) {
+            std::vector<double> Mw[3], Kw[3];
+            for (int d = 0; d < 3; d++) {
+                Mw[d].assign(nq[d], 1.0);
+                Kw[d].assign(nq[d], 1.0);
+            }
+            const double *ccp[3] = {&cc[(size_t)(3 * c) * n], &cc[(size_t)(3 * c + 1) * n],
+                                    &cc[(size_t)(3 * c + 2) * n]};
+            for (int sweep = 0; sweep < 2; sweep++) td_sweep(nq, ccp, Mw, Kw);
+            for (int d = 0; d < 3; d++) {
+                for (int q = 0; q < nq[d]; q++)
+                    YETI_CHECK(Mw[d][q] > 0.0 && Kw[d][q] > 0.0 && std::isfinite(Mw[d][q]) &&
+                                   std::isfinite(Kw[d][q]),
+                               YETI_ENUMERIC, "fast diagonalisation 'TD': weight %g / %g",
+                               Mw[d][q], Kw[d][q]);
+                tdM[c][d] = Mw[d];
+                tdK[c][d] = Kw[d];
+            }
+        }
+    }
     struct Eig {
         std::vector<double> lam, U, kd, md;
     };
-    std::map<std::tuple<int, int, int, int>, Eig> cache;
+    std::map<std::tuple<int, int, int, int, int>, Eig> cache;
     Eig *E[3][3];
     for (int c = 0; c < 3; c++)
         for (int d = 0; d < 3; d++) {
             const int lo = F.lo[c][d], hi = lo + F.m[c][d];
-            auto key = std::make_tuple(op->p[d], op->nel[d], lo, hi);
+            // 'TD' weights differ per component: no sharing between components
+            auto key = std::make_tuple(op->p[d], op->nel[d], lo, hi, td ? 3 * c + d : -1);
             auto it = cache.find(key);
             if (it == cache.end()) {
                 Eig e;
                 std::vector<double> K, M;
-                wq_1d_matrices(R[d], lo, hi, K, M);
+                if (td)
+                    wq_1d_matrices_weighted(R[d], lo, hi, tdM[c][d].data(), tdK[c][d].data(), K, M);
+                else
+                    wq_1d_matrices(R[d], lo, hi, K, M);
                 const int m = hi - lo;
                 e.kd.resize(m);
                 e.md.resize(m);
@@ -969,7 +1115,8 @@ YETI_API int yeti_wq_fd_apply(yeti_wq_op *op, const void *r, void *z, int prec, 
     YETI_CHECK(prec == YETI_PREC_F64 || prec == YETI_PREC_F32, YETI_EINVAL,
                "yeti_wq_fd_apply: prec %d", prec);
     YETI_CHECK((variant & YETI_PCG_FD) && !(variant & ~(YETI_PCG_FD | YETI_PCG_FD_SCALED |
-                                                       YETI_PCG_FD_UNIT)),
+                                                       YETI_PCG_FD_UNIT | YETI_PCG_FD_TD)) &&
+                   !((variant & YETI_PCG_FD_UNIT) && (variant & YETI_PCG_FD_TD)),
                YETI_EINVAL, "yeti_wq_fd_apply: variant %d", variant);
     DeviceGuard guard(op->ctx->device);
     const bool f32 = prec == YETI_PREC_F32;

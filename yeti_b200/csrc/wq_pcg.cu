@@ -872,7 +872,7 @@ int cgsolve_begin(CgSolve &cs, yeti_wq_op *op, cudaStream_t st, void *host_scal,
     YETI_CHECK(op && host_scal && b_host && op->coef64.ptr, YETI_EINVAL,
                "cgsolve_begin: missing operator data");
     YETI_CHECK(chunk >= 0 && chunk <= 256, YETI_EINVAL, "cgsolve_begin: chunk %d", chunk);
-    const int fd_bits = YETI_PCG_FD | YETI_PCG_FD_SCALED | YETI_PCG_FD_UNIT;
+    const int fd_bits = YETI_PCG_FD | YETI_PCG_FD_SCALED | YETI_PCG_FD_UNIT | YETI_PCG_FD_TD;
     YETI_CHECK((mode & ~(fd_bits | YETI_PCG_BICGSTAB)) == 0 &&
                    ((mode & fd_bits) == 0 || (mode & YETI_PCG_FD)),
                YETI_EINVAL, "cgsolve_begin: mode %d", mode);
@@ -1062,8 +1062,10 @@ static int pcg_run(yeti_wq_op *op, const double *b, double *x, double rtol, int 
                    int mode, yeti_cg_stats *stats, int mem, const double *dsol,
                    double *relres, double *relerr) {
     YETI_CHECK(op && b && x, YETI_EINVAL, "yeti_wq_pcg: NULL argument");
-    YETI_CHECK(mode >= 0 && mode < 32 &&
-                   ((mode & (YETI_PCG_FD_SCALED | YETI_PCG_FD_UNIT)) == 0 || (mode & YETI_PCG_FD)),
+    YETI_CHECK(mode >= 0 && mode < 64 &&
+                   ((mode & (YETI_PCG_FD_SCALED | YETI_PCG_FD_UNIT | YETI_PCG_FD_TD)) == 0 ||
+                    (mode & YETI_PCG_FD)) &&
+                   !((mode & YETI_PCG_FD_UNIT) && (mode & YETI_PCG_FD_TD)),
                YETI_EINVAL, "yeti_wq_pcg: mode %d", mode);
     YETI_CHECK(rtol > 0 && maxit > 0, YETI_EINVAL, "yeti_wq_pcg: rtol %g maxit %d", rtol, maxit);
     YETI_CHECK(op->coef64.ptr, YETI_EINVAL,

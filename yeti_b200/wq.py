@@ -20,14 +20,18 @@ from .patches import face_mask, free_mask
 WQ_F64, WQ_F32 = 1, 2
 
 # Preconditioners of yeti_wq_pcg (mode bits of include/yeti_b200.h).
-PCG_FD, PCG_FD_SCALED, PCG_FD_UNIT = 4, 8, 16
+PCG_FD, PCG_FD_SCALED, PCG_FD_UNIT, PCG_FD_TD = 4, 8, 16, 32
 FD_VARIANTS = {
     "fd": PCG_FD,                        # a[c][d] = mean S[(c,d),(c,d)]
     "fd_scaled": PCG_FD | PCG_FD_SCALED,  # ... and sqrt(diag P / diag K)
     "fd_unit": PCG_FD | PCG_FD_UNIT,      # a[c][d] = 1
+    "fd_td": PCG_FD | PCG_FD_TD,          # 1-D matrices weighted by the tensor
+                                          # decomposition of the coefficients
+    "fd_td_scaled": PCG_FD | PCG_FD_TD | PCG_FD_SCALED,
 }
 # The reference's Method strings of wq_mf_cg_3d (mf_wq_solver.f90:803-953).
-REFERENCE_METHODS = {"WP": "jacobi", "C": "fd_unit", "JM": "fd", "JMS": "fd_scaled"}
+REFERENCE_METHODS = {"WP": "jacobi", "C": "fd_unit", "JM": "fd", "JMS": "fd_scaled",
+                     "TD": "fd_td", "TDS": "fd_td_scaled"}
 
 
 def _precond_bits(precond):
@@ -197,8 +201,8 @@ class WQElasticity:
         k = 0..iterations, stopping when RelRes <= epsilon
         (wq_mf_cg_3d / wq_mf_bicgstab_3d, mf_wq_solver.f90:642-1308).
         method: 'WP' (Jacobi) or the fast-diagonalisation forms 'C', 'JM',
-        'JMS' (mf_wq_solver.f90:803-953, per displacement component).  FP64
-        throughout, as the reference."""
+        'JMS', 'TD', 'TDS' (mf_wq_solver.f90:803-953, per displacement
+        component).  FP64 throughout, as the reference."""
         if method not in REFERENCE_METHODS:
             raise NotImplementedError(
                 f"method {method!r}: supported {sorted(REFERENCE_METHODS)}")
