@@ -52,6 +52,8 @@ def parse():
     ap.add_argument("--serve-requests", type=int, default=2000)
     ap.add_argument("--serve-rate", type=float, default=25.0,
                     help="Poisson arrival rate of the serving stream (requests/s)")
+    ap.add_argument("--serve-rate-high", type=float, default=80.0,
+                    help="second serving stream near saturation (requests/s; 0: none)")
     ap.add_argument("--serve-budget-gb", type=float, default=32.0)
     ap.add_argument("--no-serve", action="store_true")
     ap.add_argument("--serve-precond", default="fd", choices=["jacobi", "fd"],
@@ -235,7 +237,7 @@ def run_reference(args):
     return 0
 
 
-def serve_stream(args, device):
+def serve_stream(args, device, rate=None):
     """The serving workload: a seeded stream of requests (cube-like NURBS
     patches, p in {2,3}, 4..32 elements per direction, 1..8 Gaussian
     right-hand sides, FP64 preconditioned Krylov solves to 1e-8:
@@ -245,13 +247,14 @@ def serve_stream(args, device):
     reqs = synthetic_requests(args.serve_requests, seed=WORKLOAD["seed"] + 7)
     budget = int(args.serve_budget_gb * (1 << 30))
     with Server(device=device, hbm_budget_bytes=budget, max_active=128) as srv:
-        out = run_stream(srv, reqs, args.serve_rate, seed=WORKLOAD["seed"] + 8, rtol=1e-8,
+        rate = args.serve_rate if rate is None else rate
+        out = run_stream(srv, reqs, rate, seed=WORKLOAD["seed"] + 8, rtol=1e-8,
                          precond=args.serve_precond, method=args.serve_method)
         st = srv.stats()
     lat = out["latency_ms"]
     its = [sum(r["iterations"]) for r in out["results"] if r is not None]
     return {"requests": len(reqs), "completed": int(len(lat)), "errors": len(out["errors"]),
-            "arrival_rate_per_s": args.serve_rate, "offered_s": out["offered_s"],
+            "arrival_rate_per_s": rate, "offered_s": out["offered_s"],
             "wall_s": out["wall_s"],
             "p50_ms": float(np.percentile(lat, 50)) if len(lat) else None,
             "p99_ms": float(np.percentile(lat, 99)) if len(lat) else None,
@@ -575,6 +578,8 @@ def main():
     serve = None
     if not args.no_serve and args.serve_requests > 0:
         serve = serve_stream(args, local)
+        if args.serve_rate_high > 0:
+            serve["high_rate"] = serve_stream(args, local, args.serve_rate_high)
     extra = None
     if rank == 0 and ws == 1 and not args.no_extra:
         extra = extra_configs(args, local)

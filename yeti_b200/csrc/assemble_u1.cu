@@ -360,87 +360,12 @@ __device__ inline double parent_det(const double J[3][3], const double *u1,
            A[0][1] * A[1][0] * A[2][2] - A[1][2] * A[2][1] * A[0][0];
 }
 
-// Shared-memory layout of one Gauss-point chunk of the stiffness kernel:
-// per point the six 1-D rows (FN dFN FM dFM FL dFL, kMaxDeg1 each), the
-// nn rational numerators, 3 nn derivative values and 16 scalars.
-constexpr int kStiffQS = 16;   // sx[3], 1/S, J (then J^-1) [9], dv
+// Shared-memory layout of one Gauss-point chunk of the stiffness and mass
+// kernels: per point the six 1-D rows (FN dFN FM dFM FL dFL, kMaxDeg1 each),
+// the nn rational numerators, 3 nn derivative values and kStiffQS scalars
+// (sx[3], 1/S, J then J^-1 [9], dv).
 __host__ __device__ inline size_t stiff_perq(int nn) {
     return (size_t)6 * kMaxDeg1 + 4 * (size_t)nn + kStiffQS;
-}
-
-// Stage A of the Gauss kernels for a chunk of points q0..q0+nqc-1
-// (shap.f90:75-178): the 1-D B-spline rows, the rational numerators R0 and
-// dR/dxi of every (point, node), the per-point 1/S (qs[3]) and dx/dxi
-// (qs[4 + 3 r + c]).  The products of every (point, node) are formed in
-// parallel; each sum over the nodes stays one thread's loop in node order,
-// so the values are those of the point-serial evaluation bit for bit.
-__device__ void basis_chunk(const int pd[3], const double *const Ud[3], const int *sni,
-                            const double *su1, const double *su2, const double *gauss,
-                            int q0, int nqc, int nn, const double *xe, const double *we,
-                            double *B1, double *R0, double *dR, double *qs) {
-    const int tid = threadIdx.x, nth = blockDim.x;
-    const int p0 = pd[0], p1 = pd[1], p2 = pd[2];
-    // A1: 1-D B-spline values and derivatives, one thread per (point, dir)
-    for (int t = tid; t < 3 * nqc; t += nth) {
-        const int ql = t / 3, d = t - 3 * ql;
-        const double tq = gauss[4 * (q0 + ql) + 1 + d];
-        const double xi = ((su2[d] - su1[d]) * tq + (su2[d] + su1[d])) * 0.5;
-        double *f = B1 + ((size_t)ql * 6 + 2 * d) * kMaxDeg1;
-        bspline_ders(sni[d], pd[d], xi, Ud[d], f, f + kMaxDeg1);
-    }
-    __syncthreads();
-    // A2: the four numerator products of every (point, node)
-    for (int t = tid; t < nqc * nn; t += nth) {
-        const int ql = t / nn, n = t - ql * nn;
-        const int i = n % (p0 + 1), j = (n / (p0 + 1)) % (p1 + 1), k = n / ((p0 + 1) * (p1 + 1));
-        const double *f = B1 + (size_t)ql * 6 * kMaxDeg1;
-        const double FN = f[p0 - i], dFN = f[kMaxDeg1 + p0 - i];
-        const double FM = f[2 * kMaxDeg1 + p1 - j], dFM = f[3 * kMaxDeg1 + p1 - j];
-        const double FL = f[4 * kMaxDeg1 + p2 - k], dFL = f[5 * kMaxDeg1 + p2 - k];
-        const double wa = we[n];
-        R0[(size_t)ql * nn + n] = FN * FM * FL * wa;
-        double *d = dR + ((size_t)ql * nn + n) * 3;
-        d[0] = dFN * FM * FL * wa;
-        d[1] = FN * dFM * FL * wa;
-        d[2] = FN * FM * dFL * wa;
-    }
-    __syncthreads();
-    // A3: the sums over the nodes (one thread per (point, sum), node order)
-    for (int t = tid; t < 4 * nqc; t += nth) {
-        const int ql = t >> 2, c = t & 3;
-        double acc = 0.0;
-        if (c == 0) {
-            const double *r = R0 + (size_t)ql * nn;
-            for (int n = 0; n < nn; n++) acc += r[n];
-            qs[(size_t)ql * kStiffQS + 3] = 1.0 / acc;
-        } else {
-            const double *d = dR + (size_t)ql * nn * 3 + (c - 1);
-            for (int n = 0; n < nn; n++) acc += d[3 * n];
-            qs[(size_t)ql * kStiffQS + c - 1] = acc;
-        }
-    }
-    __syncthreads();
-    // A4: rational derivatives dR/dxi, one thread per (point, node)
-    for (int t = tid; t < nqc * nn; t += nth) {
-        const int ql = t / nn, n = t - ql * nn;
-        const double *sq = qs + (size_t)ql * kStiffQS;
-        const double inv = sq[3];
-        const double R = R0[(size_t)ql * nn + n] * inv;
-        double *d = dR + ((size_t)ql * nn + n) * 3;
-        d[0] = (d[0] - R * sq[0]) * inv;
-        d[1] = (d[1] - R * sq[1]) * inv;
-        d[2] = (d[2] - R * sq[2]) * inv;
-    }
-    __syncthreads();
-    // A5: dx/dxi, one thread per (point, entry), node order
-    for (int t = tid; t < 9 * nqc; t += nth) {
-        const int ql = t / 9, rc = t - 9 * ql, r = rc / 3, c = rc - 3 * r;
-        const double *d = dR + (size_t)ql * nn * 3 + c;
-        double acc = 0.0;
-        for (int n = 0; n < nn; n++) acc += xe[3 * n + r] * d[3 * n];
-        qs[(size_t)ql * kStiffQS + 4 + rc] = acc;
-    }
-    __syncthreads();
 }
 
 __global__ void __launch_bounds__(256)
@@ -481,7 +406,7 @@ k_u1_stiffness(StiffArgs a) {
         const int nqc = min(a.qchunk, a.nq - q0);
         __syncthreads();
         // ---- stage A: basis derivatives at the chunk's Gauss points
-        basis_chunk(pd, Ud, sni, su1, su2, a.gauss, q0, nqc, nn, xe, we, B1, R0, dR, qs);
+        basis_chunk(pd, Ud, sni, su1, su2, a.gauss, q0, nqc, nn, xe, we, B1, R0, nn, dR, 3 * nn, qs);
         // A6: inverse Jacobian and the point's weight
         for (int ql = tid; ql < nqc; ql += nth) {
             double *sq = qs + (size_t)ql * kStiffQS;
@@ -617,7 +542,7 @@ __global__ void __launch_bounds__(256) k_u1_mass(MassArgs a) {
         const int nqc = min(a.qchunk, a.nq - q0);
         __syncthreads();
         // ---- stage A: basis values and dvol at the chunk's Gauss points
-        basis_chunk(pd, Ud, sni, su1, su2, a.gauss, q0, nqc, nn, xe, we, B1, Rq, dR, qs);
+        basis_chunk(pd, Ud, sni, su1, su2, a.gauss, q0, nqc, nn, xe, we, B1, Rq, nn, dR, 3 * nn, qs);
         for (int t = tid; t < nqc * nn; t += blockDim.x) {
             const int ql = t / nn;
             Rq[t] = Rq[t] * qs[(size_t)ql * kStiffQS + 3];

@@ -117,6 +117,25 @@ __host__ __device__ inline PtLayout pt_layout(int nn, int nadj, int nbody) {
     return L;
 }
 
+// Shared memory of one element: xe, ue, uae, we, then nq point records of
+// PtLayout, then the basis scratch (kBasisB1 + kStiffQS per point) and the
+// external-work accumulators of the (control point, component) tasks.
+__host__ __device__ inline size_t grad_smem_doubles(int nn, int nq, int nadj, const PtLayout &L,
+                                                    size_t face) {
+    const size_t vol = (size_t)nq * L.size;
+    return (size_t)(6 + 3 * nadj) * nn + nn + (vol > face ? vol : face) +
+           (size_t)nq * (kBasisB1 + kStiffQS) + (size_t)3 * nn * nadj;
+}
+
+// gradUELMAT1adj (gradUELMAT_solid.f90:18-479) of one element per CTA.
+// Stage A evaluates the basis and the point quantities: the products of
+// every (point, node) in parallel (basis_chunk), every sum over the nodes as
+// one thread's loop in node order, then the per-point tensors (one thread
+// per point).  Stage B runs one task per (control point, component c): every
+// quantity the reference indexes by c -- dJ, the strain variations, dAAI,
+// dAAE, dC and the accumulated gradient -- depends on that component alone,
+// so each task performs exactly the operations the reference performs for
+// its component, in the same order, and the results keep their bits.
 __global__ void __launch_bounds__(256) k_u1_grad(GradArgs a) {
     extern __shared__ double sm[];
     const int nn = a.nn, nadj = a.nadj;
@@ -129,9 +148,9 @@ __global__ void __launch_bounds__(256) k_u1_grad(GradArgs a) {
     __shared__ double su1[3], su2[3];
     __shared__ int sni[3];
     __shared__ int s_body[8], s_nbody;
-    const int tid = threadIdx.x;
+    const int tid = threadIdx.x, nth = blockDim.x;
     const int32_t *ien = a.ien + (size_t)e * nn;
-    for (int i = tid; i < nn; i += blockDim.x) {
+    for (int i = tid; i < nn; i += nth) {
         const int cp = ien[i];
         for (int c = 0; c < 3; c++) {
             xe[3 * i + c] = a.coords[3 * cp + c];
@@ -158,23 +177,52 @@ __global__ void __launch_bounds__(256) k_u1_grad(GradArgs a) {
     __syncthreads();
     const int nbody = s_nbody;
     const PtLayout L = pt_layout(nn, nadj, nbody);
+    const size_t face = (size_t)a.ng * a.ng * (4 * nn + 11 + 3 * nadj);
+    const size_t vol = (size_t)a.nq * L.size;
+    double *B1 = pts + (vol > face ? vol : face);
+    double *qs = B1 + (size_t)a.nq * kBasisB1;
+    double *ge_s = qs + (size_t)a.nq * kStiffQS;
     const double lambda = a.E * a.nu / (1.0 + a.nu) / (1.0 - 2.0 * a.nu);
     const double mu = a.E / 2.0 / (1.0 + a.nu);
     // ---------------- stage A: per volume point
-    for (int q = tid; q < a.nq; q += blockDim.x) {
+    {
+        const int pd[3] = {a.p0, a.p1, a.p2};
+        const double *Ud[3] = {a.U0, a.U1, a.U2};
+        // R numerators and dR/dxi into the point records, dx/dxi into qs
+        basis_chunk(pd, Ud, sni, su1, su2, a.gauss, 0, a.nq, nn, xe, we, B1, pts + L.R, L.size,
+                    pts + L.dR, L.size, qs);
+    }
+    for (int t = tid; t < a.nq * nn; t += nth) {
+        const int q = t / nn, n = t - q * nn;
+        double *R = pts + (size_t)q * L.size + L.R;
+        R[n] = R[n] * qs[(size_t)q * kStiffQS + 3];
+    }
+    if (a.compute_int) {
+        // the gradients of the state and of the adjoints: ordered sums over
+        // the nodes, one thread per (point, entry)
+        const int ns = 9 * (1 + nadj);
+        for (int t = tid; t < a.nq * ns; t += nth) {
+            const int q = t / ns, s = t - q * ns;
+            double *P = pts + (size_t)q * L.size;
+            const double *dR = P + L.dR;
+            const int k = s / 9 - 1, ic = s % 9, i = ic / 3, c = ic % 3;
+            const double *v = k < 0 ? ue : uae + 3 * nn * k;
+            double acc = 0.0;
+            for (int cp = 0; cp < nn; cp++) acc = acc + dR[3 * cp + i] * v[3 * cp + c];
+            if (k < 0) P[L.dU + ic] = acc;
+            else P[L.dUA + 9 * k + ic] = acc;
+        }
+    }
+    __syncthreads();
+    for (int q = tid; q < a.nq; q += nth) {
         double *P = pts + (size_t)q * L.size;
         const double *g = a.gauss + 4 * q;
-        double xi[3], detJac = g[0];
-        for (int i = 0; i < 3; i++) {
-            xi[i] = ((su2[i] - su1[i]) * g[1 + i] + (su2[i] + su1[i])) * 0.5;
-            detJac = detJac * 0.5 * (su2[i] - su1[i]);
-        }
-        double *R = P + L.R, *dR = P + L.dR;
-        eval_nurbs(a, sni, xi, we, R, dR);
-        double AI[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+        double detJac = g[0];
+        for (int i = 0; i < 3; i++) detJac = detJac * 0.5 * (su2[i] - su1[i]);
+        const double *R = P + L.R;
+        double AI[3][3];
         for (int i = 0; i < 3; i++)
-            for (int cp = 0; cp < nn; cp++)
-                for (int c = 0; c < 3; c++) AI[i][c] = AI[i][c] + dR[3 * cp + i] * xe[3 * cp + c];
+            for (int c = 0; c < 3; c++) AI[i][c] = qs[(size_t)q * kStiffQS + 4 + 3 * c + i];
         double AxA[3][3];
         gcross(AI[0], AI[1], AxA[2]);
         const double Area = gdot(AxA[2], AI[2]);
@@ -203,10 +251,9 @@ __global__ void __launch_bounds__(256) k_u1_grad(GradArgs a) {
             }
             for (int kl = 1; kl < 6; kl++)
                 for (int r = kl; r < 6; r++) H[r][kl - 1] = H[kl - 1][r];
-            double dU[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+            double dU[3][3];
             for (int i = 0; i < 3; i++)
-                for (int cp = 0; cp < nn; cp++)
-                    for (int c = 0; c < 3; c++) dU[i][c] = dU[i][c] + dR[3 * cp + i] * ue[3 * cp + c];
+                for (int c = 0; c < 3; c++) dU[i][c] = P[L.dU + 3 * i + c];
             double strain[6], stress[6];
             for (int ij = 0; ij < 6; ij++) {
                 const int i = c_vi[ij], j = c_vj[ij];
@@ -219,20 +266,15 @@ __global__ void __launch_bounds__(256) k_u1_grad(GradArgs a) {
                 stress[ii] = s;
             }
             for (int i = 0; i < 3; i++)
-                for (int c = 0; c < 3; c++) {
-                    P[L.AAE + 3 * i + c] = AAE[i][c];
-                    P[L.dU + 3 * i + c] = dU[i][c];
-                }
+                for (int c = 0; c < 3; c++) P[L.AAE + 3 * i + c] = AAE[i][c];
             for (int ij = 0; ij < 6; ij++) {
                 P[L.strain + ij] = strain[ij];
                 P[L.stress + ij] = stress[ij];
             }
             for (int k = 0; k < nadj; k++) {
-                double dA[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+                double dA[3][3];
                 for (int i = 0; i < 3; i++)
-                    for (int cp = 0; cp < nn; cp++)
-                        for (int c = 0; c < 3; c++)
-                            dA[i][c] = dA[i][c] + dR[3 * cp + i] * uae[3 * cp + c + 3 * nn * k];
+                    for (int c = 0; c < 3; c++) dA[i][c] = P[L.dUA + 9 * k + 3 * i + c];
                 double sA[6], tA[6];
                 for (int ij = 0; ij < 6; ij++) {
                     const int i = c_vi[ij], j = c_vj[ij];
@@ -244,8 +286,6 @@ __global__ void __launch_bounds__(256) k_u1_grad(GradArgs a) {
                     for (int jj = 0; jj < 6; jj++) s = s + H[ii][jj] * sA[jj];
                     tA[ii] = s;
                 }
-                for (int i = 0; i < 3; i++)
-                    for (int c = 0; c < 3; c++) P[L.dUA + 9 * k + 3 * i + c] = dA[i][c];
                 for (int ij = 0; ij < 6; ij++) {
                     P[L.sA + 6 * k + ij] = sA[ij];
                     P[L.tA + 6 * k + ij] = tA[ij];
@@ -288,12 +328,11 @@ __global__ void __launch_bounds__(256) k_u1_grad(GradArgs a) {
         }
     }
     __syncthreads();
-    // ---------------- stage B: one thread per control point
-    double gi[3 * kGradMaxAdj], ge[3 * kGradMaxAdj];
-    const int cp = tid;
-    const bool mine = cp < nn;
-    for (int i = 0; i < 3 * kGradMaxAdj; i++) gi[i] = ge[i] = 0.0;
-    if (mine) {
+    // ---------------- stage B: one task per (control point, component)
+    for (int task = tid; task < 3 * nn; task += nth) {
+        const int cp = task / 3, c = task - 3 * cp;
+        double gi[kGradMaxAdj], ge[kGradMaxAdj];
+        for (int k = 0; k < kGradMaxAdj; k++) gi[k] = ge[k] = 0.0;
         for (int q = 0; q < a.nq; q++) {
             const double *P = pts + (size_t)q * L.size;
             const double *dr = P + L.dR + 3 * cp;
@@ -302,93 +341,81 @@ __global__ void __launch_bounds__(256) k_u1_grad(GradArgs a) {
             if (a.compute_int) {
                 const double *AI = P + L.AI, *AAE = P + L.AAE;
                 const double *stress = P + L.stress, *strain = P + L.strain, *dU = P + L.dU;
-                double dJ[3] = {0, 0, 0};
-                for (int i = 0; i < 3; i++)
-                    for (int c = 0; c < 3; c++) dJ[c] = dJ[c] + AxA[3 * i + c] * dr[i];
-                for (int k = 0; k < nadj; k++)
-                    for (int c = 0; c < 3; c++) gi[3 * k + c] = gi[3 * k + c] - P[L.work + k] * dJ[c] * detJac;
+                double dJ = 0.0;
+                for (int i = 0; i < 3; i++) dJ = dJ + AxA[3 * i + c] * dr[i];
+                for (int k = 0; k < nadj; k++) gi[k] = gi[k] - P[L.work + k] * dJ * detJac;
                 for (int k = 0; k < nadj; k++) {
                     const double *d = P + L.dUA + 9 * k;
-                    double ev[3] = {0, 0, 0};
+                    double ev = 0.0;
                     for (int ij = 0; ij < 6; ij++) {
                         const int i = c_vi[ij], j = c_vj[ij];
-                        for (int c = 0; c < 3; c++) {
-                            if (i == j) ev[c] = ev[c] + stress[ij] * d[3 * i + c] * dr[i];
-                            else ev[c] = ev[c] + stress[ij] * d[3 * i + c] * dr[j] + stress[ij] * d[3 * j + c] * dr[i];
-                        }
+                        if (i == j) ev = ev + stress[ij] * d[3 * i + c] * dr[i];
+                        else ev = ev + stress[ij] * d[3 * i + c] * dr[j] + stress[ij] * d[3 * j + c] * dr[i];
                     }
-                    for (int c = 0; c < 3; c++) gi[3 * k + c] = gi[3 * k + c] - ev[c] * Area * detJac;
+                    gi[k] = gi[k] - ev * Area * detJac;
                 }
-                double dAAI[3][3][3], dAAE[3][3][3];
+                double dAAI[3][3], dAAE[3][3];
                 for (int j = 0; j < 3; j++)
-                    for (int i = 0; i < 3; i++)
-                        for (int c = 0; c < 3; c++)
-                            dAAI[i][j][c] = dr[i] * AI[3 * j + c] + AI[3 * i + c] * dr[j];
+                    for (int i = 0; i < 3; i++) dAAI[i][j] = dr[i] * AI[3 * j + c] + AI[3 * i + c] * dr[j];
                 for (int i = 0; i < 3; i++)
-                    for (int j = 0; j < 3; j++)
-                        for (int c = 0; c < 3; c++) dAAE[i][j][c] = 0.0;
+                    for (int j = 0; j < 3; j++) dAAE[i][j] = 0.0;
                 for (int j = 0; j < 3; j++)
                     for (int i = 0; i < 3; i++)
                         for (int l = 0; l < 3; l++)
                             for (int k = 0; k < 3; k++)
-                                for (int c = 0; c < 3; c++)
-                                    dAAE[i][j][c] = dAAE[i][j][c] - AAE[3 * i + k] * AAE[3 * l + j] * dAAI[k][l][c];
-                double vA[3 * kGradMaxAdj];
+                                dAAE[i][j] = dAAE[i][j] - AAE[3 * i + k] * AAE[3 * l + j] * dAAI[k][l];
+                double vA[kGradMaxAdj];
                 for (int k = 0; k < nadj; k++) {
                     const double *tA = P + L.tA + 6 * k;
-                    double ev[3] = {0, 0, 0};
+                    double ev = 0.0;
                     for (int ij = 0; ij < 6; ij++) {
                         const int i = c_vi[ij], j = c_vj[ij];
-                        for (int c = 0; c < 3; c++) {
-                            if (i == j) ev[c] = ev[c] + tA[ij] * dU[3 * i + c] * dr[i];
-                            else ev[c] = ev[c] + tA[ij] * dU[3 * i + c] * dr[j] + tA[ij] * dU[3 * j + c] * dr[i];
-                        }
+                        if (i == j) ev = ev + tA[ij] * dU[3 * i + c] * dr[i];
+                        else ev = ev + tA[ij] * dU[3 * i + c] * dr[j] + tA[ij] * dU[3 * j + c] * dr[i];
                     }
-                    for (int c = 0; c < 3; c++) vA[3 * k + c] = ev[c];
+                    vA[k] = ev;
                 }
                 for (int kl = 0; kl < 6; kl++) {
                     const int k = c_vi[kl], l = c_vj[kl];
                     for (int ij = 0; ij < 6; ij++) {
                         const int i = c_vi[ij], j = c_vj[ij];
-                        double dC[3];
-                        for (int c = 0; c < 3; c++)
-                            dC[c] = lambda * dAAE[i][j][c] * AAE[3 * k + l] + lambda * AAE[3 * i + j] * dAAE[k][l][c] +
-                                    mu * dAAE[i][k][c] * AAE[3 * j + l] + mu * AAE[3 * i + k] * dAAE[j][l][c] +
-                                    mu * dAAE[i][l][c] * AAE[3 * j + k] + mu * AAE[3 * i + l] * dAAE[j][k][c];
+                        const double dC =
+                            lambda * dAAE[i][j] * AAE[3 * k + l] + lambda * AAE[3 * i + j] * dAAE[k][l] +
+                            mu * dAAE[i][k] * AAE[3 * j + l] + mu * AAE[3 * i + k] * dAAE[j][l] +
+                            mu * dAAE[i][l] * AAE[3 * j + k] + mu * AAE[3 * i + l] * dAAE[j][k];
                         for (int kk = 0; kk < nadj; kk++)
-                            for (int c = 0; c < 3; c++)
-                                vA[3 * kk + c] = vA[3 * kk + c] + dC[c] * strain[ij] * P[L.sA + 6 * kk + kl];
+                            vA[kk] = vA[kk] + dC * strain[ij] * P[L.sA + 6 * kk + kl];
                     }
                 }
-                for (int k = 0; k < nadj; k++)
-                    for (int c = 0; c < 3; c++) gi[3 * k + c] = gi[3 * k + c] - vA[3 * k + c] * Area * detJac;
+                for (int k = 0; k < nadj; k++) gi[k] = gi[k] - vA[k] * Area * detJac;
             }
             if (a.compute_ext) {
                 for (int b = 0; b < nbody; b++) {
                     const double *lf = P + L.body + 6 * b, *vd = lf + 3;
                     const int nl = s_body[b];
-                    double dJ[3] = {0, 0, 0};
-                    for (int i = 0; i < 3; i++)
-                        for (int c = 0; c < 3; c++) dJ[c] = dJ[c] + AxA[3 * i + c] * dr[i];
+                    double dJ = 0.0;
+                    for (int i = 0; i < 3; i++) dJ = dJ + AxA[3 * i + c] * dr[i];
                     for (int k = 0; k < nadj; k++) {
                         const double sf = gdot(lf, P + L.vA + 3 * k);
-                        for (int c = 0; c < 3; c++) ge[3 * k + c] = ge[3 * k + c] + sf * dJ[c] * detJac;
+                        ge[k] = ge[k] + sf * dJ * detJac;
                     }
                     for (int k = 0; k < nadj; k++) {
                         const double *ua = P + L.vA + 3 * k;
-                        double df[3] = {0, 0, 0};
-                        for (int id = 0; id < 3; id++)
-                            for (int jd = 0; jd < 3; jd++) {
-                                if (id == jd) df[jd] = df[jd] + ua[id] * (1.0 - vd[id] * vd[jd]);
-                                else df[jd] = df[jd] - ua[id] * (vd[id] * vd[jd]);
-                            }
-                        for (int c = 0; c < 3; c++) {
-                            df[c] = df[c] * (a.rho * (a.adlmag[nl] * a.adlmag[nl]) * P[L.R + cp]);
-                            ge[3 * k + c] = ge[3 * k + c] + df[c] * Area * detJac;
+                        double df = 0.0;
+                        for (int id = 0; id < 3; id++) {
+                            if (id == c) df = df + ua[id] * (1.0 - vd[id] * vd[c]);
+                            else df = df - ua[id] * (vd[id] * vd[c]);
                         }
+                        df = df * (a.rho * (a.adlmag[nl] * a.adlmag[nl]) * P[L.R + cp]);
+                        ge[k] = ge[k] + df * Area * detJac;
                     }
                 }
             }
+        }
+        double *oi = a.egi + (size_t)blockIdx.x * nadj * 3 * nn;
+        for (int k = 0; k < nadj; k++) {
+            oi[k + nadj * (c + 3 * cp)] = gi[k];
+            ge_s[task * nadj + k] = ge[k];
         }
     }
     // ---------------- surface loads (not in the reference)
@@ -402,7 +429,7 @@ __global__ void __launch_bounds__(256) k_u1_grad(GradArgs a) {
             // per face point: R (nn), dR (3nn), AJ (9), fmag, w, vA (3nadj)
             const int fs = 4 * nn + 11 + 3 * nadj;
             __syncthreads();
-            for (int q = tid; q < nf; q += blockDim.x) {
+            for (int q = tid; q < nf; q += nth) {
                 double *P = pts + (size_t)q * fs;
                 const double *g = a.gface + ((size_t)(face - 1) * nf + q) * 4;
                 double xi[3], h[3];
@@ -435,16 +462,19 @@ __global__ void __launch_bounds__(256) k_u1_grad(GradArgs a) {
                     }
             }
             __syncthreads();
-            if (mine) {
-                int ia, ib, ip, iq;
-                switch (face) { case 1: case 2: ia = 1; ib = 2; break; case 3: case 4: ia = 2; ib = 0; break; default: ia = 0; ib = 1; }
-                switch (face) {
-                    case 1: ip = 1; iq = 2; break; case 2: ip = 2; iq = 1; break;
-                    case 3: ip = 2; iq = 0; break; case 4: ip = 0; iq = 2; break;
-                    case 5: ip = 0; iq = 1; break; default: ip = 1; iq = 0; break;
-                }
-                double h[3];
-                for (int i = 0; i < 3; i++) h[i] = 0.5 * (su2[i] - su1[i]);
+            int ia, ib, ip, iq;
+            switch (face) { case 1: case 2: ia = 1; ib = 2; break; case 3: case 4: ia = 2; ib = 0; break; default: ia = 0; ib = 1; }
+            switch (face) {
+                case 1: ip = 1; iq = 2; break; case 2: ip = 2; iq = 1; break;
+                case 3: ip = 2; iq = 0; break; case 4: ip = 0; iq = 2; break;
+                case 5: ip = 0; iq = 1; break; default: ip = 1; iq = 0; break;
+            }
+            double h[3];
+            for (int i = 0; i < 3; i++) h[i] = 0.5 * (su2[i] - su1[i]);
+            for (int task = tid; task < 3 * nn; task += nth) {
+                const int cp = task / 3, c = task - 3 * cp;
+                double ge[kGradMaxAdj];
+                for (int k = 0; k < nadj; k++) ge[k] = ge_s[task * nadj + k];
                 for (int q = 0; q < nf; q++) {
                     const double *P = pts + (size_t)q * fs;
                     const double *dR = P + nn;
@@ -452,38 +482,36 @@ __global__ void __launch_bounds__(256) k_u1_grad(GradArgs a) {
                     const double fmag = P[4 * nn + 9], wq = P[4 * nn + 10];
                     for (int k = 0; k < nadj; k++) {
                         const double *ua = P + 4 * nn + 11 + 3 * k;
-                        double gg[3];
+                        double gg;
                         if (type == 0 || type == 4) {
                             const double cP = dR[3 * cp + ip] * h[ip], cQ = dR[3 * cp + iq] * h[iq];
                             double QxU[3], UxP[3];
                             gcross(AJ + 3 * iq, ua, QxU);
                             gcross(ua, AJ + 3 * ip, UxP);
-                            for (int c = 0; c < 3; c++) gg[c] = cP * QxU[c] + cQ * UxP[c];
+                            gg = cP * QxU[c] + cQ * UxP[c];
                         } else {
                             double n[3];
                             gcross(AJ + 3 * ia, AJ + 3 * ib, n);
                             const double nr = sqrt(n[0] * n[0] + n[1] * n[1] + n[2] * n[2]);
-                            for (int c = 0; c < 3; c++) n[c] = n[c] / nr;
+                            for (int cc = 0; cc < 3; cc++) n[cc] = n[cc] / nr;
                             const double cA = dR[3 * cp + ia] * h[ia], cB = dR[3 * cp + ib] * h[ib];
                             double Bxn[3], nxA[3];
                             gcross(AJ + 3 * ib, n, Bxn);
                             gcross(n, AJ + 3 * ia, nxA);
-                            for (int c = 0; c < 3; c++) gg[c] = ua[type - 1] * (cA * Bxn[c] + cB * nxA[c]);
+                            gg = ua[type - 1] * (cA * Bxn[c] + cB * nxA[c]);
                         }
-                        for (int c = 0; c < 3; c++) ge[3 * k + c] = ge[3 * k + c] + gg[c] * wq * fmag;
+                        ge[k] = ge[k] + gg * wq * fmag;
                     }
                 }
+                for (int k = 0; k < nadj; k++) ge_s[task * nadj + k] = ge[k];
             }
         }
     }
-    if (mine) {
-        double *oi = a.egi + (size_t)blockIdx.x * nadj * 3 * nn;
-        double *oe = a.ege + (size_t)blockIdx.x * nadj * 3 * nn;
-        for (int k = 0; k < nadj; k++)
-            for (int c = 0; c < 3; c++) {
-                oi[k + nadj * (c + 3 * cp)] = gi[3 * k + c];
-                oe[k + nadj * (c + 3 * cp)] = ge[3 * k + c];
-            }
+    __syncthreads();
+    double *oe = a.ege + (size_t)blockIdx.x * nadj * 3 * nn;
+    for (int task = tid; task < 3 * nn; task += nth) {
+        const int cp = task / 3, c = task - 3 * cp;
+        for (int k = 0; k < nadj; k++) oe[k + nadj * (c + 3 * cp)] = ge_s[task * nadj + k];
     }
 }
 
@@ -645,7 +673,7 @@ YETI_API int yeti_grad_lin_elast_work(yeti_ctx *ctx, const yeti_u1_model *m,
         const PtLayout L = pt_layout(P.nn, (int)nadj, max_body);
         const size_t vol = (size_t)P.nq * L.size;
         const size_t face = (size_t)P.ng * P.ng * (4 * P.nn + 11 + 3 * nadj);
-        const size_t smem = sizeof(double) * ((size_t)(6 + 3 * nadj) * P.nn + P.nn + std::max(vol, face));
+        const size_t smem = sizeof(double) * grad_smem_doubles(P.nn, P.nq, (int)nadj, L, face);
         YETI_CHECK(smem <= (size_t)smem_optin, YETI_EUNSUPPORTED,
                    "shape gradient: element needs %zu bytes of shared memory", smem);
         YETI_TRY(set_smem_optin((const void *)k_u1_grad, ctx->device, smem, "shape gradient element"));

@@ -86,6 +86,87 @@ __device__ inline void nurbs_eval_elem(int p0, int p1, int p2, const double *U0,
     }
 }
 
+constexpr int kStiffQS = 16;              // scalars per point of basis_chunk
+constexpr int kBasisB1 = 6 * kMaxDeg1;    // 1-D rows per point of basis_chunk
+
+// Stage A of the Gauss kernels for a chunk of points q0..q0+nqc-1
+// (shap.f90:75-178, evalnurbs, evaluatenurbsfcts.f:94-209): the 1-D B-spline
+// rows (B1, kBasisB1 per point), the rational numerators R0[ql rs + n] and
+// dR/dxi at dR[ql ds + 3 n + c] of every (point, node), the per-point sums
+// of the derivative numerators (qs[0..2]), 1/S (qs[3]) and dx/dxi
+// (qs[4 + 3 r + c]), kStiffQS scalars per point.  The products of every (point, node) are formed in
+// parallel; each sum over the nodes stays one thread's loop in node order,
+// so the values are those of the point-serial evaluation bit for bit.
+__device__ inline void basis_chunk(const int pd[3], const double *const Ud[3], const int *sni,
+                                   const double *su1, const double *su2, const double *gauss,
+                                   int q0, int nqc, int nn, const double *xe, const double *we,
+                                   double *B1, double *R0, int rs, double *dR, int ds,
+                                   double *qs) {
+    const int tid = threadIdx.x, nth = blockDim.x;
+    const int p0 = pd[0], p1 = pd[1], p2 = pd[2];
+    // A1: 1-D B-spline values and derivatives, one thread per (point, dir)
+    for (int t = tid; t < 3 * nqc; t += nth) {
+        const int ql = t / 3, d = t - 3 * ql;
+        const double tq = gauss[4 * (q0 + ql) + 1 + d];
+        const double xi = ((su2[d] - su1[d]) * tq + (su2[d] + su1[d])) * 0.5;
+        double *f = B1 + ((size_t)ql * 6 + 2 * d) * kMaxDeg1;
+        bspline_ders(sni[d], pd[d], xi, Ud[d], f, f + kMaxDeg1);
+    }
+    __syncthreads();
+    // A2: the four numerator products of every (point, node)
+    for (int t = tid; t < nqc * nn; t += nth) {
+        const int ql = t / nn, n = t - ql * nn;
+        const int i = n % (p0 + 1), j = (n / (p0 + 1)) % (p1 + 1), k = n / ((p0 + 1) * (p1 + 1));
+        const double *f = B1 + (size_t)ql * 6 * kMaxDeg1;
+        const double FN = f[p0 - i], dFN = f[kMaxDeg1 + p0 - i];
+        const double FM = f[2 * kMaxDeg1 + p1 - j], dFM = f[3 * kMaxDeg1 + p1 - j];
+        const double FL = f[4 * kMaxDeg1 + p2 - k], dFL = f[5 * kMaxDeg1 + p2 - k];
+        const double wa = we[n];
+        R0[(size_t)ql * rs + n] = FN * FM * FL * wa;
+        double *d = dR + (size_t)ql * ds + 3 * n;
+        d[0] = dFN * FM * FL * wa;
+        d[1] = FN * dFM * FL * wa;
+        d[2] = FN * FM * dFL * wa;
+    }
+    __syncthreads();
+    // A3: the sums over the nodes (one thread per (point, sum), node order)
+    for (int t = tid; t < 4 * nqc; t += nth) {
+        const int ql = t >> 2, c = t & 3;
+        double acc = 0.0;
+        if (c == 0) {
+            const double *r = R0 + (size_t)ql * rs;
+            for (int n = 0; n < nn; n++) acc += r[n];
+            qs[(size_t)ql * kStiffQS + 3] = 1.0 / acc;
+        } else {
+            const double *d = dR + (size_t)ql * ds + (c - 1);
+            for (int n = 0; n < nn; n++) acc += d[3 * n];
+            qs[(size_t)ql * kStiffQS + c - 1] = acc;
+        }
+    }
+    __syncthreads();
+    // A4: rational derivatives dR/dxi, one thread per (point, node)
+    for (int t = tid; t < nqc * nn; t += nth) {
+        const int ql = t / nn, n = t - ql * nn;
+        const double *sq = qs + (size_t)ql * kStiffQS;
+        const double inv = sq[3];
+        const double R = R0[(size_t)ql * rs + n] * inv;
+        double *d = dR + (size_t)ql * ds + 3 * n;
+        d[0] = (d[0] - R * sq[0]) * inv;
+        d[1] = (d[1] - R * sq[1]) * inv;
+        d[2] = (d[2] - R * sq[2]) * inv;
+    }
+    __syncthreads();
+    // A5: dx/dxi, one thread per (point, entry), node order
+    for (int t = tid; t < 9 * nqc; t += nth) {
+        const int ql = t / 9, rc = t - 9 * ql, r = rc / 3, c = rc - 3 * r;
+        const double *d = dR + (size_t)ql * ds + c;
+        double acc = 0.0;
+        for (int n = 0; n < nn; n++) acc += xe[3 * n + r] * d[3 * n];
+        qs[(size_t)ql * kStiffQS + 4 + rc] = acc;
+    }
+    __syncthreads();
+}
+
 // Gauss-Legendre nodes/weights of order n on [-1, 1] (ascending): roots of
 // the Legendre polynomial P_n by Newton iteration on its recurrence.
 void gauss_legendre_host(int n, double *x, double *w);

@@ -27,7 +27,9 @@
 // vectors (a few MB) stay in L2 between passes.
 #include <algorithm>
 #include <cmath>
+#include <deque>
 #include <map>
+#include <mutex>
 #include <tuple>
 #include <vector>
 
@@ -824,6 +826,13 @@ int wq_fd_prepare(yeti_wq_op *op, int variant, bool f32) {
     struct Eig {
         std::vector<double> lam, U, kd, md;
     };
+    // unweighted eigenpairs depend on (p, nel, lo, hi) only: operators set
+    // up back to back (the serving loop's) share them through a bounded
+    // process-wide cache; 'TD' ones are the operator's own
+    static std::mutex g_eig_mtx;
+    static std::map<std::tuple<int, int, int, int>, Eig> g_eig;
+    static std::deque<std::tuple<int, int, int, int>> g_eig_order;
+    constexpr size_t kEigCacheEntries = 512;
     std::map<std::tuple<int, int, int, int, int>, Eig> cache;
     Eig *E[3][3];
     for (int c = 0; c < 3; c++)
@@ -832,6 +841,11 @@ int wq_fd_prepare(yeti_wq_op *op, int variant, bool f32) {
             // 'TD' weights differ per component: no sharing between components
             auto key = std::make_tuple(op->p[d], op->nel[d], lo, hi, td ? 3 * c + d : -1);
             auto it = cache.find(key);
+            if (it == cache.end() && !td) {
+                std::lock_guard<std::mutex> lock(g_eig_mtx);
+                auto g = g_eig.find(std::make_tuple(op->p[d], op->nel[d], lo, hi));
+                if (g != g_eig.end()) it = cache.emplace(key, g->second).first;
+            }
             if (it == cache.end()) {
                 Eig e;
                 std::vector<double> K, M;
@@ -848,6 +862,17 @@ int wq_fd_prepare(yeti_wq_op *op, int variant, bool f32) {
                 }
                 YETI_CHECK(gen_eig(m, K, M, e.lam, e.U), YETI_ENUMERIC,
                            "fast diagonalisation: eigen decomposition failed (direction %d)", d);
+                if (!td) {
+                    std::lock_guard<std::mutex> lock(g_eig_mtx);
+                    const auto gk = std::make_tuple(op->p[d], op->nel[d], lo, hi);
+                    if (g_eig.emplace(gk, e).second) {
+                        g_eig_order.push_back(gk);
+                        if (g_eig_order.size() > kEigCacheEntries) {
+                            g_eig.erase(g_eig_order.front());
+                            g_eig_order.pop_front();
+                        }
+                    }
+                }
                 it = cache.emplace(key, std::move(e)).first;
             }
             E[c][d] = &it->second;

@@ -85,12 +85,12 @@ __device__ __forceinline__ void load_band2(const float2 *p, float2 (&w)[P + 1]) 
     for (int m = 0; m <= P; m++) w[m] = t[m];
 }
 
-// Streamed coefficient pair: read once, not kept in L1.
+// Streamed coefficient pair: read once, not kept in L1.  Not volatile: the
+// values are used, and the compiler may then issue the loads of a point
+// ahead of the products that consume them.
 __device__ __forceinline__ float2 ld_stream(const float2 *p) {
     float2 v;
-    asm volatile("ld.global.nc.L1::no_allocate.v2.f32 {%0, %1}, [%2];"
-                 : "=f"(v.x), "=f"(v.y)
-                 : "l"(p));
+    asm("ld.global.nc.L1::no_allocate.v2.f32 {%0, %1}, [%2];" : "=f"(v.x), "=f"(v.y) : "l"(p));
     return v;
 }
 

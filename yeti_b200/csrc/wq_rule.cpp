@@ -16,6 +16,10 @@
 // when underdetermined (the dgels/dgesv split of algebra.f90:87-167).
 #include <algorithm>
 #include <cmath>
+#include <deque>
+#include <map>
+#include <mutex>
+#include <utility>
 #include <vector>
 
 #include "wq_rule.h"
@@ -327,7 +331,7 @@ static void wq_rule_generalized(int p, int nel, WQRule1D &R) {
     rules(nfun1, nfun, nqp, B0w1, product_awb(B0c1, nfun1, B1c, nfun), I1, b0lo, b0hi, R.W11);
 }
 
-int wq_rule_1d(int p, int nel, WQRule1D &R) {
+static int wq_rule_1d_compute(int p, int nel, WQRule1D &R) {
     if (p < 1 || nel < 2) return -1;
     if (nel <= p + 3) {
         wq_rule_generalized(p, nel, R);
@@ -369,6 +373,39 @@ int wq_rule_1d(int p, int nel, WQRule1D &R) {
         for (int j = b1lo[i]; j <= b1hi[i]; j++)
             put(nfun - 1 - i, nqp - 1 - j, i, j, -1.0);
     return 0;
+}
+
+// The rule depends on (p, nel) only.  Operators built back to back (the
+// serving loop sets up one per request, over a few dozen distinct sizes)
+// reuse the rules of earlier ones: a bounded cache of the rules of up to 512
+// elements per direction, evicted oldest first.
+int wq_rule_1d(int p, int nel, WQRule1D &R) {
+    constexpr int kMaxCachedNel = 512;
+    constexpr size_t kMaxEntries = 256;
+    static std::mutex mtx;
+    static std::map<std::pair<int, int>, WQRule1D> cache;
+    static std::deque<std::pair<int, int>> order;
+    const auto key = std::make_pair(p, nel);
+    if (nel <= kMaxCachedNel) {
+        std::lock_guard<std::mutex> lock(mtx);
+        auto it = cache.find(key);
+        if (it != cache.end()) {
+            R = it->second;
+            return 0;
+        }
+    }
+    const int rc = wq_rule_1d_compute(p, nel, R);
+    if (rc == 0 && nel <= kMaxCachedNel) {
+        std::lock_guard<std::mutex> lock(mtx);
+        if (cache.emplace(key, R).second) {
+            order.push_back(key);
+            if (order.size() > kMaxEntries) {
+                cache.erase(order.front());
+                order.pop_front();
+            }
+        }
+    }
+    return rc;
 }
 
 }  // namespace yeti
