@@ -64,6 +64,30 @@ def test_library_rule_matches_oracle(p, nel):
         assert _rel(a, r[k]) < RULE_TOL, k
 
 
+def test_library_rule_cache_returns_the_computed_rule():
+    """The library keeps the rules of the (p, nel) it has built; a rule
+    served from that cache is the computed one bit for bit, in any order of
+    requests."""
+    from yeti_b200 import _lib
+    L = _lib.lib()
+
+    def rule(p, nel):
+        nf, nq = p + nel, 2 * (p + nel) - 1
+        arrs = [np.zeros(nq)] + [np.zeros((nf, nq)) for _ in KEYS]
+        _lib.check(L.yeti_wq_rule_1d(p, nel, *[a.ctypes.data for a in arrs]),
+                   "yeti_wq_rule_1d")
+        return arrs
+    seq = [(2, 37), (3, 41), (2, 37), (4, 29), (3, 41), (2, 37)]
+    first = {}
+    for p, nel in seq:
+        got = rule(p, nel)
+        if (p, nel) in first:
+            for a, b in zip(got, first[(p, nel)]):
+                assert a.tobytes() == b.tobytes()
+        else:
+            first[(p, nel)] = got
+
+
 def test_library_rule_rejects_bad_sizes():
     from yeti_b200 import _lib
     L = _lib.lib()

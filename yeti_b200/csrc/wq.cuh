@@ -71,13 +71,6 @@ struct WQStreamPlan {
     DevBuf tile_off, tile_pstride, seg[2], cta_seg[2];
     DevBuf err;              // int: a kernel's bounded wait gave up
     int wait_tries = 1 << 16;   // polls of a wait for a coefficient copy
-    // FP32 two-plane kernel (wq_pair.cu): w steps (two planes each), the
-    // pair-step coefficient layout, duplicated u/v bands and per-step w bands
-    size_t pair_smem = 0;
-    int pair_per_sm = 0;
-    int nstep = 0;
-    int64_t pair_ncoef = 0;   // pairs of the FP32 layout
-    DevBuf pair_tile_off, pair_sstride, pair_band[2], pair_bandw, pair_sstart, pair_qw_step;
 };
 
 // Device-side scalars of one CG solve (wq_pcg.cu); the fast-diagonalisation
@@ -128,14 +121,6 @@ int wq_stream_setup(yeti_wq_op *op, const WQRule1D R[3]);
 int wq_stream_permute(yeti_wq_op *op);
 template <class T>
 int wq_stream_apply(yeti_wq_op *op, const T *u, T *Ku, const int *done, cudaStream_t s);
-// FP32 two-plane streaming apply (wq_pair.cu): kernel attributes, band row
-// width in pairs, the coefficient permute and the launch.
-int wq_pair_prepare(yeti_wq_op *op);
-int wq_pair_band_width(int p);
-int wq_pair_permute(yeti_wq_op *op, const float *src, float2 *dst, const int64_t *qoff1,
-                    const int *const *blk1, const int *const *loc1, const int *const *nq1,
-                    const int *qw_step);
-int wq_pair_apply(yeti_wq_op *op, const float *u, float *Ku, const int *done, cudaStream_t s);
 // One FP64 preconditioned Krylov solve (CG or BiCGSTAB; Jacobi or fast
 // diagonalisation) of a WQ operator (x0 = 0) that advances in
 // chunks of iterations captured once in a CUDA graph, on its own stream and

@@ -259,8 +259,54 @@ __device__ __forceinline__ void fma44(T acc[4][4], const T g[4], const T x[4]) {
         for (int j = 0; j < 4; j++) acc[i][j] += g[i] * x[j];
 }
 
+// FP32: the 4x4 tile as pairs of columns on packed FP32x2 FMAs (each lane
+// of a pair is the scalar FMA acc += g x, so the sums keep their bits).
+__device__ __forceinline__ void fma44_2(float2 acc[4][2], const float g[4], const float2 x[2]) {
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+        const float2 gg = make_float2(g[i], g[i]);
+        acc[i][0] = __ffma2_rn(gg, x[0], acc[i][0]);
+        acc[i][1] = __ffma2_rn(gg, x[1], acc[i][1]);
+    }
+}
+
 // acc[i][j] = sum_{k < m} gp[k ldg + i] xp[k ldx + j], the next row's
 // operands loaded while the current row's products issue.
+__device__ __forceinline__ void fd_contract(const float *gp, int ldg, const float *xp, int ldx,
+                                            int m, float acc[4][4]) {
+    float2 a2[4][2];
+#pragma unroll
+    for (int i = 0; i < 4; i++) a2[i][0] = a2[i][1] = make_float2(0.f, 0.f);
+    float g0[4], g1[4];
+    float2 x0[2], x1[2];
+    auto ldx2 = [](const float *p, float2 v[2]) {
+        const float4 q = *reinterpret_cast<const float4 *>(p);
+        v[0] = make_float2(q.x, q.y);
+        v[1] = make_float2(q.z, q.w);
+    };
+    Vec4<float>::ld(gp, g0);
+    ldx2(xp, x0);
+    int k = 0;
+    for (; k + 1 < m; k += 2) {
+        Vec4<float>::ld(gp + (k + 1) * ldg, g1);
+        ldx2(xp + (k + 1) * ldx, x1);
+        fma44_2(a2, g0, x0);
+        if (k + 2 < m) {
+            Vec4<float>::ld(gp + (k + 2) * ldg, g0);
+            ldx2(xp + (k + 2) * ldx, x0);
+        }
+        fma44_2(a2, g1, x1);
+    }
+    if (k < m) fma44_2(a2, g0, x0);
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+        acc[i][0] = a2[i][0].x;
+        acc[i][1] = a2[i][0].y;
+        acc[i][2] = a2[i][1].x;
+        acc[i][3] = a2[i][1].y;
+    }
+}
+
 template <class T>
 __device__ __forceinline__ void fd_contract(const T *gp, int ldg, const T *xp, int ldx, int m,
                                             T acc[4][4]) {
@@ -728,13 +774,37 @@ __global__ void k_fd_diag_coef(const double *coef, const int64_t *tile_off, cons
     }
 }
 
+// The same gather from the element-block layout of the setup kernels
+// (operators of mixed degrees or degree > 5): point (qu, qv, qw) of block b
+// at coef[qoff[b] 45 + e nq_b + (lw nv_b + lv) nu_b + lu].
+__global__ void k_fd_diag_coef_blk(const double *coef, const int64_t *qoff,
+                                   const int *const *blk1, const int *const *loc1,
+                                   const int *const *nq1, int nbu, int nbv, int nqu, int nqv,
+                                   int nqw, double *out) {
+    const int64_t n = (int64_t)nqu * nqv * nqw;
+    for (int64_t g = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; g < n;
+         g += (int64_t)gridDim.x * blockDim.x) {
+        const int qu = (int)(g % nqu), qv = (int)((g / nqu) % nqv);
+        const int qw = (int)(g / ((int64_t)nqu * nqv));
+        const int bu = blk1[0][qu], bv = blk1[1][qv], bw = blk1[2][qw];
+        const int64_t b = bu + (int64_t)nbu * (bv + (int64_t)nbv * bw);
+        const int nu1 = nq1[0][bu], nv1 = nq1[1][bv], nw1 = nq1[2][bw];
+        const int64_t nqb = (int64_t)nu1 * nv1 * nw1;
+        const double *base = coef + qoff[b] * kWQCoef +
+                             (loc1[2][qw] * (int64_t)nv1 + loc1[1][qv]) * nu1 + loc1[0][qu];
+        for (int c = 0; c < 3; c++)
+            for (int k = 0; k < 3; k++)
+                out[(int64_t)(3 * c + k) * n + g] = base[(int64_t)sym9(3 * c + k, 3 * c + k) * nqb];
+    }
+}
+
 int wq_fd_prepare(yeti_wq_op *op, int variant, bool f32) {
     WQFdPlan &F = op->fd;
     variant &= (YETI_PCG_FD | YETI_PCG_FD_SCALED | YETI_PCG_FD_UNIT | YETI_PCG_FD_TD);
     if (F.variant == variant && (!f32 || F.g32.ptr)) return YETI_OK;
     const bool td = (variant & YETI_PCG_FD_TD) != 0;
-    YETI_CHECK(!td || (op->st.active && op->coef64.ptr), YETI_EUNSUPPORTED,
-               "fast diagonalisation 'TD': needs an operator of one degree 2..5 with FP64 data");
+    YETI_CHECK(!td || op->coef64.ptr, YETI_EUNSUPPORTED,
+               "fast diagonalisation 'TD': needs the operator's FP64 data");
     // the passes stage up to kFdSmem bytes: opt in once per device (the
     // attribute is always this maximum, so concurrent callers agree)
     YETI_TRY(fd_set_attrs<double>());
@@ -792,11 +862,39 @@ int wq_fd_prepare(yeti_wq_op *op, int variant, bool f32) {
         DevBuf dcc;
         YETI_TRY(dcc.alloc(ctx, (size_t)9 * n * sizeof(double)));
         WQStreamPlan &st = op->st;
-        k_fd_diag_coef<<<592, 256, 0, s>>>(op->coef64.as<double>(), st.tile_off.as<int64_t>(),
-                                           st.tile_pstride.as<int>(), st.tq0[0].as<int>(),
-                                           st.tnq[0].as<int>(), st.tq0[1].as<int>(),
-                                           st.tnq[1].as<int>(), st.ntile[0], nq[0], nq[1], nq[2],
-                                           dcc.as<double>());
+        DevBuf blk[3], loc[3], nqb[3], ptrs;   // block-layout maps (freed on return)
+        if (st.active) {
+            k_fd_diag_coef<<<592, 256, 0, s>>>(op->coef64.as<double>(), st.tile_off.as<int64_t>(),
+                                               st.tile_pstride.as<int>(), st.tq0[0].as<int>(),
+                                               st.tnq[0].as<int>(), st.tq0[1].as<int>(),
+                                               st.tnq[1].as<int>(), st.ntile[0], nq[0], nq[1],
+                                               nq[2], dcc.as<double>());
+        } else {
+            const int *hp[9];
+            for (int d = 0; d < 3; d++) {
+                std::vector<int> b(nq[d]), l(nq[d]), m(op->blk[d].size());
+                for (size_t k = 0; k < op->blk[d].size(); k++) {
+                    const BlkInfo &B = op->blk[d][k];
+                    m[k] = B.nq;
+                    for (int q = 0; q < B.nq; q++) {
+                        b[B.q0 + q] = (int)k;
+                        l[B.q0 + q] = q;
+                    }
+                }
+                YETI_TRY(upload(ctx, blk[d], b.data(), b.size()));
+                YETI_TRY(upload(ctx, loc[d], l.data(), l.size()));
+                YETI_TRY(upload(ctx, nqb[d], m.data(), m.size()));
+                hp[d] = blk[d].as<int>();
+                hp[3 + d] = loc[d].as<int>();
+                hp[6 + d] = nqb[d].as<int>();
+            }
+            YETI_TRY(upload(ctx, ptrs, hp, 9));
+            const int *const *dp = ptrs.as<const int *>();
+            k_fd_diag_coef_blk<<<592, 256, 0, s>>>(op->coef64.as<double>(), op->qoff.as<int64_t>(),
+                                                   dp, dp + 3, dp + 6, (int)op->blk[0].size(),
+                                                   (int)op->blk[1].size(), nq[0], nq[1], nq[2],
+                                                   dcc.as<double>());
+        }
         count_launches(1);
         YETI_CUDA(cudaGetLastError());
         std::vector<double> cc((size_t)9 * n);

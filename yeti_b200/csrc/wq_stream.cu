@@ -821,6 +821,7 @@ static int stream_prepare_kernels(yeti_wq_op *op) {
 #define YETI_CASE(PP)                                                  \
     case PP:                                                           \
         rc = stream_attr<double, PP>(op, 0);                           \
+        if (rc == YETI_OK) rc = stream_attr<float, PP>(op, 1);         \
         break;
         YETI_CASE(2)
         YETI_CASE(3)
@@ -829,12 +830,6 @@ static int stream_prepare_kernels(yeti_wq_op *op) {
 #undef YETI_CASE
         default:
             rc = YETI_EUNSUPPORTED;
-    }
-    // FP32: the two-plane kernel (wq_pair.cu)
-    if (rc == YETI_OK) rc = wq_pair_prepare(op);
-    if (rc == YETI_OK) {
-        op->st.smem[1] = op->st.pair_smem;
-        op->st.per_sm[1] = op->st.pair_per_sm;
     }
     return rc;
 }
@@ -879,41 +874,6 @@ int wq_stream_setup(yeti_wq_op *op, const WQRule1D R[3]) {
         YETI_TRY(upload_vec(ctx, st.elem[d], elem));
         YETI_TRY(upload_vec(ctx, st.band64[d], band));
         YETI_TRY(upload_vec(ctx, st.band32[d], bandf));
-        // FP32 two-plane kernel: u and v bands with every value duplicated
-        // into a pair (the planes share them); w bands per step, pairing the
-        // step's two planes (zero for a missing second plane)
-        const int PBW = wq_pair_band_width(P);
-        if (d < 2) {
-            std::vector<float> dup((size_t)nq * 6 * PBW * 2, 0.f);
-            for (int q = 0; q < nq; q++)
-                for (int k = 0; k < 6; k++)
-                    for (int m = 0; m <= P; m++) {
-                        const float v = (float)band[((size_t)q * 6 + k) * PBP + m];
-                        dup[(((size_t)q * 6 + k) * PBW + m) * 2] = v;
-                        dup[(((size_t)q * 6 + k) * PBW + m) * 2 + 1] = v;
-                    }
-            YETI_TRY(upload_vec(ctx, st.pair_band[d], dup));
-        } else {
-            std::vector<int> sstart(nel + 1, 0), qw_step(nq, 0);
-            for (int e = 0; e < nel; e++)
-                sstart[e + 1] = sstart[e] + (elem_q0[d][e + 1] - elem_q0[d][e] + 1) / 2;
-            const int nstep = sstart[nel];
-            std::vector<float> bw((size_t)nstep * 6 * PBW * 2, 0.f);
-            for (int e = 0; e < nel; e++)
-                for (int q = elem_q0[d][e]; q < elem_q0[d][e + 1]; q++) {
-                    const int k2 = q - elem_q0[d][e];
-                    const int s = sstart[e] + k2 / 2, slot = k2 % 2;
-                    qw_step[q] = (s << 1) | slot;
-                    for (int k = 0; k < 6; k++)
-                        for (int m = 0; m <= P; m++)
-                            bw[(((size_t)s * 6 + k) * PBW + m) * 2 + slot] =
-                                (float)band[((size_t)q * 6 + k) * PBP + m];
-                }
-            st.nstep = nstep;
-            YETI_TRY(upload_vec(ctx, st.pair_sstart, sstart));
-            YETI_TRY(upload_vec(ctx, st.pair_qw_step, qw_step));
-            YETI_TRY(upload_vec(ctx, st.pair_bandw, bw));
-        }
     }
     YETI_TRY(upload_vec(ctx, st.wq0, elem_q0[2]));
     std::vector<int> tq0[2], tnq[2], treg[2];
@@ -938,21 +898,6 @@ int wq_stream_setup(yeti_wq_op *op, const WQRule1D R[3]) {
     st.ncoef = toff[ntiles];
     YETI_TRY(upload_vec(ctx, st.tile_off, toff));
     YETI_TRY(upload_vec(ctx, st.tile_pstride, pstride));
-    // FP32 pair-step layout: tile-major, then w step, then entry, then point,
-    // a pair of planes per value; step blocks padded to 256 bytes
-    {
-        std::vector<int64_t> toff2(ntiles + 1, 0);
-        std::vector<int> sstride(ntiles);
-        for (int t = 0; t < ntiles; t++) {
-            const int tu = t % st.ntile[0], tv = t / st.ntile[0];
-            const int npts = tnq[0][tu] * tnq[1][tv];
-            sstride[t] = (kWQCoef * npts + 31) / 32 * 32;
-            toff2[t + 1] = toff2[t] + (int64_t)st.nstep * sstride[t];
-        }
-        st.pair_ncoef = toff2[ntiles];
-        YETI_TRY(upload_vec(ctx, st.pair_tile_off, toff2));
-        YETI_TRY(upload_vec(ctx, st.pair_sstride, sstride));
-    }
     YETI_TRY(st.err.alloc(ctx, sizeof(int)));
     YETI_CUDA(cudaMemsetAsync(st.err.ptr, 0, sizeof(int), ctx->stream));
 
@@ -1004,10 +949,8 @@ template <class T>
 static int permute_one(yeti_wq_op *op, const DevBuf &src, DevBuf &dst) {
     yeti_ctx *ctx = op->ctx;
     WQStreamPlan &st = op->st;
-    const bool f32 = sizeof(T) == 4;
-    const size_t nbytes = f32 ? st.pair_ncoef * sizeof(float2) : st.ncoef * sizeof(T);
-    YETI_TRY(dst.alloc(ctx, nbytes));
-    YETI_CUDA(cudaMemsetAsync(dst.ptr, 0, nbytes, ctx->stream));
+    YETI_TRY(dst.alloc(ctx, st.ncoef * sizeof(T)));
+    YETI_CUDA(cudaMemsetAsync(dst.ptr, 0, st.ncoef * sizeof(T), ctx->stream));
     // per-direction maps of the setup layout: point -> (block, local index)
     DevBuf blk[3], loc[3], nq1[3], ptrs;
     const int *hp[9];
@@ -1030,12 +973,6 @@ static int permute_one(yeti_wq_op *op, const DevBuf &src, DevBuf &dst) {
     }
     YETI_TRY(upload(ctx, ptrs, hp, 9));
     const int **dp = ptrs.as<const int *>();
-    if (f32) {
-        YETI_TRY(wq_pair_permute(op, src.as<float>(), dst.as<float2>(), op->qoff.as<int64_t>(), dp,
-                                 dp + 3, dp + 6, st.pair_qw_step.as<int>()));
-        YETI_CUDA(cudaStreamSynchronize(ctx->stream));
-        return YETI_OK;
-    }
     const int64_t n = (int64_t)op->nqp[0] * op->nqp[1] * op->nqp[2];
     const int grid = (int)std::min<int64_t>((n + 255) / 256, 148 * 16);
     k_wq_stream_permute<T><<<grid, 256, 0, ctx->stream>>>(
@@ -1104,18 +1041,14 @@ static int launch_stream(yeti_wq_op *op, const T *u, T *Ku, const int *done, cud
 
 template <class T>
 int wq_stream_apply(yeti_wq_op *op, const T *u, T *Ku, const int *done, cudaStream_t s) {
-    if constexpr (sizeof(T) == 4) {
-        return wq_pair_apply(op, u, Ku, done, s);
-    } else {
-        switch (op->p[0]) {
-            case 2: return launch_stream<T, 2>(op, u, Ku, done, s);
-            case 3: return launch_stream<T, 3>(op, u, Ku, done, s);
-            case 4: return launch_stream<T, 4>(op, u, Ku, done, s);
-            case 5: return launch_stream<T, 5>(op, u, Ku, done, s);
-            default:
-                set_error("WQ streaming: degree %d", op->p[0]);
-                return YETI_EUNSUPPORTED;
-        }
+    switch (op->p[0]) {
+        case 2: return launch_stream<T, 2>(op, u, Ku, done, s);
+        case 3: return launch_stream<T, 3>(op, u, Ku, done, s);
+        case 4: return launch_stream<T, 4>(op, u, Ku, done, s);
+        case 5: return launch_stream<T, 5>(op, u, Ku, done, s);
+        default:
+            set_error("WQ streaming: degree %d", op->p[0]);
+            return YETI_EUNSUPPORTED;
     }
 }
 
