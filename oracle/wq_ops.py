@@ -270,12 +270,14 @@ class WQOracle:
     def fd_1d_weighted(self, d, lo, hi, mw, kw):
         """1-D matrices of the 'TD' branch of eigen_decomposition
         (tensor_algebra.f90:1045-1071): W00 (B0 diag(mw))^T and W11 (B1
-        diag(kw))^T restricted, symmetric from the upper triangle."""
+        diag(kw))^T restricted, symmetrised by averaging with the transpose
+        (the reference hands the non-symmetric products to dsygvd, which
+        reads the upper triangle; that triangle is indefinite on rough
+        coefficient fields)."""
         R = self.rules[d]
         M = (R["W00"] @ (R["B0"] * mw[None, :]).T)[lo:hi, lo:hi]
         K = (R["W11"] @ (R["B1"] * kw[None, :]).T)[lo:hi, lo:hi]
-        up = lambda A: np.triu(A) + np.triu(A, 1).T   # noqa: E731
-        return up(K), up(M)
+        return 0.5 * (K + K.T), 0.5 * (M + M.T)
 
     def fd_setup(self, scaled=False, unit=False, td=False):
         """Per component: box, eigenpairs of K_d U = M_d U lam (scipy's

@@ -678,8 +678,12 @@ static int fd_set_attrs() {
 
 // 1-D matrices with per-point weights (eigen_decomposition's 'TD' branch,
 // tensor_algebra.f90:1045-1071): M = W00 (B0 diag(mw))^T and K = W11 (B1
-// diag(kw))^T on the rows lo..hi-1, symmetric from their upper triangle (the
-// triangle dsygvd reads, UPLO = 'U').
+// diag(kw))^T on the rows lo..hi-1, made symmetric by averaging with the
+// transpose, as the unweighted matrices are.  (The reference hands the
+// non-symmetric products to dsygvd, which reads their upper triangle; with
+// the point-to-point variation of a rough coefficient field that triangle
+// is indefinite, its eigenvalue sums negative, while the symmetric part
+// stays definite.)
 static void wq_1d_matrices_weighted(const WQRule1D &R, int lo, int hi, const double *mw,
                                     const double *kw, std::vector<double> &K,
                                     std::vector<double> &M) {
@@ -687,7 +691,7 @@ static void wq_1d_matrices_weighted(const WQRule1D &R, int lo, int hi, const dou
     K.assign((size_t)m * m, 0.0);
     M.assign((size_t)m * m, 0.0);
     for (int i = 0; i < m; i++)
-        for (int j = i; j < m; j++) {
+        for (int j = 0; j < m; j++) {
             const double *w0 = &R.W00[(size_t)(lo + i) * nq], *b0 = &R.B0[(size_t)(lo + j) * nq];
             const double *w1 = &R.W11[(size_t)(lo + i) * nq], *b1 = &R.B1[(size_t)(lo + j) * nq];
             double sm = 0.0, sk = 0.0;
@@ -695,8 +699,15 @@ static void wq_1d_matrices_weighted(const WQRule1D &R, int lo, int hi, const dou
                 sm += w0[q] * (b0[q] * mw[q]);
                 sk += w1[q] * (b1[q] * kw[q]);
             }
-            M[(size_t)i * m + j] = M[(size_t)j * m + i] = sm;
-            K[(size_t)i * m + j] = K[(size_t)j * m + i] = sk;
+            M[(size_t)i * m + j] = sm;
+            K[(size_t)i * m + j] = sk;
+        }
+    for (int i = 0; i < m; i++)
+        for (int j = i + 1; j < m; j++) {
+            const double a = 0.5 * (M[(size_t)i * m + j] + M[(size_t)j * m + i]);
+            const double b = 0.5 * (K[(size_t)i * m + j] + K[(size_t)j * m + i]);
+            M[(size_t)i * m + j] = M[(size_t)j * m + i] = a;
+            K[(size_t)i * m + j] = K[(size_t)j * m + i] = b;
         }
 }
 
