@@ -284,6 +284,56 @@ def _system_args(name):
     return [d[k] if d[k].ndim else d[k][()] for k in SYSTEM_ARG_NAMES]
 
 
+def _event_ms(fn, reps):
+    """Median device time of fn() between two CUDA events on the current
+    stream (the library's), after one warm call."""
+    import torch
+    fn()
+    ts = []
+    for _ in range(reps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        fn()
+        e1.record()
+        torch.cuda.synchronize()
+        ts.append(e0.elapsed_time(e1))
+    return statistics.median(ts)
+
+
+def fp64_peak_tflops():
+    """Measured FP64 GEMM rate (cuBLAS DGEMM 8192^3, best of 5): the FP64
+    denominator of the Gauss kernels' compute rooflines."""
+    import torch
+    n = 8192
+    A = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    B = torch.randn_like(A)
+    for _ in range(2):
+        A @ B
+    best = float("inf")
+    for _ in range(5):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        A @ B
+        e1.record()
+        torch.cuda.synchronize()
+        best = min(best, e0.elapsed_time(e1))
+    del A, B
+    return 2.0 * n ** 3 / (best / 1e3) / 1e12
+
+
+def stiffness_flops(nq, nn, nel):
+    """FP64 operations of k_u1_stiffness: per (point, node pair) the nine
+    B_i^T D B_j entries (72), per (point, node) the basis stage (60)."""
+    return nel * nq * (nn * (nn + 1) // 2 * 72 + nn * 60)
+
+
+def gradient_flops(nq, nn, nel, nadj=1):
+    """FP64 operations of k_u1_grad: per (point, control point, component)
+    the interior-work derivative terms (dJ, the strain variation, dAAI, the
+    81-term dAAE, the 36 dC products: about 1150 with one adjoint)."""
+    return nel * nq * nn * 3 * 1150 * nadj
+
+
 def extra_configs(args, device):
     """The other configurations of the path, each beside its CPU oracle:
     U1 Gauss assembly of the p=2 16x4x4 cantilever (COO), the compliance
@@ -323,8 +373,14 @@ def extra_configs(args, device):
     Uo = np.zeros(n1)
     Uo[idof1] = spla.spsolve(K1[idof1, :][:, idof1], Fo2[idof1])
     t_cpu_solve = (time.perf_counter() - t0) * 1e3
+    peak64 = fp64_peak_tflops()
+    t_ev = _event_ms(lambda: sys_linmat_lindef_static(*a1, device_out=True), 20)
+    fl1 = stiffness_flops(27, 27, 256)
+    out["fp64_gemm_tflops_measured"] = peak64
     out["assembly_p2_16x4x4"] = {
         "nb_data": int(kd.size), "gpu_ms_device_out": t_gpu, "gpu_ms_host_buffers": t_gpu_host,
+        "gpu_ms_events_device_out": t_ev, "stiffness_gflop": fl1 / 1e9,
+        "fp64_frac_of_measured_dgemm": fl1 / (t_ev / 1e3) / 1e12 / peak64,
         "cpu_oracle_ms": t_cpu, "cpu_cores": oracle.threads(),
         "bit_identical": bool(np.array_equal(kd, ko) and np.array_equal(F, Fo)),
         "assemble_and_solve_ms": t_solve, "cpu_oracle_assemble_and_solve_ms": t_cpu_solve,
@@ -355,13 +411,18 @@ def extra_configs(args, device):
     grad_from_system_args(a3, sol, adj)
     t_g = _median_ms(lambda: grad_from_system_args(a3, sol, adj), 5, sync)
     gi, ge = grad_from_system_args(a3, sol, adj)
+    t_gev = _event_ms(lambda: grad_from_system_args(a3, sol, adj), 5)
+    fl3 = gradient_flops(27, 27, 2048)
     t0 = time.perf_counter()
     oi, oe = oracle.grad_lin_elast_work(a3, sol, adj)
     t_go = (time.perf_counter() - t0) * 1e3
     ref = np.concatenate([oi.ravel(), oe.ravel()])
     got = np.concatenate([gi.ravel(), ge.ravel()])
     out["gradient_p2_32x32x2"] = {
-        "nb_cp": int(sol.shape[1]), "gpu_ms_host_buffers": t_g, "cpu_oracle_ms": t_go,
+        "nb_cp": int(sol.shape[1]), "gpu_ms_host_buffers": t_g, "gpu_ms_events": t_gev,
+        "gradient_gflop": fl3 / 1e9,
+        "fp64_frac_of_measured_dgemm": fl3 / (t_gev / 1e3) / 1e12 / peak64,
+        "cpu_oracle_ms": t_go,
         "cpu_cores": oracle.threads(), "max_rel_diff_vs_oracle": float(np.abs(got - ref).max() / np.abs(ref).max())}
     # volume and its shape gradient on the C3 geometry (the constraint of the
     # shape optimisation beside the compliance)

@@ -47,10 +47,16 @@ namespace yeti {
 
 namespace {
 
-constexpr int kTQ = 16;          // max points of a tile per direction
-constexpr int kNE = kTQ / 2;     // max elements of a regular tile
-constexpr int kThreads = 256;    // one thread per point of a plane tile
+#ifndef YETI_WQ_TV
+#define YETI_WQ_TV 16
+#endif
+constexpr int kTQ = 16;          // max points of a tile along u
+constexpr int kTV = YETI_WQ_TV;  // max points of a tile along v (16 or 8)
+constexpr int kNE = kTQ / 2;     // max elements of a regular tile along u
+constexpr int kNEV = kTV / 2;    // ... along v
+constexpr int kThreads = kTQ * kTV;   // one thread per point of a plane tile
 constexpr int kWarps = kThreads / 32;
+constexpr int kCtasPerSm = 512 / kThreads;   // 2 (16 x 16 tiles) or 4 (16 x 8)
 constexpr int kHS = 2 * kTQ + 1; // channel stride of a warp's h block
 
 constexpr int cmax(int a, int b) { return a > b ? a : b; }
@@ -69,26 +75,27 @@ template <int P>
 struct Dims {
     static constexpr int PB = P + 1;
     static constexpr int PBP = round4(PB);     // padded band row
-    static constexpr int NFM = kNE + P;        // max functions of a tile
+    static constexpr int NFM = kNE + P;        // max functions of a tile along u
+    static constexpr int NFV = kNEV + P;       // ... along v
     static constexpr int GS = gstride(NFM);
-    static constexpr int Y = round4(2 * 3 * NFM * NFM);
+    static constexpr int Y = round4(2 * 3 * NFV * NFM);
     static constexpr int ZHP = round4(cmax(9 * 2 * NFM, 27 * kHS));   // Z, then h
     static constexpr int GP = round4(27 * GS);                        // G
-    static constexpr int K = 9 * NFM * NFM * 2;                       // aliases the Z/h parts
-    static constexpr int TAB = kTQ * 6 * PBP;
+    static constexpr int K = 9 * NFV * NFM * 2;                       // aliases the Z/h parts
+    static constexpr int TAB = kTQ * 6 * PBP;                         // u (v: kTV rows)
     static constexpr int OFF_ZH = Y;
     static constexpr int OFF_G = OFF_ZH + kWarps * ZHP;
     static constexpr int OFF_TAB = OFF_G + kWarps * GP;
-    static constexpr int TOTAL = OFF_TAB + 2 * TAB;
-    static constexpr int NCOL = 3 * NFM * NFM;
+    static constexpr int TOTAL = OFF_TAB + TAB + kTV * 6 * PBP;
+    static constexpr int NCOL = 3 * NFV * NFM;
     static constexpr int CPT = (NCOL + kThreads - 1) / kThreads;
-    static constexpr int CB = kTQ * kTQ * 45;   // one plane's coefficients (staged kernels)
+    static constexpr int CB = kTQ * kTV * 45;   // one plane's coefficients (staged kernels)
     static_assert(K <= kWarps * ZHP, "K must fit in the Z/h parts");
     // values, then the staged coefficient block (FP32), the two rel tables
     // and the mbarrier
     template <class T>
     static constexpr size_t smem_bytes() {
-        return (size_t)(TOTAL + (sizeof(T) == 4 ? CB : 0)) * sizeof(T) + 2 * kTQ * sizeof(int) +
+        return (size_t)(TOTAL + (sizeof(T) == 4 ? CB : 0)) * sizeof(T) + (kTQ + kTV) * sizeof(int) +
                sizeof(uint64_t);
     }
 };
@@ -194,8 +201,8 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, int tr
 // points; 2 the first element owns p+1 points, the others two (the first
 // tile); 3 the last element owns p+2 points, the others two (the last tile);
 // 0 anything else (run-time walk).
-__host__ __device__ constexpr int pat_nemax(int P, int pat) {
-    return pat == 1 ? kNE : pat == 2 ? 1 + (kTQ - (P + 1)) / 2 : 1 + (kTQ - (P + 2)) / 2;
+__host__ __device__ constexpr int pat_nemax(int P, int pat, int tq = kTQ) {
+    return pat == 1 ? tq / 2 : pat == 2 ? 1 + (tq - (P + 1)) / 2 : 1 + (tq - (P + 2)) / 2;
 }
 // first point of element e in a tile of pattern pat
 __host__ __device__ constexpr int pat_q0(int P, int pat, int e) {
@@ -269,7 +276,7 @@ __device__ __forceinline__ void walk_u_generic(const T *h, T *g, const T *tab, i
 template <class T, int P, int PAT>
 __device__ __forceinline__ void walk_v(const T *gb, T *kp, const T *tab, int ka, int ne) {
     using D = Dims<P>;
-    constexpr int PBP = D::PBP, NEM = pat_nemax(P, PAT), NF = NEM + P, NFM = D::NFM;
+    constexpr int PBP = D::PBP, NEM = pat_nemax(P, PAT, kTV), NF = NEM + P, NFM = D::NFM;
     constexpr int GS = D::GS, GP = D::GP;
     T A0[NF], A1[NF];
 #pragma unroll
@@ -371,7 +378,7 @@ struct StreamArgs {
 };
 
 template <class T, int P>
-__global__ void __launch_bounds__(kThreads, 2) k_wq_apply_stream(StreamArgs<T> a) {
+__global__ void __launch_bounds__(kThreads, kCtasPerSm) k_wq_apply_stream(StreamArgs<T> a) {
     using D = Dims<P>;
     constexpr int PB = D::PB, PBP = D::PBP, NFM = D::NFM, CPT = D::CPT;
     constexpr int GS = D::GS, GP = D::GP, ZHP = D::ZHP;
@@ -389,7 +396,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_wq_apply_stream(StreamArgs<T> a
     T *const cbuf = sm + D::TOTAL;
     int *const relu = reinterpret_cast<int *>(sm + D::TOTAL + (kStaged ? D::CB : 0));
     int *const relv = relu + kTQ;
-    uint64_t *const bar = reinterpret_cast<uint64_t *>(relv + kTQ);
+    uint64_t *const bar = reinterpret_cast<uint64_t *>(relv + kTV);
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     uint32_t phase = 0;
     if constexpr (kStaged) {
@@ -420,12 +427,10 @@ __global__ void __launch_bounds__(kThreads, 2) k_wq_apply_stream(StreamArgs<T> a
         for (int i = tid; i < kTQ * 6 * PBP; i += kThreads) {
             const int q = i / (6 * PBP), r = i - q * (6 * PBP);
             tabu[i] = q < nqu ? a.band[0][(size_t)(qu0 + q) * 6 * PBP + r] : T(0);
-            tabv[i] = q < nqv ? a.band[1][(size_t)(qv0 + q) * 6 * PBP + r] : T(0);
+            if (q < kTV) tabv[i] = q < nqv ? a.band[1][(size_t)(qv0 + q) * 6 * PBP + r] : T(0);
         }
-        if (tid < kTQ) {
-            relu[tid] = tid < nqu ? a.elem[0][qu0 + tid] - fu0 : 0;
-            relv[tid] = tid < nqv ? a.elem[1][qv0 + tid] - fv0 : 0;
-        }
+        if (tid < kTQ) relu[tid] = tid < nqu ? a.elem[0][qu0 + tid] - fu0 : 0;
+        if (tid < kTV) relv[tid] = tid < nqv ? a.elem[1][qv0 + tid] - fv0 : 0;
         const uint32_t cbytes = (uint32_t)((npts * kWQCoef * (int)sizeof(T) + 15) & ~15);
         if constexpr (kStaged) {
             if (tid == 0) bulk_load(cbuf, coef_t + (int64_t)a.wq0[sg.y] * pstride, cbytes, bar);
@@ -513,8 +518,8 @@ __global__ void __launch_bounds__(kThreads, 2) k_wq_apply_stream(StreamArgs<T> a
                             y1 += b1[m] * x[cc][m];
                         }
                         const int c = cinfo[cc] & 3, k = cinfo[cc] >> 3;
-                        RY[c * NFM * NFM + k] = y0;
-                        RY[(3 + c) * NFM * NFM + k] = y1;
+                        RY[c * D::NFV * NFM + k] = y0;
+                        RY[(3 + c) * D::NFV * NFM + k] = y1;
                     }
                 }
                 if constexpr (kStaged) {
@@ -544,8 +549,8 @@ __global__ void __launch_bounds__(kThreads, 2) k_wq_apply_stream(StreamArgs<T> a
                             load_band<P>(tabv + (qv * 6 + 1) * PBP, b1);
 #pragma unroll
                             for (int c = 0; c < 3; c++) {
-                                const T *y0 = RY + (c * NFM + rv) * NFM + fu;
-                                const T *y1 = RY + ((3 + c) * NFM + rv) * NFM + fu;
+                                const T *y0 = RY + (c * D::NFV + rv) * NFM + fu;
+                                const T *y1 = RY + ((3 + c) * D::NFV + rv) * NFM + fu;
                                 T z0 = 0, z1 = 0, z2 = 0;
 #pragma unroll
                                 for (int m = 0; m < PB; m++) {
@@ -658,7 +663,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_wq_apply_stream(StreamArgs<T> a
                     const int ik = d_ik, fu = d_fu;
                     const int ka = 2 + 2 * (ik % 3 == 1);   // W_{[k==v], 0}
                     const T *gb = RG + (ik * 3) * GS + fu;
-                    T *kp = RZH + (ik * NFM * NFM + fu) * 2;
+                    T *kp = RZH + (ik * D::NFV * NFM + fu) * 2;
                     switch (patv) {
                         case 1: walk_v<T, P, 1>(gb, kp, tabv, ka, nev); break;
                         case 2: walk_v<T, P, 2>(gb, kp, tabv, ka, nev); break;
@@ -678,11 +683,11 @@ __global__ void __launch_bounds__(kThreads, 2) k_wq_apply_stream(StreamArgs<T> a
                     for (int cc = 0; cc < CPT; cc++) {
                         if (!(cinfo[cc] & 4)) continue;
                         const int i = cinfo[cc] & 3, kidx = cinfo[cc] >> 3;
-                        const T *kb = RZH + ((i * 3) * NFM * NFM + kidx) * 2;
+                        const T *kb = RZH + ((i * 3) * D::NFV * NFM + kidx) * 2;
                         T k00, k01, k10, k11, k20, k21;
                         load_pair(kb, k00, k01);
-                        load_pair(kb + 2 * NFM * NFM, k10, k11);
-                        load_pair(kb + 4 * NFM * NFM, k20, k21);
+                        load_pair(kb + 2 * D::NFV * NFM, k10, k11);
+                        load_pair(kb + 4 * D::NFV * NFM, k20, k21);
                         const T s00 = k00 + k10, s01 = k01 + k11;
 #pragma unroll
                         for (int m = 0; m < PB; m++)
@@ -713,22 +718,24 @@ __global__ void __launch_bounds__(kThreads, 2) k_wq_apply_stream(StreamArgs<T> a
 }
 
 // ------------------------------------------------------------------ host
-// Tiles of whole elements with at most kTQ points: the first and last tiles
-// take the boundary elements (which own more than two points) and as many
-// neighbours as fit; the elements between (two points each) are split into
-// balanced regular tiles of at most kNE elements.
+// Tiles of whole elements with at most maxq points (kTQ along u, kTV along
+// v): the first and last tiles take the boundary elements (which own more
+// than two points) and as many neighbours as fit; the elements between (two
+// points each) are split into balanced regular tiles of at most maxq / 2
+// elements.
 static void make_tiles(const std::vector<int> &elem_q0, int nel, std::vector<int> &q0,
-                       std::vector<int> &nq, std::vector<int> &reg) {
+                       std::vector<int> &nq, std::vector<int> &reg, int maxq) {
+    const int maxe = maxq / 2;
     q0.clear();
     nq.clear();
     reg.clear();
     auto pts = [&](int a, int b) { return elem_q0[b] - elem_q0[a]; };   // elements [a, b)
     int first_end = 1;
-    while (first_end < nel && pts(0, first_end + 1) <= kTQ) first_end++;
+    while (first_end < nel && pts(0, first_end + 1) <= maxq) first_end++;
     int last_begin = nel;
     if (first_end < nel) {
         last_begin = nel - 1;
-        while (last_begin - 1 >= first_end && pts(last_begin - 1, nel) <= kTQ) last_begin--;
+        while (last_begin - 1 >= first_end && pts(last_begin - 1, nel) <= maxq) last_begin--;
     }
     // walk pattern of a tile (see walk_u): 1 all elements own two points,
     // 2 only the first element of the patch differs, 3 only the last
@@ -748,7 +755,7 @@ static void make_tiles(const std::vector<int> &elem_q0, int nel, std::vector<int
     add(0, first_end);
     const int nmid = last_begin - first_end;
     if (nmid > 0) {
-        const int t = (nmid + kNE - 1) / kNE;
+        const int t = (nmid + maxe - 1) / maxe;
         for (int k = 0; k < t; k++)
             add(first_end + (int)((int64_t)nmid * k / t), first_end + (int)((int64_t)nmid * (k + 1) / t));
     }
@@ -878,7 +885,7 @@ int wq_stream_setup(yeti_wq_op *op, const WQRule1D R[3]) {
     YETI_TRY(upload_vec(ctx, st.wq0, elem_q0[2]));
     std::vector<int> tq0[2], tnq[2], treg[2];
     for (int d = 0; d < 2; d++) {
-        make_tiles(elem_q0[d], op->nel[d], tq0[d], tnq[d], treg[d]);
+        make_tiles(elem_q0[d], op->nel[d], tq0[d], tnq[d], treg[d], d == 0 ? kTQ : kTV);
         YETI_TRY(upload_vec(ctx, st.treg[d], treg[d]));
         st.ntile[d] = (int)tq0[d].size();
         YETI_TRY(upload_vec(ctx, st.tq0[d], tq0[d]));
