@@ -62,6 +62,9 @@ def parse():
                     help="Krylov method of the served solves")
     ap.add_argument("--no-extra", action="store_true",
                     help="skip the assembly, gradient and p=4 block measurements")
+    ap.add_argument("--only-extra", action="store_true",
+                    help="run only the assembly, mass, gradient, volume and p=4 block "
+                         "measurements (one JSON line with other_configs)")
     return ap.parse_args()
 
 
@@ -520,6 +523,10 @@ def main():
     ctx = _lib.default_context(local)
     ctx.set_stream(torch.cuda.current_stream(dev))
     L = _lib.lib()
+    if args.only_extra:
+        if rank == 0:
+            print(json.dumps({"other_configs": extra_configs(args, local)}), flush=True)
+        return 0
     seed = replica_seed(rank)
     P = cube_patch(tuple(args.nel), args.p, perturb=0.2, wrange=(0.8, 1.2), seed=seed)
     t0 = time.perf_counter()

@@ -34,7 +34,7 @@ __device__ __constant__ int c_vi[6] = {0, 1, 2, 0, 0, 1};
 __device__ __constant__ int c_vj[6] = {0, 1, 2, 1, 2, 2};
 
 struct GradArgs {
-    int p0, p1, p2, nn, nq, ng, nadj;
+    int p0, p1, p2, nn, nq, ng, nadj, qchunk;
     int compute_int, compute_ext, include_surface;
     const double *U0, *U1, *U2;
     const double *gauss;      // volume rule (4 * nq)
@@ -121,10 +121,11 @@ __host__ __device__ inline PtLayout pt_layout(int nn, int nadj, int nbody) {
 // PtLayout, then the basis scratch (kBasisB1 + kStiffQS per point) and the
 // external-work accumulators of the (control point, component) tasks.
 __host__ __device__ inline size_t grad_smem_doubles(int nn, int nq, int nadj, const PtLayout &L,
-                                                    size_t face) {
+                                                    size_t face, int qchunk) {
     const size_t vol = (size_t)nq * L.size;
     return (size_t)(6 + 3 * nadj) * nn + nn + (vol > face ? vol : face) +
-           (size_t)nq * (kBasisB1 + kStiffQS) + (size_t)3 * nn * nadj;
+           (size_t)nq * (kBasisB1 + kStiffQS) + (size_t)2 * 3 * nn * nadj +
+           (size_t)3 * nn * qchunk * 3 * nadj;
 }
 
 // gradUELMAT1adj (gradUELMAT_solid.f90:18-479) of one element per CTA.
@@ -328,22 +329,33 @@ __global__ void __launch_bounds__(256) k_u1_grad(GradArgs a) {
         }
     }
     __syncthreads();
-    // ---------------- stage B: one task per (control point, component)
-    for (int task = tid; task < 3 * nn; task += nth) {
-        const int cp = task / 3, c = task - 3 * cp;
-        double gi[kGradMaxAdj], ge[kGradMaxAdj];
-        for (int k = 0; k < kGradMaxAdj; k++) gi[k] = ge[k] = 0.0;
-        for (int q = 0; q < a.nq; q++) {
-            const double *P = pts + (size_t)q * L.size;
-            const double *dr = P + L.dR + 3 * cp;
-            const double Area = P[L.area], detJac = P[L.dj];
-            const double *AxA = P + L.AxA;
-            if (a.compute_int) {
+    // ---------------- stage B: interior work, per (control point, component,
+    // point) in parallel.  Each thread forms the three terms the reference
+    // subtracts from the gradient at its point (work dJ detJ, the
+    // stress-times-strain-variation term, the material-variation term); one
+    // thread per (control point, component) then subtracts them in point
+    // order, the reference's order, so the sums keep their bits.  Points are
+    // taken in chunks of a.qchunk (the term buffer).
+    double *gi_s = ge_s + (size_t)3 * nn * nadj;   // 3 nn nadj accumulators
+    double *terms = gi_s + (size_t)3 * nn * nadj;  // 3 nn qchunk 3 nadj terms
+    for (int t = tid; t < 3 * nn * nadj; t += nth) gi_s[t] = 0.0;
+    if (a.compute_int) {
+        for (int q0 = 0; q0 < a.nq; q0 += a.qchunk) {
+            const int nqc = min(a.qchunk, a.nq - q0);
+            __syncthreads();
+            for (int t = tid; t < 3 * nn * nqc; t += nth) {
+                const int task = t / nqc, ql = t - task * nqc, q = q0 + ql;
+                const int cp = task / 3, c = task - 3 * cp;
+                const double *P = pts + (size_t)q * L.size;
+                const double *dr = P + L.dR + 3 * cp;
+                const double Area = P[L.area], detJac = P[L.dj];
+                const double *AxA = P + L.AxA;
                 const double *AI = P + L.AI, *AAE = P + L.AAE;
                 const double *stress = P + L.stress, *strain = P + L.strain, *dU = P + L.dU;
+                double *tt = terms + ((size_t)task * a.qchunk + ql) * 3 * nadj;
                 double dJ = 0.0;
                 for (int i = 0; i < 3; i++) dJ = dJ + AxA[3 * i + c] * dr[i];
-                for (int k = 0; k < nadj; k++) gi[k] = gi[k] - P[L.work + k] * dJ * detJac;
+                for (int k = 0; k < nadj; k++) tt[3 * k] = P[L.work + k] * dJ * detJac;
                 for (int k = 0; k < nadj; k++) {
                     const double *d = P + L.dUA + 9 * k;
                     double ev = 0.0;
@@ -352,7 +364,7 @@ __global__ void __launch_bounds__(256) k_u1_grad(GradArgs a) {
                         if (i == j) ev = ev + stress[ij] * d[3 * i + c] * dr[i];
                         else ev = ev + stress[ij] * d[3 * i + c] * dr[j] + stress[ij] * d[3 * j + c] * dr[i];
                     }
-                    gi[k] = gi[k] - ev * Area * detJac;
+                    tt[3 * k + 1] = ev * Area * detJac;
                 }
                 double dAAI[3][3], dAAE[3][3];
                 for (int j = 0; j < 3; j++)
@@ -387,9 +399,34 @@ __global__ void __launch_bounds__(256) k_u1_grad(GradArgs a) {
                             vA[kk] = vA[kk] + dC * strain[ij] * P[L.sA + 6 * kk + kl];
                     }
                 }
-                for (int k = 0; k < nadj; k++) gi[k] = gi[k] - vA[k] * Area * detJac;
+                for (int k = 0; k < nadj; k++) tt[3 * k + 2] = vA[k] * Area * detJac;
             }
-            if (a.compute_ext) {
+            __syncthreads();
+            for (int task = tid; task < 3 * nn; task += nth)
+                for (int k = 0; k < nadj; k++) {
+                    double g = gi_s[task * nadj + k];
+                    for (int ql = 0; ql < nqc; ql++) {
+                        const double *tt = terms + ((size_t)task * a.qchunk + ql) * 3 * nadj + 3 * k;
+                        g = g - tt[0];
+                        g = g - tt[1];
+                        g = g - tt[2];
+                    }
+                    gi_s[task * nadj + k] = g;
+                }
+        }
+    }
+    // ---------------- stage B': body-load work, one task per (control
+    // point, component), points in order
+    for (int task = tid; task < 3 * nn; task += nth) {
+        const int cp = task / 3, c = task - 3 * cp;
+        double ge[kGradMaxAdj];
+        for (int k = 0; k < kGradMaxAdj; k++) ge[k] = 0.0;
+        if (a.compute_ext && nbody > 0) {
+            for (int q = 0; q < a.nq; q++) {
+                const double *P = pts + (size_t)q * L.size;
+                const double *dr = P + L.dR + 3 * cp;
+                const double Area = P[L.area], detJac = P[L.dj];
+                const double *AxA = P + L.AxA;
                 for (int b = 0; b < nbody; b++) {
                     const double *lf = P + L.body + 6 * b, *vd = lf + 3;
                     const int nl = s_body[b];
@@ -414,7 +451,7 @@ __global__ void __launch_bounds__(256) k_u1_grad(GradArgs a) {
         }
         double *oi = a.egi + (size_t)blockIdx.x * nadj * 3 * nn;
         for (int k = 0; k < nadj; k++) {
-            oi[k + nadj * (c + 3 * cp)] = gi[k];
+            oi[k + nadj * (c + 3 * cp)] = gi_s[task * nadj + k];
             ge_s[task * nadj + k] = ge[k];
         }
     }
@@ -673,7 +710,11 @@ YETI_API int yeti_grad_lin_elast_work(yeti_ctx *ctx, const yeti_u1_model *m,
         const PtLayout L = pt_layout(P.nn, (int)nadj, max_body);
         const size_t vol = (size_t)P.nq * L.size;
         const size_t face = (size_t)P.ng * P.ng * (4 * P.nn + 11 + 3 * nadj);
-        const size_t smem = sizeof(double) * grad_smem_doubles(P.nn, P.nq, (int)nadj, L, face);
+        // term buffer of stage B: up to 6144 doubles (48 KB), whole chunks of points
+        const int qchunk = (int)std::max<int64_t>(
+            1, std::min<int64_t>(P.nq, 6144 / (9 * (int64_t)P.nn * nadj)));
+        g.qchunk = qchunk;
+        const size_t smem = sizeof(double) * grad_smem_doubles(P.nn, P.nq, (int)nadj, L, face, qchunk);
         YETI_CHECK(smem <= (size_t)smem_optin, YETI_EUNSUPPORTED,
                    "shape gradient: element needs %zu bytes of shared memory", smem);
         YETI_TRY(set_smem_optin((const void *)k_u1_grad, ctx->device, smem, "shape gradient element"));
