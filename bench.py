@@ -330,6 +330,62 @@ def stiffness_flops(nq, nn, nel):
     return nel * nq * (nn * (nn + 1) // 2 * 72 + nn * 60)
 
 
+def stiffness_sf_flops(n, g, nel):
+    """FP64 operations of k_u1_stiffness_sf per its loops (2 per
+    multiply-add): the per-point geometry pass (nn sums of 16 values) and,
+    for each of the six blocks, the w, v and u contractions."""
+    nu, nv, nw = n
+    nn, nq = nu * nv * nw, g ** 3
+    blk = (16 * nw * g ** 3 + 12 * nw ** 2 * g ** 3 + 9 * nv * nw ** 2 * g ** 2 +
+           6 * nv ** 2 * nw ** 2 * g ** 2 + 4 * nu * nv ** 2 * nw ** 2 * g)
+    out = 6 * blk + (3 + 3 * 0.5) * nn * nn * 2 * g   # diagonal blocks: half the pairs
+    return nel * 2 * (out + nq * nn * 18 + 6 * 16 * nq * 6)
+
+
+def assembly_beyond_p2(device, seed):
+    """U1 COO assembly of perturbed rational cubes of degree 3 and 4 with the
+    pair kernel (bit-identical to the oracle) and the sum-factorised kernel,
+    device times of the element kernels from the context's CUDA-event
+    timers, and the oracle (OpenMP) on the same model."""
+    import oracle
+    from yeti_b200._lib import Context
+    from yeti_b200.patches import cube_patch, u1_system_args
+    from yeti_b200.stiffmtrx_elemstorage import sys_linmat_lindef_static
+    ctx = Context(device)
+    out = {}
+    for tag, nel, p in (("p3_16x16x16", (16, 16, 16), 3), ("p4_12x12x12", (12, 12, 12), 4)):
+        args = u1_system_args(cube_patch(nel, p, perturb=0.1, wrange=(0.8, 1.2), seed=seed),
+                              E=1.0, nu=0.3)
+        nelt = nel[0] * nel[1] * nel[2]
+        nn, g = (p + 1) ** 3, p + 1
+        r = {"elements": nelt, "nb_data": int(args[1])}
+        for kern, name in (("pairs", "k_u1_stiffness"), ("sumfact", "k_u1_stiffness_sf")):
+            sys_linmat_lindef_static(*args, ctx=ctx, device_out=True, element_kernel=kern)
+            ctx.set_timing(True)
+            reps = 3
+            for _ in range(reps):
+                sys_linmat_lindef_static(*args, ctx=ctx, device_out=True, element_kernel=kern)
+            r[f"{kern}_kernel_ms_events"] = ctx.kernel_ms(name) / reps
+            ctx.set_timing(False)
+        k_p = sys_linmat_lindef_static(*args, ctx=ctx)[0]
+        k_s = sys_linmat_lindef_static(*args, ctx=ctx, element_kernel="sumfact")[0]
+        t0 = time.perf_counter()
+        k_o = oracle.sys_linmat_lindef_static(*args)[0]
+        r["cpu_oracle_ms"] = (time.perf_counter() - t0) * 1e3
+        r["cpu_cores"] = oracle.threads()
+        r["pairs_bit_identical"] = bool(np.array_equal(k_p, k_o))
+        r["sumfact_max_rel_diff_vs_oracle"] = float(np.abs(k_s - k_o).max() / np.abs(k_o).max())
+        r["pairs_gflop"] = stiffness_flops(g ** 3, nn, nelt) / 1e9
+        r["sumfact_gflop"] = stiffness_sf_flops((p + 1,) * 3, g, nelt) / 1e9
+        r["sumfact_speedup_vs_pairs"] = r["pairs_kernel_ms_events"] / r["sumfact_kernel_ms_events"]
+        # the COO output (value + row + col, 16 B a slot) is the HBM floor
+        r["sumfact_hbm_gbs_output"] = int(args[1]) * 16 / (r["sumfact_kernel_ms_events"] / 1e3) / 1e9
+        del k_p, k_s, k_o
+        out[tag] = r
+    ctx.close()
+    return out
+
+
 def gradient_flops(nq, nn, nel, nadj=1):
     """FP64 operations of k_u1_grad: per (point, control point, component)
     the interior-work derivative terms (dJ, the strain variation, dAAI, the
@@ -406,6 +462,14 @@ def extra_configs(args, device):
     t_mo = (time.perf_counter() - t0) * 1e3
     out["mass_matrix_p2_16x4x4"] = {"gpu_ms_device_out": t_m, "cpu_oracle_ms": t_mo,
                                     "cpu_cores": oracle.threads(), "bit_identical": bool(np.array_equal(md, mo))}
+
+    asm = assembly_beyond_p2(device, WORKLOAD["seed"] + 7)
+    for tag, r in asm.items():
+        r["pairs_fp64_frac_of_measured_dgemm"] = (r["pairs_gflop"] / (r["pairs_kernel_ms_events"] / 1e3)
+                                                  / 1e3 / peak64)
+        r["sumfact_fp64_frac_of_measured_dgemm"] = (r["sumfact_gflop"] / (r["sumfact_kernel_ms_events"] / 1e3)
+                                                    / 1e3 / peak64)
+        out["assembly_" + tag] = r
     # C3: shape gradient (adjoint kernel; parity vs the CPU oracle)
     a3 = _system_args("quarter_annulus_p2_32x32x2")
     U, _ = _solve(a3, np.asarray(a3[2], dtype=np.float64))

@@ -71,6 +71,15 @@ int yeti_ctx_set_stream(yeti_ctx *ctx, void *stream);
 int yeti_ctx_synchronize(yeti_ctx *ctx);
 /* Bytes of device memory currently held by the context's objects. */
 size_t yeti_ctx_bytes_in_use(const yeti_ctx *ctx);
+/* Device-time accounting (no counterpart in the reference).  With timing
+ * on, the element kernels of the Gauss-quadrature calls ("k_u1_stiffness",
+ * "k_u1_stiffness_sf", "k_u1_mass", "k_u1_grad") are bracketed by CUDA
+ * events on the context's stream and their durations summed per name;
+ * yeti_ctx_set_timing() clears the sums.  Each timed launch waits for its
+ * end event, so leave timing off outside measurements. */
+int yeti_ctx_set_timing(yeti_ctx *ctx, int on);
+/* Summed device milliseconds of `kernel` since timing was set; -1 if none. */
+double yeti_ctx_kernel_ms(yeti_ctx *ctx, const char *kernel);
 
 /* ------------------------------------------------------------------------
  * U1 element stiffness + COO assembly (drop-in for sys_linmat_lindef_static)
@@ -117,6 +126,22 @@ typedef struct {
 int yeti_assemble_u1_coo(yeti_ctx *ctx, const yeti_u1_model *model,
                          int64_t nb_data, double *kdata, int32_t *krow,
                          int32_t *kcol, double *F, int mem);
+/* The same, with a choice of element kernel (no counterpart in the
+ * reference, whose element routine is the pair loop):
+ *   YETI_STIFF_PAIRS    one thread per control-point pair summing over the
+ *                       Gauss points in the reference's operation order
+ *                       (bit-identical to it; what yeti_assemble_u1_coo runs);
+ *   YETI_STIFF_SUMFACT  B^T D B contracted direction by direction over the
+ *                       1-D basis tables (sum factorisation): the same slots,
+ *                       values equal to rounding (not bit for bit), fewer
+ *                       operations from degree 3 on.  Needs NBINT = g^3 with
+ *                       g <= 8 and the element's buffers in shared memory
+ *                       (degree <= 5 at g = p+1), else YETI_EUNSUPPORTED. */
+#define YETI_STIFF_PAIRS 0
+#define YETI_STIFF_SUMFACT 1
+int yeti_assemble_u1_coo_ex(yeti_ctx *ctx, const yeti_u1_model *model,
+                            int64_t nb_data, double *kdata, int32_t *krow,
+                            int32_t *kcol, double *F, int mem, int kernel);
 /* Consistent mass matrix of the active U1 elements in the same COO slot
  * order (replaces massmtrx.build_cmassmatrix: build_CMASSMatrix,
  * src/yeti_iga/main/compute_CMASSMatrix.f:30-199, with UMASSMAT_byCP's U1

@@ -208,3 +208,105 @@ def test_gpu_rejects_unsupported_element(cuda_ok):
     args[10] = "U3"   # shell patch
     with pytest.raises(YetiError):
         sys_linmat_lindef_static(*args)
+
+
+# ------------------------------------------- sum-factorised element kernel
+# Synthetic U1 cubes beyond the fixtures' degree 2: (elements, degrees,
+# perturbation, weight range).  Mixed degrees keep one Gauss count per
+# direction (max p + 1), as the reference's NBINT does.
+SF_PATCHES = {
+    "p3_3x3x2": ((3, 3, 2), 3, 0.2, (0.8, 1.2)),
+    "p4_2x2x2": ((2, 2, 2), 4, 0.1, (0.8, 1.2)),
+    "p234_2x3x2": ((2, 3, 2), (2, 3, 4), 0.15, (0.9, 1.1)),
+    "p5_2x1x1": ((2, 1, 1), 5, 0.1, None),
+}
+
+
+def _sf_args(name):
+    from yeti_b200.patches import cube_patch, u1_system_args
+    nel, p, pert, wr = SF_PATCHES[name]
+    return u1_system_args(cube_patch(nel, p, perturb=pert, wrange=wr, seed=11), E=210.0, nu=0.3)
+
+
+def test_u1_system_args_match_the_reference_layout():
+    """The synthetic model builder reproduces the IEN / Nijk / weight / knot
+    layout that the reference's preprocessing wrote for the p=2 cantilever."""
+    from yeti_b200.patches import u1_system_args
+    from yeti_b200.stiffmtrx_elemstorage import SYSTEM_ARG_NAMES
+    d, args = load_fixture("cantilever_p2_16x4x4")
+    mine = u1_system_args({"p": (2, 2, 2), "nel": (16, 4, 4), "cps": np.asarray(d["COORDS3D"]),
+                           "weights": np.ones(int(d["nb_cp"]))}, E=210000.0, nu=0.3)
+    for name, a, b in zip(SYSTEM_ARG_NAMES, args, mine):
+        if name in ("activeElement", "IEN", "Nkv", "Ukv", "Nijk", "weight", "Jpqr", "NBINT", "NNODE",
+                    "MATERIAL_PROPERTIES", "nb_elem", "nb_cp", "nb_dof_tot"):
+            np.testing.assert_array_equal(np.asarray(a).ravel(), np.asarray(b).ravel(), err_msg=name)
+    k0 = oracle.sys_linmat_lindef_static(*args)[0]
+    k1 = oracle.sys_linmat_lindef_static(*mine)[0]
+    np.testing.assert_array_equal(k0, k1)
+
+
+def _check_close(k0, r0, c0, k1, r1, c1):
+    np.testing.assert_array_equal(r1, r0)
+    np.testing.assert_array_equal(c1, c0)
+    assert np.linalg.norm(k1 - k0) <= TOL * np.linalg.norm(k0)
+    assert np.abs(k1 - k0).max() <= TOL * np.abs(k0).max()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", FIXTURES)
+def test_gpu_sumfact_matches_oracle_on_fixtures(cuda_ok, name):
+    from yeti_b200.stiffmtrx_elemstorage import sys_linmat_lindef_static
+    d, args = load_fixture(name)
+    k0, r0, c0, f0 = oracle.sys_linmat_lindef_static(*args)
+    k1, r1, c1, f1 = sys_linmat_lindef_static(*args, element_kernel="sumfact")
+    _check_close(k0, r0, c0, k1, r1, c1)
+    np.testing.assert_array_equal(f1, f0)   # the load vector is the same kernel's
+    if int(d["nb_dof_free"]) < int(d["nb_dof_tot"]) and np.linalg.norm(f0) > 0:
+        s0 = _solve(d, k0, r0, c0, f0)
+        s1 = _solve(d, k1, r1, c1, f1)
+        assert np.linalg.norm(s1 - s0) <= TOL * np.linalg.norm(s0)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", list(SF_PATCHES))
+def test_gpu_sumfact_and_pairs_match_oracle_beyond_degree_two(cuda_ok, name):
+    from yeti_b200.stiffmtrx_elemstorage import sys_linmat_lindef_static
+    args = _sf_args(name)
+    k0, r0, c0, _ = oracle.sys_linmat_lindef_static(*args)
+    k1, r1, c1, _ = sys_linmat_lindef_static(*args, element_kernel="sumfact")
+    _check_close(k0, r0, c0, k1, r1, c1)
+    k2, r2, c2, _ = sys_linmat_lindef_static(*args)
+    np.testing.assert_array_equal(k2, k0)
+    np.testing.assert_array_equal(r2, r0)
+    np.testing.assert_array_equal(c2, c0)
+
+
+@pytest.mark.gpu
+def test_gpu_sumfact_rejects_a_partial_gauss_rule(cuda_ok):
+    from yeti_b200._lib import YetiError
+    from yeti_b200.patches import cube_patch, u1_system_args
+    from yeti_b200.stiffmtrx_elemstorage import sys_linmat_lindef_static
+    args = u1_system_args(cube_patch((2, 2, 2), 2), nbint=26)
+    with pytest.raises(YetiError, match="EUNSUPPORTED"):
+        sys_linmat_lindef_static(*args, element_kernel="sumfact")
+    with pytest.raises(ValueError):
+        sys_linmat_lindef_static(*args, element_kernel="fast")
+
+
+@pytest.mark.gpu
+def test_gpu_context_times_the_element_kernels(cuda_ok):
+    from yeti_b200._lib import Context
+    from yeti_b200.stiffmtrx_elemstorage import sys_linmat_lindef_static
+    args = _sf_args("p3_3x3x2")
+    ctx = Context(0)
+    assert ctx.kernel_ms("k_u1_stiffness") is None
+    ctx.set_timing(True)
+    sys_linmat_lindef_static(*args, ctx=ctx)
+    sys_linmat_lindef_static(*args, ctx=ctx, element_kernel="sumfact")
+    t_pairs, t_sf = ctx.kernel_ms("k_u1_stiffness"), ctx.kernel_ms("k_u1_stiffness_sf")
+    assert t_pairs is not None and t_pairs > 0 and t_sf is not None and t_sf > 0
+    ctx.set_timing(False)
+    assert ctx.kernel_ms("k_u1_stiffness") is None
+    sys_linmat_lindef_static(*args, ctx=ctx)
+    assert ctx.kernel_ms("k_u1_stiffness") is None
+    ctx.close()

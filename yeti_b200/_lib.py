@@ -17,6 +17,7 @@ ERRORS = {-1: "EINVAL", -2: "ECUDA", -3: "ENOMEM", -4: "EUNSUPPORTED",
           -5: "ETIMEDOUT", -6: "EBREAKDOWN", -7: "ENUMERIC", -8: "ENOTCONV"}
 MEM_HOST, MEM_DEVICE = 0, 1
 PREC_F64, PREC_F32 = 0, 1
+STIFF_PAIRS, STIFF_SUMFACT = 0, 1
 
 _lib = None
 _lock = threading.Lock()
@@ -95,6 +96,8 @@ def _declare(lib):
         "yeti_ctx_set_stream": (i32, [vp, vp]),
         "yeti_ctx_synchronize": (i32, [vp]),
         "yeti_ctx_bytes_in_use": (ctypes.c_size_t, [vp]),
+        "yeti_ctx_set_timing": (i32, [vp, i32]),
+        "yeti_ctx_kernel_ms": (ctypes.c_double, [vp, ctypes.c_char_p]),
         "yeti_serve_open": (i32, [i32, ctypes.c_size_t, i32, ctypes.POINTER(vp)]),
         "yeti_serve_submit": (i32, [vp, ctypes.POINTER(ServeRequest), ctypes.POINTER(i64)]),
         "yeti_serve_poll": (i32, [vp, i64, vp, ctypes.POINTER(ServeResult)]),
@@ -104,6 +107,8 @@ def _declare(lib):
         "yeti_serve_close": (i32, [vp]),
         "yeti_assemble_u1_coo": (i32, [vp, ctypes.POINTER(U1Model), i64, vp,
                                        vp, vp, vp, i32]),
+        "yeti_assemble_u1_coo_ex": (i32, [vp, ctypes.POINTER(U1Model), i64, vp,
+                                          vp, vp, vp, i32, i32]),
         "yeti_wq_setup": (i32, [vp, vp, vp, vp, vp, dbl, dbl, vp, i32,
                                 ctypes.POINTER(vp)]),
         "yeti_wq_destroy": (i32, [vp]),
@@ -199,6 +204,16 @@ class Context:
 
     def bytes_in_use(self):
         return int(lib().yeti_ctx_bytes_in_use(self.handle))
+
+    def set_timing(self, on=True):
+        """Sum the device time of the element kernels per name (CUDA events
+        on the context's stream); clears the sums."""
+        check(lib().yeti_ctx_set_timing(self.handle, int(bool(on))), "yeti_ctx_set_timing")
+
+    def kernel_ms(self, kernel):
+        """Summed device ms of `kernel` since set_timing(); None if none."""
+        v = float(lib().yeti_ctx_kernel_ms(self.handle, kernel.encode()))
+        return None if v < 0 else v
 
     def close(self):
         if getattr(self, "handle", None):

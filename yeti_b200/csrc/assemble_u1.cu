@@ -818,14 +818,16 @@ static bool in_list(const int64_t *l, int64_t n, int64_t v) {
 
 using namespace yeti;
 
-YETI_API int yeti_assemble_u1_coo(yeti_ctx *ctx, const yeti_u1_model *m,
-                                  int64_t nb_data, double *kdata,
-                                  int32_t *krow, int32_t *kcol, double *F,
-                                  int mem) {
+YETI_API int yeti_assemble_u1_coo_ex(yeti_ctx *ctx, const yeti_u1_model *m,
+                                     int64_t nb_data, double *kdata,
+                                     int32_t *krow, int32_t *kcol, double *F,
+                                     int mem, int kernel) {
     YETI_CHECK(ctx && m && kdata && krow && kcol && F, YETI_EINVAL,
                "yeti_assemble_u1_coo: NULL argument");
     YETI_CHECK(mem == YETI_MEM_HOST || mem == YETI_MEM_DEVICE, YETI_EINVAL,
                "yeti_assemble_u1_coo: bad mem flag %d", mem);
+    YETI_CHECK(kernel == YETI_STIFF_PAIRS || kernel == YETI_STIFF_SUMFACT, YETI_EINVAL,
+               "yeti_assemble_u1_coo: bad element kernel %d", kernel);
     DeviceGuard guard(ctx->device);
     U1Model M;
     YETI_TRY(u1_prepare(ctx, m, M));
@@ -917,15 +919,21 @@ YETI_API int yeti_assemble_u1_coo(yeti_ctx *ctx, const yeti_u1_model *m,
         a.mu = P.E / (2.0 * (1.0 + P.nu));
         a.kdata = k_; a.krow = r_; a.kcol = c_;
         const size_t smem = fixed + perq * qchunk;
-        int64_t left = P.nactive, off = 0;
-        while (left > 0) {   // grid.x limit
-            int64_t n = std::min<int64_t>(left, 1 << 30);
-            StiffArgs b = a;
-            b.ien += off * P.nn; b.w += off * P.nn; b.span += off * 3; b.slot += off;
-            k_u1_stiffness<<<(unsigned)n, 256, smem, ctx->stream>>>(b);
-            count_launches(1);
-            YETI_CUDA(cudaGetLastError());
-            left -= n; off += n;
+        if (kernel == YETI_STIFF_SUMFACT) {
+            KernelTimer timer(ctx, "k_u1_stiffness_sf");
+            YETI_TRY(launch_u1_stiffness_sf(ctx, P, a.coords, a.lam, a.mu, k_, r_, c_, smem_cap));
+        } else {
+            KernelTimer timer(ctx, "k_u1_stiffness");
+            int64_t left = P.nactive, off = 0;
+            while (left > 0) {   // grid.x limit
+                int64_t n = std::min<int64_t>(left, 1 << 30);
+                StiffArgs b = a;
+                b.ien += off * P.nn; b.w += off * P.nn; b.span += off * 3; b.slot += off;
+                k_u1_stiffness<<<(unsigned)n, 256, smem, ctx->stream>>>(b);
+                count_launches(1);
+                YETI_CUDA(cudaGetLastError());
+                left -= n; off += n;
+            }
         }
         // ---- distributed loads of this patch's elements
         std::vector<int32_t> elems, tptr(1, 0);
@@ -1075,6 +1083,13 @@ YETI_API int yeti_assemble_u1_coo(yeti_ctx *ctx, const yeti_u1_model *m,
     return YETI_OK;
 }
 
+YETI_API int yeti_assemble_u1_coo(yeti_ctx *ctx, const yeti_u1_model *m,
+                                  int64_t nb_data, double *kdata,
+                                  int32_t *krow, int32_t *kcol, double *F,
+                                  int mem) {
+    return yeti_assemble_u1_coo_ex(ctx, m, nb_data, kdata, krow, kcol, F, mem, YETI_STIFF_PAIRS);
+}
+
 YETI_API int yeti_assemble_u1_mass_coo(yeti_ctx *ctx, const yeti_u1_model *m,
                                        int64_t nb_data, double *mdata, int32_t *mrow,
                                        int32_t *mcol, int mem) {
@@ -1132,6 +1147,7 @@ YETI_API int yeti_assemble_u1_mass_coo(yeti_ctx *ctx, const yeti_u1_model *m,
         a.rho = P.rho;
         a.mdata = m_; a.mrow = r_; a.mcol = c_;
         const size_t smem = fixed + perq * qchunk;
+        KernelTimer timer(ctx, "k_u1_mass");
         int64_t left = P.nactive, off = 0;
         while (left > 0) {   // grid.x limit
             const int64_t n = std::min<int64_t>(left, 1 << 30);

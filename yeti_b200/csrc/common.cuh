@@ -4,6 +4,8 @@
 #include <atomic>
 #include <cstdint>
 #include <cstdio>
+#include <map>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -53,6 +55,10 @@ struct yeti_ctx {
     // allocate with cudaMallocAsync / cudaFreeAsync on `stream` (no implicit
     // device synchronisation; for contexts driven by the serving loop)
     bool stream_ordered = false;
+    // device-time accounting of the element kernels (yeti_ctx_set_timing)
+    bool timing = false;
+    std::mutex timing_mu;
+    std::map<std::string, double> kernel_ms;
 };
 
 namespace yeti {
@@ -132,6 +138,18 @@ bool is_device_pointer(const void *p);
 // concurrently cannot lower the limit under each other's launch.  Fails with
 // YETI_EUNSUPPORTED when `need` dynamic bytes exceed it.
 int set_smem_optin(const void *func, int device, size_t need, const char *what);
+
+// With the context's timing on, the device time of the work enqueued on
+// ctx->stream during the object's lifetime (CUDA events on that stream,
+// waited for on destruction) is added to ctx->kernel_ms[name]; with timing
+// off it does nothing.
+struct KernelTimer {
+    yeti_ctx *ctx;
+    const char *name;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    KernelTimer(yeti_ctx *c, const char *n);
+    ~KernelTimer();
+};
 
 // Process-wide count of kernel launches issued by the library (reported by
 // yeti_kernel_launches(); lets callers verify the device path ran).

@@ -139,3 +139,44 @@ YETI_API int yeti_ctx_synchronize(yeti_ctx *ctx) {
 YETI_API size_t yeti_ctx_bytes_in_use(const yeti_ctx *ctx) {
     return ctx ? ctx->bytes_in_use.load() : 0;
 }
+
+namespace yeti {
+
+KernelTimer::KernelTimer(yeti_ctx *c, const char *n) : ctx(c), name(n) {
+    if (!ctx || !ctx->timing) return;
+    if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess ||
+        cudaEventRecord(e0, ctx->stream) != cudaSuccess) {
+        if (e0) cudaEventDestroy(e0);
+        if (e1) cudaEventDestroy(e1);
+        e0 = e1 = nullptr;
+    }
+}
+
+KernelTimer::~KernelTimer() {
+    if (!e0) return;
+    float ms = 0.f;
+    if (cudaEventRecord(e1, ctx->stream) == cudaSuccess && cudaEventSynchronize(e1) == cudaSuccess &&
+        cudaEventElapsedTime(&ms, e0, e1) == cudaSuccess) {
+        std::lock_guard<std::mutex> lk(ctx->timing_mu);
+        ctx->kernel_ms[name] += ms;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+}
+
+}  // namespace yeti
+
+YETI_API int yeti_ctx_set_timing(yeti_ctx *ctx, int on) {
+    YETI_CHECK(ctx, YETI_EINVAL, "yeti_ctx_set_timing: ctx is NULL");
+    std::lock_guard<std::mutex> lk(ctx->timing_mu);
+    ctx->timing = on != 0;
+    ctx->kernel_ms.clear();
+    return YETI_OK;
+}
+
+YETI_API double yeti_ctx_kernel_ms(yeti_ctx *ctx, const char *kernel) {
+    if (!ctx || !kernel) return -1.0;
+    std::lock_guard<std::mutex> lk(ctx->timing_mu);
+    auto it = ctx->kernel_ms.find(kernel);
+    return it == ctx->kernel_ms.end() ? -1.0 : it->second;
+}

@@ -718,6 +718,7 @@ YETI_API int yeti_grad_lin_elast_work(yeti_ctx *ctx, const yeti_u1_model *m,
         YETI_CHECK(smem <= (size_t)smem_optin, YETI_EUNSUPPORTED,
                    "shape gradient: element needs %zu bytes of shared memory", smem);
         YETI_TRY(set_smem_optin((const void *)k_u1_grad, ctx->device, smem, "shape gradient element"));
+        KernelTimer timer(ctx, "k_u1_grad");
         k_u1_grad<<<(unsigned)elems.size(), 256, smem, s>>>(g);
         count_launches(1);
         YETI_CUDA(cudaGetLastError());

@@ -41,4 +41,10 @@ struct U1Model {
 // elements, build_system_elemStorage.f90:156-293) and upload the geometry.
 int u1_prepare(yeti_ctx *ctx, const yeti_u1_model *m, U1Model &out);
 
+// Element stiffness of one patch's active elements by the sum-factorised
+// kernel (stiff_sf.cu), written into the COO slots of the pair kernel.
+int launch_u1_stiffness_sf(yeti_ctx *ctx, const U1Patch &P, const double *coords,
+                           double lam, double mu, double *kdata, int32_t *krow,
+                           int32_t *kcol, size_t smem_cap);
+
 }  // namespace yeti

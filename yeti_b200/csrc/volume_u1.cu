@@ -138,12 +138,36 @@ __global__ void __launch_bounds__(128) k_u1_volume(VolArgs a) {
             }
 }
 
-// vol = sum of the terms in order (one thread: the reference's running sum)
-__global__ void k_volume_sum(const double *vterm, int64_t n, double *vol) {
-    if (blockIdx.x != 0 || threadIdx.x != 0) return;
+// vol = sum of the terms in order (the reference's running sum).  The
+// block brings the terms into shared memory in coalesced chunks; one thread
+// adds them in order, from shared memory, while nothing else is waited for.
+constexpr int kVolChunk = 4096;
+__global__ void __launch_bounds__(1024) k_volume_sum(const double *vterm, int64_t n, double *vol) {
+    __shared__ double buf[kVolChunk];
     double v = 0.0;
-    for (int64_t i = 0; i < n; i++) v = v + vterm[i];
-    *vol = v;
+    for (int64_t c0 = 0; c0 < n; c0 += kVolChunk) {
+        const int m = (int)(n - c0 < kVolChunk ? n - c0 : kVolChunk);
+        __syncthreads();
+        for (int i = threadIdx.x; i < m; i += blockDim.x) buf[i] = vterm[c0 + i];
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            int i = 0;
+            for (; i + 8 <= m; i += 8) {
+                const double t0 = buf[i], t1 = buf[i + 1], t2 = buf[i + 2], t3 = buf[i + 3];
+                const double t4 = buf[i + 4], t5 = buf[i + 5], t6 = buf[i + 6], t7 = buf[i + 7];
+                v = v + t0;
+                v = v + t1;
+                v = v + t2;
+                v = v + t3;
+                v = v + t4;
+                v = v + t5;
+                v = v + t6;
+                v = v + t7;
+            }
+            for (; i < m; i++) v = v + buf[i];
+        }
+    }
+    if (threadIdx.x == 0) *vol = v;
 }
 
 // grad[j] = sum over the terms idx[ptr[j] .. ptr[j+1]) in order
@@ -233,7 +257,7 @@ YETI_API int yeti_volume_u1(yeti_ctx *ctx, const yeti_u1_model *m, double *vol,
         YETI_CUDA(cudaGetLastError());
         goff += nt * P.nn * 3;
     }
-    k_volume_sum<<<1, 32, 0, s>>>(dvt.as<double>(), nterm, dv.as<double>());
+    k_volume_sum<<<1, 1024, 0, s>>>(dvt.as<double>(), nterm, dv.as<double>());
     count_launches(1);
     YETI_CUDA(cudaGetLastError());
     if (want_grad) {

@@ -49,6 +49,75 @@ def cube_patch(nel, p, size=(1.0, 1.0, 1.0), perturb=0.0, wrange=None,
             "weights": np.ascontiguousarray(weights)}
 
 
+def u1_system_args(patch, E=1.0, nu=0.3, rho=0.0, nbint=None):
+    """The 38 positional arguments of ``sys_linmat_lindef_static`` (the
+    order of ``IGAparametrization.get_inputs4system_elemStorage()``,
+    IGA_parametrization.py:1705-1716) for a single U1 patch from
+    :func:`cube_patch`: every element active, no loads and no boundary
+    conditions (all dofs free), NBINT = (max p + 1)^3 unless given.
+
+    IEN lists each element's control points in the reference's descending
+    local order: local node (i, j, k) is the control point of tensor index
+    (span_u - 1 - i, span_v - 1 - j, span_w - 1 - k), spans 1-based."""
+    p, nel = patch["p"], patch["nel"]
+    n = [p[d] + nel[d] for d in range(3)]
+    kvs = [np.concatenate([np.zeros(p[d] + 1), np.arange(1, nel[d]) / nel[d],
+                           np.ones(p[d] + 1)]) for d in range(3)]
+    nb_cp = n[0] * n[1] * n[2]
+    nb_elem = nel[0] * nel[1] * nel[2]
+    nn = (p[0] + 1) * (p[1] + 1) * (p[2] + 1)
+    ew, ev, eu = np.meshgrid(np.arange(nel[2]), np.arange(nel[1]),
+                             np.arange(nel[0]), indexing="ij")
+    nijk = np.stack([eu.ravel() + p[0] + 1, ev.ravel() + p[1] + 1,
+                     ew.ravel() + p[2] + 1])           # (3, nb_elem)
+    k, j, i = np.meshgrid(np.arange(p[2] + 1), np.arange(p[1] + 1),
+                          np.arange(p[0] + 1), indexing="ij")
+    i, j, k = i.ravel(), j.ravel(), k.ravel()            # local node order
+    iu = nijk[0][:, None] - 1 - i[None, :]
+    iv = nijk[1][:, None] - 1 - j[None, :]
+    iw = nijk[2][:, None] - 1 - k[None, :]
+    cp0 = iu + n[0] * (iv + n[1] * iw)                  # (nb_elem, nn), 0-based
+    ien = (cp0 + 1).astype(np.int64).ravel()
+    weight = np.asarray(patch["weights"], dtype=np.float64)[cp0].ravel()
+    ng = max(p) + 1
+    nbint = ng ** 3 if nbint is None else int(nbint)
+    ndof = 3 * nb_cp
+    return [
+        np.ones(nb_elem, dtype=np.int64),                      # activeElement
+        float(nb_elem * (9 * nn * (nn - 1) // 2 + 6 * nn)),    # nb_data
+        np.asarray(patch["cps"], dtype=np.float64),            # COORDS3D
+        ien,                                                   # IEN
+        np.array([nb_elem], dtype=np.int64),                   # nb_elem_patch
+        np.array([[len(kv)] for kv in kvs], dtype=np.int64),   # Nkv (3, 1)
+        np.concatenate(kvs),                                   # Ukv
+        nijk.astype(np.int64),                                 # Nijk
+        weight,                                                # weight
+        np.array([[p[0]], [p[1]], [p[2]]], dtype=np.int64),    # Jpqr
+        np.array("U1"),                                        # ELT_TYPE
+        np.array([1.0]), np.array([1], dtype=np.int64),        # PROPS, JPROPS
+        np.array([[E], [nu]], dtype=np.float64),               # MATERIAL_PROPERTIES
+        np.array([3], dtype=np.int64),                         # n_mat_props
+        np.array([rho], dtype=np.float64),                     # RHO
+        np.array("/THREED"),                                   # TENSOR
+        np.zeros(0, dtype=np.int64),                           # indDLoad
+        np.zeros(0, dtype=np.int64),                           # JDLType
+        np.zeros(0, dtype=np.float64),                         # ADLMAG
+        np.zeros(0, dtype=np.int64),                           # load_target_nbelem
+        np.zeros(0, dtype=np.float64),                         # load_additionalInfos
+        np.zeros(0, dtype=np.int64),                           # nb_load_additionalInfos
+        np.zeros((2, 0), dtype=np.float64),                    # bc_values
+        np.zeros(0, dtype=np.int64),                           # bc_target
+        np.zeros(0, dtype=np.int64),                           # bc_target_nbelem
+        np.arange(1, ndof + 1, dtype=np.int64),                # ind_dof_free
+        ndof,                                                  # nb_dof_free
+        3,                                                     # MCRD
+        np.array([nbint], dtype=np.int64),                     # NBINT
+        np.array([nn], dtype=np.int64),                        # NNODE
+        np.zeros((1, nb_cp), dtype=np.float64),                # nodal_dist
+        0, 0, 1, nb_elem, nb_cp, ndof,   # nb_bc, nb_load, nb_patch, nb_elem, nb_cp, nb_dof_tot
+    ]
+
+
 def face_mask(clamp_faces):
     """dirichlet[6*c + f] array from {'u0': comps, 'w1': comps, ...}."""
     names = ["u0", "u1", "v0", "v1", "w0", "w1"]

@@ -117,7 +117,8 @@ def pack_u1_model(activeElement, nb_data, COORDS3D, IEN, nb_elem_patch, Nkv,
     return PackedModel(arrays, s, int(nb_data), nb_dof_tot)
 
 
-def sys_linmat_lindef_static(*args, ctx=None, device_out=False, **kwargs):
+def sys_linmat_lindef_static(*args, ctx=None, device_out=False,
+                             element_kernel="pairs", **kwargs):
     """GPU twin of ``stiffmtrx_elemstorage.sys_linmat_lindef_static``.
 
     Positional arguments: the 38 items of
@@ -125,7 +126,16 @@ def sys_linmat_lindef_static(*args, ctx=None, device_out=False, **kwargs):
     (``IGA_parametrization.py:1705-1716``).  Returns numpy
     ``(Kdata float64, Krow int32, Kcol int32, F float64)``; with
     ``device_out=True`` the four are torch CUDA tensors instead.
+
+    ``element_kernel``: ``"pairs"`` (default) sums each control-point pair's
+    block over the Gauss points in the reference's operation order, so the
+    values are bit-identical to it; ``"sumfact"`` contracts BᵀDB direction by
+    direction over the 1-D basis tables (same slots, values equal to
+    rounding, far fewer operations from degree 3 on).
     """
+    kinds = {"pairs": _lib.STIFF_PAIRS, "sumfact": _lib.STIFF_SUMFACT}
+    if element_kernel not in kinds:
+        raise ValueError(f"element_kernel must be one of {sorted(kinds)}")
     pm = pack_u1_model(*args, **kwargs)
     ctx = ctx or _lib.default_context()
     n = pm.nb_data
@@ -143,7 +153,8 @@ def sys_linmat_lindef_static(*args, ctx=None, device_out=False, **kwargs):
         kcol = np.empty(n, dtype=np.int32)
         F = np.empty(pm.nb_dof_tot, dtype=np.float64)
         mem = MEM_HOST
-    check(lib().yeti_assemble_u1_coo(ctx.handle, pm.struct, n, ptr(kdata),
-                                     ptr(krow), ptr(kcol), ptr(F), mem),
+    check(lib().yeti_assemble_u1_coo_ex(ctx.handle, pm.struct, n, ptr(kdata),
+                                        ptr(krow), ptr(kcol), ptr(F), mem,
+                                        kinds[element_kernel]),
           "yeti_assemble_u1_coo")
     return kdata, krow, kcol, F
