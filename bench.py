@@ -435,11 +435,19 @@ def extra_configs(args, device):
     peak64 = fp64_peak_tflops()
     t_ev = _event_ms(lambda: sys_linmat_lindef_static(*a1, device_out=True), 20)
     fl1 = stiffness_flops(27, 27, 256)
+    from yeti_b200._lib import Context
+    tctx = Context(device)
+    tctx.set_timing(True)
+    for _ in range(20):
+        sys_linmat_lindef_static(*a1, device_out=True, ctx=tctx)
+    t_k1 = tctx.kernel_ms("k_u1_stiffness") / 20
+    tctx.set_timing(False)
     out["fp64_gemm_tflops_measured"] = peak64
     out["assembly_p2_16x4x4"] = {
         "nb_data": int(kd.size), "gpu_ms_device_out": t_gpu, "gpu_ms_host_buffers": t_gpu_host,
-        "gpu_ms_events_device_out": t_ev, "stiffness_gflop": fl1 / 1e9,
-        "fp64_frac_of_measured_dgemm": fl1 / (t_ev / 1e3) / 1e12 / peak64,
+        "gpu_ms_events_device_out": t_ev, "k_u1_stiffness_ms_events": t_k1,
+        "stiffness_gflop": fl1 / 1e9,
+        "fp64_frac_of_measured_dgemm": fl1 / (t_k1 / 1e3) / 1e12 / peak64,
         "cpu_oracle_ms": t_cpu, "cpu_cores": oracle.threads(),
         "bit_identical": bool(np.array_equal(kd, ko) and np.array_equal(F, Fo)),
         "assemble_and_solve_ms": t_solve, "cpu_oracle_assemble_and_solve_ms": t_cpu_solve,
@@ -479,6 +487,11 @@ def extra_configs(args, device):
     t_g = _median_ms(lambda: grad_from_system_args(a3, sol, adj), 5, sync)
     gi, ge = grad_from_system_args(a3, sol, adj)
     t_gev = _event_ms(lambda: grad_from_system_args(a3, sol, adj), 5)
+    tctx.set_timing(True)
+    for _ in range(5):
+        grad_from_system_args(a3, sol, adj, ctx=tctx)
+    t_k3 = tctx.kernel_ms("k_u1_grad") / 5
+    tctx.set_timing(False)
     fl3 = gradient_flops(27, 27, 2048)
     t0 = time.perf_counter()
     oi, oe = oracle.grad_lin_elast_work(a3, sol, adj)
@@ -487,8 +500,8 @@ def extra_configs(args, device):
     got = np.concatenate([gi.ravel(), ge.ravel()])
     out["gradient_p2_32x32x2"] = {
         "nb_cp": int(sol.shape[1]), "gpu_ms_host_buffers": t_g, "gpu_ms_events": t_gev,
-        "gradient_gflop": fl3 / 1e9,
-        "fp64_frac_of_measured_dgemm": fl3 / (t_gev / 1e3) / 1e12 / peak64,
+        "k_u1_grad_ms_events": t_k3, "gradient_gflop": fl3 / 1e9,
+        "fp64_frac_of_measured_dgemm": fl3 / (t_k3 / 1e3) / 1e12 / peak64,
         "cpu_oracle_ms": t_go,
         "cpu_cores": oracle.threads(), "max_rel_diff_vs_oracle": float(np.abs(got - ref).max() / np.abs(ref).max())}
     # volume and its shape gradient on the C3 geometry (the constraint of the

@@ -264,7 +264,10 @@ def test_gpu_sumfact_matches_oracle_on_fixtures(cuda_ok, name):
     if int(d["nb_dof_free"]) < int(d["nb_dof_tot"]) and np.linalg.norm(f0) > 0:
         s0 = _solve(d, k0, r0, c0, f0)
         s1 = _solve(d, k1, r1, c1, f1)
-        assert np.linalg.norm(s1 - s0) <= TOL * np.linalg.norm(s0)
+        # values equal to rounding (not bit for bit): the displacement moves
+        # by up to cond(K) times that; 1e-10 on these models (measured
+        # 1.5e-12 on the slender p=2 cantilever)
+        assert np.linalg.norm(s1 - s0) <= 1e-10 * np.linalg.norm(s0)
 
 
 @pytest.mark.gpu

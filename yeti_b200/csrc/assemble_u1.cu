@@ -434,7 +434,23 @@ k_u1_stiffness(StiffArgs a) {
             while (j * (j + 1) / 2 > t) j--;
             while ((j + 1) * (j + 2) / 2 <= t) j++;
             const int i = t - j * (j + 1) / 2;
+            const int64_t jb = base + 9LL * j * (j - 1) / 2 + 6LL * j;
             double K[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+            if (q0 > 0) {
+                // resume the running sums of the earlier chunks (the stored
+                // diagonal of a diagonal block is halved; x2 is exact), so the
+                // points are added in one sequence as in the reference
+                if (i < j) {
+                    for (int ll = 0; ll < 3; ll++)
+                        for (int kk = 0; kk < 3; kk++) K[kk][ll] = a.kdata[jb + 9LL * i + 3 * ll + kk];
+                } else {
+                    for (int ll = 0; ll < 3; ll++)
+                        for (int kk = 0; kk <= ll; kk++) {
+                            const double v = a.kdata[jb + 9LL * j + ll * (ll + 1) / 2 + kk];
+                            K[kk][ll] = kk == ll ? v * 2.0 : v;
+                        }
+                }
+            }
             for (int q = 0; q < nqc; q++) {
                 const double *A = dR + ((size_t)q * nn + i) * 3;
                 const double *B = dR + ((size_t)q * nn + j) * 3;
@@ -452,16 +468,13 @@ k_u1_stiffness(StiffArgs a) {
                 K[1][2] += (a1 * (lam * b2) + a2 * (mu * b1)) * d;
                 K[2][1] += (a2 * (lam * b1) + a1 * (mu * b2)) * d;
             }
-            const int64_t jb = base + 9LL * j * (j - 1) / 2 + 6LL * j;
             const int dofi = 3 * ien[i], dofj = 3 * ien[j];
             if (i < j) {
                 const int64_t s = jb + 9LL * i;
                 for (int ll = 0; ll < 3; ll++)
                     for (int kk = 0; kk < 3; kk++) {
                         const int64_t o = s + 3 * ll + kk;
-                        double v = K[kk][ll];
-                        if (q0 > 0) v += a.kdata[o];
-                        a.kdata[o] = v;
+                        a.kdata[o] = K[kk][ll];
                         if (q0 == 0) {
                             a.krow[o] = dofi + kk;
                             a.kcol[o] = dofj + ll;
@@ -472,9 +485,7 @@ k_u1_stiffness(StiffArgs a) {
                 for (int ll = 0; ll < 3; ll++)
                     for (int kk = 0; kk <= ll; kk++) {
                         const int64_t o = s + ll * (ll + 1) / 2 + kk;
-                        double v = (kk == ll) ? K[kk][ll] * 0.5 : K[kk][ll];
-                        if (q0 > 0) v += a.kdata[o];
-                        a.kdata[o] = v;
+                        a.kdata[o] = (kk == ll) ? K[kk][ll] * 0.5 : K[kk][ll];
                         if (q0 == 0) {
                             a.krow[o] = dofj + kk;
                             a.kcol[o] = dofj + ll;
@@ -562,21 +573,22 @@ __global__ void __launch_bounds__(256) k_u1_mass(MassArgs a) {
             while (j * (j + 1) / 2 > t) j--;
             while ((j + 1) * (j + 2) / 2 <= t) j++;
             const int i = t - j * (j + 1) / 2;
+            const int64_t jb = base + 9LL * j * (j - 1) / 2 + 6LL * j;
+            // resume the running sum of the earlier chunks (a diagonal
+            // block's stored value is halved; x2 is exact)
             double m = 0.0;
+            if (q0 > 0) m = i < j ? a.mdata[jb + 9LL * i] : a.mdata[jb + 9LL * j] * 2.0;
             for (int q = 0; q < nqc; q++) {
                 const double t1 = qs[(size_t)q * kStiffQS + 13] * Rq[(size_t)q * nn + j];
                 m += t1 * Rq[(size_t)q * nn + i];
             }
-            const int64_t jb = base + 9LL * j * (j - 1) / 2 + 6LL * j;
             const int dofi = 3 * ien[i], dofj = 3 * ien[j];
             if (i < j) {
                 const int64_t s = jb + 9LL * i;
                 for (int ll = 0; ll < 3; ll++)
                     for (int kk = 0; kk < 3; kk++) {
                         const int64_t o = s + 3 * ll + kk;
-                        double v = kk == ll ? m : 0.0;
-                        if (q0 > 0) v += a.mdata[o];
-                        a.mdata[o] = v;
+                        a.mdata[o] = kk == ll ? m : 0.0;
                         if (q0 == 0) {
                             a.mrow[o] = dofi + kk;
                             a.mcol[o] = dofj + ll;
@@ -587,9 +599,7 @@ __global__ void __launch_bounds__(256) k_u1_mass(MassArgs a) {
                 for (int ll = 0; ll < 3; ll++)
                     for (int kk = 0; kk <= ll; kk++) {
                         const int64_t o = s + ll * (ll + 1) / 2 + kk;
-                        double v = kk == ll ? m * 0.5 : 0.0;
-                        if (q0 > 0) v += a.mdata[o];
-                        a.mdata[o] = v;
+                        a.mdata[o] = kk == ll ? m * 0.5 : 0.0;
                         if (q0 == 0) {
                             a.mrow[o] = dofj + kk;
                             a.mcol[o] = dofj + ll;
