@@ -331,15 +331,18 @@ def stiffness_flops(nq, nn, nel):
 
 
 def stiffness_sf_flops(n, g, nel):
-    """FP64 operations of k_u1_stiffness_sf per its loops (2 per
-    multiply-add): the per-point geometry pass (nn sums of 16 values) and,
-    for each of the six blocks, the w, v and u contractions."""
-    nu, nv, nw = n
-    nn, nq = nu * nv * nw, g ** 3
-    blk = (16 * nw * g ** 3 + 12 * nw ** 2 * g ** 3 + 9 * nv * nw ** 2 * g ** 2 +
-           6 * nv ** 2 * nw ** 2 * g ** 2 + 4 * nu * nv ** 2 * nw ** 2 * g)
-    out = 6 * blk + (3 + 3 * 0.5) * nn * nn * 2 * g   # diagonal blocks: half the pairs
-    return nel * 2 * (out + nq * nn * 18 + 6 * 16 * nq * 6)
+    """FP64 operations of k_u1_stiffness_sf per its loops (a multiply-add
+    counts 2): the per-point geometry pass (nn sums of 16 values), then per
+    pair i3 <= j3 of w indices the w, v and u contractions of the nine G_rs,
+    and per written node pair the 3x3 block (about 40)."""
+    n1, n2, n3 = n
+    nn, nq = n1 * n2 * n3, g ** 3
+    step1 = 9 * g ** 3 * 31
+    step2 = 18 * n2 * g * (6 * g + 6 * n2 * g)
+    step3 = 9 * n1 * n2 ** 2 * (6 * g + 4 * n1 * g)
+    per_elem = (n3 * (n3 + 1) // 2 * (step1 + step2 + step3) + nn * (nn + 1) // 2 * 40 +
+                nq * nn * 36)
+    return nel * per_elem
 
 
 def assembly_beyond_p2(device, seed):

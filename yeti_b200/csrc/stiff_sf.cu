@@ -3,7 +3,7 @@
 // UELMAT.f90:109-171), with the B^T D B contraction done direction by
 // direction over the 1-D basis tables instead of pair by pair.  The sums run
 // in another order, so the values agree with the reference to rounding
-// (relative 1e-13 on the test meshes), not bit for bit.
+// (relative 1e-14 on the test meshes), not bit for bit.
 //
 // Factorisation
 // -------------
@@ -16,28 +16,28 @@
 // over the four kinds kappa = value, d/du, d/dv, d/dw of the tensor product
 // (Phi^value = N_a, Phi^u = N1' N2 N3, ...) with the point coefficients
 // c^{d}_r = Jinv[d][r] / W and c^{value}_r = -sum_d W_d Jinv[d][r] / W^2.
-// The 3x3 block (k, l) of the element matrix is then
+// For the isotropic D of stiffmatrix.F90:167-216 the 3x3 block of a node
+// pair is
 //
-//     K_kl(a, b) = w_a w_b sum_q sum_{kappa,eta} Phi^kappa_a Phi^eta_b M^{kappa eta}_kl(q),
-//     M^{kappa eta}_kl = dv (lam c^kappa_k c^eta_l + mu c^kappa_l c^eta_k
-//                            + [k = l] mu sum_r c^kappa_r c^eta_r),
+//     K_kl(a, b) = lam G_kl + mu G_lk + [k = l] mu (G_00 + G_11 + G_22),
+//     G_rs(a, b) = sum_q dv(q) dR_a/dx_r dR_b/dx_s,
 //
-// (isotropic D of stiffmatrix.F90:167-216), and each sum over q is
-// contracted along w, then v, then u.  Kinds that share their 1-D factors in
-// the remaining directions are added before a contraction: after w the
-// value and d/dw kinds fall together (class 0), d/du is class 1, d/dv class
-// 2; after v only the (value or derivative) kind along u remains.  Per block
-// the three steps cost 16 n^2 g^3, 9 n^4 g^2 and 4 n^6 g multiply-adds (n =
-// p+1 functions, g Gauss points per direction), against about 22 n^6 g^3
-// for the pair loop.
+// so the nine integrals G_rs carry the element matrix; they are contracted
+// along w, then v, then u.  After the w contraction the value and d/dw kinds
+// share their factors in u and v (class 0), d/du is class 1 and d/dv class
+// 2; after v only the kind along u (value or derivative) remains.  Each
+// contraction runs one side (the row node a) and then the other (b).  For
+// one pair (i3, j3) of w indices the steps cost about 81 g^3,
+// 30 n2 g^3 + 27 n2^2 g^2 and 36 n1 n2^2 g + 18 n1^2 n2^2 g multiply-adds
+// (n = p+1 functions, g Gauss points per direction); only the pairs
+// i3 <= j3 are needed, the slots hold the upper triangle.
 //
-// One CTA per element; the six blocks (k <= l) run in turn, each through
-// shared memory: M (16 per point), T1 (class pairs x i3 j3 x q1 q2) and T2
-// (kind pairs along u x i2 j2 x i3 j3 x q1, for a chunk of i3 at a time).
-// Every COO value is written once: block (k, l) gives entry (k, l) of pair
-// (a, b) for a < b, entry (l, k) of pair (b, a) for a > b (k < l only: the
-// diagonal blocks are symmetric) and the upper triangle of the diagonal
-// pair, halved on its diagonal.
+// One CTA per element.  Shared memory holds the point coefficients (13 per
+// point), T1 = G_rs per class pair and (q1, q2), T2 per u-kind pair, i2, j2
+// and q1, and the contracted G_rs of a chunk of j2 values; every node pair's
+// nine (diagonal pair: six) slot values are formed and written together by
+// one thread, consecutive threads taking consecutive row nodes, whose slots
+// are contiguous.
 #include "nurbs.cuh"
 #include "u1_model.cuh"
 
@@ -49,9 +49,9 @@ constexpr int kSfMaxG = 8;   // Gauss points per direction (template instances)
 struct SfArgs {
     int n[3];        // functions per direction (p+1)
     int p[3];
-    int nn, ng, nq, i3c;
+    int nn, j2c;     // nodes; j2 values per output chunk
     const double *U[3];
-    const double *gauss;   // 4 * ng^3: weight, t1, t2, t3 (t3 fastest)
+    const double *gauss;   // 4 * g^3: weight, t1, t2, t3 (t3 fastest)
     const double *coords;
     const int32_t *ien;
     const double *w;
@@ -63,11 +63,11 @@ struct SfArgs {
 };
 
 // Shared-memory doubles of one CTA.
-size_t sf_smem_doubles(const int n[3], int ng, int i3c) {
-    const size_t nn = (size_t)n[0] * n[1] * n[2], nq = (size_t)ng * ng * ng;
-    const size_t t2 = 4 * (size_t)n[1] * n[1] * i3c * n[2] * ng;
-    return 4 * nn + 2 * (size_t)ng * (n[0] + n[1] + n[2]) + 13 * nq +
-           9 * (size_t)n[2] * n[2] * ng * ng + (t2 > 16 * nq ? t2 : 16 * nq);
+size_t sf_smem_doubles(const int n[3], int g, int j2c) {
+    const size_t nn = (size_t)n[0] * n[1] * n[2], nq = (size_t)g * g * g;
+    return 4 * nn + (nn + 1) / 2 + 2 * (size_t)g * (n[0] + n[1] + n[2]) + 13 * nq +
+           81 * (size_t)g * g + 36 * (size_t)n[1] * n[1] * g +
+           9 * (size_t)n[0] * n[1] * n[0] * j2c;
 }
 
 __device__ __forceinline__ double det3(const double J[3][3]) {
@@ -79,21 +79,25 @@ __device__ __forceinline__ double det3(const double J[3][3]) {
 template <int G>
 __global__ void __launch_bounds__(kSfThreads) k_u1_stiffness_sf(SfArgs a) {
     extern __shared__ double smem[];
-    constexpr int ng = G, nq = G * G * G;
-    const int nu = a.n[0], nv = a.n[1], nw = a.n[2], nn = a.nn;
-    double *xe = smem;                       // 3 nn
-    double *we = xe + 3 * nn;                // nn
-    double *tab = we + nn;                   // A_d[kind][i][q], d = u, v, w
-    double *A1 = tab, *A2 = A1 + 2 * nu * ng, *A3 = A2 + 2 * nv * ng;
-    double *cq = A3 + 2 * nw * ng;           // 13 nq: c[kind][r], dv
-    double *T1 = cq + 13 * nq;               // 9 nw^2 ng^2
-    double *MT = T1 + 9 * nw * nw * ng * ng; // M (16 nq), then T2
+    constexpr int g = G, gg = G * G, nq = G * G * G;
+    const int n1 = a.n[0], n2 = a.n[1], n3 = a.n[2], nn = a.nn, j2c = a.j2c;
+    const int n12 = n1 * n2;
+    double *xe = smem;                        // 3 nn
+    double *we = xe + 3 * nn;                 // nn
+    int *sien = reinterpret_cast<int *>(we + nn);   // nn ints
+    double *A1 = we + nn + (nn + 1) / 2;      // A_d[kind][i][q], d = u, v, w
+    double *A2 = A1 + 2 * n1 * g, *A3 = A2 + 2 * n2 * g;
+    double *cq = A3 + 2 * n3 * g;             // 13 nq: c[kind][r], dv
+    double *T1 = cq + 13 * nq;                // [rs][ck ce][q1 q2]
+    double *T2 = T1 + 81 * gg;                // [rs][al be][i2][j2][q1]
+    double *OB = T2 + 36 * n2 * n2 * g;       // [rs][a12][b12 of the chunk]
     __shared__ double su1[3], su2[3];
     __shared__ int sni[3];
     const int e = blockIdx.x, tid = threadIdx.x;
     const int32_t *ien = a.ien + (size_t)e * nn;
     for (int i = tid; i < nn; i += kSfThreads) {
         const int cp = ien[i];
+        sien[i] = cp;
         xe[3 * i] = a.coords[3 * cp];
         xe[3 * i + 1] = a.coords[3 * cp + 1];
         xe[3 * i + 2] = a.coords[3 * cp + 2];
@@ -108,9 +112,9 @@ __global__ void __launch_bounds__(kSfThreads) k_u1_stiffness_sf(SfArgs a) {
     __syncthreads();
     // ---- 1-D tables: local index i uses the span's function p - i
     // (descending local node order of the reference's IEN)
-    if (tid < 3 * ng) {
-        const int d = tid / ng, q = tid - d * ng;
-        const int qq = d == 0 ? q * ng * ng : (d == 1 ? q * ng : q);
+    if (tid < 3 * g) {
+        const int d = tid / g, q = tid - d * g;
+        const int qq = d == 0 ? q * gg : (d == 1 ? q * g : q);
         const double t = a.gauss[4 * qq + 1 + d];
         const double xi = ((su2[d] - su1[d]) * t + (su2[d] + su1[d])) * 0.5;
         double N[kMaxDeg1], dN[kMaxDeg1];
@@ -118,23 +122,23 @@ __global__ void __launch_bounds__(kSfThreads) k_u1_stiffness_sf(SfArgs a) {
         const int nd = a.n[d];
         double *A = d == 0 ? A1 : (d == 1 ? A2 : A3);
         for (int i = 0; i < nd; i++) {
-            A[i * ng + q] = N[a.p[d] - i];
-            A[(nd + i) * ng + q] = dN[a.p[d] - i];
+            A[i * g + q] = N[a.p[d] - i];
+            A[(nd + i) * g + q] = dN[a.p[d] - i];
         }
     }
     __syncthreads();
     // ---- per point: W, dW, x sums -> Jacobian, its inverse, dv, c
     for (int q = tid; q < nq; q += kSfThreads) {
-        const int q1 = q / (ng * ng), q2 = (q / ng) % ng, q3 = q % ng;
+        const int q1 = q / gg, q2 = (q / g) % g, q3 = q % g;
         double W = 0, Wd[3] = {0, 0, 0}, P[4][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
         int n = 0;
-        for (int i3 = 0; i3 < nw; i3++) {
-            const double c0 = A3[i3 * ng + q3], c1 = A3[(nw + i3) * ng + q3];
-            for (int i2 = 0; i2 < nv; i2++) {
-                const double b0 = A2[i2 * ng + q2], b1 = A2[(nv + i2) * ng + q2];
+        for (int i3 = 0; i3 < n3; i3++) {
+            const double c0 = A3[i3 * g + q3], c1 = A3[(n3 + i3) * g + q3];
+            for (int i2 = 0; i2 < n2; i2++) {
+                const double b0 = A2[i2 * g + q2], b1 = A2[(n2 + i2) * g + q2];
                 const double v23 = b0 * c0, d2 = b1 * c0, d3 = b0 * c1;
-                for (int i1 = 0; i1 < nu; i1++, n++) {
-                    const double a0 = A1[i1 * ng + q1], a1 = A1[(nu + i1) * ng + q1];
+                for (int i1 = 0; i1 < n1; i1++, n++) {
+                    const double a0 = A1[i1 * g + q1], a1 = A1[(n1 + i1) * g + q1];
                     const double wn = we[n];
                     const double ph[4] = {a0 * v23 * wn, a1 * v23 * wn, a0 * d2 * wn, a0 * d3 * wn};
                     W += ph[0];
@@ -173,157 +177,157 @@ __global__ void __launch_bounds__(kSfThreads) k_u1_stiffness_sf(SfArgs a) {
     }
     const int64_t base = a.slot[e];
     const double lam = a.lam, mu = a.mu;
-    const int ngg = ng * ng;
-    for (int kl = 0; kl < 6; kl++) {
-        const int k = kl < 3 ? kl : (kl == 5 ? 1 : 0);
-        const int l = kl < 3 ? kl : (kl == 3 ? 1 : 2);
-        __syncthreads();
-        // ---- M^{kappa eta}(q), kinds 0 value, 1 u, 2 v, 3 w
-        for (int t = tid; t < 16 * nq; t += kSfThreads) {
-            const int ke = t / nq, q = t - ke * nq, ka = ke >> 2, et = ke & 3;
-            const double *c = cq + 13 * q;
-            const double *ck = c + 3 * ka, *ce = c + 3 * et;
-            double m = lam * ck[k] * ce[l] + mu * ck[l] * ce[k];
-            if (k == l) m += mu * (ck[0] * ce[0] + ck[1] * ce[1] + ck[2] * ce[2]);
-            MT[t] = m * c[12];
-        }
-        __syncthreads();
-        // ---- step 1 (w): T1[ck,ce][i3][j3][q1 q2], classes 0 {value, w}, 1 {u}, 2 {v}
-        for (int t = tid; t < 3 * nw * ngg; t += kSfThreads) {
-            const int ck = t / (nw * ngg), r = t - ck * nw * ngg, i3 = r / ngg, q12 = r - i3 * ngg;
-            double X[4][G];   // X[eta][q3] = sum_{kappa in ck} A3[kappa is w][i3][q3] M
-#pragma unroll
-            for (int q3 = 0; q3 < G; q3++) {
-                {
-                    const int q = q12 * ng + q3;
-#pragma unroll
-                    for (int et = 0; et < 4; et++) {
-                        double x;
-                        if (ck == 0)
-                            x = A3[i3 * ng + q3] * MT[(0 * 4 + et) * nq + q] +
-                                A3[(nw + i3) * ng + q3] * MT[(3 * 4 + et) * nq + q];
-                        else
-                            x = A3[i3 * ng + q3] * MT[(ck * 4 + et) * nq + q];
-                        X[et][q3] = x;
-                    }
-                }
-            }
-#pragma unroll
-            for (int ce = 0; ce < 3; ce++)
-                for (int j3 = 0; j3 < nw; j3++) {
-                    double s = 0;
-#pragma unroll
-                    for (int q3 = 0; q3 < G; q3++) {
-                        {
-                            const double b0 = A3[j3 * ng + q3];
-                            if (ce == 0)
-                                s += b0 * X[0][q3] + A3[(nw + j3) * ng + q3] * X[3][q3];
-                            else
-                                s += b0 * X[ce][q3];
-                        }
-                    }
-                    T1[((ck * 3 + ce) * nw * nw + i3 * nw + j3) * ngg + q12] = s;
-                }
-        }
-        for (int i3s = 0; i3s < nw; i3s += a.i3c) {
-            const int i3n = min(a.i3c, nw - i3s);
+    for (int i3 = 0; i3 < n3; i3++)
+        for (int j3 = i3; j3 < n3; j3++) {
             __syncthreads();
-            // ---- step 2 (v): T2[al,be][i2][j2][i3l][j3][q1]; along u the
-            // classes 0 and 2 carry the value kind, class 1 the derivative
-            for (int t = tid; t < 2 * nv * i3n * nw * ng; t += kSfThreads) {
+            // ---- step 1 (w): T1[rs][ck ce][q1 q2] = sum_q3 dv Pa_r Pb_s, with
+            // P^{class}_r(i3, q) = sum_{kinds of the class} A3[kind along w][i3][q3] c_r
+            for (int t = tid; t < 9 * gg; t += kSfThreads) {
+                const int cc = t / gg, q12 = t - cc * gg, ck = cc / 3, ce = cc - 3 * ck;
+                double acc[9];
+#pragma unroll
+                for (int k = 0; k < 9; k++) acc[k] = 0.0;
+#pragma unroll
+                for (int q3 = 0; q3 < G; q3++) {
+                    const double *c = cq + 13 * (q12 * g + q3);
+                    const double ai0 = A3[i3 * g + q3], bj0 = A3[j3 * g + q3];
+                    double pa[3], pb[3];
+                    if (ck == 0) {
+                        const double ai1 = A3[(n3 + i3) * g + q3];
+#pragma unroll
+                        for (int r = 0; r < 3; r++) pa[r] = ai0 * c[r] + ai1 * c[9 + r];
+                    } else {
+#pragma unroll
+                        for (int r = 0; r < 3; r++) pa[r] = ai0 * c[3 * ck + r];
+                    }
+                    if (ce == 0) {
+                        const double bj1 = A3[(n3 + j3) * g + q3];
+#pragma unroll
+                        for (int s = 0; s < 3; s++) pb[s] = bj0 * c[s] + bj1 * c[9 + s];
+                    } else {
+#pragma unroll
+                        for (int s = 0; s < 3; s++) pb[s] = bj0 * c[3 * ce + s];
+                    }
+                    const double dv = c[12];
+#pragma unroll
+                    for (int r = 0; r < 3; r++) {
+                        const double pd = pa[r] * dv;
+#pragma unroll
+                        for (int s = 0; s < 3; s++) acc[3 * r + s] += pd * pb[s];
+                    }
+                }
+#pragma unroll
+                for (int rs = 0; rs < 9; rs++) T1[(rs * 9 + cc) * gg + q12] = acc[rs];
+            }
+            __syncthreads();
+            // ---- step 2 (v): T2[rs][al be][i2][j2][q1]; along u the classes
+            // 0 and 2 carry the value kind, class 1 the derivative
+            for (int t = tid; t < 18 * n2 * g; t += kSfThreads) {
                 int r = t;
-                const int q1 = r % ng; r /= ng;
-                const int j3 = r % nw; r /= nw;
-                const int i3l = r % i3n; r /= i3n;
-                const int i2 = r % nv; r /= nv;
-                const int al = r;
-                const int i3 = i3s + i3l;
-                double V[3][G];   // V[ce][q2] = sum_{ck: u-kind al} A2 T1
+                const int q1 = r % g; r /= g;
+                const int i2 = r % n2; r /= n2;
+                const int al = r & 1, rs = r >> 1;
+                const double *t1 = T1 + rs * 9 * gg + q1 * g;
+                double V[3][G];   // V[ce][q2] = sum_{ck of u-kind al} A2 T1
 #pragma unroll
                 for (int q2 = 0; q2 < G; q2++) {
-                    {
-                        const int o = (i3 * nw + j3) * ngg + q1 * ng + q2;
-                        const double b0 = A2[i2 * ng + q2];
+                    const double b0 = A2[i2 * g + q2];
+                    if (al == 0) {
+                        const double b1 = A2[(n2 + i2) * g + q2];
 #pragma unroll
-                        for (int ce = 0; ce < 3; ce++) {
-                            const int so = ce * nw * nw * ngg + o;
-                            V[ce][q2] = al == 0
-                                ? b0 * T1[0 * 3 * nw * nw * ngg + so] +
-                                      A2[(nv + i2) * ng + q2] * T1[2 * 3 * nw * nw * ngg + so]
-                                : b0 * T1[1 * 3 * nw * nw * ngg + so];
-                        }
+                        for (int ce = 0; ce < 3; ce++)
+                            V[ce][q2] = b0 * t1[(0 * 3 + ce) * gg + q2] + b1 * t1[(2 * 3 + ce) * gg + q2];
+                    } else {
+#pragma unroll
+                        for (int ce = 0; ce < 3; ce++) V[ce][q2] = b0 * t1[(1 * 3 + ce) * gg + q2];
                     }
                 }
+                double *t2 = T2 + ((size_t)(rs * 4 + al * 2) * n2 + i2) * n2 * g + q1;
+                for (int j2 = 0; j2 < n2; j2++) {
+                    double s0 = 0.0, s1 = 0.0;
 #pragma unroll
-                for (int be = 0; be < 2; be++)
-                    for (int j2 = 0; j2 < nv; j2++) {
-                        double s = 0;
-#pragma unroll
-                        for (int q2 = 0; q2 < G; q2++) {
-                            {
-                                const double c0 = A2[j2 * ng + q2];
-                                s += be == 0 ? c0 * V[0][q2] + A2[(nv + j2) * ng + q2] * V[2][q2]
-                                             : c0 * V[1][q2];
-                            }
-                        }
-                        MT[((((al * 2 + be) * nv + i2) * nv + j2) * i3n + i3l) * nw * ng + j3 * ng + q1] = s;
+                    for (int q2 = 0; q2 < G; q2++) {
+                        const double c0 = A2[j2 * g + q2];
+                        s0 += c0 * V[0][q2] + A2[(n2 + j2) * g + q2] * V[2][q2];
+                        s1 += c0 * V[1][q2];
                     }
+                    t2[j2 * g] = s0;                         // be = 0
+                    t2[(size_t)n2 * n2 * g + j2 * g] = s1;   // be = 1
+                }
             }
-            __syncthreads();
-            // ---- step 3 (u) and the COO writes
-            for (int t = tid; t < nu * nv * i3n * nv * nw; t += kSfThreads) {
-                int r = t;
-                const int j3 = r % nw; r /= nw;
-                const int j2 = r % nv; r /= nv;
-                const int i3l = r % i3n; r /= i3n;
-                const int i2 = r % nv; r /= nv;
-                const int i1 = r;
-                const int ia = i1 + nu * (i2 + nv * (i3s + i3l));
-                double Uu[2][G];   // U[be][q1] = sum_al A1[al][i1][q1] T2[al,be]
+            for (int j2s = 0; j2s < n2; j2s += j2c) {
+                const int j2n = min(j2c, n2 - j2s), nb = n1 * j2n;
+                __syncthreads();
+                // ---- step 3 (u): OB[rs][a12][b12] for j2 in the chunk
+                for (int t = tid; t < 9 * n12 * j2n; t += kSfThreads) {
+                    int r = t;
+                    const int j2l = r % j2n; r /= j2n;
+                    const int a12 = r % n12;
+                    const int rs = r / n12;
+                    const int i1 = a12 % n1, i2 = a12 / n1, j2 = j2s + j2l;
+                    double Uu[2][G];   // Uu[be][q1] = sum_al A1[al][i1][q1] T2[rs][al be]
 #pragma unroll
-                for (int q1 = 0; q1 < G; q1++) {
-                    {
-                        const double a0 = A1[i1 * ng + q1], a1 = A1[(nu + i1) * ng + q1];
+                    for (int q1 = 0; q1 < G; q1++) {
+                        const double a0 = A1[i1 * g + q1], a1 = A1[(n1 + i1) * g + q1];
 #pragma unroll
                         for (int be = 0; be < 2; be++) {
-                            const size_t o0 = ((((0 * 2 + be) * nv + i2) * nv + j2) * i3n + i3l) * nw * ng + j3 * ng + q1;
-                            const size_t o1 = ((((1 * 2 + be) * nv + i2) * nv + j2) * i3n + i3l) * nw * ng + j3 * ng + q1;
-                            Uu[be][q1] = a0 * MT[o0] + a1 * MT[o1];
+                            const double *t2 = T2 + (((size_t)(rs * 4 + be) * n2 + i2) * n2 + j2) * g + q1;
+                            Uu[be][q1] = a0 * t2[0] + a1 * t2[(size_t)2 * n2 * n2 * g];
                         }
                     }
-                }
-                const double wa = we[ia];
-                const int dofa = 3 * ien[ia];
-                for (int j1 = 0; j1 < nu; j1++) {
-                    const int ib = j1 + nu * (j2 + nv * j3);
-                    if (k == l && ia > ib) continue;
-                    double s = 0;
+                    double *ob = OB + ((size_t)rs * n12 + a12) * nb + j2l * n1;
+                    for (int j1 = 0; j1 < n1; j1++) {
+                        double s = 0.0;
 #pragma unroll
-                    for (int q1 = 0; q1 < G; q1++)
-                        s += A1[j1 * ng + q1] * Uu[0][q1] + A1[(nu + j1) * ng + q1] * Uu[1][q1];
-                    s *= wa * we[ib];
-                    const int dofb = 3 * ien[ib];
-                    int64_t o;
-                    int row, col;
-                    if (ia != ib) {
-                        const int i = ia < ib ? ia : ib, j = ia < ib ? ib : ia;
-                        const int kk = ia < ib ? k : l, ll = ia < ib ? l : k;
-                        o = base + 9LL * j * (j - 1) / 2 + 6LL * j + 9LL * i + 3 * ll + kk;
-                        row = (ia < ib ? dofa : dofb) + kk;
-                        col = (ia < ib ? dofb : dofa) + ll;
-                    } else {
-                        o = base + 9LL * ia * (ia - 1) / 2 + 15LL * ia + l * (l + 1) / 2 + k;
-                        if (k == l) s *= 0.5;
-                        row = dofa + k;
-                        col = dofa + l;
+                        for (int q1 = 0; q1 < G; q1++)
+                            s += A1[j1 * g + q1] * Uu[0][q1] + A1[(n1 + j1) * g + q1] * Uu[1][q1];
+                        ob[j1] = s;
                     }
-                    a.kdata[o] = s;
-                    a.krow[o] = row;
-                    a.kcol[o] = col;
+                }
+                __syncthreads();
+                // ---- the pairs' 3x3 blocks into their COO slots; consecutive
+                // threads take consecutive row nodes (contiguous slots)
+                for (int t = tid; t < n12 * nb; t += kSfThreads) {
+                    const int a12 = t % n12, bl = t / n12;
+                    const int ia = a12 + n12 * i3;
+                    const int ib = bl % n1 + n1 * (j2s + bl / n1) + n12 * j3;
+                    if (ia > ib) continue;
+                    const double wab = we[ia] * we[ib];
+                    double Gm[9];
+#pragma unroll
+                    for (int rs = 0; rs < 9; rs++) Gm[rs] = OB[((size_t)rs * n12 + a12) * nb + bl] * wab;
+                    const double tr = mu * (Gm[0] + Gm[4] + Gm[8]);
+                    const int dofa = 3 * sien[ia], dofb = 3 * sien[ib];
+                    if (ia < ib) {
+                        const int64_t s0 = base + 9LL * ib * (ib - 1) / 2 + 6LL * ib + 9LL * ia;
+#pragma unroll
+                        for (int ll = 0; ll < 3; ll++)
+#pragma unroll
+                            for (int kk = 0; kk < 3; kk++) {
+                                double v = lam * Gm[3 * kk + ll] + mu * Gm[3 * ll + kk];
+                                if (kk == ll) v += tr;
+                                const int64_t o = s0 + 3 * ll + kk;
+                                a.kdata[o] = v;
+                                a.krow[o] = dofa + kk;
+                                a.kcol[o] = dofb + ll;
+                            }
+                    } else {
+                        const int64_t s0 = base + 9LL * ia * (ia - 1) / 2 + 15LL * ia;
+#pragma unroll
+                        for (int ll = 0; ll < 3; ll++)
+#pragma unroll
+                            for (int kk = 0; kk <= ll; kk++) {
+                                double v = lam * Gm[3 * kk + ll] + mu * Gm[3 * ll + kk];
+                                if (kk == ll) v = (v + tr) * 0.5;
+                                const int64_t o = s0 + ll * (ll + 1) / 2 + kk;
+                                a.kdata[o] = v;
+                                a.krow[o] = dofa + kk;
+                                a.kcol[o] = dofa + ll;
+                            }
+                    }
                 }
             }
         }
-    }
 }
 
 int launch_u1_stiffness_sf(yeti_ctx *ctx, const U1Patch &P, const double *coords,
@@ -338,19 +342,19 @@ int launch_u1_stiffness_sf(yeti_ctx *ctx, const U1Patch &P, const double *coords
         a.n[d] = P.p[d] + 1;
     }
     a.nn = P.nn;
-    a.ng = P.ng;
-    a.nq = P.nq;
-    // the largest chunk of i3 whose buffers leave room for two CTAs per SM
-    // (one when even a single i3 does not)
-    const size_t two = smem_cap / 2 > 1024 ? smem_cap / 2 - 1024 : 0;
-    int i3c = a.n[2];
-    while (i3c > 1 && sf_smem_doubles(a.n, a.ng, i3c) * sizeof(double) > two) i3c--;
-    const size_t smem = sf_smem_doubles(a.n, a.ng, i3c) * sizeof(double);
+    // the largest chunk of j2 whose buffers leave room for two CTAs per SM
+    // (a single j2 when none does)
+    int per_sm = 0;
+    YETI_CUDA(cudaDeviceGetAttribute(&per_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, ctx->device));
+    const size_t two = (size_t)per_sm / 2 > 2048 ? (size_t)per_sm / 2 - 2048 : 0;
+    int j2c = a.n[1];
+    while (j2c > 1 && sf_smem_doubles(a.n, P.ng, j2c) * sizeof(double) > two) j2c--;
+    const size_t smem = sf_smem_doubles(a.n, P.ng, j2c) * sizeof(double);
     YETI_CHECK(smem <= smem_cap, YETI_EUNSUPPORTED,
                "sum-factorised stiffness: an element of degrees (%d,%d,%d) "
                "with %d Gauss points per direction does not fit shared memory",
                P.p[0], P.p[1], P.p[2], P.ng);
-    a.i3c = i3c;
+    a.j2c = j2c;
     a.U[0] = P.knots.as<double>();
     a.U[1] = a.U[0] + P.nkv[0];
     a.U[2] = a.U[1] + P.nkv[1];
