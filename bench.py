@@ -54,6 +54,9 @@ def parse():
                     help="Poisson arrival rate of the serving stream (requests/s)")
     ap.add_argument("--serve-rate-high", type=float, default=80.0,
                     help="second serving stream near saturation (requests/s; 0: none)")
+    ap.add_argument("--serve-rate-capacity", type=float, default=160.0,
+                    help="third serving stream above the 80/s point, to show the "
+                         "sustained capacity (requests/s; 0: none)")
     ap.add_argument("--serve-budget-gb", type=float, default=32.0)
     ap.add_argument("--no-serve", action="store_true")
     ap.add_argument("--serve-precond", default="fd", choices=["jacobi", "fd"],
@@ -262,6 +265,7 @@ def serve_stream(args, device, rate=None):
             "p50_ms": float(np.percentile(lat, 50)) if len(lat) else None,
             "p99_ms": float(np.percentile(lat, 99)) if len(lat) else None,
             "solved_dof_per_s": out["solved_dofs"] / out["wall_s"],
+            "completed_per_s": len(lat) / out["wall_s"],
             "cg_iterations_total": int(sum(its)), "peak_active": st["peak_active"],
             "thread_ms": {"setup": st["setup_ms"], "retire": st["retire_ms"],
                           "poll": st["poll_ms"]},
@@ -728,6 +732,8 @@ def main():
         serve = serve_stream(args, local)
         if args.serve_rate_high > 0:
             serve["high_rate"] = serve_stream(args, local, args.serve_rate_high)
+        if args.serve_rate_capacity > 0:
+            serve["capacity_rate"] = serve_stream(args, local, args.serve_rate_capacity)
     extra = None
     if rank == 0 and ws == 1 and not args.no_extra:
         extra = extra_configs(args, local)

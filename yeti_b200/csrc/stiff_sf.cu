@@ -221,67 +221,81 @@ __global__ void __launch_bounds__(kSfThreads) k_u1_stiffness_sf(SfArgs a) {
             }
             __syncthreads();
             // ---- step 2 (v): T2[rs][al be][i2][j2][q1]; along u the classes
-            // 0 and 2 carry the value kind, class 1 the derivative
-            for (int t = tid; t < 18 * n2 * g; t += kSfThreads) {
+            // 0 and 2 carry the value kind, class 1 the derivative.  One task
+            // per (rs, i2, q1) for both u-kinds al, so each A2 value read
+            // serves six multiply-adds.
+            for (int t = tid; t < 9 * n2 * g; t += kSfThreads) {
                 int r = t;
                 const int q1 = r % g; r /= g;
-                const int i2 = r % n2; r /= n2;
-                const int al = r & 1, rs = r >> 1;
+                const int i2 = r % n2;
+                const int rs = r / n2;
                 const double *t1 = T1 + rs * 9 * gg + q1 * g;
-                double V[3][G];   // V[ce][q2] = sum_{ck of u-kind al} A2 T1
+                double V[2][3][G];   // V[al][ce][q2] = sum_{ck of u-kind al} A2 T1
 #pragma unroll
                 for (int q2 = 0; q2 < G; q2++) {
-                    const double b0 = A2[i2 * g + q2];
-                    if (al == 0) {
-                        const double b1 = A2[(n2 + i2) * g + q2];
+                    const double b0 = A2[i2 * g + q2], b1 = A2[(n2 + i2) * g + q2];
 #pragma unroll
-                        for (int ce = 0; ce < 3; ce++)
-                            V[ce][q2] = b0 * t1[(0 * 3 + ce) * gg + q2] + b1 * t1[(2 * 3 + ce) * gg + q2];
-                    } else {
-#pragma unroll
-                        for (int ce = 0; ce < 3; ce++) V[ce][q2] = b0 * t1[(1 * 3 + ce) * gg + q2];
+                    for (int ce = 0; ce < 3; ce++) {
+                        V[0][ce][q2] = b0 * t1[(0 * 3 + ce) * gg + q2] + b1 * t1[(2 * 3 + ce) * gg + q2];
+                        V[1][ce][q2] = b0 * t1[(1 * 3 + ce) * gg + q2];
                     }
                 }
-                double *t2 = T2 + ((size_t)(rs * 4 + al * 2) * n2 + i2) * n2 * g + q1;
+                double *t2 = T2 + ((size_t)rs * 4 * n2 + i2) * n2 * g + q1;
+                const size_t sk = (size_t)n2 * n2 * g;   // stride of the (al, be) index
                 for (int j2 = 0; j2 < n2; j2++) {
-                    double s0 = 0.0, s1 = 0.0;
+                    double s00 = 0.0, s01 = 0.0, s10 = 0.0, s11 = 0.0;
 #pragma unroll
                     for (int q2 = 0; q2 < G; q2++) {
-                        const double c0 = A2[j2 * g + q2];
-                        s0 += c0 * V[0][q2] + A2[(n2 + j2) * g + q2] * V[2][q2];
-                        s1 += c0 * V[1][q2];
+                        const double c0 = A2[j2 * g + q2], c1 = A2[(n2 + j2) * g + q2];
+                        s00 += c0 * V[0][0][q2] + c1 * V[0][2][q2];
+                        s01 += c0 * V[0][1][q2];
+                        s10 += c0 * V[1][0][q2] + c1 * V[1][2][q2];
+                        s11 += c0 * V[1][1][q2];
                     }
-                    t2[j2 * g] = s0;                         // be = 0
-                    t2[(size_t)n2 * n2 * g + j2 * g] = s1;   // be = 1
+                    t2[j2 * g] = s00;
+                    t2[sk + j2 * g] = s01;
+                    t2[2 * sk + j2 * g] = s10;
+                    t2[3 * sk + j2 * g] = s11;
                 }
             }
             for (int j2s = 0; j2s < n2; j2s += j2c) {
                 const int j2n = min(j2c, n2 - j2s), nb = n1 * j2n;
                 __syncthreads();
-                // ---- step 3 (u): OB[rs][a12][b12] for j2 in the chunk
-                for (int t = tid; t < 9 * n12 * j2n; t += kSfThreads) {
+                // ---- step 3 (u): OB[rs][a12][b12] for j2 in the chunk; one
+                // task per (r, a12, j2) for the three s, so each A1 value read
+                // serves six multiply-adds
+                for (int t = tid; t < 3 * n12 * j2n; t += kSfThreads) {
                     int r = t;
                     const int j2l = r % j2n; r /= j2n;
                     const int a12 = r % n12;
-                    const int rs = r / n12;
+                    const int rr = r / n12;
                     const int i1 = a12 % n1, i2 = a12 / n1, j2 = j2s + j2l;
-                    double Uu[2][G];   // Uu[be][q1] = sum_al A1[al][i1][q1] T2[rs][al be]
+                    const size_t sk = (size_t)n2 * n2 * g;
+                    double Uu[3][2][G];   // Uu[s][be][q1] = sum_al A1[al][i1][q1] T2[3rr+s][al be]
 #pragma unroll
                     for (int q1 = 0; q1 < G; q1++) {
                         const double a0 = A1[i1 * g + q1], a1 = A1[(n1 + i1) * g + q1];
 #pragma unroll
-                        for (int be = 0; be < 2; be++) {
-                            const double *t2 = T2 + (((size_t)(rs * 4 + be) * n2 + i2) * n2 + j2) * g + q1;
-                            Uu[be][q1] = a0 * t2[0] + a1 * t2[(size_t)2 * n2 * n2 * g];
+                        for (int ss = 0; ss < 3; ss++) {
+                            const double *t2 = T2 + (((size_t)(3 * rr + ss) * 4 * n2 + i2) * n2 + j2) * g + q1;
+                            Uu[ss][0][q1] = a0 * t2[0] + a1 * t2[2 * sk];
+                            Uu[ss][1][q1] = a0 * t2[sk] + a1 * t2[3 * sk];
                         }
                     }
-                    double *ob = OB + ((size_t)rs * n12 + a12) * nb + j2l * n1;
+                    double *ob = OB + ((size_t)(3 * rr) * n12 + a12) * nb + j2l * n1;
+                    const size_t so = (size_t)n12 * nb;   // stride of rs in OB
                     for (int j1 = 0; j1 < n1; j1++) {
-                        double s = 0.0;
+                        double o0 = 0.0, o1 = 0.0, o2 = 0.0;
 #pragma unroll
-                        for (int q1 = 0; q1 < G; q1++)
-                            s += A1[j1 * g + q1] * Uu[0][q1] + A1[(n1 + j1) * g + q1] * Uu[1][q1];
-                        ob[j1] = s;
+                        for (int q1 = 0; q1 < G; q1++) {
+                            const double c0 = A1[j1 * g + q1], c1 = A1[(n1 + j1) * g + q1];
+                            o0 += c0 * Uu[0][0][q1] + c1 * Uu[0][1][q1];
+                            o1 += c0 * Uu[1][0][q1] + c1 * Uu[1][1][q1];
+                            o2 += c0 * Uu[2][0][q1] + c1 * Uu[2][1][q1];
+                        }
+                        ob[j1] = o0;
+                        ob[so + j1] = o1;
+                        ob[2 * so + j1] = o2;
                     }
                 }
                 __syncthreads();
@@ -349,6 +363,8 @@ int launch_u1_stiffness_sf(yeti_ctx *ctx, const U1Patch &P, const double *coords
     const size_t two = (size_t)per_sm / 2 > 2048 ? (size_t)per_sm / 2 - 2048 : 0;
     int j2c = a.n[1];
     while (j2c > 1 && sf_smem_doubles(a.n, P.ng, j2c) * sizeof(double) > two) j2c--;
+    const int nchunk = (a.n[1] + j2c - 1) / j2c;
+    j2c = (a.n[1] + nchunk - 1) / nchunk;   // chunks of even size
     const size_t smem = sf_smem_doubles(a.n, P.ng, j2c) * sizeof(double);
     YETI_CHECK(smem <= smem_cap, YETI_EUNSUPPORTED,
                "sum-factorised stiffness: an element of degrees (%d,%d,%d) "
