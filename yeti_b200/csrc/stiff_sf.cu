@@ -63,11 +63,14 @@ struct SfArgs {
 };
 
 // Shared-memory doubles of one CTA.
+// The control-point coordinates (3 nn) are needed only by the per-point
+// pass and share their space with T1/T2/OB.
 size_t sf_smem_doubles(const int n[3], int g, int j2c) {
     const size_t nn = (size_t)n[0] * n[1] * n[2], nq = (size_t)g * g * g;
-    return 4 * nn + (nn + 1) / 2 + 2 * (size_t)g * (n[0] + n[1] + n[2]) + 13 * nq +
-           81 * (size_t)g * g + 36 * (size_t)n[1] * n[1] * g +
-           9 * (size_t)n[0] * n[1] * n[0] * j2c;
+    const size_t work = 81 * (size_t)g * g + 36 * (size_t)n[1] * n[1] * g +
+                        9 * (size_t)n[0] * n[1] * n[0] * j2c;
+    return nn + (nn + 1) / 2 + 2 * (size_t)g * (n[0] + n[1] + n[2]) + 13 * nq +
+           (work > 3 * nn ? work : 3 * nn);
 }
 
 __device__ __forceinline__ double det3(const double J[3][3]) {
@@ -82,8 +85,7 @@ __global__ void __launch_bounds__(kSfThreads) k_u1_stiffness_sf(SfArgs a) {
     constexpr int g = G, gg = G * G, nq = G * G * G;
     const int n1 = a.n[0], n2 = a.n[1], n3 = a.n[2], nn = a.nn, j2c = a.j2c;
     const int n12 = n1 * n2;
-    double *xe = smem;                        // 3 nn
-    double *we = xe + 3 * nn;                 // nn
+    double *we = smem;                        // nn
     int *sien = reinterpret_cast<int *>(we + nn);   // nn ints
     double *A1 = we + nn + (nn + 1) / 2;      // A_d[kind][i][q], d = u, v, w
     double *A2 = A1 + 2 * n1 * g, *A3 = A2 + 2 * n2 * g;
@@ -91,6 +93,7 @@ __global__ void __launch_bounds__(kSfThreads) k_u1_stiffness_sf(SfArgs a) {
     double *T1 = cq + 13 * nq;                // [rs][ck ce][q1 q2]
     double *T2 = T1 + 81 * gg;                // [rs][al be][i2][j2][q1]
     double *OB = T2 + 36 * n2 * n2 * g;       // [rs][a12][b12 of the chunk]
+    double *xe = T1;                          // 3 nn, per-point pass only
     __shared__ double su1[3], su2[3];
     __shared__ int sni[3];
     const int e = blockIdx.x, tid = threadIdx.x;
