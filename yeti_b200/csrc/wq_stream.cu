@@ -201,11 +201,13 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, int tr
 
 // ---------------------------------------------------------------- walks
 // Tile patterns of one direction (host flag): 1 every element owns two
-// points; 2 the first element owns p+1 points, the others two (the first
+// points and the tile is full (tq / 2 elements: the walks' element count is
+// a compile-time constant); 4 every element owns two points, fewer
+// elements; 2 the first element owns p+1 points, the others two (the first
 // tile); 3 the last element owns p+2 points, the others two (the last tile);
 // 0 anything else (run-time walk).
 __host__ __device__ constexpr int pat_nemax(int P, int pat, int tq = kTQ) {
-    return pat == 1 ? tq / 2 : pat == 2 ? 1 + (tq - (P + 1)) / 2 : 1 + (tq - (P + 2)) / 2;
+    return pat == 1 || pat == 4 ? tq / 2 : pat == 2 ? 1 + (tq - (P + 1)) / 2 : 1 + (tq - (P + 2)) / 2;
 }
 // first point of element e in a tile of pattern pat
 __host__ __device__ constexpr int pat_q0(int P, int pat, int e) {
@@ -216,8 +218,9 @@ __host__ __device__ constexpr int pat_q0(int P, int pat, int e) {
 // walked element by element with the accumulators of the element's p+1
 // functions named at compile time.
 template <class T, int P, int PAT>
-__device__ __forceinline__ void walk_u(const T *h, T *g, const T *tab, int kind, int ne) {
+__device__ __forceinline__ void walk_u(const T *h, T *g, const T *tab, int kind, int ne_rt) {
     constexpr int PBP = round4(P + 1), NEM = pat_nemax(P, PAT), NF = NEM + P;
+    const int ne = PAT == 1 ? NEM : ne_rt;
     T a[NF];
 #pragma unroll
     for (int f = 0; f < NF; f++) a[f] = T(0);
@@ -277,9 +280,10 @@ __device__ __forceinline__ void walk_u_generic(const T *h, T *g, const T *tab, i
 // (trial l != v), wb at ka+1 (trial l == v).  G of row qv of the tile lives
 // in the block of warp qv/2: gb + (qv/2)*GP + (qv%2)*NFM + l*GS.
 template <class T, int P, int PAT>
-__device__ __forceinline__ void walk_v(const T *gb, T *kp, const T *tab, int ka, int ne) {
+__device__ __forceinline__ void walk_v(const T *gb, T *kp, const T *tab, int ka, int ne_rt) {
     using D = Dims<P>;
     constexpr int PBP = D::PBP, NEM = pat_nemax(P, PAT, kTV), NF = NEM + P, NFM = D::NFM;
+    const int ne = PAT == 1 ? NEM : ne_rt;
     constexpr int GS = D::GS, GP = D::GP;
     T A0[NF], A1[NF];
 #pragma unroll
@@ -365,7 +369,7 @@ struct StreamArgs {
     const int *tile_pstride;   // coefficients per w plane of a tile (padded)
     const int *tq0[2];         // first point of a u / v tile
     const int *tnq[2];         // points of a u / v tile
-    const int *treg[2];        // tile pattern (walk_u): 1 regular, 2 first, 3 last, 0 other
+    const int *treg[2];        // tile pattern (walk_u): 1 regular full, 4 regular, 2 first, 3 last, 0 other
     int ntile[2];
     const int *elem[3];        // element owning each point
     const T *band[3];          // [nqp][6][round4(p+1)]: B0 B1 W00 W01 W10 W11
@@ -414,7 +418,7 @@ __global__ void __launch_bounds__(kThreads, kCtasPerSm) k_wq_apply_stream(Stream
         const int qu0 = a.tq0[0][tu], nqu = a.tnq[0][tu];
         const int qv0 = a.tq0[1][tv], nqv = a.tnq[1][tv];
         const int patu = a.treg[0][tu], patv = a.treg[1][tv];
-        const bool regu = patu == 1, regv = patv == 1;
+        const bool regu = patu == 1 || patu == 4, regv = patv == 1 || patv == 4;
         const int fu0 = a.elem[0][qu0], fv0 = a.elem[1][qv0];
         const int nfu = a.elem[0][qu0 + nqu - 1] + PB - fu0;
         const int nfv = a.elem[1][qv0 + nqv - 1] + PB - fv0;
@@ -648,6 +652,7 @@ __global__ void __launch_bounds__(kThreads, kCtasPerSm) k_wq_apply_stream(Stream
                             T *gr = gp + ch * GS + row * NFM;
                             switch (patu) {
                                 case 1: walk_u<T, P, 1>(hr, gr, tabu, kind, neu); break;
+                                case 4: walk_u<T, P, 4>(hr, gr, tabu, kind, neu); break;
                                 case 2: walk_u<T, P, 2>(hr, gr, tabu, kind, neu); break;
                                 case 3: walk_u<T, P, 3>(hr, gr, tabu, kind, neu); break;
                                 default: walk_u_generic<T, P>(hr, gr, tabu, kind, relu, nqu);
@@ -669,6 +674,7 @@ __global__ void __launch_bounds__(kThreads, kCtasPerSm) k_wq_apply_stream(Stream
                     T *kp = RZH + (ik * D::NFV * NFM + fu) * 2;
                     switch (patv) {
                         case 1: walk_v<T, P, 1>(gb, kp, tabv, ka, nev); break;
+                        case 4: walk_v<T, P, 4>(gb, kp, tabv, ka, nev); break;
                         case 2: walk_v<T, P, 2>(gb, kp, tabv, ka, nev); break;
                         case 3: walk_v<T, P, 3>(gb, kp, tabv, ka, nev); break;
                         default: walk_v_generic<T, P>(gb, kp, tabv, ka, relv, nqv);
@@ -740,15 +746,16 @@ static void make_tiles(const std::vector<int> &elem_q0, int nel, std::vector<int
         last_begin = nel - 1;
         while (last_begin - 1 >= first_end && pts(last_begin - 1, nel) <= maxq) last_begin--;
     }
-    // walk pattern of a tile (see walk_u): 1 all elements own two points,
-    // 2 only the first element of the patch differs, 3 only the last
+    // walk pattern of a tile (see walk_u): 1 all elements own two points and
+    // the tile is full, 4 all own two, 2 only the first element of the patch
+    // differs, 3 only the last
     auto add = [&](int a, int b) {
         bool inner2 = true;   // elements other than the patch's first / last own 2
         for (int e = a; e < b; e++)
             if (e != 0 && e != nel - 1) inner2 = inner2 && (pts(e, e + 1) == 2);
         const bool has_first = a == 0, has_last = b == nel;
         int pat = 0;
-        if (inner2 && !has_first && !has_last) pat = 1;
+        if (inner2 && !has_first && !has_last) pat = b - a == maxe ? 1 : 4;
         else if (inner2 && has_first && !has_last) pat = 2;
         else if (inner2 && has_last && !has_first) pat = 3;
         q0.push_back(elem_q0[a]);
@@ -916,15 +923,13 @@ int wq_stream_setup(yeti_wq_op *op, const WQRule1D R[3]) {
     int nsm = 0;
     YETI_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, ctx->device));
     // segments: (tile, element range) cut from the tile-major sequence so
-    // that every CTA gets about the same number of point-planes
+    // that every CTA gets about the same number of tile planes (a plane of a
+    // narrow tile costs a CTA about as much as a full one: the same stages,
+    // barriers and walks, with lanes idle)
     for (int which = 0; which < 2; which++) {
         // item (t, e) goes to CTA floor(work before it * ncta / total work);
         // consecutive items of one CTA and one tile form a segment
-        int64_t total = 0;
-        for (int t = 0; t < ntiles; t++) {
-            const int tu = t % st.ntile[0], tv = t / st.ntile[0];
-            total += (int64_t)tnq[0][tu] * tnq[1][tv] * nqw;
-        }
+        const int64_t total = (int64_t)ntiles * nqw;
         const int64_t nitems = (int64_t)ntiles * op->nel[2];
         const int ncta = (int)std::max<int64_t>(
             1, std::min<int64_t>((int64_t)nsm * st.per_sm[which], nitems));
@@ -933,11 +938,9 @@ int wq_stream_setup(yeti_wq_op *op, const WQRule1D R[3]) {
         int64_t before = 0;
         int last_cta = -1;
         for (int t = 0; t < ntiles; t++) {
-            const int tu = t % st.ntile[0], tv = t / st.ntile[0];
-            const int64_t npts = (int64_t)tnq[0][tu] * tnq[1][tv];
             for (int e = 0; e < op->nel[2]; e++) {
                 const int c = (int)std::min<int64_t>(ncta - 1, before * ncta / total);
-                before += npts * (elem_q0[2][e + 1] - elem_q0[2][e]);
+                before += elem_q0[2][e + 1] - elem_q0[2][e];
                 if (c != last_cta || seg.empty() || seg.back().x != t) {
                     for (int k = last_cta + 1; k <= c; k++) cta_seg[k] = (int)seg.size();
                     seg.push_back(make_int4(t, e, e + 1, 0));
