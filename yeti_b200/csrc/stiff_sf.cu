@@ -79,8 +79,9 @@ __device__ __forceinline__ double det3(const double J[3][3]) {
            J[0][2] * (J[1][0] * J[2][1] - J[1][1] * J[2][0]);
 }
 
+// Three CTAs per SM for g <= 4 (registers capped at 85), two above.
 template <int G>
-__global__ void __launch_bounds__(kSfThreads) k_u1_stiffness_sf(SfArgs a) {
+__global__ void __launch_bounds__(kSfThreads, G <= 4 ? 3 : 2) k_u1_stiffness_sf(SfArgs a) {
     extern __shared__ double smem[];
     constexpr int g = G, gg = G * G, nq = G * G * G;
     const int n1 = a.n[0], n2 = a.n[1], n3 = a.n[2], nn = a.nn, j2c = a.j2c;
