@@ -4,9 +4,9 @@
 //
 // Work decomposition
 // ------------------
-// The (u, v) point grid is cut into tiles of at most 16 x 16 points made of
-// whole elements; a CTA takes a tile and a range of elements along w and
-// marches through the w point planes of that range.  Every WQ point belongs
+// The (u, v) point grid is cut into tiles of at most 16 x YETI_WQ_TV (8)
+// points made of whole elements; a CTA takes a tile and a range of elements
+// along w and marches through the w point planes of that range.  Every WQ point belongs
 // to one element and, in each direction, its B0/B1/W** rows are non-zero for
 // the p+1 functions elem(q)..elem(q)+p only (checked on the host), so every
 // 1-D contraction is a band of width p+1.  Per plane:
