@@ -194,6 +194,8 @@ typedef struct {
 #define YETI_WQ_F64 1     /* keep FP64 operator data                    */
 #define YETI_WQ_F32 2     /* keep FP32 operator data                    */
 
+/* p[d] in 2..8 and nel[d] >= 2 per direction (the WQ rule's construction
+ * needs two elements); otherwise YETI_EINVAL. */
 int yeti_wq_setup(yeti_ctx *ctx, const int32_t p[3], const int32_t nel[3],
                   const double *cps, const double *weights, double E,
                   double nu, const uint8_t dirichlet[18], int prec_mask,

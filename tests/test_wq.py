@@ -29,6 +29,18 @@ STREAM_CASES = [
     ((10, 24, 4), (3, 3, 3), 0.2, (0.8, 1.2), {"v0": (0, 1, 2)}),
 ]
 
+# Thin patches (two elements, the fewest the WQ rule takes): tiles that are
+# first and last at once, one tile along u with many along v and back.
+THIN_CASES = [
+    ((2, 2, 2), (2, 2, 2), 0.1, (0.9, 1.1), None),
+    ((2, 3, 2), (3, 3, 3), 0.1, (0.9, 1.1), {"w0": (0, 1, 2)}),
+    ((2, 2, 5), (4, 4, 4), 0.1, (0.9, 1.1), None),
+    ((16, 2, 2), (2, 2, 2), 0.1, (0.9, 1.1), {"u0": (0, 1, 2)}),
+    ((2, 17, 2), (3, 3, 3), 0.1, (0.9, 1.1), None),
+    ((33, 2, 2), (2, 2, 2), 0.1, (0.9, 1.1), {"v1": (1,)}),
+    ((3, 2, 2), (5, 5, 5), 0.1, (0.9, 1.1), None),
+]
+
 
 def _rel(a, b):
     return np.linalg.norm(a - b) / np.linalg.norm(b)
@@ -83,7 +95,7 @@ def _pair(case, E=1.0, nu=0.3, seed=7):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("case", CASES + STREAM_CASES)
+@pytest.mark.parametrize("case", CASES + STREAM_CASES + THIN_CASES)
 def test_gpu_apply_diag_force_match_oracle(cuda_ok, case):
     op, ref = _pair(case)
     rng = np.random.default_rng(11)
@@ -102,6 +114,15 @@ def test_gpu_apply_diag_force_match_oracle(cuda_ok, case):
     m = op.free_mask == 0
     if m.any():
         assert np.abs(k1[m]).max() == 0.0
+
+
+@pytest.mark.gpu
+def test_gpu_setup_rejects_a_single_element_direction(cuda_ok):
+    from yeti_b200._lib import YetiError
+    from yeti_b200.wq import WQElasticity
+    P = cube_patch((1, 3, 2), (2, 2, 2))
+    with pytest.raises(YetiError, match="EINVAL"):
+        WQElasticity(P, 1.0, 0.3, None)
 
 
 @pytest.mark.gpu
