@@ -22,6 +22,7 @@ namespace yeti {
 
 constexpr int kRedBlocks = 592;     // 4 x 148 SMs
 constexpr int kRedThreads = 256;
+constexpr int kFusedThreads = 1024; // k_cg_fused: one CTA per SM
 constexpr int kChunk = 16;          // iterations enqueued per host check
 
 // Sum of nparts partials (single block, fixed order).
@@ -78,10 +79,13 @@ __device__ __forceinline__ double block_sum_all(double v, double *sh) {
 // vector is kept across a barrier (p, r and the inverse diagonal are read
 // again from L2; z = dinv r is recomputed from the stored r, the same value);
 // every block sums the partials in the same fixed order, so all blocks take
-// the same alpha, beta and stop decision and the results equal the
-// three-kernel path's.  parts: 3 * gridDim.x doubles.
+// the same alpha, beta and stop decision.  One CTA of kFusedThreads per SM
+// (fewer blocks to meet at each grid barrier than 4 x 256-thread CTAs: 2 us
+// less per iteration at 64^3); its partial sums are taken over its own
+// blocks, so the results can differ from the three-kernel path's in the last
+// bits.  parts: 3 * gridDim.x doubles.
 template <class T>
-__global__ void __launch_bounds__(kRedThreads, 4)   // 4 x 148 = kRedBlocks co-resident
+__global__ void __launch_bounds__(kFusedThreads, 1)
 k_cg_fused(T *x, T *r, T *p, T *Ap, const T *dinv, int64_t n, double *parts, CGScal *s) {
     __shared__ double sh[32];
     if (s->done) return;   // read by every block before anyone can set it
@@ -710,19 +714,20 @@ static int ensure_workspace(yeti_wq_op *op, bool f32) {
 // device flag is set).
 // dinv == nullptr: the fast-diagonalisation preconditioner gives z, r.z and
 // beta after the update.
-// Can the iteration's vector work run as one cooperative k_cg_fused launch
-// (all kRedBlocks blocks co-resident)?
+// Grid of the cooperative k_cg_fused launch (one CTA per SM, all
+// co-resident), or 0 when the iteration cannot run as one.
 template <class T>
-static bool cg_fused_ok(const yeti_wq_op *op) {
+static int cg_fused_grid(const yeti_wq_op *op) {
     int dev = op->ctx->device, coop = 0, sms = 0, per_sm = 0;
     if (cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev) != cudaSuccess ||
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_cg_fused<T>, kRedThreads, 0) !=
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_cg_fused<T>, kFusedThreads, 0) !=
             cudaSuccess) {
         (void)cudaGetLastError();
-        return false;
+        return 0;
     }
-    return coop && (int64_t)per_sm * sms >= kRedBlocks;
+    if (!coop || per_sm < 1) return 0;
+    return std::min(sms, kRedBlocks);   // parts holds 3 x kRedBlocks partials
 }
 
 template <class T>
@@ -731,13 +736,14 @@ static int cg_chunk(yeti_wq_op *op, int prec, T *x, T *r, T *z, T *p, T *Ap,
     cudaStream_t s = op->ctx->stream;
     const int64_t n = op->ndof;
     double *parts = op->parts.as<double>();
-    if (dinv && !pause && cg_fused_ok<T>(op)) {
+    const int fgrid = dinv && !pause ? cg_fused_grid<T>(op) : 0;
+    if (fgrid > 0) {
         for (int k = 0; k < kChunk; k++) {
             YETI_TRY(wq_apply_dev(op, p, Ap, prec, &ds->done, s));
             int64_t nn = n;
             void *args[] = {&x, &r, &p, &Ap, (void *)&dinv, &nn, &parts, &ds};
-            YETI_CUDA(cudaLaunchCooperativeKernel((const void *)k_cg_fused<T>, dim3(kRedBlocks),
-                                                  dim3(kRedThreads), args, 0, s));
+            YETI_CUDA(cudaLaunchCooperativeKernel((const void *)k_cg_fused<T>, dim3(fgrid),
+                                                  dim3(kFusedThreads), args, 0, s));
             count_launches(1);
         }
         YETI_CUDA(cudaGetLastError());
