@@ -706,12 +706,16 @@ def main():
     for mixed in (False, True):
         op.pcg(b, rtol=args.rtol, mixed=mixed, precond="fd")   # builds the plan
         torch.cuda.synchronize()
-        e0.record()
-        for _ in range(max(1, args.steps)):
+        # each solve timed alone, the median kept: one host stall between
+        # two calls on a shared machine would otherwise double a 17 ms mean
+        tf = []
+        for _ in range(max(3, args.steps)):
+            e0.record()
             xf, stf = op.pcg(b, rtol=args.rtol, mixed=mixed, precond="fd")
-        e1.record()
-        torch.cuda.synchronize()
-        msf = e0.elapsed_time(e1) / max(1, args.steps)
+            e1.record()
+            torch.cuda.synchronize()
+            tf.append(e0.elapsed_time(e1))
+        msf = float(np.median(tf))
         fd["mixed" if mixed else "fp64"] = {
             "value": ws * op.nfree / (msf / 1e3), "ms_per_step": msf,
             "iterations": stf["iterations"], "outer_iterations": stf["outer_iterations"],
