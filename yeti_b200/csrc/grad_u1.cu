@@ -708,7 +708,6 @@ YETI_API int yeti_grad_lin_elast_work(yeti_ctx *ctx, const yeti_u1_model *m,
         g.egi = bi.as<double>();
         g.ege = be.as<double>();
         const PtLayout L = pt_layout(P.nn, (int)nadj, max_body);
-        const size_t vol = (size_t)P.nq * L.size;
         const size_t face = (size_t)P.ng * P.ng * (4 * P.nn + 11 + 3 * nadj);
         // term buffer of stage B: up to 6144 doubles (48 KB), whole chunks of points
         const int qchunk = (int)std::max<int64_t>(
