@@ -118,6 +118,56 @@ def u1_system_args(patch, E=1.0, nu=0.3, rho=0.0, nbint=None):
     ]
 
 
+def u1_system_args_multi(patches, materials=None, rho=0.0):
+    """The 38 arguments of ``sys_linmat_lindef_static`` for several U1
+    patches side by side in one model: control points numbered patch after
+    patch (no shared control points), elements, knots, IEN, spans and
+    weights concatenated in patch order, ``ELT_TYPE`` 'U1U1...', ``TENSOR``
+    '/THREED/THREED...', one (E, nu) per patch from ``materials`` (default
+    (1, 0.3)) and the Gauss points per element of each patch its own
+    (max p + 1)^3."""
+    per = [u1_system_args(P) for P in patches]
+    npatch = len(per)
+    materials = materials or [(1.0, 0.3)] * npatch
+    ncps = [int(a[36]) for a in per]
+    off = np.cumsum([0] + ncps[:-1])
+    nb_cp = int(sum(ncps))
+    nb_elem = int(sum(int(a[35]) for a in per))
+    nb_data = float(sum(float(a[1]) for a in per))
+    coords = np.concatenate([np.asarray(a[2]) for a in per], axis=1)
+    ien = np.concatenate([np.asarray(a[3]) + o for a, o in zip(per, off)])
+    nkv = np.concatenate([np.asarray(a[5]) for a in per], axis=1)
+    ndof = 3 * nb_cp
+    return [
+        np.ones(nb_elem, dtype=np.int64),
+        nb_data,
+        coords,
+        ien.astype(np.int64),
+        np.array([int(a[35]) for a in per], dtype=np.int64),
+        nkv.astype(np.int64),
+        np.concatenate([np.asarray(a[6]) for a in per]),
+        np.concatenate([np.asarray(a[7]) for a in per], axis=1).astype(np.int64),
+        np.concatenate([np.asarray(a[8]) for a in per]),
+        np.concatenate([np.asarray(a[9]) for a in per], axis=1).astype(np.int64),
+        np.array("U1" * npatch),
+        np.ones(npatch), np.ones(npatch, dtype=np.int64),
+        np.array([[E for E, _ in materials], [nu for _, nu in materials]], dtype=np.float64),
+        np.full(npatch, 3, dtype=np.int64),
+        np.full(npatch, rho, dtype=np.float64),
+        np.array("/THREED" * npatch),
+        np.zeros(0, dtype=np.int64), np.zeros(0, dtype=np.int64), np.zeros(0, dtype=np.float64),
+        np.zeros(0, dtype=np.int64), np.zeros(0, dtype=np.float64), np.zeros(0, dtype=np.int64),
+        np.zeros((2, 0), dtype=np.float64), np.zeros(0, dtype=np.int64), np.zeros(0, dtype=np.int64),
+        np.arange(1, ndof + 1, dtype=np.int64),
+        ndof,
+        3,
+        np.concatenate([np.asarray(a[29]) for a in per]).astype(np.int64),
+        np.concatenate([np.asarray(a[30]) for a in per]).astype(np.int64),
+        np.zeros((1, nb_cp), dtype=np.float64),
+        0, 0, npatch, nb_elem, nb_cp, ndof,
+    ]
+
+
 def face_mask(clamp_faces):
     """dirichlet[6*c + f] array from {'u0': comps, 'w1': comps, ...}."""
     names = ["u0", "u1", "v0", "v1", "w0", "w1"]
