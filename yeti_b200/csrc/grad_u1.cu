@@ -13,7 +13,9 @@
 //
 // Kernel design: one CTA per active element.  Stage A: one thread per
 // quadrature point computes the basis, covariant frame, metrics, strains and
-// stresses of the state and adjoint fields into shared memory.  Stage B: one
+// stresses of the state and adjoint fields into shared memory (all the
+// points when their records fit, else chunk by chunk, every sum continued
+// across the chunks in point order).  Stage B: one
 // thread per control point accumulates its (nadj x 3) derivative over the
 // points in order.  A second kernel sums element contributions per control
 // point in element order (deterministic).  Compiled without FMA contraction
@@ -34,7 +36,7 @@ __device__ __constant__ int c_vi[6] = {0, 1, 2, 0, 0, 1};
 __device__ __constant__ int c_vj[6] = {0, 1, 2, 1, 2, 2};
 
 struct GradArgs {
-    int p0, p1, p2, nn, nq, ng, nadj, qchunk;
+    int p0, p1, p2, nn, nq, ng, nadj, qchunk, pchunk;
     int compute_int, compute_ext, include_surface;
     const double *U0, *U1, *U2;
     const double *gauss;      // volume rule (4 * nq)
@@ -117,14 +119,16 @@ __host__ __device__ inline PtLayout pt_layout(int nn, int nadj, int nbody) {
     return L;
 }
 
-// Shared memory of one element: xe, ue, uae, we, then nq point records of
-// PtLayout, then the basis scratch (kBasisB1 + kStiffQS per point) and the
-// external-work accumulators of the (control point, component) tasks.
-__host__ __device__ inline size_t grad_smem_doubles(int nn, int nq, int nadj, const PtLayout &L,
+// Shared memory of one element: xe, ue, uae, we, then the point records
+// (PtLayout) of one chunk of pchunk points, then the basis scratch
+// (kBasisB1 + kStiffQS per point of the chunk), the external- and
+// internal-work accumulators of the (control point, component) tasks and
+// the term buffer of stage B (qchunk points).
+__host__ __device__ inline size_t grad_smem_doubles(int nn, int pchunk, int nadj, const PtLayout &L,
                                                     size_t face, int qchunk) {
-    const size_t vol = (size_t)nq * L.size;
+    const size_t vol = (size_t)pchunk * L.size;
     return (size_t)(6 + 3 * nadj) * nn + nn + (vol > face ? vol : face) +
-           (size_t)nq * (kBasisB1 + kStiffQS) + (size_t)2 * 3 * nn * nadj +
+           (size_t)pchunk * (kBasisB1 + kStiffQS) + (size_t)2 * 3 * nn * nadj +
            (size_t)3 * nn * qchunk * 3 * nadj;
 }
 
@@ -179,280 +183,293 @@ __global__ void __launch_bounds__(256) k_u1_grad(GradArgs a) {
     const int nbody = s_nbody;
     const PtLayout L = pt_layout(nn, nadj, nbody);
     const size_t face = (size_t)a.ng * a.ng * (4 * nn + 11 + 3 * nadj);
-    const size_t vol = (size_t)a.nq * L.size;
+    const int pc = a.pchunk;
+    const size_t vol = (size_t)pc * L.size;
     double *B1 = pts + (vol > face ? vol : face);
-    double *qs = B1 + (size_t)a.nq * kBasisB1;
-    double *ge_s = qs + (size_t)a.nq * kStiffQS;
+    double *qs = B1 + (size_t)pc * kBasisB1;
+    double *ge_s = qs + (size_t)pc * kStiffQS;
+    double *gi_s = ge_s + (size_t)3 * nn * nadj;   // 3 nn nadj accumulators
+    double *terms = gi_s + (size_t)3 * nn * nadj;  // 3 nn qchunk 3 nadj terms
     const double lambda = a.E * a.nu / (1.0 + a.nu) / (1.0 - 2.0 * a.nu);
     const double mu = a.E / 2.0 / (1.0 + a.nu);
-    // ---------------- stage A: per volume point
-    {
-        const int pd[3] = {a.p0, a.p1, a.p2};
-        const double *Ud[3] = {a.U0, a.U1, a.U2};
-        // R numerators and dR/dxi into the point records, dx/dxi into qs
-        basis_chunk(pd, Ud, sni, su1, su2, a.gauss, 0, a.nq, nn, xe, we, B1, pts + L.R, L.size,
-                    pts + L.dR, L.size, qs);
-    }
-    for (int t = tid; t < a.nq * nn; t += nth) {
-        const int q = t / nn, n = t - q * nn;
-        double *R = pts + (size_t)q * L.size + L.R;
-        R[n] = R[n] * qs[(size_t)q * kStiffQS + 3];
-    }
-    if (a.compute_int) {
-        // the gradients of the state and of the adjoints: ordered sums over
-        // the nodes, one thread per (point, entry)
-        const int ns = 9 * (1 + nadj);
-        for (int t = tid; t < a.nq * ns; t += nth) {
-            const int q = t / ns, s = t - q * ns;
-            double *P = pts + (size_t)q * L.size;
-            const double *dR = P + L.dR;
-            const int k = s / 9 - 1, ic = s % 9, i = ic / 3, c = ic % 3;
-            const double *v = k < 0 ? ue : uae + 3 * nn * k;
-            double acc = 0.0;
-            for (int cp = 0; cp < nn; cp++) acc = acc + dR[3 * cp + i] * v[3 * cp + c];
-            if (k < 0) P[L.dU + ic] = acc;
-            else P[L.dUA + 9 * k + ic] = acc;
+    for (int t = tid; t < 3 * nn * nadj; t += nth) gi_s[t] = ge_s[t] = 0.0;
+    // The points are taken in chunks of pc (their records in shared memory);
+    // every accumulator continues over the chunks in point order, so the
+    // sums are the same sequences as over all points at once.
+    for (int p0 = 0; p0 < a.nq; p0 += pc) {
+        const int np = min(pc, a.nq - p0);
+        __syncthreads();
+        // ---------------- stage A: per volume point of the chunk
+        {
+            const int pd[3] = {a.p0, a.p1, a.p2};
+            const double *Ud[3] = {a.U0, a.U1, a.U2};
+            // R numerators and dR/dxi into the point records, dx/dxi into qs
+            basis_chunk(pd, Ud, sni, su1, su2, a.gauss, p0, np, nn, xe, we, B1, pts + L.R, L.size,
+                        pts + L.dR, L.size, qs);
         }
-    }
-    __syncthreads();
-    for (int q = tid; q < a.nq; q += nth) {
-        double *P = pts + (size_t)q * L.size;
-        const double *g = a.gauss + 4 * q;
-        double detJac = g[0];
-        for (int i = 0; i < 3; i++) detJac = detJac * 0.5 * (su2[i] - su1[i]);
-        const double *R = P + L.R;
-        double AI[3][3];
-        for (int i = 0; i < 3; i++)
-            for (int c = 0; c < 3; c++) AI[i][c] = qs[(size_t)q * kStiffQS + 4 + 3 * c + i];
-        double AxA[3][3];
-        gcross(AI[0], AI[1], AxA[2]);
-        const double Area = gdot(AxA[2], AI[2]);
-        gcross(AI[1], AI[2], AxA[0]);
-        gcross(AI[2], AI[0], AxA[1]);
-        for (int i = 0; i < 3; i++)
-            for (int c = 0; c < 3; c++) {
-                P[L.AI + 3 * i + c] = AI[i][c];
-                P[L.AxA + 3 * i + c] = AxA[i][c];
-            }
-        P[L.area] = Area;
-        P[L.dj] = detJac;
+        for (int t = tid; t < np * nn; t += nth) {
+            const int q = t / nn, n = t - q * nn;
+            double *R = pts + (size_t)q * L.size + L.R;
+            R[n] = R[n] * qs[(size_t)q * kStiffQS + 3];
+        }
         if (a.compute_int) {
-            double AAI[3][3], AAE[3][3];
+            // the gradients of the state and of the adjoints: ordered sums over
+            // the nodes, one thread per (point, entry)
+            const int ns = 9 * (1 + nadj);
+            for (int t = tid; t < np * ns; t += nth) {
+                const int q = t / ns, s = t - q * ns;
+                double *P = pts + (size_t)q * L.size;
+                const double *dR = P + L.dR;
+                const int k = s / 9 - 1, ic = s % 9, i = ic / 3, c = ic % 3;
+                const double *v = k < 0 ? ue : uae + 3 * nn * k;
+                double acc = 0.0;
+                for (int cp = 0; cp < nn; cp++) acc = acc + dR[3 * cp + i] * v[3 * cp + c];
+                if (k < 0) P[L.dU + ic] = acc;
+                else P[L.dUA + 9 * k + ic] = acc;
+            }
+        }
+        __syncthreads();
+        for (int ql = tid; ql < np; ql += nth) {
+            const int q = ql;   // the point's record and basis scratch (chunk-local)
+            double *P = pts + (size_t)q * L.size;
+            const double *g = a.gauss + 4 * (p0 + ql);
+            double detJac = g[0];
+            for (int i = 0; i < 3; i++) detJac = detJac * 0.5 * (su2[i] - su1[i]);
+            const double *R = P + L.R;
+            double AI[3][3];
             for (int i = 0; i < 3; i++)
-                for (int j = 0; j < 3; j++) AAI[i][j] = gdot(AI[i], AI[j]);
-            ginv3(AAI, AAE);
-            double H[6][6];
-            for (int kl = 0; kl < 6; kl++) {
-                const int k = c_vi[kl], l = c_vj[kl];
-                for (int ij = 0; ij <= kl; ij++) {
-                    const int i = c_vi[ij], j = c_vj[ij];
-                    H[ij][kl] = lambda * AAE[i][j] * AAE[k][l] +
-                                mu * (AAE[i][k] * AAE[j][l] + AAE[i][l] * AAE[j][k]);
+                for (int c = 0; c < 3; c++) AI[i][c] = qs[(size_t)q * kStiffQS + 4 + 3 * c + i];
+            double AxA[3][3];
+            gcross(AI[0], AI[1], AxA[2]);
+            const double Area = gdot(AxA[2], AI[2]);
+            gcross(AI[1], AI[2], AxA[0]);
+            gcross(AI[2], AI[0], AxA[1]);
+            for (int i = 0; i < 3; i++)
+                for (int c = 0; c < 3; c++) {
+                    P[L.AI + 3 * i + c] = AI[i][c];
+                    P[L.AxA + 3 * i + c] = AxA[i][c];
                 }
-            }
-            for (int kl = 1; kl < 6; kl++)
-                for (int r = kl; r < 6; r++) H[r][kl - 1] = H[kl - 1][r];
-            double dU[3][3];
-            for (int i = 0; i < 3; i++)
-                for (int c = 0; c < 3; c++) dU[i][c] = P[L.dU + 3 * i + c];
-            double strain[6], stress[6];
-            for (int ij = 0; ij < 6; ij++) {
-                const int i = c_vi[ij], j = c_vj[ij];
-                if (i == j) strain[ij] = gdot(AI[i], dU[i]);
-                else strain[ij] = gdot(AI[i], dU[j]) + gdot(AI[j], dU[i]);
-            }
-            for (int ii = 0; ii < 6; ii++) {
-                double s = 0.0;
-                for (int jj = 0; jj < 6; jj++) s = s + H[ii][jj] * strain[jj];
-                stress[ii] = s;
-            }
-            for (int i = 0; i < 3; i++)
-                for (int c = 0; c < 3; c++) P[L.AAE + 3 * i + c] = AAE[i][c];
-            for (int ij = 0; ij < 6; ij++) {
-                P[L.strain + ij] = strain[ij];
-                P[L.stress + ij] = stress[ij];
-            }
-            for (int k = 0; k < nadj; k++) {
-                double dA[3][3];
+            P[L.area] = Area;
+            P[L.dj] = detJac;
+            if (a.compute_int) {
+                double AAI[3][3], AAE[3][3];
                 for (int i = 0; i < 3; i++)
-                    for (int c = 0; c < 3; c++) dA[i][c] = P[L.dUA + 9 * k + 3 * i + c];
-                double sA[6], tA[6];
+                    for (int j = 0; j < 3; j++) AAI[i][j] = gdot(AI[i], AI[j]);
+                ginv3(AAI, AAE);
+                double H[6][6];
+                for (int kl = 0; kl < 6; kl++) {
+                    const int k = c_vi[kl], l = c_vj[kl];
+                    for (int ij = 0; ij <= kl; ij++) {
+                        const int i = c_vi[ij], j = c_vj[ij];
+                        H[ij][kl] = lambda * AAE[i][j] * AAE[k][l] +
+                                    mu * (AAE[i][k] * AAE[j][l] + AAE[i][l] * AAE[j][k]);
+                    }
+                }
+                for (int kl = 1; kl < 6; kl++)
+                    for (int r = kl; r < 6; r++) H[r][kl - 1] = H[kl - 1][r];
+                double dU[3][3];
+                for (int i = 0; i < 3; i++)
+                    for (int c = 0; c < 3; c++) dU[i][c] = P[L.dU + 3 * i + c];
+                double strain[6], stress[6];
                 for (int ij = 0; ij < 6; ij++) {
                     const int i = c_vi[ij], j = c_vj[ij];
-                    if (i == j) sA[ij] = gdot(AI[i], dA[i]);
-                    else sA[ij] = gdot(AI[i], dA[j]) + gdot(AI[j], dA[i]);
+                    if (i == j) strain[ij] = gdot(AI[i], dU[i]);
+                    else strain[ij] = gdot(AI[i], dU[j]) + gdot(AI[j], dU[i]);
                 }
                 for (int ii = 0; ii < 6; ii++) {
                     double s = 0.0;
-                    for (int jj = 0; jj < 6; jj++) s = s + H[ii][jj] * sA[jj];
-                    tA[ii] = s;
+                    for (int jj = 0; jj < 6; jj++) s = s + H[ii][jj] * strain[jj];
+                    stress[ii] = s;
                 }
-                for (int ij = 0; ij < 6; ij++) {
-                    P[L.sA + 6 * k + ij] = sA[ij];
-                    P[L.tA + 6 * k + ij] = tA[ij];
-                }
-            }
-            for (int k = 0; k < nadj; k++) P[L.work + k] = 0.0;
-            for (int ij = 0; ij < 6; ij++)
-                for (int k = 0; k < nadj; k++)
-                    P[L.work + k] = P[L.work + k] + P[L.sA + 6 * k + ij] * stress[ij];
-        }
-        if (a.compute_ext && nbody > 0) {
-            for (int k = 0; k < nadj; k++)
-                for (int c = 0; c < 3; c++) {
-                    double s = 0.0;
-                    for (int cp = 0; cp < nn; cp++) s = s + R[cp] * uae[3 * cp + c + 3 * nn * k];
-                    P[L.vA + 3 * k + c] = s;
-                }
-            // centrifugal loads: the reference advances its info cursor by
-            // 2*MCRD for every centrifugal load acting on the element
-            int loadcount = 0;
-            for (int b = 0; b < nbody; b++) {
-                const int nl = s_body[b];
-                double pg[3] = {0, 0, 0}, A[3], B[3], vd[3], ag[3];
-                for (int cp = 0; cp < nn; cp++)
-                    for (int c = 0; c < 3; c++) pg[c] = pg[c] + R[cp] * xe[3 * cp + c];
-                for (int c = 0; c < 3; c++) A[c] = a.addinfos[loadcount + c];
-                loadcount += 3;
-                for (int c = 0; c < 3; c++) B[c] = a.addinfos[loadcount + c];
-                loadcount += 3;
-                for (int c = 0; c < 3; c++) vd[c] = B[c] - A[c];
-                const double nr = sqrt(vd[0] * vd[0] + vd[1] * vd[1] + vd[2] * vd[2]);
-                for (int c = 0; c < 3; c++) vd[c] = vd[c] / nr;
-                for (int c = 0; c < 3; c++) ag[c] = pg[c] - A[c];
-                const double sc = gdot(ag, vd);
-                for (int c = 0; c < 3; c++) {
-                    P[L.body + 6 * b + c] = a.rho * (a.adlmag[nl] * a.adlmag[nl]) * (ag[c] - sc * vd[c]);
-                    P[L.body + 6 * b + 3 + c] = vd[c];
-                }
-            }
-        }
-    }
-    __syncthreads();
-    // ---------------- stage B: interior work, per (control point, component,
-    // point) in parallel.  Each thread forms the three terms the reference
-    // subtracts from the gradient at its point (work dJ detJ, the
-    // stress-times-strain-variation term, the material-variation term); one
-    // thread per (control point, component) then subtracts them in point
-    // order, the reference's order, so the sums keep their bits.  Points are
-    // taken in chunks of a.qchunk (the term buffer).
-    double *gi_s = ge_s + (size_t)3 * nn * nadj;   // 3 nn nadj accumulators
-    double *terms = gi_s + (size_t)3 * nn * nadj;  // 3 nn qchunk 3 nadj terms
-    for (int t = tid; t < 3 * nn * nadj; t += nth) gi_s[t] = 0.0;
-    if (a.compute_int) {
-        for (int q0 = 0; q0 < a.nq; q0 += a.qchunk) {
-            const int nqc = min(a.qchunk, a.nq - q0);
-            __syncthreads();
-            for (int t = tid; t < 3 * nn * nqc; t += nth) {
-                const int task = t / nqc, ql = t - task * nqc, q = q0 + ql;
-                const int cp = task / 3, c = task - 3 * cp;
-                const double *P = pts + (size_t)q * L.size;
-                const double *dr = P + L.dR + 3 * cp;
-                const double Area = P[L.area], detJac = P[L.dj];
-                const double *AxA = P + L.AxA;
-                const double *AI = P + L.AI, *AAE = P + L.AAE;
-                const double *stress = P + L.stress, *strain = P + L.strain, *dU = P + L.dU;
-                double *tt = terms + ((size_t)task * a.qchunk + ql) * 3 * nadj;
-                double dJ = 0.0;
-                for (int i = 0; i < 3; i++) dJ = dJ + AxA[3 * i + c] * dr[i];
-                for (int k = 0; k < nadj; k++) tt[3 * k] = P[L.work + k] * dJ * detJac;
-                for (int k = 0; k < nadj; k++) {
-                    const double *d = P + L.dUA + 9 * k;
-                    double ev = 0.0;
-                    for (int ij = 0; ij < 6; ij++) {
-                        const int i = c_vi[ij], j = c_vj[ij];
-                        if (i == j) ev = ev + stress[ij] * d[3 * i + c] * dr[i];
-                        else ev = ev + stress[ij] * d[3 * i + c] * dr[j] + stress[ij] * d[3 * j + c] * dr[i];
-                    }
-                    tt[3 * k + 1] = ev * Area * detJac;
-                }
-                double dAAI[3][3], dAAE[3][3];
-                for (int j = 0; j < 3; j++)
-                    for (int i = 0; i < 3; i++) dAAI[i][j] = dr[i] * AI[3 * j + c] + AI[3 * i + c] * dr[j];
                 for (int i = 0; i < 3; i++)
-                    for (int j = 0; j < 3; j++) dAAE[i][j] = 0.0;
-                for (int j = 0; j < 3; j++)
+                    for (int c = 0; c < 3; c++) P[L.AAE + 3 * i + c] = AAE[i][c];
+                for (int ij = 0; ij < 6; ij++) {
+                    P[L.strain + ij] = strain[ij];
+                    P[L.stress + ij] = stress[ij];
+                }
+                for (int k = 0; k < nadj; k++) {
+                    double dA[3][3];
                     for (int i = 0; i < 3; i++)
-                        for (int l = 0; l < 3; l++)
-                            for (int k = 0; k < 3; k++)
-                                dAAE[i][j] = dAAE[i][j] - AAE[3 * i + k] * AAE[3 * l + j] * dAAI[k][l];
-                double vA[kGradMaxAdj];
-                for (int k = 0; k < nadj; k++) {
-                    const double *tA = P + L.tA + 6 * k;
-                    double ev = 0.0;
+                        for (int c = 0; c < 3; c++) dA[i][c] = P[L.dUA + 9 * k + 3 * i + c];
+                    double sA[6], tA[6];
                     for (int ij = 0; ij < 6; ij++) {
                         const int i = c_vi[ij], j = c_vj[ij];
-                        if (i == j) ev = ev + tA[ij] * dU[3 * i + c] * dr[i];
-                        else ev = ev + tA[ij] * dU[3 * i + c] * dr[j] + tA[ij] * dU[3 * j + c] * dr[i];
+                        if (i == j) sA[ij] = gdot(AI[i], dA[i]);
+                        else sA[ij] = gdot(AI[i], dA[j]) + gdot(AI[j], dA[i]);
                     }
-                    vA[k] = ev;
-                }
-                for (int kl = 0; kl < 6; kl++) {
-                    const int k = c_vi[kl], l = c_vj[kl];
+                    for (int ii = 0; ii < 6; ii++) {
+                        double s = 0.0;
+                        for (int jj = 0; jj < 6; jj++) s = s + H[ii][jj] * sA[jj];
+                        tA[ii] = s;
+                    }
                     for (int ij = 0; ij < 6; ij++) {
-                        const int i = c_vi[ij], j = c_vj[ij];
-                        const double dC =
-                            lambda * dAAE[i][j] * AAE[3 * k + l] + lambda * AAE[3 * i + j] * dAAE[k][l] +
-                            mu * dAAE[i][k] * AAE[3 * j + l] + mu * AAE[3 * i + k] * dAAE[j][l] +
-                            mu * dAAE[i][l] * AAE[3 * j + k] + mu * AAE[3 * i + l] * dAAE[j][k];
-                        for (int kk = 0; kk < nadj; kk++)
-                            vA[kk] = vA[kk] + dC * strain[ij] * P[L.sA + 6 * kk + kl];
+                        P[L.sA + 6 * k + ij] = sA[ij];
+                        P[L.tA + 6 * k + ij] = tA[ij];
                     }
                 }
-                for (int k = 0; k < nadj; k++) tt[3 * k + 2] = vA[k] * Area * detJac;
+                for (int k = 0; k < nadj; k++) P[L.work + k] = 0.0;
+                for (int ij = 0; ij < 6; ij++)
+                    for (int k = 0; k < nadj; k++)
+                        P[L.work + k] = P[L.work + k] + P[L.sA + 6 * k + ij] * stress[ij];
             }
-            __syncthreads();
-            for (int task = tid; task < 3 * nn; task += nth)
-                for (int k = 0; k < nadj; k++) {
-                    double g = gi_s[task * nadj + k];
-                    for (int ql = 0; ql < nqc; ql++) {
-                        const double *tt = terms + ((size_t)task * a.qchunk + ql) * 3 * nadj + 3 * k;
-                        g = g - tt[0];
-                        g = g - tt[1];
-                        g = g - tt[2];
+            if (a.compute_ext && nbody > 0) {
+                for (int k = 0; k < nadj; k++)
+                    for (int c = 0; c < 3; c++) {
+                        double s = 0.0;
+                        for (int cp = 0; cp < nn; cp++) s = s + R[cp] * uae[3 * cp + c + 3 * nn * k];
+                        P[L.vA + 3 * k + c] = s;
                     }
-                    gi_s[task * nadj + k] = g;
-                }
-        }
-    }
-    // ---------------- stage B': body-load work, one task per (control
-    // point, component), points in order
-    for (int task = tid; task < 3 * nn; task += nth) {
-        const int cp = task / 3, c = task - 3 * cp;
-        double ge[kGradMaxAdj];
-        for (int k = 0; k < kGradMaxAdj; k++) ge[k] = 0.0;
-        if (a.compute_ext && nbody > 0) {
-            for (int q = 0; q < a.nq; q++) {
-                const double *P = pts + (size_t)q * L.size;
-                const double *dr = P + L.dR + 3 * cp;
-                const double Area = P[L.area], detJac = P[L.dj];
-                const double *AxA = P + L.AxA;
+                // centrifugal loads: the reference advances its info cursor by
+                // 2*MCRD for every centrifugal load acting on the element
+                int loadcount = 0;
                 for (int b = 0; b < nbody; b++) {
-                    const double *lf = P + L.body + 6 * b, *vd = lf + 3;
                     const int nl = s_body[b];
+                    double pg[3] = {0, 0, 0}, A[3], B[3], vd[3], ag[3];
+                    for (int cp = 0; cp < nn; cp++)
+                        for (int c = 0; c < 3; c++) pg[c] = pg[c] + R[cp] * xe[3 * cp + c];
+                    for (int c = 0; c < 3; c++) A[c] = a.addinfos[loadcount + c];
+                    loadcount += 3;
+                    for (int c = 0; c < 3; c++) B[c] = a.addinfos[loadcount + c];
+                    loadcount += 3;
+                    for (int c = 0; c < 3; c++) vd[c] = B[c] - A[c];
+                    const double nr = sqrt(vd[0] * vd[0] + vd[1] * vd[1] + vd[2] * vd[2]);
+                    for (int c = 0; c < 3; c++) vd[c] = vd[c] / nr;
+                    for (int c = 0; c < 3; c++) ag[c] = pg[c] - A[c];
+                    const double sc = gdot(ag, vd);
+                    for (int c = 0; c < 3; c++) {
+                        P[L.body + 6 * b + c] = a.rho * (a.adlmag[nl] * a.adlmag[nl]) * (ag[c] - sc * vd[c]);
+                        P[L.body + 6 * b + 3 + c] = vd[c];
+                    }
+                }
+            }
+        }
+        __syncthreads();
+        // ---------------- stage B: interior work, per (control point, component,
+        // point) in parallel.  Each thread forms the three terms the reference
+        // subtracts from the gradient at its point (work dJ detJ, the
+        // stress-times-strain-variation term, the material-variation term); one
+        // thread per (control point, component) then subtracts them in point
+        // order, the reference's order, so the sums keep their bits.  Points are
+        // taken in chunks of a.qchunk (the term buffer).
+        if (a.compute_int) {
+            for (int q0 = 0; q0 < np; q0 += a.qchunk) {
+                const int nqc = min(a.qchunk, np - q0);
+                __syncthreads();
+                for (int t = tid; t < 3 * nn * nqc; t += nth) {
+                    const int task = t / nqc, ql = t - task * nqc, q = q0 + ql;
+                    const int cp = task / 3, c = task - 3 * cp;
+                    const double *P = pts + (size_t)q * L.size;
+                    const double *dr = P + L.dR + 3 * cp;
+                    const double Area = P[L.area], detJac = P[L.dj];
+                    const double *AxA = P + L.AxA;
+                    const double *AI = P + L.AI, *AAE = P + L.AAE;
+                    const double *stress = P + L.stress, *strain = P + L.strain, *dU = P + L.dU;
+                    double *tt = terms + ((size_t)task * a.qchunk + ql) * 3 * nadj;
                     double dJ = 0.0;
                     for (int i = 0; i < 3; i++) dJ = dJ + AxA[3 * i + c] * dr[i];
+                    for (int k = 0; k < nadj; k++) tt[3 * k] = P[L.work + k] * dJ * detJac;
                     for (int k = 0; k < nadj; k++) {
-                        const double sf = gdot(lf, P + L.vA + 3 * k);
-                        ge[k] = ge[k] + sf * dJ * detJac;
-                    }
-                    for (int k = 0; k < nadj; k++) {
-                        const double *ua = P + L.vA + 3 * k;
-                        double df = 0.0;
-                        for (int id = 0; id < 3; id++) {
-                            if (id == c) df = df + ua[id] * (1.0 - vd[id] * vd[c]);
-                            else df = df - ua[id] * (vd[id] * vd[c]);
+                        const double *d = P + L.dUA + 9 * k;
+                        double ev = 0.0;
+                        for (int ij = 0; ij < 6; ij++) {
+                            const int i = c_vi[ij], j = c_vj[ij];
+                            if (i == j) ev = ev + stress[ij] * d[3 * i + c] * dr[i];
+                            else ev = ev + stress[ij] * d[3 * i + c] * dr[j] + stress[ij] * d[3 * j + c] * dr[i];
                         }
-                        df = df * (a.rho * (a.adlmag[nl] * a.adlmag[nl]) * P[L.R + cp]);
-                        ge[k] = ge[k] + df * Area * detJac;
+                        tt[3 * k + 1] = ev * Area * detJac;
+                    }
+                    double dAAI[3][3], dAAE[3][3];
+                    for (int j = 0; j < 3; j++)
+                        for (int i = 0; i < 3; i++) dAAI[i][j] = dr[i] * AI[3 * j + c] + AI[3 * i + c] * dr[j];
+                    for (int i = 0; i < 3; i++)
+                        for (int j = 0; j < 3; j++) dAAE[i][j] = 0.0;
+                    for (int j = 0; j < 3; j++)
+                        for (int i = 0; i < 3; i++)
+                            for (int l = 0; l < 3; l++)
+                                for (int k = 0; k < 3; k++)
+                                    dAAE[i][j] = dAAE[i][j] - AAE[3 * i + k] * AAE[3 * l + j] * dAAI[k][l];
+                    double vA[kGradMaxAdj];
+                    for (int k = 0; k < nadj; k++) {
+                        const double *tA = P + L.tA + 6 * k;
+                        double ev = 0.0;
+                        for (int ij = 0; ij < 6; ij++) {
+                            const int i = c_vi[ij], j = c_vj[ij];
+                            if (i == j) ev = ev + tA[ij] * dU[3 * i + c] * dr[i];
+                            else ev = ev + tA[ij] * dU[3 * i + c] * dr[j] + tA[ij] * dU[3 * j + c] * dr[i];
+                        }
+                        vA[k] = ev;
+                    }
+                    for (int kl = 0; kl < 6; kl++) {
+                        const int k = c_vi[kl], l = c_vj[kl];
+                        for (int ij = 0; ij < 6; ij++) {
+                            const int i = c_vi[ij], j = c_vj[ij];
+                            const double dC =
+                                lambda * dAAE[i][j] * AAE[3 * k + l] + lambda * AAE[3 * i + j] * dAAE[k][l] +
+                                mu * dAAE[i][k] * AAE[3 * j + l] + mu * AAE[3 * i + k] * dAAE[j][l] +
+                                mu * dAAE[i][l] * AAE[3 * j + k] + mu * AAE[3 * i + l] * dAAE[j][k];
+                            for (int kk = 0; kk < nadj; kk++)
+                                vA[kk] = vA[kk] + dC * strain[ij] * P[L.sA + 6 * kk + kl];
+                        }
+                    }
+                    for (int k = 0; k < nadj; k++) tt[3 * k + 2] = vA[k] * Area * detJac;
+                }
+                __syncthreads();
+                for (int task = tid; task < 3 * nn; task += nth)
+                    for (int k = 0; k < nadj; k++) {
+                        double g = gi_s[task * nadj + k];
+                        for (int ql = 0; ql < nqc; ql++) {
+                            const double *tt = terms + ((size_t)task * a.qchunk + ql) * 3 * nadj + 3 * k;
+                            g = g - tt[0];
+                            g = g - tt[1];
+                            g = g - tt[2];
+                        }
+                        gi_s[task * nadj + k] = g;
+                    }
+            }
+        }
+        // ---------------- stage B': body-load work, one task per (control
+        // point, component), points in order
+        for (int task = tid; task < 3 * nn; task += nth) {
+            const int cp = task / 3, c = task - 3 * cp;
+            double ge[kGradMaxAdj];
+            for (int k = 0; k < kGradMaxAdj; k++) ge[k] = k < nadj ? ge_s[task * nadj + k] : 0.0;
+            if (a.compute_ext && nbody > 0) {
+                for (int q = 0; q < np; q++) {
+                    const double *P = pts + (size_t)q * L.size;
+                    const double *dr = P + L.dR + 3 * cp;
+                    const double Area = P[L.area], detJac = P[L.dj];
+                    const double *AxA = P + L.AxA;
+                    for (int b = 0; b < nbody; b++) {
+                        const double *lf = P + L.body + 6 * b, *vd = lf + 3;
+                        const int nl = s_body[b];
+                        double dJ = 0.0;
+                        for (int i = 0; i < 3; i++) dJ = dJ + AxA[3 * i + c] * dr[i];
+                        for (int k = 0; k < nadj; k++) {
+                            const double sf = gdot(lf, P + L.vA + 3 * k);
+                            ge[k] = ge[k] + sf * dJ * detJac;
+                        }
+                        for (int k = 0; k < nadj; k++) {
+                            const double *ua = P + L.vA + 3 * k;
+                            double df = 0.0;
+                            for (int id = 0; id < 3; id++) {
+                                if (id == c) df = df + ua[id] * (1.0 - vd[id] * vd[c]);
+                                else df = df - ua[id] * (vd[id] * vd[c]);
+                            }
+                            df = df * (a.rho * (a.adlmag[nl] * a.adlmag[nl]) * P[L.R + cp]);
+                            ge[k] = ge[k] + df * Area * detJac;
+                        }
                     }
                 }
             }
+            for (int k = 0; k < nadj; k++) ge_s[task * nadj + k] = ge[k];
         }
+    }   // point chunks
+    __syncthreads();
+    {
         double *oi = a.egi + (size_t)blockIdx.x * nadj * 3 * nn;
-        for (int k = 0; k < nadj; k++) {
-            oi[k + nadj * (c + 3 * cp)] = gi_s[task * nadj + k];
-            ge_s[task * nadj + k] = ge[k];
+        for (int task = tid; task < 3 * nn; task += nth) {
+            const int cp = task / 3, c = task - 3 * cp;
+            for (int k = 0; k < nadj; k++) oi[k + nadj * (c + 3 * cp)] = gi_s[task * nadj + k];
         }
     }
     // ---------------- surface loads (not in the reference)
@@ -712,8 +729,15 @@ YETI_API int yeti_grad_lin_elast_work(yeti_ctx *ctx, const yeti_u1_model *m,
         // term buffer of stage B: up to 6144 doubles (48 KB), whole chunks of points
         const int qchunk = (int)std::max<int64_t>(
             1, std::min<int64_t>(P.nq, 6144 / (9 * (int64_t)P.nn * nadj)));
-        g.qchunk = qchunk;
-        const size_t smem = sizeof(double) * grad_smem_doubles(P.nn, P.nq, (int)nadj, L, face, qchunk);
+        // point records: all the points when they fit, else the largest
+        // chunk that does (at least the term buffer's)
+        int pchunk = P.nq;
+        while (pchunk > qchunk &&
+               sizeof(double) * grad_smem_doubles(P.nn, pchunk, (int)nadj, L, face, qchunk) > (size_t)smem_optin)
+            pchunk--;
+        g.qchunk = std::min(qchunk, pchunk);
+        g.pchunk = pchunk;
+        const size_t smem = sizeof(double) * grad_smem_doubles(P.nn, pchunk, (int)nadj, L, face, g.qchunk);
         YETI_CHECK(smem <= (size_t)smem_optin, YETI_EUNSUPPORTED,
                    "shape gradient: element needs %zu bytes of shared memory", smem);
         YETI_TRY(set_smem_optin((const void *)k_u1_grad, ctx->device, smem, "shape gradient element"));
