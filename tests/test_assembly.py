@@ -313,3 +313,24 @@ def test_gpu_context_times_the_element_kernels(cuda_ok):
     sys_linmat_lindef_static(*args, ctx=ctx)
     assert ctx.kernel_ms("k_u1_stiffness") is None
     ctx.close()
+
+
+def test_u1_system_args_reproduce_the_cantilever_loads_and_clamps():
+    """With the clamp and face-load options the builder writes the loads,
+    boundary conditions and free-dof list the reference's preprocessing
+    wrote for the p=2 cantilever (U23 on the face x=10, clamped x=0)."""
+    from yeti_b200.patches import u1_system_args
+    from yeti_b200.stiffmtrx_elemstorage import SYSTEM_ARG_NAMES
+    d, args = load_fixture("cantilever_p2_16x4x4")
+    mine = u1_system_args({"p": (2, 2, 2), "nel": (16, 4, 4), "cps": np.asarray(d["COORDS3D"]),
+                           "weights": np.ones(int(d["nb_cp"]))}, E=210000.0, nu=0.3,
+                          clamp_u0=True, load_u1=(3, -1.0))
+    for name, a, b in zip(SYSTEM_ARG_NAMES, args, mine):
+        if name in ("indDLoad", "JDLType", "ADLMAG", "load_target_nbelem", "bc_values",
+                    "bc_target", "bc_target_nbelem", "ind_dof_free", "nb_dof_free", "nb_bc",
+                    "nb_load"):
+            np.testing.assert_array_equal(np.asarray(a).ravel(), np.asarray(b).ravel(), err_msg=name)
+    k0, _, _, f0 = oracle.sys_linmat_lindef_static(*args)
+    k1, _, _, f1 = oracle.sys_linmat_lindef_static(*mine)
+    np.testing.assert_array_equal(k0, k1)
+    np.testing.assert_array_equal(f0, f1)

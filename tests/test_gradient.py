@@ -128,3 +128,54 @@ def _gpu_compliance(args, X):
     from yeti_b200.gradient import _solve
     U, F = _solve(args, X)
     return 0.5 * U @ F
+
+
+# ------------------------------------------- degrees beyond 2 (synthetic)
+# (degrees, elements, load 'U2<type>' on the face u = 1 with its magnitude)
+HIGH = [(4, (2, 1, 1), (3, -1.0)), ((3, 2, 4), (2, 2, 1), (0, 1.0))]
+
+
+def _high_args(p, nel, load):
+    from yeti_b200.patches import cube_patch, u1_system_args
+    P = cube_patch(nel, p, size=(2.0, 1.0, 1.0), perturb=0.1, wrange=(0.9, 1.1), seed=9)
+    return u1_system_args(P, E=100.0, nu=0.3, clamp_u0=True, load_u1=load)
+
+
+@pytest.mark.parametrize("p,nel,load", HIGH)
+def test_oracle_gradient_high_degree_with_traction_vs_fd(p, nel, load):
+    """p=4 and mixed degrees (3,2,4), clamped face u=0, a fixed-direction
+    traction / a normal pressure on the face u=1: AN with the surface term
+    vs central FD on 8 seeded control points x 3 coordinates."""
+    from yeti_b200.stiffmtrx_elemstorage import SYSTEM_ARG_NAMES
+    args = _high_args(p, nel, load)
+    d = dict(zip(SYSTEM_ARG_NAMES, args))
+    X0 = np.asarray(args[2], dtype=float)
+    C0, U = _oracle_compliance(d, args, X0)
+    sol = U.reshape(-1, 3).T
+    gi, ge = oracle.grad_lin_elast_work(args, sol, 0.5 * sol[None], include_surface=True)
+    g = gi[0] + 2.0 * ge[0]
+    sel = np.random.default_rng(3).choice(X0.shape[1], size=8, replace=False)
+    fd = _fd(lambda X: _oracle_compliance(d, args, X)[0], X0, sel)
+    an = np.array([g[c, cp] for cp in sel for c in range(3)])
+    assert np.linalg.norm(an - fd) / np.linalg.norm(fd) < 1e-6
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("p,nel,load", HIGH)
+def test_gpu_gradient_high_degree_vs_fd_and_oracle(cuda_ok, p, nel, load):
+    from yeti_b200.gradient import compliance_and_gradient, grad_from_system_args
+    args = _high_args(p, nel, load)
+    X0 = np.asarray(args[2], dtype=float)
+    C0, g = compliance_and_gradient(args)
+    sel = np.random.default_rng(3).choice(X0.shape[1], size=8, replace=False)
+    fd = _fd(lambda X: _gpu_compliance(args, X), X0, sel)
+    an = np.array([g[c, cp] for cp in sel for c in range(3)])
+    assert np.linalg.norm(an - fd) / np.linalg.norm(fd) < 1e-6
+    # and the kernel equals the oracle bit for bit on the same state
+    rng = np.random.default_rng(4)
+    sol = rng.standard_normal((3, X0.shape[1]))
+    adj = rng.standard_normal((2, 3, X0.shape[1]))
+    gi, ge = grad_from_system_args(args, sol, adj, include_surface=True)
+    oi, oe = oracle.grad_lin_elast_work(args, sol, adj, include_surface=True)
+    np.testing.assert_array_equal(gi, oi)
+    np.testing.assert_array_equal(ge, oe)

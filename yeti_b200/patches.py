@@ -49,12 +49,18 @@ def cube_patch(nel, p, size=(1.0, 1.0, 1.0), perturb=0.0, wrange=None,
             "weights": np.ascontiguousarray(weights)}
 
 
-def u1_system_args(patch, E=1.0, nu=0.3, rho=0.0, nbint=None):
+def u1_system_args(patch, E=1.0, nu=0.3, rho=0.0, nbint=None, clamp_u0=False,
+                   load_u1=None):
     """The 38 positional arguments of ``sys_linmat_lindef_static`` (the
     order of ``IGAparametrization.get_inputs4system_elemStorage()``,
     IGA_parametrization.py:1705-1716) for a single U1 patch from
-    :func:`cube_patch`: every element active, no loads and no boundary
-    conditions (all dofs free), NBINT = (max p + 1)^3 unless given.
+    :func:`cube_patch`: every element active, NBINT = (max p + 1)^3 unless
+    given.  Without options no loads and no boundary conditions (all dofs
+    free).  ``clamp_u0``: the three displacement components of the control
+    points on the face u = 0 prescribed to zero; ``load_u1 = (type, mag)``:
+    the distributed load 'U2<type>' (face 2, the face u = 1: type 0 normal
+    pressure, 1..3 a fixed direction) of magnitude mag on the elements of
+    that face.
 
     IEN lists each element's control points in the reference's descending
     local order: local node (i, j, k) is the control point of tensor index
@@ -82,6 +88,35 @@ def u1_system_args(patch, E=1.0, nu=0.3, rho=0.0, nbint=None):
     ng = max(p) + 1
     nbint = ng ** 3 if nbint is None else int(nbint)
     ndof = 3 * nb_cp
+    if clamp_u0:
+        face_cps = (np.arange(n[1] * n[2]) * n[0] + 1).astype(np.int64)   # iu = 0
+        bc_values = np.array([[1.0, 2.0, 3.0], [0.0, 0.0, 0.0]])
+        bc_target = np.concatenate([face_cps] * 3)
+        bc_nb = np.full(3, face_cps.size, dtype=np.int64)
+        fixed = np.zeros(ndof, dtype=bool)
+        for c in range(3):
+            fixed[3 * (face_cps - 1) + c] = True
+        free = np.flatnonzero(~fixed) + 1
+        ind_dof_free = np.concatenate([free, np.flatnonzero(fixed) + 1]).astype(np.int64)
+        nb_dof_free, nb_bc = int(free.size), 3
+    else:
+        bc_values = np.zeros((2, 0))
+        bc_target = np.zeros(0, dtype=np.int64)
+        bc_nb = np.zeros(0, dtype=np.int64)
+        ind_dof_free = np.arange(1, ndof + 1, dtype=np.int64)
+        nb_dof_free, nb_bc = ndof, 0
+    if load_u1 is not None:
+        typ, mag = load_u1
+        face_el = (np.flatnonzero(eu.ravel() == nel[0] - 1) + 1).astype(np.int64)
+        loads = [face_el, np.array([20 + int(typ)], dtype=np.int64),
+                 np.array([float(mag)]), np.array([face_el.size], dtype=np.int64),
+                 np.zeros(0, dtype=np.float64), np.zeros(1, dtype=np.int64)]
+        nb_load = 1
+    else:
+        loads = [np.zeros(0, dtype=np.int64), np.zeros(0, dtype=np.int64),
+                 np.zeros(0, dtype=np.float64), np.zeros(0, dtype=np.int64),
+                 np.zeros(0, dtype=np.float64), np.zeros(0, dtype=np.int64)]
+        nb_load = 0
     return [
         np.ones(nb_elem, dtype=np.int64),                      # activeElement
         float(nb_elem * (9 * nn * (nn - 1) // 2 + 6 * nn)),    # nb_data
@@ -99,22 +134,17 @@ def u1_system_args(patch, E=1.0, nu=0.3, rho=0.0, nbint=None):
         np.array([3], dtype=np.int64),                         # n_mat_props
         np.array([rho], dtype=np.float64),                     # RHO
         np.array("/THREED"),                                   # TENSOR
-        np.zeros(0, dtype=np.int64),                           # indDLoad
-        np.zeros(0, dtype=np.int64),                           # JDLType
-        np.zeros(0, dtype=np.float64),                         # ADLMAG
-        np.zeros(0, dtype=np.int64),                           # load_target_nbelem
-        np.zeros(0, dtype=np.float64),                         # load_additionalInfos
-        np.zeros(0, dtype=np.int64),                           # nb_load_additionalInfos
-        np.zeros((2, 0), dtype=np.float64),                    # bc_values
-        np.zeros(0, dtype=np.int64),                           # bc_target
-        np.zeros(0, dtype=np.int64),                           # bc_target_nbelem
-        np.arange(1, ndof + 1, dtype=np.int64),                # ind_dof_free
-        ndof,                                                  # nb_dof_free
+        *loads,   # indDLoad, JDLType, ADLMAG, load_target_nbelem, infos, nb infos
+        bc_values,                                             # bc_values
+        bc_target,                                             # bc_target
+        bc_nb,                                                 # bc_target_nbelem
+        ind_dof_free,                                          # ind_dof_free
+        nb_dof_free,                                           # nb_dof_free
         3,                                                     # MCRD
         np.array([nbint], dtype=np.int64),                     # NBINT
         np.array([nn], dtype=np.int64),                        # NNODE
         np.zeros((1, nb_cp), dtype=np.float64),                # nodal_dist
-        0, 0, 1, nb_elem, nb_cp, ndof,   # nb_bc, nb_load, nb_patch, nb_elem, nb_cp, nb_dof_tot
+        nb_bc, nb_load, 1, nb_elem, nb_cp, ndof,   # nb_bc, nb_load, nb_patch, nb_elem, nb_cp, nb_dof_tot
     ]
 
 
