@@ -97,7 +97,8 @@ def u1_system_args(patch, E=1.0, nu=0.3, rho=0.0, nbint=None, clamp_u0=False,
         for c in range(3):
             fixed[3 * (face_cps - 1) + c] = True
         free = np.flatnonzero(~fixed) + 1
-        ind_dof_free = np.concatenate([free, np.flatnonzero(fixed) + 1]).astype(np.int64)
+        ind_dof_free = np.zeros(ndof, dtype=np.int64)   # free dofs first, zeros after
+        ind_dof_free[:free.size] = free
         nb_dof_free, nb_bc = int(free.size), 3
     else:
         bc_values = np.zeros((2, 0))
