@@ -33,11 +33,12 @@
 // i3 <= j3 are needed, the slots hold the upper triangle.
 //
 // One CTA per element.  Shared memory holds the point coefficients (13 per
-// point), T1 = G_rs per class pair and (q1, q2), T2 per u-kind pair, i2, j2
-// and q1, and the contracted G_rs of a chunk of j2 values; every node pair's
-// nine (diagonal pair: six) slot values are formed and written together by
-// one thread, consecutive threads taking consecutive row nodes, whose slots
-// are contiguous.
+// point), T1 = G_rs per class pair and (q1, q2), and T2 per u-kind pair, i2,
+// j2 and q1.  The u contraction runs in lane groups of three (one r each,
+// the three s in registers); the group's first lane gathers the nine G_rs of
+// a node pair with warp shuffles and writes the pair's nine (diagonal pair:
+// six) slot values, consecutive groups taking consecutive row nodes, whose
+// slots are contiguous.
 #include "nurbs.cuh"
 #include "u1_model.cuh"
 
@@ -49,7 +50,7 @@ constexpr int kSfMaxG = 8;   // Gauss points per direction (template instances)
 struct SfArgs {
     int n[3];        // functions per direction (p+1)
     int p[3];
-    int nn, j2c;     // nodes; j2 values per output chunk
+    int nn;          // nodes
     const double *U[3];
     const double *gauss;   // 4 * g^3: weight, t1, t2, t3 (t3 fastest)
     const double *coords;
@@ -64,11 +65,10 @@ struct SfArgs {
 
 // Shared-memory doubles of one CTA.
 // The control-point coordinates (3 nn) are needed only by the per-point
-// pass and share their space with T1/T2/OB.
-size_t sf_smem_doubles(const int n[3], int g, int j2c) {
+// pass and share their space with T1/T2.
+size_t sf_smem_doubles(const int n[3], int g) {
     const size_t nn = (size_t)n[0] * n[1] * n[2], nq = (size_t)g * g * g;
-    const size_t work = 81 * (size_t)g * g + 36 * (size_t)n[1] * n[1] * g +
-                        9 * (size_t)n[0] * n[1] * n[0] * j2c;
+    const size_t work = 81 * (size_t)g * g + 36 * (size_t)n[1] * n[1] * g;
     return nn + (nn + 1) / 2 + 2 * (size_t)g * (n[0] + n[1] + n[2]) + 13 * nq +
            (work > 3 * nn ? work : 3 * nn);
 }
@@ -84,7 +84,7 @@ template <int G>
 __global__ void __launch_bounds__(kSfThreads, G <= 4 ? 3 : 2) k_u1_stiffness_sf(SfArgs a) {
     extern __shared__ double smem[];
     constexpr int g = G, gg = G * G, nq = G * G * G;
-    const int n1 = a.n[0], n2 = a.n[1], n3 = a.n[2], nn = a.nn, j2c = a.j2c;
+    const int n1 = a.n[0], n2 = a.n[1], n3 = a.n[2], nn = a.nn;
     const int n12 = n1 * n2;
     double *we = smem;                        // nn
     int *sien = reinterpret_cast<int *>(we + nn);   // nn ints
@@ -93,7 +93,6 @@ __global__ void __launch_bounds__(kSfThreads, G <= 4 ? 3 : 2) k_u1_stiffness_sf(
     double *cq = A3 + 2 * n3 * g;             // 13 nq: c[kind][r], dv
     double *T1 = cq + 13 * nq;                // [rs][ck ce][q1 q2]
     double *T2 = T1 + 81 * gg;                // [rs][al be][i2][j2][q1]
-    double *OB = T2 + 36 * n2 * n2 * g;       // [rs][a12][b12 of the chunk]
     double *xe = T1;                          // 3 nn, per-point pass only
     __shared__ double su1[3], su2[3];
     __shared__ int sni[3];
@@ -179,7 +178,7 @@ __global__ void __launch_bounds__(kSfThreads, G <= 4 ? 3 : 2) k_u1_stiffness_sf(
         }
         c[12] = a.gauss[4 * q] * fabs(det * hs);
     }
-    const int64_t base = a.slot[e];
+    const int64_t base_slot = a.slot[e];
     const double lam = a.lam, mu = a.mu;
     for (int i3 = 0; i3 < n3; i3++)
         for (int j3 = i3; j3 < n3; j3++) {
@@ -262,19 +261,22 @@ __global__ void __launch_bounds__(kSfThreads, G <= 4 ? 3 : 2) k_u1_stiffness_sf(
                     t2[3 * sk + j2 * g] = s11;
                 }
             }
-            for (int j2s = 0; j2s < n2; j2s += j2c) {
-                const int j2n = min(j2c, n2 - j2s), nb = n1 * j2n;
-                __syncthreads();
-                // ---- step 3 (u): OB[rs][a12][b12] for j2 in the chunk; one
-                // task per (r, a12, j2) for the three s, so each A1 value read
-                // serves six multiply-adds
-                for (int t = tid; t < 3 * n12 * j2n; t += kSfThreads) {
-                    int r = t;
-                    const int j2l = r % j2n; r /= j2n;
-                    const int a12 = r % n12;
-                    const int rr = r / n12;
-                    const int i1 = a12 % n1, i2 = a12 / n1, j2 = j2s + j2l;
-                    const size_t sk = (size_t)n2 * n2 * g;
+            __syncthreads();
+            // ---- steps 3 (u) and 4 (the COO slot): lanes in groups of three
+            // (r = 0, 1, 2) per (a12, j2), ten groups per warp; each lane
+            // contracts the three G_rs of its r along u, the group's first
+            // lane gathers the other six through warp shuffles and writes the
+            // pair's slot (consecutive groups take consecutive row nodes,
+            // whose slots are contiguous)
+            {
+                const int warp = tid >> 5, lane = tid & 31, gl = lane / 3, rr = lane - 3 * gl;
+                const int ngroups = n12 * n2;
+                const size_t sk = (size_t)n2 * n2 * g;
+                for (int g0 = 10 * warp; g0 < ngroups; g0 += 10 * (kSfThreads / 32)) {
+                    const int grp = g0 + gl;
+                    const bool act = gl < 10 && grp < ngroups;
+                    const int a12 = act ? grp % n12 : 0, j2 = act ? grp / n12 : 0;
+                    const int i1 = a12 % n1, i2 = a12 / n1;
                     double Uu[3][2][G];   // Uu[s][be][q1] = sum_al A1[al][i1][q1] T2[3rr+s][al be]
 #pragma unroll
                     for (int q1 = 0; q1 < G; q1++) {
@@ -286,62 +288,57 @@ __global__ void __launch_bounds__(kSfThreads, G <= 4 ? 3 : 2) k_u1_stiffness_sf(
                             Uu[ss][1][q1] = a0 * t2[sk] + a1 * t2[3 * sk];
                         }
                     }
-                    double *ob = OB + ((size_t)(3 * rr) * n12 + a12) * nb + j2l * n1;
-                    const size_t so = (size_t)n12 * nb;   // stride of rs in OB
+                    const int ia = a12 + n12 * i3;
+                    const int base = 3 * gl;
                     for (int j1 = 0; j1 < n1; j1++) {
-                        double o0 = 0.0, o1 = 0.0, o2 = 0.0;
+                        double o[3] = {0.0, 0.0, 0.0};
 #pragma unroll
                         for (int q1 = 0; q1 < G; q1++) {
                             const double c0 = A1[j1 * g + q1], c1 = A1[(n1 + j1) * g + q1];
-                            o0 += c0 * Uu[0][0][q1] + c1 * Uu[0][1][q1];
-                            o1 += c0 * Uu[1][0][q1] + c1 * Uu[1][1][q1];
-                            o2 += c0 * Uu[2][0][q1] + c1 * Uu[2][1][q1];
+#pragma unroll
+                            for (int ss = 0; ss < 3; ss++) o[ss] += c0 * Uu[ss][0][q1] + c1 * Uu[ss][1][q1];
                         }
-                        ob[j1] = o0;
-                        ob[so + j1] = o1;
-                        ob[2 * so + j1] = o2;
-                    }
-                }
-                __syncthreads();
-                // ---- the pairs' 3x3 blocks into their COO slots; consecutive
-                // threads take consecutive row nodes (contiguous slots)
-                for (int t = tid; t < n12 * nb; t += kSfThreads) {
-                    const int a12 = t % n12, bl = t / n12;
-                    const int ia = a12 + n12 * i3;
-                    const int ib = bl % n1 + n1 * (j2s + bl / n1) + n12 * j3;
-                    if (ia > ib) continue;
-                    const double wab = we[ia] * we[ib];
-                    double Gm[9];
+                        double Gm[9];
 #pragma unroll
-                    for (int rs = 0; rs < 9; rs++) Gm[rs] = OB[((size_t)rs * n12 + a12) * nb + bl] * wab;
-                    const double tr = mu * (Gm[0] + Gm[4] + Gm[8]);
-                    const int dofa = 3 * sien[ia], dofb = 3 * sien[ib];
-                    if (ia < ib) {
-                        const int64_t s0 = base + 9LL * ib * (ib - 1) / 2 + 6LL * ib + 9LL * ia;
+                        for (int ss = 0; ss < 3; ss++) {
+                            Gm[ss] = o[ss];
+                            Gm[3 + ss] = __shfl_sync(0xffffffffu, o[ss], (base + 1) & 31);
+                            Gm[6 + ss] = __shfl_sync(0xffffffffu, o[ss], (base + 2) & 31);
+                        }
+                        const int ib = j1 + n1 * j2 + n12 * j3;
+                        if (!act || rr != 0 || ia > ib) continue;
+                        const double wab = we[ia] * we[ib];
 #pragma unroll
-                        for (int ll = 0; ll < 3; ll++)
+                        for (int rs = 0; rs < 9; rs++) Gm[rs] *= wab;
+                        const double tr = mu * (Gm[0] + Gm[4] + Gm[8]);
+                        const int dofa = 3 * sien[ia], dofb = 3 * sien[ib];
+                        if (ia < ib) {
+                            const int64_t s0 = base_slot + 9LL * ib * (ib - 1) / 2 + 6LL * ib + 9LL * ia;
 #pragma unroll
-                            for (int kk = 0; kk < 3; kk++) {
-                                double v = lam * Gm[3 * kk + ll] + mu * Gm[3 * ll + kk];
-                                if (kk == ll) v += tr;
-                                const int64_t o = s0 + 3 * ll + kk;
-                                a.kdata[o] = v;
-                                a.krow[o] = dofa + kk;
-                                a.kcol[o] = dofb + ll;
-                            }
-                    } else {
-                        const int64_t s0 = base + 9LL * ia * (ia - 1) / 2 + 15LL * ia;
+                            for (int ll = 0; ll < 3; ll++)
 #pragma unroll
-                        for (int ll = 0; ll < 3; ll++)
+                                for (int kk = 0; kk < 3; kk++) {
+                                    double v = lam * Gm[3 * kk + ll] + mu * Gm[3 * ll + kk];
+                                    if (kk == ll) v += tr;
+                                    const int64_t oo = s0 + 3 * ll + kk;
+                                    a.kdata[oo] = v;
+                                    a.krow[oo] = dofa + kk;
+                                    a.kcol[oo] = dofb + ll;
+                                }
+                        } else {
+                            const int64_t s0 = base_slot + 9LL * ia * (ia - 1) / 2 + 15LL * ia;
 #pragma unroll
-                            for (int kk = 0; kk <= ll; kk++) {
-                                double v = lam * Gm[3 * kk + ll] + mu * Gm[3 * ll + kk];
-                                if (kk == ll) v = (v + tr) * 0.5;
-                                const int64_t o = s0 + ll * (ll + 1) / 2 + kk;
-                                a.kdata[o] = v;
-                                a.krow[o] = dofa + kk;
-                                a.kcol[o] = dofa + ll;
-                            }
+                            for (int ll = 0; ll < 3; ll++)
+#pragma unroll
+                                for (int kk = 0; kk <= ll; kk++) {
+                                    double v = lam * Gm[3 * kk + ll] + mu * Gm[3 * ll + kk];
+                                    if (kk == ll) v = (v + tr) * 0.5;
+                                    const int64_t oo = s0 + ll * (ll + 1) / 2 + kk;
+                                    a.kdata[oo] = v;
+                                    a.krow[oo] = dofa + kk;
+                                    a.kcol[oo] = dofa + ll;
+                                }
+                        }
                     }
                 }
             }
@@ -360,21 +357,11 @@ int launch_u1_stiffness_sf(yeti_ctx *ctx, const U1Patch &P, const double *coords
         a.n[d] = P.p[d] + 1;
     }
     a.nn = P.nn;
-    // the largest chunk of j2 whose buffers leave room for two CTAs per SM
-    // (a single j2 when none does)
-    int per_sm = 0;
-    YETI_CUDA(cudaDeviceGetAttribute(&per_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, ctx->device));
-    const size_t two = (size_t)per_sm / 2 > 2048 ? (size_t)per_sm / 2 - 2048 : 0;
-    int j2c = a.n[1];
-    while (j2c > 1 && sf_smem_doubles(a.n, P.ng, j2c) * sizeof(double) > two) j2c--;
-    const int nchunk = (a.n[1] + j2c - 1) / j2c;
-    j2c = (a.n[1] + nchunk - 1) / nchunk;   // chunks of even size
-    const size_t smem = sf_smem_doubles(a.n, P.ng, j2c) * sizeof(double);
+    const size_t smem = sf_smem_doubles(a.n, P.ng) * sizeof(double);
     YETI_CHECK(smem <= smem_cap, YETI_EUNSUPPORTED,
                "sum-factorised stiffness: an element of degrees (%d,%d,%d) "
                "with %d Gauss points per direction does not fit shared memory",
                P.p[0], P.p[1], P.p[2], P.ng);
-    a.j2c = j2c;
     a.U[0] = P.knots.as<double>();
     a.U[1] = a.U[0] + P.nkv[0];
     a.U[2] = a.U[1] + P.nkv[1];
