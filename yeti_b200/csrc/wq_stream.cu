@@ -21,7 +21,7 @@
 //   C  forward u + pointwise, one lane per point: F[l][j] = d u_j / d xi_l,
 //                  then h[i][k][l] = sum_j S[(i,k),(j,l)] F[l][j] with the
 //                  45 streamed coefficients of the point (the HBM stream)
-//   G  backward u: one lane per (row, channel (i,k,l)) walks the row,
+//   G  backward u: one lane per channel (i,k,l) walks the warp's two rows,
 //                  weights W^{[k==u][l==u]}
 //   -- barrier --
 //   D  backward v: one thread per (i, k, fu) walks the column over the tile's
@@ -65,31 +65,29 @@ constexpr int kHS = 2 * kTQ + 1; // channel stride of a warp's h block
 constexpr int cmax(int a, int b) { return a > b ? a : b; }
 constexpr int round4(int a) { return (a + 3) / 4 * 4; }
 
-// Channel stride of a warp's G block: at least two rows of NFM, and chosen
-// so that stage D's threads ((i,k)-major, fu fastest) of consecutive (i,k)
-// fall on disjoint banks.
-constexpr int gstride(int nfm) {
-    int g = 2 * nfm;
-    while (!((3 * g) % 32 >= nfm && (3 * g) % 32 <= 32 - nfm)) g++;
-    return g;
-}
-
 template <int P>
 struct Dims {
     static constexpr int PB = P + 1;
     static constexpr int PBP = round4(PB);     // padded band row
+    static constexpr int TS = 6 * PBP + 4;     // table row of one point: six bands, padded so
+                                               // that the 16-byte loads of consecutive points
+                                               // fall on different banks
     static constexpr int NFM = kNE + P;        // max functions of a tile along u
     static constexpr int NFV = kNEV + P;       // ... along v
-    static constexpr int GS = gstride(NFM);
     static constexpr int Y = round4(2 * 3 * NFV * NFM);
     static constexpr int ZHP = round4(cmax(9 * 2 * NFM, 27 * kHS));   // Z, then h
-    static constexpr int GP = round4(27 * GS);                        // G
+    // a warp's G block: [row][function][channel], the 27 channels
+    // consecutive (stage G's lanes are channels; stage D's threads, with
+    // the 9 (i,k) fastest, read 3 (i,k) + l at a function stride of 27:
+    // banks 3 * tid, all distinct)
+    static constexpr int RS = 27 * NFM;                               // row of G
+    static constexpr int GP = round4(2 * RS);                         // G
     static constexpr int K = 9 * NFV * NFM * 2;                       // aliases the Z/h parts
-    static constexpr int TAB = kTQ * 6 * PBP;                         // u (v: kTV rows)
+    static constexpr int TAB = kTQ * TS;                              // u (v: kTV rows)
     static constexpr int OFF_ZH = Y;
     static constexpr int OFF_G = OFF_ZH + kWarps * ZHP;
     static constexpr int OFF_TAB = OFF_G + kWarps * GP;
-    static constexpr int TOTAL = OFF_TAB + TAB + kTV * 6 * PBP;
+    static constexpr int TOTAL = OFF_TAB + TAB + kTV * TS;
     static constexpr int NCOL = 3 * NFV * NFM;
     static constexpr int CPT = (NCOL + kThreads - 1) / kThreads;
     static constexpr int CB = kTQ * kTV * 45;   // one plane's coefficients (staged kernels)
@@ -214,16 +212,20 @@ __host__ __device__ constexpr int pat_q0(int P, int pat, int e) {
     return pat == 2 ? (e == 0 ? 0 : P + 1 + 2 * (e - 1)) : 2 * e;
 }
 
-// Backward u of one channel of one row: g[f] = sum_q W_kind(q, f - rel(q)) h[q],
-// walked element by element with the accumulators of the element's p+1
-// functions named at compile time.
+// Backward u of one channel of a warp's two rows: g[f] = sum_q W_kind(q,
+// f - rel(q)) h[q], walked element by element with the accumulators of the
+// element's p+1 functions named at compile time; one band row serves both
+// rows.  h: row 0 at h[q], row 1 at h[kTQ + q]; g: function f of row r at
+// g[r * RS + 27 f] (the G block's channel stride is 1).
 template <class T, int P, int PAT>
 __device__ __forceinline__ void walk_u(const T *h, T *g, const T *tab, int kind, int ne_rt) {
-    constexpr int PBP = round4(P + 1), NEM = pat_nemax(P, PAT), NF = NEM + P;
+    using D = Dims<P>;
+    constexpr int TS = D::TS, PBP = D::PBP, RS = D::RS;
+    constexpr int NEM = pat_nemax(P, PAT), NF = NEM + P;
     const int ne = PAT == 1 ? NEM : ne_rt;
-    T a[NF];
+    T a0[NF], a1[NF];
 #pragma unroll
-    for (int f = 0; f < NF; f++) a[f] = T(0);
+    for (int f = 0; f < NF; f++) a0[f] = a1[f] = T(0);
 #pragma unroll
     for (int e = 0; e < NEM; e++) {
         if (e < ne) {
@@ -234,57 +236,76 @@ __device__ __forceinline__ void walk_u(const T *h, T *g, const T *tab, int kind,
                 if (pt < np) {
                     const int q = q0 + pt;
                     T w[P + 1];
-                    load_band<P>(tab + (q * 6 + kind) * PBP, w);
-                    const T x = h[q];
+                    load_band<P>(tab + q * TS + kind * PBP, w);
+                    const T x0 = h[q], x1 = h[kTQ + q];
 #pragma unroll
-                    for (int m = 0; m <= P; m++) a[e + m] += w[m] * x;
+                    for (int m = 0; m <= P; m++) {
+                        a0[e + m] += w[m] * x0;
+                        a1[e + m] += w[m] * x1;
+                    }
                 }
             }
-            g[e] = a[e];
+            g[27 * e] = a0[e];
+            g[RS + 27 * e] = a1[e];
         }
     }
 #pragma unroll
     for (int f = 1; f < NF; f++)
-        if (f >= ne && f < ne + P) g[f] = a[f];
+        if (f >= ne && f < ne + P) {
+            g[27 * f] = a0[f];
+            g[RS + 27 * f] = a1[f];
+        }
 }
 
 template <class T, int P>
 __device__ __forceinline__ void walk_u_generic(const T *h, T *g, const T *tab, int kind,
                                                const int *rel, int nq) {
-    constexpr int PBP = round4(P + 1);
-    T a[P + 1];
+    using D = Dims<P>;
+    constexpr int TS = D::TS, PBP = D::PBP, RS = D::RS;
+    T a0[P + 1], a1[P + 1];
 #pragma unroll
-    for (int m = 0; m <= P; m++) a[m] = T(0);
+    for (int m = 0; m <= P; m++) a0[m] = a1[m] = T(0);
     int cur = 0;
     for (int q = 0; q < nq; q++) {
         const int r = rel[q];
         if (r != cur) {
-            g[cur] = a[0];
+            g[27 * cur] = a0[0];
+            g[RS + 27 * cur] = a1[0];
 #pragma unroll
-            for (int m = 0; m < P; m++) a[m] = a[m + 1];
-            a[P] = T(0);
+            for (int m = 0; m < P; m++) {
+                a0[m] = a0[m + 1];
+                a1[m] = a1[m + 1];
+            }
+            a0[P] = a1[P] = T(0);
             cur = r;
         }
         T w[P + 1];
-        load_band<P>(tab + (q * 6 + kind) * PBP, w);
-        const T x = h[q];
+        load_band<P>(tab + q * TS + kind * PBP, w);
+        const T x0 = h[q], x1 = h[kTQ + q];
 #pragma unroll
-        for (int m = 0; m <= P; m++) a[m] += w[m] * x;
+        for (int m = 0; m <= P; m++) {
+            a0[m] += w[m] * x0;
+            a1[m] += w[m] * x1;
+        }
     }
 #pragma unroll
-    for (int m = 0; m <= P; m++) g[cur + m] = a[m];
+    for (int m = 0; m <= P; m++) {
+        g[27 * (cur + m)] = a0[m];
+        g[RS + 27 * (cur + m)] = a1[m];
+    }
 }
 
 // Backward v of the three channels (i,k,l=0..2) of one fu column, merged on
 // the w key: kp[fv] = (sum wa g0 + wb g1, sum wa g2), wa at table row ka
 // (trial l != v), wb at ka+1 (trial l == v).  G of row qv of the tile lives
-// in the block of warp qv/2: gb + (qv/2)*GP + (qv%2)*NFM + l*GS.
+// in the block of warp qv/2: gb + (qv/2)*GP + (qv%2)*RS + l; the pairs of K
+// are NFM * 18 apart from one fv to the next.
 template <class T, int P, int PAT>
 __device__ __forceinline__ void walk_v(const T *gb, T *kp, const T *tab, int ka, int ne_rt) {
     using D = Dims<P>;
-    constexpr int PBP = D::PBP, NEM = pat_nemax(P, PAT, kTV), NF = NEM + P, NFM = D::NFM;
+    constexpr int PBP = D::PBP, TS = D::TS, NEM = pat_nemax(P, PAT, kTV), NF = NEM + P;
+    constexpr int KS = D::NFM * 18, RS = D::RS, GP = D::GP;
     const int ne = PAT == 1 ? NEM : ne_rt;
-    constexpr int GS = D::GS, GP = D::GP;
     T A0[NF], A1[NF];
 #pragma unroll
     for (int f = 0; f < NF; f++) A0[f] = A1[f] = T(0);
@@ -298,10 +319,10 @@ __device__ __forceinline__ void walk_v(const T *gb, T *kp, const T *tab, int ka,
                 if (pt < np) {
                     const int q = q0 + pt;
                     T wa[P + 1], wb[P + 1];
-                    load_band<P>(tab + (q * 6 + ka) * PBP, wa);
-                    load_band<P>(tab + (q * 6 + ka + 1) * PBP, wb);
-                    const T *g = gb + (q >> 1) * GP + (q & 1) * NFM;
-                    const T x0 = g[0], x1 = g[GS], x2 = g[2 * GS];
+                    load_band<P>(tab + q * TS + ka * PBP, wa);
+                    load_band<P>(tab + q * TS + (ka + 1) * PBP, wb);
+                    const T *g = gb + (q >> 1) * GP + (q & 1) * RS;
+                    const T x0 = g[0], x1 = g[1], x2 = g[2];
 #pragma unroll
                     for (int m = 0; m <= P; m++) {
                         A0[e + m] += wa[m] * x0 + wb[m] * x1;
@@ -309,19 +330,19 @@ __device__ __forceinline__ void walk_v(const T *gb, T *kp, const T *tab, int ka,
                     }
                 }
             }
-            store_pair(kp + e * (2 * NFM), A0[e], A1[e]);
+            store_pair(kp + e * KS, A0[e], A1[e]);
         }
     }
 #pragma unroll
     for (int f = 1; f < NF; f++)
-        if (f >= ne && f < ne + P) store_pair(kp + f * (2 * NFM), A0[f], A1[f]);
+        if (f >= ne && f < ne + P) store_pair(kp + f * KS, A0[f], A1[f]);
 }
 
 template <class T, int P>
 __device__ __forceinline__ void walk_v_generic(const T *gb, T *kp, const T *tab, int ka,
                                                const int *rel, int nq) {
     using D = Dims<P>;
-    constexpr int PBP = D::PBP, NFM = D::NFM, GS = D::GS, GP = D::GP;
+    constexpr int PBP = D::PBP, TS = D::TS, KS = D::NFM * 18, RS = D::RS, GP = D::GP;
     T A0[P + 1], A1[P + 1];
 #pragma unroll
     for (int m = 0; m <= P; m++) A0[m] = A1[m] = T(0);
@@ -329,7 +350,7 @@ __device__ __forceinline__ void walk_v_generic(const T *gb, T *kp, const T *tab,
     for (int q = 0; q < nq; q++) {
         const int r = rel[q];
         if (r != cur) {
-            store_pair(kp + cur * (2 * NFM), A0[0], A1[0]);
+            store_pair(kp + cur * KS, A0[0], A1[0]);
 #pragma unroll
             for (int m = 0; m < P; m++) {
                 A0[m] = A0[m + 1];
@@ -339,10 +360,10 @@ __device__ __forceinline__ void walk_v_generic(const T *gb, T *kp, const T *tab,
             cur = r;
         }
         T wa[P + 1], wb[P + 1];
-        load_band<P>(tab + (q * 6 + ka) * PBP, wa);
-        load_band<P>(tab + (q * 6 + ka + 1) * PBP, wb);
-        const T *g = gb + (q >> 1) * GP + (q & 1) * NFM;
-        const T x0 = g[0], x1 = g[GS], x2 = g[2 * GS];
+        load_band<P>(tab + q * TS + ka * PBP, wa);
+        load_band<P>(tab + q * TS + (ka + 1) * PBP, wb);
+        const T *g = gb + (q >> 1) * GP + (q & 1) * RS;
+        const T x0 = g[0], x1 = g[1], x2 = g[2];
 #pragma unroll
         for (int m = 0; m <= P; m++) {
             A0[m] += wa[m] * x0 + wb[m] * x1;
@@ -350,7 +371,7 @@ __device__ __forceinline__ void walk_v_generic(const T *gb, T *kp, const T *tab,
         }
     }
 #pragma unroll
-    for (int m = 0; m <= P; m++) store_pair(kp + (cur + m) * (2 * NFM), A0[m], A1[m]);
+    for (int m = 0; m <= P; m++) store_pair(kp + (cur + m) * KS, A0[m], A1[m]);
 }
 
 __device__ __forceinline__ int relu_last_plus1(const int *elem, int q0, int nq, int f0) {
@@ -388,7 +409,7 @@ template <class T, int P>
 __global__ void __launch_bounds__(kThreads, kCtasPerSm) k_wq_apply_stream(StreamArgs<T> a) {
     using D = Dims<P>;
     constexpr int PB = D::PB, PBP = D::PBP, NFM = D::NFM, CPT = D::CPT;
-    constexpr int GS = D::GS, GP = D::GP, ZHP = D::ZHP;
+    constexpr int TS = D::TS, GP = D::GP, ZHP = D::ZHP;
     // FP32: each plane's coefficient block is brought into shared memory by a
     // bulk copy issued one plane ahead; FP64 reads it from HBM directly
     constexpr bool kStaged = sizeof(T) == 4;
@@ -433,8 +454,8 @@ __global__ void __launch_bounds__(kThreads, kCtasPerSm) k_wq_apply_stream(Stream
         __syncthreads();   // the previous segment is done with the tables
         for (int i = tid; i < kTQ * 6 * PBP; i += kThreads) {
             const int q = i / (6 * PBP), r = i - q * (6 * PBP);
-            tabu[i] = q < nqu ? a.band[0][(size_t)(qu0 + q) * 6 * PBP + r] : T(0);
-            if (q < kTV) tabv[i] = q < nqv ? a.band[1][(size_t)(qv0 + q) * 6 * PBP + r] : T(0);
+            tabu[q * TS + r] = q < nqu ? a.band[0][(size_t)(qu0 + q) * 6 * PBP + r] : T(0);
+            if (q < kTV) tabv[q * TS + r] = q < nqv ? a.band[1][(size_t)(qv0 + q) * 6 * PBP + r] : T(0);
         }
         if (tid < kTQ) relu[tid] = tid < nqu ? a.elem[0][qu0 + tid] - fu0 : 0;
         if (tid < kTV) relv[tid] = tid < nqv ? a.elem[1][qv0 + tid] - fv0 : 0;
@@ -442,9 +463,9 @@ __global__ void __launch_bounds__(kThreads, kCtasPerSm) k_wq_apply_stream(Stream
         if constexpr (kStaged) {
             if (tid == 0) bulk_load(cbuf, coef_t + (int64_t)a.wq0[sg.y] * pstride, cbytes, bar);
         }
-        // stage D thread: (ik, fu)
+        // stage D thread: (ik, fu), the nine ik fastest
         const bool d_act = tid < 9 * nfu;
-        const int d_ik = d_act ? tid / nfu : 0, d_fu = d_act ? tid - d_ik * nfu : 0;
+        const int d_fu = d_act ? tid / 9 : 0, d_ik = d_act ? tid - 9 * d_fu : 0;
 
         // columns (c, fv, fu) of this thread: stages A and E
         const int ncol = 3 * nfv * nfu;
@@ -552,8 +573,8 @@ __global__ void __launch_bounds__(kThreads, kCtasPerSm) k_wq_apply_stream(Stream
                             const int qv = 2 * warp + row;
                             const int rv = regv ? (qv >> 1) : relv[qv];
                             T b0[PB], b1[PB];
-                            load_band<P>(tabv + (qv * 6 + 0) * PBP, b0);
-                            load_band<P>(tabv + (qv * 6 + 1) * PBP, b1);
+                            load_band<P>(tabv + qv * TS, b0);
+                            load_band<P>(tabv + qv * TS + PBP, b1);
 #pragma unroll
                             for (int c = 0; c < 3; c++) {
                                 const T *y0 = RY + (c * D::NFV + rv) * NFM + fu;
@@ -581,8 +602,8 @@ __global__ void __launch_bounds__(kThreads, kCtasPerSm) k_wq_apply_stream(Stream
                         if (act) {
                             const int ru = regu ? (qu >> 1) : relu[qu];
                             T b0[PB], b1[PB];
-                            load_band<P>(tabu + (qu * 6 + 0) * PBP, b0);
-                            load_band<P>(tabu + (qu * 6 + 1) * PBP, b1);
+                            load_band<P>(tabu + qu * TS, b0);
+                            load_band<P>(tabu + qu * TS + PBP, b1);
 #pragma unroll
                             for (int l = 0; l < 3; l++)
 #pragma unroll
@@ -642,21 +663,20 @@ __global__ void __launch_bounds__(kThreads, kCtasPerSm) k_wq_apply_stream(Stream
                         }
                     }
                     __syncwarp();
-                    // ---- G: backward u, lane (row, channel), 54 walks per warp
-                    for (int wk = lane; wk < 54; wk += 32) {
-                        const int row = wk & 1, ch = wk >> 1;
-                        if (row < nrow) {
-                            const int k = (ch / 3) % 3, l = ch % 3;
-                            const int kind = 2 + 2 * (k == 0) + (l == 0);   // W_{[k==u][l==u]}
-                            const T *hr = zh + ch * kHS + row * kTQ;
-                            T *gr = gp + ch * GS + row * NFM;
-                            switch (patu) {
-                                case 1: walk_u<T, P, 1>(hr, gr, tabu, kind, neu); break;
-                                case 4: walk_u<T, P, 4>(hr, gr, tabu, kind, neu); break;
-                                case 2: walk_u<T, P, 2>(hr, gr, tabu, kind, neu); break;
-                                case 3: walk_u<T, P, 3>(hr, gr, tabu, kind, neu); break;
-                                default: walk_u_generic<T, P>(hr, gr, tabu, kind, relu, nqu);
-                            }
+                    // ---- G: backward u, lane = channel (i,k,l), both rows of the warp
+                    // (with one row the second walks stale values that nothing reads)
+                    if (lane < 27) {
+                        const int ch = lane;
+                        const int k = (ch / 3) % 3, l = ch % 3;
+                        const int kind = 2 + 2 * (k == 0) + (l == 0);   // W_{[k==u][l==u]}
+                        const T *hr = zh + ch * kHS;
+                        T *gr = gp + ch;
+                        switch (patu) {
+                            case 1: walk_u<T, P, 1>(hr, gr, tabu, kind, neu); break;
+                            case 4: walk_u<T, P, 4>(hr, gr, tabu, kind, neu); break;
+                            case 2: walk_u<T, P, 2>(hr, gr, tabu, kind, neu); break;
+                            case 3: walk_u<T, P, 3>(hr, gr, tabu, kind, neu); break;
+                            default: walk_u_generic<T, P>(hr, gr, tabu, kind, relu, nqu);
                         }
                     }
                 }
@@ -670,8 +690,8 @@ __global__ void __launch_bounds__(kThreads, kCtasPerSm) k_wq_apply_stream(Stream
                 if (d_act) {
                     const int ik = d_ik, fu = d_fu;
                     const int ka = 2 + 2 * (ik % 3 == 1);   // W_{[k==v], 0}
-                    const T *gb = RG + (ik * 3) * GS + fu;
-                    T *kp = RZH + (ik * D::NFV * NFM + fu) * 2;
+                    const T *gb = RG + fu * 27 + ik * 3;
+                    T *kp = RZH + (fu * 9 + ik) * 2;
                     switch (patv) {
                         case 1: walk_v<T, P, 1>(gb, kp, tabv, ka, nev); break;
                         case 4: walk_v<T, P, 4>(gb, kp, tabv, ka, nev); break;
@@ -692,11 +712,11 @@ __global__ void __launch_bounds__(kThreads, kCtasPerSm) k_wq_apply_stream(Stream
                     for (int cc = 0; cc < CPT; cc++) {
                         if (!(cinfo[cc] & 4)) continue;
                         const int i = cinfo[cc] & 3, kidx = cinfo[cc] >> 3;
-                        const T *kb = RZH + ((i * 3) * D::NFV * NFM + kidx) * 2;
+                        const T *kb = RZH + (kidx * 9 + i * 3) * 2;   // K[fv][fu][ik][2]
                         T k00, k01, k10, k11, k20, k21;
                         load_pair(kb, k00, k01);
-                        load_pair(kb + 2 * D::NFV * NFM, k10, k11);
-                        load_pair(kb + 4 * D::NFV * NFM, k20, k21);
+                        load_pair(kb + 2, k10, k11);
+                        load_pair(kb + 4, k20, k21);
                         const T s00 = k00 + k10, s01 = k01 + k11;
 #pragma unroll
                         for (int m = 0; m < PB; m++)
