@@ -24,8 +24,10 @@
 //   G  backward u: one lane per channel (i,k,l) walks the warp's two rows,
 //                  weights W^{[k==u][l==u]}
 //   -- barrier --
-//   D  backward v: one thread per (i, k, fu) walks the column over the tile's
-//                  rows; channels merged on (l == w): K[i][k][fv][fu][lw]
+//   D  backward v: one thread per (i, k) and two fu (FP32; one fu in FP64)
+//                  walks the columns over the tile's rows (one pair of band
+//                  rows serves both); channels merged on (l == w):
+//                  K[fv][fu][i][k][lw]
 //   -- barrier --
 //   E  backward w: accumulation into a register ring of output planes
 //                  e..e+p; plane e is complete after element e and is added
@@ -295,20 +297,26 @@ __device__ __forceinline__ void walk_u_generic(const T *h, T *g, const T *tab, i
     }
 }
 
-// Backward v of the three channels (i,k,l=0..2) of one fu column, merged on
-// the w key: kp[fv] = (sum wa g0 + wb g1, sum wa g2), wa at table row ka
-// (trial l != v), wb at ka+1 (trial l == v).  G of row qv of the tile lives
-// in the block of warp qv/2: gb + (qv/2)*GP + (qv%2)*RS + l; the pairs of K
-// are NFM * 18 apart from one fv to the next.
-template <class T, int P, int PAT>
-__device__ __forceinline__ void walk_v(const T *gb, T *kp, const T *tab, int ka, int ne_rt) {
+// Backward v of the three channels (i,k,l=0..2) of two fu columns (fu and
+// fu + dfu: one pair of band rows serves both), merged on the w key:
+// kp[fv] = (sum wa g0 + wb g1, sum wa g2), wa at table row ka (trial
+// l != v), wb at ka+1 (trial l == v).  G of row qv of the tile lives in the
+// block of warp qv/2: gb + (qv/2)*GP + (qv%2)*RS + l (second column: + 27
+// dfu); the pairs of K are NFM * 18 apart from one fv to the next (second
+// column: + 18 dfu).  two = false: the second column is not stored.  NC = 1:
+// one column only (FP64, whose registers do not hold two).
+template <class T, int P, int PAT, int NC>
+__device__ __forceinline__ void walk_v(const T *gb, T *kp, int dfu, bool two, const T *tab, int ka,
+                                       int ne_rt) {
     using D = Dims<P>;
     constexpr int PBP = D::PBP, TS = D::TS, NEM = pat_nemax(P, PAT, kTV), NF = NEM + P;
     constexpr int KS = D::NFM * 18, RS = D::RS, GP = D::GP;
     const int ne = PAT == 1 ? NEM : ne_rt;
-    T A0[NF], A1[NF];
+    const int dg = 27 * dfu;
+    T *const kp1 = kp + 18 * dfu;
+    T A0[NF], A1[NF], B0[NF], B1[NF];
 #pragma unroll
-    for (int f = 0; f < NF; f++) A0[f] = A1[f] = T(0);
+    for (int f = 0; f < NF; f++) A0[f] = A1[f] = B0[f] = B1[f] = T(0);
 #pragma unroll
     for (int e = 0; e < NEM; e++) {
         if (e < ne) {
@@ -328,35 +336,52 @@ __device__ __forceinline__ void walk_v(const T *gb, T *kp, const T *tab, int ka,
                         A0[e + m] += wa[m] * x0 + wb[m] * x1;
                         A1[e + m] += wa[m] * x2;
                     }
+                    if constexpr (NC == 2) {
+                        const T y0 = g[dg], y1 = g[dg + 1], y2 = g[dg + 2];
+#pragma unroll
+                        for (int m = 0; m <= P; m++) {
+                            B0[e + m] += wa[m] * y0 + wb[m] * y1;
+                            B1[e + m] += wa[m] * y2;
+                        }
+                    }
                 }
             }
             store_pair(kp + e * KS, A0[e], A1[e]);
+            if (NC == 2 && two) store_pair(kp1 + e * KS, B0[e], B1[e]);
         }
     }
 #pragma unroll
     for (int f = 1; f < NF; f++)
-        if (f >= ne && f < ne + P) store_pair(kp + f * KS, A0[f], A1[f]);
+        if (f >= ne && f < ne + P) {
+            store_pair(kp + f * KS, A0[f], A1[f]);
+            if (NC == 2 && two) store_pair(kp1 + f * KS, B0[f], B1[f]);
+        }
 }
 
-template <class T, int P>
-__device__ __forceinline__ void walk_v_generic(const T *gb, T *kp, const T *tab, int ka,
-                                               const int *rel, int nq) {
+template <class T, int P, int NC>
+__device__ __forceinline__ void walk_v_generic(const T *gb, T *kp, int dfu, bool two, const T *tab,
+                                               int ka, const int *rel, int nq) {
     using D = Dims<P>;
     constexpr int PBP = D::PBP, TS = D::TS, KS = D::NFM * 18, RS = D::RS, GP = D::GP;
-    T A0[P + 1], A1[P + 1];
+    const int dg = 27 * dfu;
+    T *const kp1 = kp + 18 * dfu;
+    T A0[P + 1], A1[P + 1], B0[P + 1], B1[P + 1];
 #pragma unroll
-    for (int m = 0; m <= P; m++) A0[m] = A1[m] = T(0);
+    for (int m = 0; m <= P; m++) A0[m] = A1[m] = B0[m] = B1[m] = T(0);
     int cur = 0;
     for (int q = 0; q < nq; q++) {
         const int r = rel[q];
         if (r != cur) {
             store_pair(kp + cur * KS, A0[0], A1[0]);
+            if (NC == 2 && two) store_pair(kp1 + cur * KS, B0[0], B1[0]);
 #pragma unroll
             for (int m = 0; m < P; m++) {
                 A0[m] = A0[m + 1];
                 A1[m] = A1[m + 1];
+                B0[m] = B0[m + 1];
+                B1[m] = B1[m + 1];
             }
-            A0[P] = A1[P] = T(0);
+            A0[P] = A1[P] = B0[P] = B1[P] = T(0);
             cur = r;
         }
         T wa[P + 1], wb[P + 1];
@@ -369,9 +394,20 @@ __device__ __forceinline__ void walk_v_generic(const T *gb, T *kp, const T *tab,
             A0[m] += wa[m] * x0 + wb[m] * x1;
             A1[m] += wa[m] * x2;
         }
+        if constexpr (NC == 2) {
+            const T y0 = g[dg], y1 = g[dg + 1], y2 = g[dg + 2];
+#pragma unroll
+            for (int m = 0; m <= P; m++) {
+                B0[m] += wa[m] * y0 + wb[m] * y1;
+                B1[m] += wa[m] * y2;
+            }
+        }
     }
 #pragma unroll
-    for (int m = 0; m <= P; m++) store_pair(kp + (cur + m) * KS, A0[m], A1[m]);
+    for (int m = 0; m <= P; m++) {
+        store_pair(kp + (cur + m) * KS, A0[m], A1[m]);
+        if (NC == 2 && two) store_pair(kp1 + (cur + m) * KS, B0[m], B1[m]);
+    }
 }
 
 __device__ __forceinline__ int relu_last_plus1(const int *elem, int q0, int nq, int f0) {
@@ -463,9 +499,13 @@ __global__ void __launch_bounds__(kThreads, kCtasPerSm) k_wq_apply_stream(Stream
         if constexpr (kStaged) {
             if (tid == 0) bulk_load(cbuf, coef_t + (int64_t)a.wq0[sg.y] * pstride, cbytes, bar);
         }
-        // stage D thread: (ik, fu), the nine ik fastest
-        const bool d_act = tid < 9 * nfu;
+        // stage D thread: (ik, fu) and (ik, fu + nfp), the nine ik fastest
+        // (FP64: one fu, nfp = nfu)
+        constexpr int kDC = sizeof(T) == 4 ? 2 : 1;
+        const int nfp = kDC == 2 ? (nfu + 1) >> 1 : nfu;
+        const bool d_act = tid < 9 * nfp;
         const int d_fu = d_act ? tid / 9 : 0, d_ik = d_act ? tid - 9 * d_fu : 0;
+        const bool d_two = d_fu + nfp < nfu;
 
         // columns (c, fv, fu) of this thread: stages A and E
         const int ncol = 3 * nfv * nfu;
@@ -686,18 +726,18 @@ __global__ void __launch_bounds__(kThreads, kCtasPerSm) k_wq_apply_stream(Stream
                     if (tid == 0 && qw + 1 < a.wq0[sg.z])
                         bulk_load(cbuf, coef_t + (int64_t)(qw + 1) * pstride, cbytes, bar);
                 }
-                // ---- D: backward v, thread (i, k, fu); K aliases the Z/h parts
+                // ---- D: backward v, thread (i, k) x two fu; K aliases the Z/h parts
                 if (d_act) {
                     const int ik = d_ik, fu = d_fu;
                     const int ka = 2 + 2 * (ik % 3 == 1);   // W_{[k==v], 0}
                     const T *gb = RG + fu * 27 + ik * 3;
                     T *kp = RZH + (fu * 9 + ik) * 2;
                     switch (patv) {
-                        case 1: walk_v<T, P, 1>(gb, kp, tabv, ka, nev); break;
-                        case 4: walk_v<T, P, 4>(gb, kp, tabv, ka, nev); break;
-                        case 2: walk_v<T, P, 2>(gb, kp, tabv, ka, nev); break;
-                        case 3: walk_v<T, P, 3>(gb, kp, tabv, ka, nev); break;
-                        default: walk_v_generic<T, P>(gb, kp, tabv, ka, relv, nqv);
+                        case 1: walk_v<T, P, 1, kDC>(gb, kp, d_two ? nfp : 0, d_two, tabv, ka, nev); break;
+                        case 4: walk_v<T, P, 4, kDC>(gb, kp, d_two ? nfp : 0, d_two, tabv, ka, nev); break;
+                        case 2: walk_v<T, P, 2, kDC>(gb, kp, d_two ? nfp : 0, d_two, tabv, ka, nev); break;
+                        case 3: walk_v<T, P, 3, kDC>(gb, kp, d_two ? nfp : 0, d_two, tabv, ka, nev); break;
+                        default: walk_v_generic<T, P, kDC>(gb, kp, d_two ? nfp : 0, d_two, tabv, ka, relv, nqv);
                     }
                 }
                 __syncthreads();
