@@ -14,6 +14,7 @@
 //   A  forward w : Y_t[c][fv][fu] = sum_m Bt_w(qw,m) X[c][fv][fu][e+m]
 //                  (one thread per (c, fv, fu) column; X for functions
 //                  e..e+p lives in a register ring that advances with e)
+//                  (computed for the next plane beside stage D of this one)
 //   -- barrier --
 //   each warp owns two point rows qv of the tile and runs, with warp
 //   synchronisation only:
@@ -547,10 +548,31 @@ __global__ void __launch_bounds__(kThreads, kCtasPerSm) k_wq_apply_stream(Stream
         auto retire = [&](int cc, int fw, T v) {
             if ((cinfo[cc] & 4) && !clamped_w(cc, fw)) atomicAdd(&a.Ku[cbase[cc] + plane * fw], v);
         };
+        // ---- A: forward w of plane qa into RY
+        auto stage_a = [&](int qa) {
+            const T *bwa = a.band[2] + (size_t)qa * 6 * PBP;
+            T b0[PB], b1[PB];
+            load_band<P>(bwa, b0);
+            load_band<P>(bwa + PBP, b1);
+#pragma unroll
+            for (int cc = 0; cc < CPT; cc++) {
+                if (!(cinfo[cc] & 4)) continue;
+                T y0 = 0, y1 = 0;
+#pragma unroll
+                for (int m = 0; m < PB; m++) {
+                    y0 += b0[m] * x[cc][m];
+                    y1 += b1[m] * x[cc][m];
+                }
+                const int c = cinfo[cc] & 3, k = cinfo[cc] >> 3;
+                RY[c * D::NFV * NFM + k] = y0;
+                RY[(3 + c) * D::NFV * NFM + k] = y1;
+            }
+        };
 #pragma unroll
         for (int cc = 0; cc < CPT; cc++)
 #pragma unroll
-            for (int m = 0; m < P; m++) x[cc][m] = load_x(cc, sg.y + m);
+            for (int m = 0; m <= P; m++) x[cc][m] = load_x(cc, sg.y + m);
+        stage_a(a.wq0[sg.y]);
         if (!kStaged) {
             const char *p0 = reinterpret_cast<const char *>(coef_t + (int64_t)a.wq0[sg.y] * pstride);
             for (int off = tid * 128; off < pbytes; off += kThreads * 128) prefetch_l2(p0 + off);
@@ -558,10 +580,7 @@ __global__ void __launch_bounds__(kThreads, kCtasPerSm) k_wq_apply_stream(Stream
 
         for (int e = sg.y; e < sg.z; e++) {
 #pragma unroll
-            for (int cc = 0; cc < CPT; cc++) {
-                x[cc][P] = load_x(cc, e + P);
-                acc[cc][P] = T(0);
-            }
+            for (int cc = 0; cc < CPT; cc++) acc[cc][P] = T(0);
             const int qw_end = a.wq0[e + 1];
             for (int qw = a.wq0[e]; qw < qw_end; qw++) {
                 const T *bw = a.band[2] + (size_t)qw * 6 * PBP;
@@ -570,25 +589,6 @@ __global__ void __launch_bounds__(kThreads, kCtasPerSm) k_wq_apply_stream(Stream
                     // the next plane into L2 (FP32 stages it with a bulk copy)
                     const char *pn = reinterpret_cast<const char *>(coef_t + (int64_t)(qw + 1) * pstride);
                     for (int off = tid * 128; off < pbytes; off += kThreads * 128) prefetch_l2(pn + off);
-                }
-                // ---- A: forward w
-                {
-                    T b0[PB], b1[PB];
-                    load_band<P>(bw, b0);
-                    load_band<P>(bw + PBP, b1);
-#pragma unroll
-                    for (int cc = 0; cc < CPT; cc++) {
-                        if (!(cinfo[cc] & 4)) continue;
-                        T y0 = 0, y1 = 0;
-#pragma unroll
-                        for (int m = 0; m < PB; m++) {
-                            y0 += b0[m] * x[cc][m];
-                            y1 += b1[m] * x[cc][m];
-                        }
-                        const int c = cinfo[cc] & 3, k = cinfo[cc] >> 3;
-                        RY[c * D::NFV * NFM + k] = y0;
-                        RY[(3 + c) * D::NFV * NFM + k] = y1;
-                    }
                 }
                 if constexpr (kStaged) {
                     // this plane's coefficient block has landed in shared memory
@@ -740,6 +740,19 @@ __global__ void __launch_bounds__(kThreads, kCtasPerSm) k_wq_apply_stream(Stream
                         default: walk_v_generic<T, P, kDC>(gb, kp, d_two ? nfp : 0, d_two, tabv, ka, relv, nqv);
                     }
                 }
+                // ---- A of the next plane, beside D (RY is free once B is done);
+                // at an element's last plane the u ring advances first
+                if (qw + 1 < a.wq0[sg.z]) {
+                    if (qw + 1 == qw_end) {
+#pragma unroll
+                        for (int cc = 0; cc < CPT; cc++) {
+#pragma unroll
+                            for (int m = 0; m < P; m++) x[cc][m] = x[cc][m + 1];
+                            x[cc][P] = load_x(cc, e + 1 + P);
+                        }
+                    }
+                    stage_a(qw + 1);
+                }
                 __syncthreads();
                 // ---- E: backward w into the register ring of output planes
                 {
@@ -763,19 +776,15 @@ __global__ void __launch_bounds__(kThreads, kCtasPerSm) k_wq_apply_stream(Stream
                             acc[cc][m] += w00[m] * s00 + w01[m] * s01 + w10[m] * k20 + w11[m] * k21;
                     }
                 }
-                // no barrier: the next plane's stage A writes only RY, and
-                // the next B writes the Z/h parts after the barrier that
-                // follows A
+                // no barrier: the next B writes the Z/h parts after the
+                // barrier that opens the next plane
             }
             // output plane e is complete for this element range
 #pragma unroll
             for (int cc = 0; cc < CPT; cc++) {
                 retire(cc, e, acc[cc][0]);
 #pragma unroll
-                for (int m = 0; m < P; m++) {
-                    x[cc][m] = x[cc][m + 1];
-                    acc[cc][m] = acc[cc][m + 1];
-                }
+                for (int m = 0; m < P; m++) acc[cc][m] = acc[cc][m + 1];
             }
         }
         // partial sums of the planes after the range
