@@ -35,10 +35,10 @@
 // One CTA per element.  Shared memory holds the point coefficients (13 per
 // point), T1 = G_rs per class pair and (q1, q2), and T2 per u-kind pair, i2,
 // j2 and q1.  The u contraction runs in lane groups of three (one r each,
-// the three s in registers); the group's first lane gathers the nine G_rs of
-// a node pair with warp shuffles and writes the pair's nine (diagonal pair:
-// six) slot values, consecutive groups taking consecutive row nodes, whose
-// slots are contiguous.
+// the three s in registers); lane r gathers the column G_{k,r} and the
+// diagonal from the other two with warp shuffles and writes column l = r of
+// the node pair's slot (three values; diagonal pair: r + 1), consecutive
+// groups taking consecutive row nodes, whose slots are contiguous.
 #include "nurbs.cuh"
 #include "u1_model.cuh"
 
@@ -264,10 +264,10 @@ __global__ void __launch_bounds__(kSfThreads, G <= 4 ? 3 : 2) k_u1_stiffness_sf(
             __syncthreads();
             // ---- steps 3 (u) and 4 (the COO slot): lanes in groups of three
             // (r = 0, 1, 2) per (a12, j2), ten groups per warp; each lane
-            // contracts the three G_rs of its r along u, the group's first
-            // lane gathers the other six through warp shuffles and writes the
-            // pair's slot (consecutive groups take consecutive row nodes,
-            // whose slots are contiguous)
+            // contracts the three G_rs of its r along u and, with the
+            // column G_{k,r} gathered through warp shuffles, writes column
+            // l = r of the pair's slot (consecutive groups take consecutive
+            // row nodes, whose slots are contiguous)
             {
                 const int warp = tid >> 5, lane = tid & 31, gl = lane / 3, rr = lane - 3 * gl;
                 const int ngroups = n12 * n2;
@@ -298,46 +298,59 @@ __global__ void __launch_bounds__(kSfThreads, G <= 4 ? 3 : 2) k_u1_stiffness_sf(
 #pragma unroll
                             for (int ss = 0; ss < 3; ss++) o[ss] += c0 * Uu[ss][0][q1] + c1 * Uu[ss][1][q1];
                         }
-                        double Gm[9];
-#pragma unroll
-                        for (int ss = 0; ss < 3; ss++) {
-                            Gm[ss] = o[ss];
-                            Gm[3 + ss] = __shfl_sync(0xffffffffu, o[ss], (base + 1) & 31);
-                            Gm[6 + ss] = __shfl_sync(0xffffffffu, o[ss], (base + 2) & 31);
-                        }
+                        // K_kl = lam G_kl + mu G_lk + [k=l] mu tr G.  Lane rr writes
+                        // column l = rr of the slot: it holds the row G_{rr,s} (o[s]);
+                        // the column G_{k,rr} comes from lanes k by two rotating
+                        // shuffles (at step t a lane sends o[(rr - t) mod 3], which
+                        // is what lane (rr - t) mod 3 of the group reads), the trace
+                        // from the three diagonals.
+                        const double dg = rr == 0 ? o[0] : rr == 1 ? o[1] : o[2];
+                        const double s1 = rr == 0 ? o[2] : rr == 1 ? o[0] : o[1];
+                        const double s2 = rr == 0 ? o[1] : rr == 1 ? o[2] : o[0];
+                        const int l1 = (base + (rr == 2 ? 0 : rr + 1)) & 31;   // lane (rr+1)%3
+                        const int l2 = (base + (rr == 0 ? 2 : rr - 1)) & 31;   // lane (rr+2)%3
+                        const double c1 = __shfl_sync(0xffffffffu, s1, l1);   // G_{(rr+1)%3, rr}
+                        const double c2 = __shfl_sync(0xffffffffu, s2, l2);   // G_{(rr+2)%3, rr}
+                        const double d1 = __shfl_sync(0xffffffffu, dg, l1);
+                        const double d2 = __shfl_sync(0xffffffffu, dg, l2);
                         const int ib = j1 + n1 * j2 + n12 * j3;
-                        if (!act || rr != 0 || ia > ib) continue;
+                        if (!act || ia > ib) continue;
                         const double wab = we[ia] * we[ib];
+                        // the trace summed as G_00 + G_11 + G_22 on every lane
+                        const double t0 = rr == 0 ? dg : rr == 1 ? d2 : d1;
+                        const double t1 = rr == 0 ? d1 : rr == 1 ? dg : d2;
+                        const double t2 = rr == 0 ? d2 : rr == 1 ? d1 : dg;
+                        const double tr = mu * (wab * t0 + wab * t1 + wab * t2);
+                        double col[3], row[3];
 #pragma unroll
-                        for (int rs = 0; rs < 9; rs++) Gm[rs] *= wab;
-                        const double tr = mu * (Gm[0] + Gm[4] + Gm[8]);
+                        for (int kk = 0; kk < 3; kk++) {
+                            const int dk = kk - rr;   // 0, 1 or 2 steps down the column
+                            col[kk] = wab * (dk == 0 ? dg : (dk == 1 || dk == -2) ? c1 : c2);
+                            row[kk] = wab * o[kk];
+                        }
                         const int dofa = 3 * sien[ia], dofb = 3 * sien[ib];
+                        const int ll = rr;
                         if (ia < ib) {
-                            const int64_t s0 = base_slot + 9LL * ib * (ib - 1) / 2 + 6LL * ib + 9LL * ia;
+                            const int64_t s0 = base_slot + 9LL * ib * (ib - 1) / 2 + 6LL * ib + 9LL * ia + 3 * ll;
 #pragma unroll
-                            for (int ll = 0; ll < 3; ll++)
-#pragma unroll
-                                for (int kk = 0; kk < 3; kk++) {
-                                    double v = lam * Gm[3 * kk + ll] + mu * Gm[3 * ll + kk];
-                                    if (kk == ll) v += tr;
-                                    const int64_t oo = s0 + 3 * ll + kk;
-                                    a.kdata[oo] = v;
-                                    a.krow[oo] = dofa + kk;
-                                    a.kcol[oo] = dofb + ll;
-                                }
+                            for (int kk = 0; kk < 3; kk++) {
+                                double v = lam * col[kk] + mu * row[kk];
+                                if (kk == ll) v += tr;
+                                a.kdata[s0 + kk] = v;
+                                a.krow[s0 + kk] = dofa + kk;
+                                a.kcol[s0 + kk] = dofb + ll;
+                            }
                         } else {
-                            const int64_t s0 = base_slot + 9LL * ia * (ia - 1) / 2 + 15LL * ia;
+                            const int64_t s0 = base_slot + 9LL * ia * (ia - 1) / 2 + 15LL * ia + ll * (ll + 1) / 2;
 #pragma unroll
-                            for (int ll = 0; ll < 3; ll++)
-#pragma unroll
-                                for (int kk = 0; kk <= ll; kk++) {
-                                    double v = lam * Gm[3 * kk + ll] + mu * Gm[3 * ll + kk];
-                                    if (kk == ll) v = (v + tr) * 0.5;
-                                    const int64_t oo = s0 + ll * (ll + 1) / 2 + kk;
-                                    a.kdata[oo] = v;
-                                    a.krow[oo] = dofa + kk;
-                                    a.kcol[oo] = dofa + ll;
-                                }
+                            for (int kk = 0; kk < 3; kk++) {
+                                if (kk > ll) continue;
+                                double v = lam * col[kk] + mu * row[kk];
+                                if (kk == ll) v = (v + tr) * 0.5;
+                                a.kdata[s0 + kk] = v;
+                                a.krow[s0 + kk] = dofa + kk;
+                                a.kcol[s0 + kk] = dofa + ll;
+                            }
                         }
                     }
                 }
