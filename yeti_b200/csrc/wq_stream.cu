@@ -42,6 +42,7 @@
 // While a plane is processed, the next plane's coefficient block
 // (contiguous, 256-byte aligned) is prefetched into L2.
 #include <algorithm>
+#include <cstring>
 #include <numeric>
 
 #include "wq.cuh"
@@ -220,12 +221,19 @@ __host__ __device__ constexpr int pat_q0(int P, int pat, int e) {
 // element's p+1 functions named at compile time; one band row serves both
 // rows.  h: row 0 at h[q], row 1 at h[kTQ + q]; g: function f of row r at
 // g[r * RS + 27 f] (the G block's channel stride is 1).
-template <class T, int P, int PAT>
+template <class T, int P, int PAT, bool PER>
 __device__ __forceinline__ void walk_u(const T *h, T *g, const T *tab, int kind, int ne_rt) {
     using D = Dims<P>;
     constexpr int TS = D::TS, PBP = D::PBP, RS = D::RS;
     constexpr int NEM = pat_nemax(P, PAT), NF = NEM + P;
     const int ne = PAT == 1 ? NEM : ne_rt;
+    // periodic tile: every element's two points have the band rows of the
+    // tile's first two points, read once
+    T wr[2][P + 1];
+    if constexpr (PER) {
+        load_band<P>(tab + kind * PBP, wr[0]);
+        load_band<P>(tab + TS + kind * PBP, wr[1]);
+    }
     T a0[NF], a1[NF];
 #pragma unroll
     for (int f = 0; f < NF; f++) a0[f] = a1[f] = T(0);
@@ -239,7 +247,12 @@ __device__ __forceinline__ void walk_u(const T *h, T *g, const T *tab, int kind,
                 if (pt < np) {
                     const int q = q0 + pt;
                     T w[P + 1];
-                    load_band<P>(tab + q * TS + kind * PBP, w);
+                    if constexpr (PER) {
+#pragma unroll
+                        for (int m = 0; m <= P; m++) w[m] = wr[pt & 1][m];
+                    } else {
+                        load_band<P>(tab + q * TS + kind * PBP, w);
+                    }
                     const T x0 = h[q], x1 = h[kTQ + q];
 #pragma unroll
                     for (int m = 0; m <= P; m++) {
@@ -306,13 +319,21 @@ __device__ __forceinline__ void walk_u_generic(const T *h, T *g, const T *tab, i
 // dfu); the pairs of K are NFM * 18 apart from one fv to the next (second
 // column: + 18 dfu).  two = false: the second column is not stored.  NC = 1:
 // one column only (FP64, whose registers do not hold two).
-template <class T, int P, int PAT, int NC>
+template <class T, int P, int PAT, int NC, bool PER>
 __device__ __forceinline__ void walk_v(const T *gb, T *kp, int dfu, bool two, const T *tab, int ka,
                                        int ne_rt) {
     using D = Dims<P>;
     constexpr int PBP = D::PBP, TS = D::TS, NEM = pat_nemax(P, PAT, kTV), NF = NEM + P;
     constexpr int KS = D::NFM * 18, RS = D::RS, GP = D::GP;
     const int ne = PAT == 1 ? NEM : ne_rt;
+    // periodic tile: the band rows of the tile's first two points, read once
+    T war[2][P + 1], wbr[2][P + 1];
+    if constexpr (PER) {
+        load_band<P>(tab + ka * PBP, war[0]);
+        load_band<P>(tab + (ka + 1) * PBP, wbr[0]);
+        load_band<P>(tab + TS + ka * PBP, war[1]);
+        load_band<P>(tab + TS + (ka + 1) * PBP, wbr[1]);
+    }
     const int dg = 27 * dfu;
     T *const kp1 = kp + 18 * dfu;
     T A0[NF], A1[NF], B0[NF], B1[NF];
@@ -328,8 +349,16 @@ __device__ __forceinline__ void walk_v(const T *gb, T *kp, int dfu, bool two, co
                 if (pt < np) {
                     const int q = q0 + pt;
                     T wa[P + 1], wb[P + 1];
-                    load_band<P>(tab + q * TS + ka * PBP, wa);
-                    load_band<P>(tab + q * TS + (ka + 1) * PBP, wb);
+                    if constexpr (PER) {
+#pragma unroll
+                        for (int m = 0; m <= P; m++) {
+                            wa[m] = war[pt & 1][m];
+                            wb[m] = wbr[pt & 1][m];
+                        }
+                    } else {
+                        load_band<P>(tab + q * TS + ka * PBP, wa);
+                        load_band<P>(tab + q * TS + (ka + 1) * PBP, wb);
+                    }
                     const T *g = gb + (q >> 1) * GP + (q & 1) * RS;
                     const T x0 = g[0], x1 = g[1], x2 = g[2];
 #pragma unroll
@@ -475,7 +504,9 @@ __global__ void __launch_bounds__(kThreads, kCtasPerSm) k_wq_apply_stream(Stream
         const int tu = sg.x % a.ntile[0], tv = sg.x / a.ntile[0];
         const int qu0 = a.tq0[0][tu], nqu = a.tnq[0][tu];
         const int qv0 = a.tq0[1][tv], nqv = a.tnq[1][tv];
-        const int patu = a.treg[0][tu], patv = a.treg[1][tv];
+        // pattern in bits 0..2, bit 3: periodic band rows (pattern 1 or 4)
+        const int patu = a.treg[0][tu] & 7, patv = a.treg[1][tv] & 7;
+        const bool peru = (a.treg[0][tu] & 8) != 0, perv = (a.treg[1][tv] & 8) != 0;
         const bool regu = patu == 1 || patu == 4, regv = patv == 1 || patv == 4;
         const int fu0 = a.elem[0][qu0], fv0 = a.elem[1][qv0];
         const int nfu = a.elem[0][qu0 + nqu - 1] + PB - fu0;
@@ -712,10 +743,16 @@ __global__ void __launch_bounds__(kThreads, kCtasPerSm) k_wq_apply_stream(Stream
                         const T *hr = zh + ch * kHS;
                         T *gr = gp + ch;
                         switch (patu) {
-                            case 1: walk_u<T, P, 1>(hr, gr, tabu, kind, neu); break;
-                            case 4: walk_u<T, P, 4>(hr, gr, tabu, kind, neu); break;
-                            case 2: walk_u<T, P, 2>(hr, gr, tabu, kind, neu); break;
-                            case 3: walk_u<T, P, 3>(hr, gr, tabu, kind, neu); break;
+                            case 1:
+                                if (peru) walk_u<T, P, 1, true>(hr, gr, tabu, kind, neu);
+                                else walk_u<T, P, 1, false>(hr, gr, tabu, kind, neu);
+                                break;
+                            case 4:
+                                if (peru) walk_u<T, P, 4, true>(hr, gr, tabu, kind, neu);
+                                else walk_u<T, P, 4, false>(hr, gr, tabu, kind, neu);
+                                break;
+                            case 2: walk_u<T, P, 2, false>(hr, gr, tabu, kind, neu); break;
+                            case 3: walk_u<T, P, 3, false>(hr, gr, tabu, kind, neu); break;
                             default: walk_u_generic<T, P>(hr, gr, tabu, kind, relu, nqu);
                         }
                     }
@@ -733,10 +770,16 @@ __global__ void __launch_bounds__(kThreads, kCtasPerSm) k_wq_apply_stream(Stream
                     const T *gb = RG + fu * 27 + ik * 3;
                     T *kp = RZH + (fu * 9 + ik) * 2;
                     switch (patv) {
-                        case 1: walk_v<T, P, 1, kDC>(gb, kp, d_two ? nfp : 0, d_two, tabv, ka, nev); break;
-                        case 4: walk_v<T, P, 4, kDC>(gb, kp, d_two ? nfp : 0, d_two, tabv, ka, nev); break;
-                        case 2: walk_v<T, P, 2, kDC>(gb, kp, d_two ? nfp : 0, d_two, tabv, ka, nev); break;
-                        case 3: walk_v<T, P, 3, kDC>(gb, kp, d_two ? nfp : 0, d_two, tabv, ka, nev); break;
+                        case 1:
+                            if (perv) walk_v<T, P, 1, kDC, true>(gb, kp, d_two ? nfp : 0, d_two, tabv, ka, nev);
+                            else walk_v<T, P, 1, kDC, false>(gb, kp, d_two ? nfp : 0, d_two, tabv, ka, nev);
+                            break;
+                        case 4:
+                            if (perv) walk_v<T, P, 4, kDC, true>(gb, kp, d_two ? nfp : 0, d_two, tabv, ka, nev);
+                            else walk_v<T, P, 4, kDC, false>(gb, kp, d_two ? nfp : 0, d_two, tabv, ka, nev);
+                            break;
+                        case 2: walk_v<T, P, 2, kDC, false>(gb, kp, d_two ? nfp : 0, d_two, tabv, ka, nev); break;
+                        case 3: walk_v<T, P, 3, kDC, false>(gb, kp, d_two ? nfp : 0, d_two, tabv, ka, nev); break;
                         default: walk_v_generic<T, P, kDC>(gb, kp, d_two ? nfp : 0, d_two, tabv, ka, relv, nqv);
                     }
                 }
@@ -929,6 +972,7 @@ int wq_stream_setup(yeti_wq_op *op, const WQRule1D R[3]) {
     WQStreamPlan &st = op->st;
     const int P = op->p[0], PBP = (P + 1 + 3) / 4 * 4;
     std::vector<int> elem_q0[3];
+    std::vector<double> band_uv[2];
     for (int d = 0; d < 3; d++) {
         const int nel = op->nel[d], nq = op->nqp[d];
         // element ownership of the points (first element p+1 points, last
@@ -957,6 +1001,7 @@ int wq_stream_setup(yeti_wq_op *op, const WQRule1D R[3]) {
                                     d, f, q);
                 }
         std::vector<float> bandf(band.begin(), band.end());
+        if (d < 2) band_uv[d] = band;
         YETI_TRY(upload_vec(ctx, st.elem[d], elem));
         YETI_TRY(upload_vec(ctx, st.band64[d], band));
         YETI_TRY(upload_vec(ctx, st.band32[d], bandf));
@@ -965,6 +1010,19 @@ int wq_stream_setup(yeti_wq_op *op, const WQRule1D R[3]) {
     std::vector<int> tq0[2], tnq[2], treg[2];
     for (int d = 0; d < 2; d++) {
         make_tiles(elem_q0[d], op->nel[d], tq0[d], tnq[d], treg[d], d == 0 ? kTQ : kTV);
+        // a regular tile whose points' band rows repeat, bit for bit, those
+        // of its first two points (interior elements of a uniform knot
+        // vector) is flagged (bit 3): its walks read two rows once
+        const size_t row = (size_t)6 * PBP;
+        for (size_t t = 0; t < treg[d].size(); t++) {
+            if (treg[d][t] != 1 && treg[d][t] != 4) continue;
+            const double *b0 = band_uv[d].data() + (size_t)tq0[d][t] * row;
+            bool per = tnq[d][t] >= 2;
+            for (int q = 2; per && q < tnq[d][t]; q++)
+                per = std::memcmp(b0 + (size_t)q * row, b0 + (size_t)(q & 1) * row,
+                                  row * sizeof(double)) == 0;
+            if (per) treg[d][t] |= 8;
+        }
         YETI_TRY(upload_vec(ctx, st.treg[d], treg[d]));
         st.ntile[d] = (int)tq0[d].size();
         YETI_TRY(upload_vec(ctx, st.tq0[d], tq0[d]));
