@@ -1260,14 +1260,14 @@ static int pcg_run(yeti_wq_op *op, const double *b, double *x, double rtol, int 
     } else if (mixed && !bicg) {
         // FP32 CG with reliable updates: the Krylov iteration runs in FP32
         // and is never restarted; whenever its recursive residual has
-        // dropped 10x (or reached the tolerance), the solution correction is
+        // dropped 100x (or reached the tolerance), the solution correction is
         // folded into the FP64 solution, the true residual is recomputed with
         // the FP64 operator and replaces the FP32 one (search direction kept,
         // rescaled).
         float *V = op->ws32.as<float>();
         float *r32 = V, *z32 = V + n, *p32 = V + 2 * n, *Ap32 = V + 3 * n, *d32 = V + 4 * n;
         const float *dinv32 = fd ? nullptr : op->dinv32.as<float>();
-        const double delta2 = 1e-2;   // replace when ||r|| fell by 10x
+        const double delta2 = 1e-4;   // replace when ||r|| fell by 100x
         // with FD: on the device, when ||r|| fell by 100x (FP32 tracks that)
         const double kFdPause2 = 1e-4;
         double rr64 = 0.0;
